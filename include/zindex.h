@@ -1,0 +1,141 @@
+/*
+ * zindex.h — C ABI of the B200 Zindex query path (libzindex_b200.so).
+ *
+ * The reference (Malfoy/Zindex, crate `zorindex`) is a Rust program with no
+ * FFI; its query entry points are library functions called by the CLI. Each
+ * declaration below names the reference function or behaviour it replaces
+ * (paths relative to the reference project). Plain pointers and sizes only:
+ * no CUDA or torch types cross this boundary except the opaque `stream`
+ * argument of zx_query_device (a cudaStream_t passed as void*).
+ *
+ * Errors: every int-returning function returns ZX_OK (0) or one of the ZX_E*
+ * codes; zx_last_error() returns the calling thread's last message. No
+ * exception crosses the boundary. Ownership: the library owns the index and
+ * its device memory; the caller owns every buffer it passes in.
+ * Threading: an index handle may be shared; each query call uses a private
+ * workspace unless stated otherwise.
+ */
+#ifndef ZINDEX_B200_H
+#define ZINDEX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZX_OK 0
+#define ZX_EINVAL 1       /* invalid argument */
+#define ZX_EFORMAT 2      /* malformed index, manifest or query input */
+#define ZX_EIO 3          /* file system error */
+#define ZX_ENOMEM 4       /* HBM / host memory exhausted, or admission refused */
+#define ZX_ECUDA 5        /* CUDA runtime error */
+#define ZX_ETIMEOUT 6     /* a bounded device wait expired */
+#define ZX_EUNSUPPORTED 7 /* index feature the GPU path does not implement */
+
+typedef struct zx_index zx_index;
+
+typedef struct zx_info {
+  uint32_t version;           /* manifest "version" */
+  uint32_t k;                 /* window span: k-mer length / minimizer window */
+  uint32_t hashes;            /* H */
+  uint32_t fingerprint_bits;  /* b */
+  uint32_t index_mode;        /* 0 kmers, 1 minimizers, 2 modimizers, 3 findere */
+  uint32_t minimizer_size;    /* m */
+  uint64_t seed;
+  uint64_t colors;
+  uint64_t banks;
+  uint64_t classes;           /* source size classes */
+  uint64_t resident_bytes;    /* HBM held by the index */
+  uint64_t gather_bytes_per_seed; /* fingerprint-plane bytes read per seed, all classes */
+  uint64_t abandoned_hashes;
+  int recovery;               /* manifest abandoned_recovery */
+} zx_info;
+
+typedef struct zx_launch {
+  int team;           /* lanes sharing one seed: 1, 2, 4, 8, 16 or 32 */
+  int warps;          /* warps per block, 1..16 */
+  int blocks;         /* grid size; 0 = fill the device */
+  int smem_counters;  /* 1 = per-block shared colour counters, 0 = global atomics */
+} zx_launch;
+
+/* Thread-local message of the last failed call on this thread. */
+const char* zx_last_error(void);
+
+/* Load and validate an index directory and make it resident in HBM of
+ * `device`. Replaces Index::load_mode / load_with_recovery
+ * (src/power_merge/storage.rs:2273-2707) and the bank readers
+ * (bank_io.rs:235-292, abandoned_io.rs:4-130). hbm_budget = 0 admits the
+ * index if it fits in free device memory minus 4 GiB; otherwise the index must
+ * fit in hbm_budget bytes (ZX_ENOMEM if not). */
+int zx_open(const char* index_dir, int device, uint64_t hbm_budget, zx_index** out);
+
+/* Release the index and its device memory. */
+void zx_close(zx_index* index);
+
+/* Index geometry (manifest fields, storage.rs:132-214). */
+int zx_index_info(const zx_index* index, zx_info* out);
+
+/* Name and unique_kmers of colour c (manifest colors[c], storage.rs:57-63). */
+const char* zx_color_name(const zx_index* index, uint64_t color);
+uint64_t zx_color_unique_kmers(const zx_index* index, uint64_t color);
+
+/* Aggregate query of a FASTA/FASTQ file (plain, gzip or zstd): the hot path
+ * of query_command_with_memory (storage.rs:3731-3767; query_aggregate,
+ * query_stream.rs:864-946). counts receives one 64-bit match count per colour
+ * (matches[] of print_aggregate); *total the number of query features (the
+ * ratio denominator, total_features); *probes the feature probes
+ * (stack_probes). recover = 0 disables abandoned-key recovery
+ * (query_command_with_recovery, storage.rs:3722-3729). */
+int zx_query_file(zx_index* index, const char* query_path, int recover, uint64_t* counts,
+                  uint64_t* total, uint64_t* probes);
+
+/* Aggregate query of records in host memory: record r is
+ * bases[offsets[r] .. offsets[r+1]) (raw sequence bytes; non-ACGT bytes split
+ * seeds as the reference parser's split_non_actg does, src/lib.rs:27-33).
+ * Batched: all records go through one launch sequence. */
+int zx_query_host(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
+                  uint64_t records, int recover, uint64_t* counts, uint64_t* total);
+
+/* As zx_query_host, but one record per launch sequence with default tiles
+ * (the plain GPU form, kept for comparison). */
+int zx_query_host_plain(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
+                        uint64_t records, int recover, uint64_t* counts, uint64_t* total);
+
+/* Asynchronous query of a batch already in device memory of the index's GPU.
+ * d_bases / d_offsets / d_counts / d_total are device pointers; counts and
+ * total are ACCUMULATED (the caller zeroes them). stream is a cudaStream_t
+ * (NULL = the legacy default stream). use_graph != 0 captures the launch
+ * sequence as a CUDA graph on first use of a batch shape and replays it after.
+ * Uses the index's shared workspace: callers serialise calls per index. */
+int zx_query_device(zx_index* index, const uint8_t* d_bases, uint64_t nbases,
+                    const uint64_t* d_offsets, uint64_t records, int recover,
+                    uint64_t* d_counts, uint64_t* d_total, void* stream, int use_graph);
+
+/* Seeds of host records, in record and window order, as the reference's
+ * scan_index_features emits them (src/lib.rs:574-642). *count receives the
+ * total number of seeds; at most cap are written. */
+int zx_extract_seeds(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
+                     uint64_t records, uint64_t* out, uint64_t cap, uint64_t* count);
+
+/* Launch configuration of the batched kernels (autotuner / planner hook;
+ * never changes results). */
+int zx_get_launch(const zx_index* index, zx_launch* out);
+int zx_set_launch(zx_index* index, const zx_launch* launch);
+int zx_default_launch(const zx_index* index, zx_launch* out);
+
+/* Write the aggregate report exactly as print_aggregate does
+ * (storage.rs:3817-3844): stdout-style TSV
+ * "color\tmatches\tratio\tunique_kmers" with rows whose ratio >= min_ratio to
+ * out_path (NULL = stdout), and the "#query\t..." statistics line to stderr
+ * when stats != 0. query_label is printed as the query path. */
+int zx_write_aggregate(const zx_index* index, const char* query_label, const uint64_t* counts,
+                       uint64_t total, uint64_t probes, double min_ratio, double seconds,
+                       const char* out_path, int stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZINDEX_B200_H */

@@ -1,0 +1,54 @@
+// TEST INFRASTRUCTURE ONLY. The oracle is the checker for the CUDA query path
+// and the timed CPU baseline; the product never links, loads or runs it.
+//
+// C entry points of liboracle.so, a CPU restatement of the Zindex (zorindex)
+// query algorithm. Each function names the reference code it follows.
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// splitmix64 (utils/ocm-minimizers/src/lib.rs:47-53).
+uint64_t oracle_splitmix64(uint64_t x);
+
+// Seed extraction of one sequence chunk exactly as scan_index_features
+// (src/lib.rs:574-642) would emit it, including the split at non-ACGT bytes.
+// mode: 0 kmers, 1 minimizers (open-closed mod), 2 modimizers, 3 findere.
+// Writes at most `cap` keys; *count receives the full number of keys.
+int oracle_features(const uint8_t* seq, size_t len, int mode, int k, int m, uint64_t seed,
+                    uint64_t sampling, int findere_z, int homopolymer, uint64_t* out, size_t cap,
+                    size_t* count);
+
+// Window-by-window open-closed mod-minimizer reference
+// (src/open_closed_minimizers.rs:43-85), for an all-ACGT `seq`.
+int oracle_ocm_slow(const uint8_t* seq, size_t len, int k, int m, uint64_t seed, uint64_t* pos_out,
+                    uint64_t* key_out, size_t cap, size_t* count);
+
+// Aggregate query of a FASTA/FASTQ file against an index directory
+// (query_command_with_memory, src/power_merge/storage.rs:3731-3767).
+// counts must hold `colors` entries. Returns 0 or a nonzero error; the message
+// is available from oracle_last_error().
+int oracle_query_file(const char* index_dir, const char* query_path, int threads, int recover,
+                      uint64_t* counts, size_t colors, uint64_t* total, uint64_t* probes);
+
+// Same query over sequences already in memory: record r spans
+// bases[offsets[r] .. offsets[r+1]).
+int oracle_query_records(const char* index_dir, const uint8_t* bases, const uint64_t* offsets,
+                         size_t records, int threads, int recover, uint64_t* counts, size_t colors,
+                         uint64_t* total, uint64_t* probes);
+
+// Number of colours of an index (manifest "colors").
+int oracle_index_colors(const char* index_dir, size_t* colors);
+
+// Render the aggregate TSV of print_aggregate (storage.rs:3817-3844) into buf.
+int oracle_format_aggregate(const char* index_dir, const uint64_t* counts, uint64_t total,
+                            double min_ratio, char* buf, size_t cap, size_t* written);
+
+const char* oracle_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,234 @@
+"""Parity of the CUDA query path with the oracle (bit-exact counts and totals).
+
+Every test here runs the GPU through the C ABI (libzindex_b200.so) and compares
+with the oracle's restatement of the reference query on the same index and
+query records. Indexes are built by zx_build from seeded synthetic genomes.
+"""
+import subprocess
+
+import numpy as np
+import pytest
+
+import helpers
+from helpers import build_index, dna, make_genomes, sample_reads
+
+pytestmark = pytest.mark.gpu
+
+_INDEXES = {}
+
+
+def index_for(tmp_path_factory, colors=6, length=30000, seed=5, **opts):
+    key = (colors, length, seed, tuple(sorted(opts.items())))
+    if key not in _INDEXES:
+        d = tmp_path_factory.mktemp("ix")
+        fof = make_genomes(d / "genomes", colors, length, seed)
+        build_index(fof, d / "index", **opts)
+        genomes = [dna(length, seed + c) for c in range(colors)]
+        _INDEXES[key] = (d / "index", genomes)
+    return _INDEXES[key]
+
+
+def reads_for(genomes, seed=11, n=300, length=150, **kw):
+    rng = np.random.default_rng(seed)
+    return sample_reads(genomes, rng, n, length, **kw)
+
+
+def gpu_vs_oracle(oracle, index_dir, records, recover=True, plain=False):
+    import zindex_b200 as zx
+
+    bases, offsets = zx.pack_records(records)
+    with zx.Index(index_dir) as ix:
+        got, total = ix.query_records(bases, offsets, recover=recover, plain=plain)
+    want, want_total = oracle.query_records(index_dir, bases, offsets, recover=recover)
+    assert total == want_total
+    np.testing.assert_array_equal(got, want)
+    return got, total
+
+
+KMER_CASES = [
+    dict(k=31, H=4, b=8),
+    dict(k=21, H=3, b=4),
+    dict(k=32, H=2, b=16),
+    dict(k=33, H=4, b=8),
+    dict(k=63, H=8, b=2),
+    dict(k=15, H=16, b=1),
+    dict(k=27, H=32, b=32),
+]
+
+
+@pytest.mark.parametrize("case", KMER_CASES, ids=lambda c: "k{k}-H{H}-b{b}".format(**c))
+def test_kmers_match_oracle(gpu, oracle, tmp_path_factory, case):
+    ix, genomes = index_for(tmp_path_factory, mode="kmers", **case)
+    gpu_vs_oracle(oracle, ix, reads_for(genomes, n_runs=0.1, lower=0.01))
+
+
+@pytest.mark.parametrize("H", [2, 3, 4, 8, 16, 32])
+@pytest.mark.parametrize("b", [1, 2, 4, 8, 16, 32])
+def test_hash_and_width_sweep(gpu, oracle, tmp_path_factory, H, b):
+    ix, genomes = index_for(tmp_path_factory, colors=5, length=8000, mode="kmers", k=25, H=H, b=b)
+    gpu_vs_oracle(oracle, ix, reads_for(genomes, n=120, length=120))
+
+
+MIN_CASES = [
+    dict(k=49, m=31, H=3, b=16),
+    dict(k=31, m=21, H=4, b=8),
+    dict(k=19, m=12, H=4, b=8),
+    dict(k=15, m=15, H=4, b=8),
+    dict(k=9, m=5, H=3, b=4),
+    dict(k=101, m=31, H=4, b=8),
+]
+
+
+@pytest.mark.parametrize("case", MIN_CASES, ids=lambda c: "k{k}-m{m}".format(**c))
+def test_minimizers_match_oracle(gpu, oracle, tmp_path_factory, case):
+    ix, genomes = index_for(tmp_path_factory, mode="minimizers", **case)
+    gpu_vs_oracle(oracle, ix, reads_for(genomes, length=600, n=120, n_runs=0.2, lower=0.01))
+
+
+@pytest.mark.parametrize("case", [dict(k=31, d=4), dict(k=49, d=8), dict(k=21, d=1)],
+                         ids=lambda c: "k{k}-d{d}".format(**c))
+def test_modimizers_match_oracle(gpu, oracle, tmp_path_factory, case):
+    ix, genomes = index_for(tmp_path_factory, mode="modimizers", H=4, b=8, **case)
+    gpu_vs_oracle(oracle, ix, reads_for(genomes, length=400, n=150, n_runs=0.1))
+
+
+def test_multi_member_groups(gpu, oracle, tmp_path_factory):
+    ix, genomes = index_for(tmp_path_factory, colors=8, mode="kmers", k=31, H=4, b=4,
+                            groups="0,1,2;3,5;6,7")
+    gpu_vs_oracle(oracle, ix, reads_for(genomes, n=400))
+
+
+def test_hash_partitions(gpu, oracle, tmp_path_factory):
+    ix, genomes = index_for(tmp_path_factory, colors=6, length=60000, mode="kmers", k=31, H=4,
+                            b=8, max_size="64KiB")
+    import json
+
+    manifest = json.loads((ix / "manifest.json").read_text())
+    assert any("routing" in b for b in manifest["banks"]), "expected a partitioned class"
+    gpu_vs_oracle(oracle, ix, reads_for(genomes, n=400))
+
+
+def test_promoted_size_classes(gpu, oracle, tmp_path_factory):
+    d = tmp_path_factory.mktemp("classes")
+    genomes = [dna(n, 77 + i) for i, n in enumerate([3000, 9000, 20000, 70000, 5000])]
+    lines = []
+    for i, g in enumerate(genomes):
+        p = d / f"g{i}.fa"
+        helpers.write_fasta(p, [g])
+        lines.append(f"g{i}\t{p}")
+    (d / "fof.tsv").write_text("\n".join(lines) + "\n")
+    ix = build_index(d / "fof.tsv", d / "index", k=31, H=4, b=8, min_docs=1)
+    gpu_vs_oracle(oracle, ix, reads_for(genomes, n=300))
+
+
+def test_recovery_disabled_and_dropped(gpu, oracle, tmp_path_factory):
+    ix, genomes = index_for(tmp_path_factory, mode="kmers", k=31, H=4, b=8)
+    reads = reads_for(genomes, n=300)
+    with_rec, _ = gpu_vs_oracle(oracle, ix, reads, recover=True)
+    without, _ = gpu_vs_oracle(oracle, ix, reads, recover=False)
+    assert (with_rec >= without).all()
+    ix2, genomes2 = index_for(tmp_path_factory, seed=9, mode="kmers", k=31, H=4, b=8,
+                              drop_abandoned=True)
+    gpu_vs_oracle(oracle, ix2, reads_for(genomes2, n=200))
+
+
+def test_edge_records(gpu, oracle, tmp_path_factory):
+    ix, genomes = index_for(tmp_path_factory, mode="kmers", k=31, H=4, b=8)
+    g = genomes[0]
+    records = [b"", b"ACGT", g[:30], g[:31], b"N" * 100, g[:500].lower(),
+               g[1000:1100] + b"NNN" + g[2000:2100], b"acgtn" * 40, g[:2000],
+               bytes(g[5000:5300].replace(b"A", b"R"))]
+    gpu_vs_oracle(oracle, ix, records)
+    gpu_vs_oracle(oracle, ix, [])
+
+
+def test_plain_form_equals_batched(gpu, oracle, tmp_path_factory):
+    ix, genomes = index_for(tmp_path_factory, mode="kmers", k=31, H=4, b=8)
+    reads = reads_for(genomes, n=40, length=300)
+    batched, t1 = gpu_vs_oracle(oracle, ix, reads)
+    plain, t2 = gpu_vs_oracle(oracle, ix, reads, plain=True)
+    np.testing.assert_array_equal(batched, plain)
+    assert t1 == t2
+
+
+@pytest.mark.parametrize("mode,case", [
+    ("kmers", dict(k=31)), ("kmers", dict(k=32)), ("kmers", dict(k=45)), ("kmers", dict(k=1)),
+    ("minimizers", dict(k=49, m=31)), ("minimizers", dict(k=31, m=15)),
+    ("minimizers", dict(k=7, m=7)), ("modimizers", dict(k=31, d=3)),
+    ("modimizers", dict(k=40, d=5)),
+], ids=lambda v: str(v))
+def test_extraction_matches_oracle_in_order(gpu, oracle, tmp_path_factory, mode, case):
+    import zindex_b200 as zx
+
+    ix, genomes = index_for(tmp_path_factory, colors=2, length=5000, mode=mode, H=4, b=8, **case)
+    rng = np.random.default_rng(3)
+    records = [helpers.mutate(dna(int(rng.integers(0, 3000)), s), rng, n_runs=3, lower=0.05)
+               for s in range(40)]
+    records += [b"", b"N" * 50, dna(70000, 99)]
+    bases, offsets = zx.pack_records(records)
+    with zx.Index(ix) as index:
+        got = index.extract_seeds(bases, offsets)
+    k = case["k"]
+    want = np.concatenate([oracle.features(r, mode=mode, k=k, m=case.get("m", 21),
+                                           sampling=case.get("d", 16)) for r in records])
+    np.testing.assert_array_equal(got, want)
+
+
+def test_cli_output_is_byte_identical(gpu, oracle, tmp_path_factory):
+    ix, genomes = index_for(tmp_path_factory, mode="kmers", k=31, H=4, b=8)
+    q = tmp_path_factory.mktemp("cli") / "q.fa"
+    helpers.write_fasta(q, reads_for(genomes, n=100))
+    ours = subprocess.run([str(helpers.ZORINDEX), "query", "-i", str(ix), "-q", str(q)],
+                          check=True, capture_output=True)
+    ref = subprocess.run([str(helpers.ORACLE_DIR / "_build" / "zx_oracle"), "query", "-i", str(ix),
+                          "-q", str(q)], check=True, capture_output=True)
+    assert ours.stdout == ref.stdout
+    ours_stats = [l for l in ours.stderr.decode().splitlines() if l.startswith("#query")][0]
+    ref_stats = [l for l in ref.stderr.decode().splitlines() if l.startswith("#query")][0]
+    assert ours_stats.split("elapsed_s")[0] == ref_stats.split("elapsed_s")[0]
+    for ratio in ("0.001", "0.5"):
+        a = subprocess.run([str(helpers.ZORINDEX), "query", "-i", str(ix), "-q", str(q), "-a", ratio],
+                           check=True, capture_output=True)
+        b = subprocess.run([str(helpers.ORACLE_DIR / "_build" / "zx_oracle"), "query", "-i", str(ix),
+                            "-q", str(q), "-a", ratio], check=True, capture_output=True)
+        assert a.stdout == b.stdout
+
+
+def test_device_api_with_graph_replay(gpu, oracle, tmp_path_factory):
+    import torch
+
+    import zindex_b200 as zx
+
+    ix, genomes = index_for(tmp_path_factory, mode="kmers", k=31, H=4, b=8)
+    reads = reads_for(genomes, n=500)
+    bases, offsets = zx.pack_records(reads)
+    want, want_total = oracle.query_records(ix, bases, offsets)
+    dev = torch.device("cuda:0")
+    d_bases = torch.from_numpy(bases).to(dev)
+    d_off = torch.from_numpy(offsets.view(np.int64)).to(dev)
+    with zx.Index(ix) as index:
+        for _ in range(3):
+            d_counts = torch.zeros(index.colors, dtype=torch.int64, device=dev)
+            d_total = torch.zeros(1, dtype=torch.int64, device=dev)
+            stream = torch.cuda.current_stream().cuda_stream
+            index.query_device(d_bases.data_ptr(), len(bases), d_off.data_ptr(), len(reads),
+                               d_counts.data_ptr(), d_total.data_ptr(), stream=stream)
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(d_counts.cpu().numpy().astype(np.uint64), want)
+            assert int(d_total.item()) == want_total
+
+
+@pytest.mark.parametrize("team,warps", [(1, 4), (2, 2), (8, 8), (32, 1), (4, 16)])
+def test_launch_configurations_do_not_change_results(gpu, oracle, tmp_path_factory, team, warps):
+    import zindex_b200 as zx
+
+    ix, genomes = index_for(tmp_path_factory, colors=40, length=4000, mode="kmers", k=31, H=4, b=8)
+    reads = reads_for(genomes, n=300)
+    bases, offsets = zx.pack_records(reads)
+    want, want_total = oracle.query_records(ix, bases, offsets)
+    with zx.Index(ix) as index:
+        for smem in (0, 1):
+            index.set_launch(team, warps, 0, smem)
+            got, total = index.query_records(bases, offsets)
+            np.testing.assert_array_equal(got, want)
+            assert total == want_total

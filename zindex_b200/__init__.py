@@ -1,0 +1,173 @@
+"""zindex_b200 — the Zindex (zorindex) query hot path on NVIDIA B200.
+
+Host-side mirror of the reference's query interface:
+
+* ``Index(index_dir)`` loads and validates an index directory into HBM
+  (Index::load_mode, src/power_merge/storage.rs:2273-2707).
+* ``Index.query_file(path)`` / ``Index.query_records(bases, offsets)`` return
+  per-colour match counts and the feature total, the numbers behind
+  ``print_aggregate`` (storage.rs:3817-3844).
+* ``query_command(index_dir, query, min_ratio, recover)`` prints the aggregate
+  TSV like ``query_command_with_recovery`` (storage.rs:3722-3744).
+
+All compute runs in the CUDA kernels of libzindex_b200.so; this module only
+moves buffers across the C ABI (include/zindex.h).
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+from ctypes import POINTER, byref, c_uint64, c_void_p
+from pathlib import Path
+from typing import Optional, Sequence, Tuple, Union
+
+import numpy as np
+
+from . import _lib
+from ._lib import ZxError, ZxInfo, ZxLaunch
+
+__all__ = ["Index", "ZxError", "query_command", "pack_records", "LIB_DIR"]
+
+LIB_DIR = _lib.LIB_DIR
+INDEX_MODES = ("kmers", "minimizers", "modimizers", "findere")
+
+
+def _p64(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_uint64))
+
+
+def pack_records(records: Sequence[Union[bytes, str]]) -> Tuple[np.ndarray, np.ndarray]:
+    """Concatenate sequences into (bases uint8, offsets uint64[n+1])."""
+    parts = [r.encode() if isinstance(r, str) else bytes(r) for r in records]
+    offsets = np.zeros(len(parts) + 1, dtype=np.uint64)
+    if parts:
+        offsets[1:] = np.cumsum([len(p) for p in parts], dtype=np.uint64)
+    bases = np.frombuffer(b"".join(parts), dtype=np.uint8).copy()
+    return bases, offsets
+
+
+class Index:
+    """An index directory made resident in HBM of one GPU."""
+
+    def __init__(self, index_dir: Union[str, Path], device: int = 0, hbm_budget: int = 0):
+        lib = _lib.load()
+        handle = c_void_p()
+        _lib.check(lib.zx_open(str(index_dir).encode(), int(device), int(hbm_budget), byref(handle)))
+        self._h = handle
+        self.path = Path(index_dir)
+        info = ZxInfo()
+        _lib.check(lib.zx_index_info(self._h, byref(info)))
+        self.info = info
+        self.colors = int(info.colors)
+        self.names = [lib.zx_color_name(self._h, c).decode() for c in range(self.colors)]
+        self.unique_kmers = [int(lib.zx_color_unique_kmers(self._h, c)) for c in range(self.colors)]
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().zx_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- queries --------------------------------------------------------------
+    @property
+    def mode(self) -> str:
+        return INDEX_MODES[self.info.index_mode]
+
+    def query_file(self, path: Union[str, Path], recover: bool = True):
+        """(counts uint64[colors], total, probes) for a FASTA/FASTQ file."""
+        counts = np.zeros(self.colors, dtype=np.uint64)
+        total, probes = c_uint64(), c_uint64()
+        _lib.check(_lib.load().zx_query_file(self._h, str(path).encode(), int(recover),
+                                            _p64(counts), byref(total), byref(probes)))
+        return counts, int(total.value), int(probes.value)
+
+    def query_records(self, bases: np.ndarray, offsets: np.ndarray, recover: bool = True,
+                      plain: bool = False):
+        """(counts, total) for records bases[offsets[r]:offsets[r+1]] in host memory."""
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        counts = np.zeros(self.colors, dtype=np.uint64)
+        total = c_uint64()
+        fn = _lib.load().zx_query_host_plain if plain else _lib.load().zx_query_host
+        _lib.check(fn(self._h, bases.ctypes.data_as(c_void_p), _p64(offsets), len(offsets) - 1,
+                      int(recover), _p64(counts), byref(total)))
+        return counts, int(total.value)
+
+    def query_device(self, d_bases: int, nbases: int, d_offsets: int, records: int,
+                     d_counts: int, d_total: int, stream: int = 0, recover: bool = True,
+                     use_graph: bool = True) -> None:
+        """Enqueue a query of a device-resident batch (raw device pointers)."""
+        _lib.check(_lib.load().zx_query_device(self._h, c_void_p(d_bases), nbases,
+                                              c_void_p(d_offsets), records, int(recover),
+                                              c_void_p(d_counts), c_void_p(d_total),
+                                              c_void_p(stream), int(use_graph)))
+
+    def extract_seeds(self, bases: np.ndarray, offsets: np.ndarray) -> np.ndarray:
+        """Seeds of the records in record/window order (extraction only)."""
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        count = c_uint64()
+        lib = _lib.load()
+        _lib.check(lib.zx_extract_seeds(self._h, bases.ctypes.data_as(c_void_p), _p64(offsets),
+                                        len(offsets) - 1, None, 0, byref(count)))
+        out = np.zeros(max(1, count.value), dtype=np.uint64)
+        _lib.check(lib.zx_extract_seeds(self._h, bases.ctypes.data_as(c_void_p), _p64(offsets),
+                                        len(offsets) - 1, _p64(out), len(out), byref(count)))
+        return out[: count.value]
+
+    # -- launch configuration -------------------------------------------------
+    def launch(self) -> dict:
+        l = ZxLaunch()
+        _lib.check(_lib.load().zx_get_launch(self._h, byref(l)))
+        return {"team": l.team, "warps": l.warps, "blocks": l.blocks, "smem_counters": l.smem_counters}
+
+    def default_launch(self) -> dict:
+        l = ZxLaunch()
+        _lib.check(_lib.load().zx_default_launch(self._h, byref(l)))
+        return {"team": l.team, "warps": l.warps, "blocks": l.blocks, "smem_counters": l.smem_counters}
+
+    def set_launch(self, team: int, warps: int, blocks: int = 0, smem_counters: Optional[int] = None):
+        if smem_counters is None:
+            smem_counters = self.default_launch()["smem_counters"]
+        l = ZxLaunch(int(team), int(warps), int(blocks), int(smem_counters))
+        _lib.check(_lib.load().zx_set_launch(self._h, byref(l)))
+
+    # -- output ---------------------------------------------------------------
+    def format_aggregate(self, counts, total: int, min_ratio: float = 0.0) -> str:
+        """The stdout TSV of print_aggregate (storage.rs:3817-3844)."""
+        lines = ["color\tmatches\tratio\tunique_kmers"]
+        for c in range(self.colors):
+            ratio = 0.0 if total == 0 else int(counts[c]) / total
+            if ratio >= min_ratio:
+                lines.append(f"{self.names[c]}\t{int(counts[c])}\t{ratio:.8f}\t{self.unique_kmers[c]}")
+        return "\n".join(lines) + "\n"
+
+    def write_aggregate(self, label: str, counts, total: int, probes: int, min_ratio: float = 0.0,
+                        seconds: float = 0.0, out_path: Optional[str] = None, stats: bool = True):
+        counts = np.ascontiguousarray(counts, dtype=np.uint64)
+        _lib.check(_lib.load().zx_write_aggregate(
+            self._h, label.encode(), _p64(counts), int(total), int(probes), float(min_ratio),
+            float(seconds), out_path.encode() if out_path else None, int(stats)))
+
+
+def query_command(index_dir, query, min_ratio: float = 0.0, recover: bool = True,
+                  device: int = 0) -> None:
+    """Print the aggregate query report, as `zorindex query -i DIR -q FILE -a R`."""
+    if not 0.0 <= min_ratio <= 1.0:
+        raise ValueError("--min-ratio must be in [0, 1]")
+    with Index(index_dir, device=device) as ix:
+        t0 = time.perf_counter()
+        counts, total, probes = ix.query_file(query, recover=recover)
+        ix.write_aggregate(str(query), counts, total, probes, min_ratio, time.perf_counter() - t0)

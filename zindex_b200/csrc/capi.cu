@@ -1,0 +1,213 @@
+// extern "C" boundary (include/zindex.h). Converts zx::Error and CUDA
+// failures into status codes plus a thread-local message.
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/zindex.h"
+#include "engine.h"
+#include "host/error.h"
+#include "host/fastx.h"
+
+struct zx_index {
+  std::unique_ptr<zx::Engine> engine;
+  std::mutex mu;  // guards the shared workspace
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F&& body) {
+  try {
+    body();
+    g_last_error.clear();
+    return ZX_OK;
+  } catch (const zx::Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host memory exhausted";
+    return ZX_ENOMEM;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return ZX_EINVAL;
+  }
+}
+
+void fill_launch(const zx::QueryLaunch& l, zx_launch* out) {
+  out->team = l.team;
+  out->warps = l.warps;
+  out->blocks = l.blocks;
+  out->smem_counters = l.smem_counters;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* zx_last_error(void) { return g_last_error.c_str(); }
+
+int zx_open(const char* index_dir, int device, uint64_t hbm_budget, zx_index** out) {
+  return guarded([&] {
+    zx::check(index_dir && out, zx::kEInval, "null argument");
+    *out = nullptr;
+    zx::OpenOptions o;
+    o.device = device;
+    o.hbm_budget = hbm_budget;
+    auto ix = std::make_unique<zx_index>();
+    ix->engine = std::make_unique<zx::Engine>(index_dir, o);
+    *out = ix.release();
+  });
+}
+
+void zx_close(zx_index* index) { delete index; }
+
+int zx_index_info(const zx_index* index, zx_info* out) {
+  return guarded([&] {
+    zx::check(index && out, zx::kEInval, "null argument");
+    const zx::Manifest& m = index->engine->manifest();
+    memset(out, 0, sizeof *out);
+    out->version = m.version;
+    out->k = (uint32_t)m.k;
+    out->hashes = (uint32_t)m.hashes;
+    out->fingerprint_bits = (uint32_t)m.fingerprint_bits;
+    out->index_mode = (uint32_t)m.index_mode;
+    out->minimizer_size = (uint32_t)m.minimizer_size;
+    out->seed = m.seed;
+    out->colors = m.colors.size();
+    out->banks = m.banks.size();
+    out->classes = m.classes.size();
+    out->resident_bytes = index->engine->resident_bytes();
+    out->gather_bytes_per_seed = index->engine->gather_bytes_per_seed();
+    out->abandoned_hashes = m.abandoned_hashes;
+    out->recovery = m.abandoned_recovery ? 1 : 0;
+  });
+}
+
+const char* zx_color_name(const zx_index* index, uint64_t color) {
+  if (!index || color >= index->engine->manifest().colors.size()) return nullptr;
+  return index->engine->manifest().colors[color].name.c_str();
+}
+
+uint64_t zx_color_unique_kmers(const zx_index* index, uint64_t color) {
+  if (!index || color >= index->engine->manifest().colors.size()) return 0;
+  return index->engine->manifest().colors[color].unique_kmers;
+}
+
+int zx_query_host(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
+                  uint64_t records, int recover, uint64_t* counts, uint64_t* total) {
+  return guarded([&] {
+    zx::check(index && offsets && counts && total && (bases || !offsets[records]), zx::kEInval,
+              "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    auto& e = *index->engine;
+    e.query_host(e.default_workspace(), bases, offsets[records], offsets, records, recover != 0,
+                 counts, total);
+  });
+}
+
+int zx_query_host_plain(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
+                        uint64_t records, int recover, uint64_t* counts, uint64_t* total) {
+  return guarded([&] {
+    zx::check(index && offsets && counts && total && (bases || !offsets[records]), zx::kEInval,
+              "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    auto& e = *index->engine;
+    e.query_host_plain(e.default_workspace(), bases, offsets[records], offsets, records,
+                       recover != 0, counts, total);
+  });
+}
+
+int zx_query_file(zx_index* index, const char* query_path, int recover, uint64_t* counts,
+                  uint64_t* total, uint64_t* probes) {
+  return guarded([&] {
+    zx::check(index && query_path && counts && total, zx::kEInval, "null argument");
+    zx::RecordBatch batch = zx::read_fastx(query_path, false);
+    std::lock_guard<std::mutex> lock(index->mu);
+    auto& e = *index->engine;
+    e.query_host(e.default_workspace(), batch.bases.data(), batch.bases.size(),
+                 batch.offsets.data(), batch.records(), recover != 0, counts, total);
+    if (probes) *probes = *total;
+  });
+}
+
+int zx_query_device(zx_index* index, const uint8_t* d_bases, uint64_t nbases,
+                    const uint64_t* d_offsets, uint64_t records, int recover,
+                    uint64_t* d_counts, uint64_t* d_total, void* stream, int use_graph) {
+  return guarded([&] {
+    zx::check(index && d_offsets && d_counts && d_total, zx::kEInval, "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    auto& e = *index->engine;
+    e.query_device(e.default_workspace(), d_bases, nbases, d_offsets, records, recover != 0,
+                   d_counts, reinterpret_cast<unsigned long long*>(d_total),
+                   static_cast<cudaStream_t>(stream), use_graph != 0);
+  });
+}
+
+int zx_extract_seeds(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
+                     uint64_t records, uint64_t* out, uint64_t cap, uint64_t* count) {
+  return guarded([&] {
+    zx::check(index && offsets && count, zx::kEInval, "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    auto& e = *index->engine;
+    std::vector<uint64_t> keys;
+    e.extract_host(e.default_workspace(), bases, offsets[records], offsets, records, keys);
+    *count = keys.size();
+    if (out) memcpy(out, keys.data(), std::min<uint64_t>(cap, keys.size()) * 8);
+  });
+}
+
+int zx_get_launch(const zx_index* index, zx_launch* out) {
+  return guarded([&] {
+    zx::check(index && out, zx::kEInval, "null argument");
+    fill_launch(index->engine->launch(), out);
+  });
+}
+
+int zx_default_launch(const zx_index* index, zx_launch* out) {
+  return guarded([&] {
+    zx::check(index && out, zx::kEInval, "null argument");
+    fill_launch(index->engine->default_launch(), out);
+  });
+}
+
+int zx_set_launch(zx_index* index, const zx_launch* l) {
+  return guarded([&] {
+    zx::check(index && l, zx::kEInval, "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    index->engine->set_launch(zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters});
+  });
+}
+
+int zx_write_aggregate(const zx_index* index, const char* query_label, const uint64_t* counts,
+                       uint64_t total, uint64_t probes, double min_ratio, double seconds,
+                       const char* out_path, int stats) {
+  return guarded([&] {
+    zx::check(index && counts, zx::kEInval, "null argument");
+    const zx::Manifest& m = index->engine->manifest();
+    if (stats)
+      fprintf(stderr,
+              "#query\t%s\tk=%llu\tindex_mode=%s\ttotal_features=%llu\tstack_probes=%llu\t"
+              "bank_probes=%llu\telapsed_s=%.6f\n",
+              query_label ? query_label : "", (unsigned long long)m.k,
+              zx::index_mode_label(m.index_mode), (unsigned long long)total,
+              (unsigned long long)probes, (unsigned long long)(probes * m.classes.size()),
+              seconds);
+    FILE* f = out_path ? fopen(out_path, "w") : stdout;
+    if (!f) zx::raise(zx::kEIo, std::string("cannot create ") + out_path);
+    fputs("color\tmatches\tratio\tunique_kmers\n", f);
+    for (size_t c = 0; c < m.colors.size(); ++c) {
+      double ratio = total == 0 ? 0.0 : (double)counts[c] / (double)total;
+      if (!(ratio >= min_ratio)) continue;
+      fprintf(f, "%s\t%llu\t%.8f\t%llu\n", m.colors[c].name.c_str(), (unsigned long long)counts[c],
+              ratio, (unsigned long long)m.colors[c].unique_kmers);
+    }
+    if (out_path) fclose(f);
+    else fflush(f);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,689 @@
+// Host runtime of the GPU query path (see engine.h).
+//
+// Index loading restates Index::load_mode (src/power_merge/storage.rs:
+// 2273-2707) for fingerprint-first banks: the manifest is validated, every
+// bank stream is decoded (bank_io.rs:235-292) and checked against its header
+// (validate_bank_header, storage.rs:2208-2231), and the recovery file is
+// decoded (abandoned_io.rs:4-130) into the device directory described in
+// kernels/device_index.cuh. All banks stay resident ("--query-memory all",
+// storage.rs:3745-3766): HBM holds the whole filter payload.
+#include "engine.h"
+
+#include <cub/device/device_scan.cuh>
+
+#include "kernels/query_kernels.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <thread>
+
+#include "host/error.h"
+#include "host/zstd_io.h"
+#include "zx_hash.h"
+
+namespace zx {
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) raise(kECuda, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+uint64_t round_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+
+template <class T>
+void dev_alloc(T** p, uint64_t count, const char* what) {
+  *p = nullptr;
+  if (!count) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    raise(kENoMem, std::string("device allocation failed for ") + what + ": " +
+                       cudaGetErrorString(e));
+  }
+}
+
+template <class T>
+void host_alloc(T** p, uint64_t count) {
+  *p = nullptr;
+  if (!count) count = 1;
+  cuda_check(cudaMallocHost((void**)p, count * sizeof(T)), "cudaMallocHost");
+}
+
+__global__ void repack_rows_kernel(const uint8_t* __restrict__ src, uint64_t rows,
+                                   uint32_t row_bytes, uint32_t stride, uint8_t* __restrict__ dst) {
+  uint64_t total = rows * stride;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t r = i / stride;
+    uint32_t c = (uint32_t)(i % stride);
+    dst[i] = c < row_bytes ? src[r * row_bytes + c] : 0;
+  }
+}
+
+uint64_t le64(const uint8_t* p) {
+  uint64_t v = 0;
+  for (int i = 7; i >= 0; --i) v = (v << 8) | p[i];
+  return v;
+}
+
+struct RecoveryRecords {
+  std::vector<uint32_t> hashes;
+  std::vector<uint64_t> starts;  // hashes + 1
+  std::vector<uint32_t> origins;
+};
+
+// AbandonedReader (src/power_merge/abandoned_io.rs:4-130) with its checks.
+RecoveryRecords read_recovery(const std::string& dir, const Manifest& m) {
+  RecoveryRecords r;
+  std::vector<uint8_t> raw = read_file_bytes(dir + "/abandoned.zormap.zst");
+  std::vector<uint8_t> d = zstd_decode_all(raw.data(), raw.size());
+  check_format(d.size() >= 8, "invalid abandoned map magic");
+  bool delta = !memcmp(d.data(), "ZORABN2\0", 8);
+  check_format(delta || !memcmp(d.data(), "ZORABN1\0", 8), "invalid abandoned map magic");
+  size_t p = 8;
+  auto var = [&]() -> uint32_t {
+    uint32_t v = 0;
+    for (int shift = 0; shift <= 28; shift += 7) {
+      check_format(p < d.size(), "truncated abandoned map");
+      uint8_t byte = d[p++];
+      check_format(shift != 28 || byte <= 15, "abandoned variable integer overflow");
+      v |= (uint32_t)(byte & 127) << shift;
+      if (!(byte & 128)) return v;
+    }
+    raise(kEFormat, "abandoned variable integer overflow");
+  };
+  auto u32 = [&]() -> uint32_t {
+    check_format(p + 4 <= d.size(), "truncated abandoned map");
+    uint32_t v = (uint32_t)d[p] | ((uint32_t)d[p + 1] << 8) | ((uint32_t)d[p + 2] << 16) |
+                 ((uint32_t)d[p + 3] << 24);
+    p += 4;
+    return v;
+  };
+  const uint64_t colors = m.colors.size();
+  r.hashes.reserve(m.abandoned_hashes);
+  r.starts.reserve(m.abandoned_hashes + 1);
+  r.origins.reserve(m.abandoned_origins);
+  uint32_t prev = 0;
+  for (uint64_t rec = 0; rec < m.abandoned_hashes; ++rec) {
+    uint32_t h;
+    if (delta) {
+      uint32_t dh = var();
+      check_format(rec == 0 || dh != 0, "unsorted/duplicate abandoned hashes");
+      check_format((uint64_t)prev + dh <= 0xFFFFFFFFull, "abandoned hash delta overflow");
+      h = prev + dh;
+    } else {
+      h = u32();
+    }
+    check_format(rec == 0 || prev < h, "unsorted/duplicate abandoned hashes");
+    prev = h;
+    uint32_t count = delta ? var() : u32();
+    check_format(count > 0 && count <= colors, "invalid abandoned origin count");
+    check_format(count <= m.abandoned_origins - r.origins.size(),
+                 "abandoned origins exceed manifest");
+    r.hashes.push_back(h);
+    r.starts.push_back(r.origins.size());
+    uint32_t po = 0;
+    for (uint32_t c = 0; c < count; ++c) {
+      uint32_t o;
+      if (delta) {
+        uint32_t dd = var();
+        check_format(c == 0 || dd != 0, "duplicate abandoned origins");
+        check_format((uint64_t)po + dd <= 0xFFFFFFFFull, "abandoned origin delta overflow");
+        o = po + dd;
+      } else {
+        o = u32();
+      }
+      check_format(o < colors, "invalid abandoned dataset ID");
+      check_format(c == 0 || o > po, "unsorted/duplicate abandoned origins");
+      r.origins.push_back(o);
+      po = o;
+    }
+  }
+  check_format(r.origins.size() == m.abandoned_origins,
+               "abandoned origin count differs from manifest");
+  check_format(p == d.size(), "unexpected abandoned map data");
+  r.starts.push_back(r.origins.size());
+  return r;
+}
+
+}  // namespace
+
+Workspace::~Workspace() {
+  release_graphs();
+  void* dev[] = {bases, offsets, packed, invalid, tile_counts, tile_first, tiles,
+                 scan_tmp, partial, counts, total, keys_out, keys_count};
+  for (void* p : dev)
+    if (p) cudaFree(p);
+  void* host[] = {h_bases, h_offsets, h_counts, h_total};
+  for (void* p : host)
+    if (p) cudaFreeHost(p);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void Workspace::release_graphs() {
+  for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+  graphs.clear();
+}
+
+Engine::Engine(const std::string& dir, const OpenOptions& options) { load(dir, options); }
+
+Engine::~Engine() {
+  ws_.reset();
+  cudaSetDevice(device_);
+  for (void* p : allocations_) cudaFree(p);
+  if (d_ix_rec_) cudaFree(d_ix_rec_);
+  if (d_ix_norec_) cudaFree(d_ix_norec_);
+}
+
+int Engine::span() const { return (int)m_.k; }
+
+void Engine::load(const std::string& dir, const OpenOptions& options) {
+  m_ = load_manifest(dir);
+  device_ = options.device;
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  cudaDeviceProp prop;
+  cuda_check(cudaGetDeviceProperties(&prop, device_), "cudaGetDeviceProperties");
+  sms_ = prop.multiProcessorCount;
+  check(m_.classes.size() <= (size_t)kMaxClasses, kEUnsupported, "too many source classes");
+  check(m_.index_mode != kFindere, kEUnsupported,
+        "findere indexes are not supported by the GPU query path yet");
+  for (auto& b : m_.banks)
+    check(b.fingerprint_first, kEUnsupported,
+          "legacy interleaved (non fingerprint-first) banks are not supported; rebuild the index");
+
+  // Seed parameters from the manifest (the query takes every setting from it).
+  sp_.mode = m_.index_mode;
+  sp_.k = (int)m_.k;
+  sp_.m = (int)m_.minimizer_size;
+  sp_.klen = m_.index_mode == kFindere ? (int)(m_.k - m_.findere_z) : (int)m_.k;
+  sp_.seed = m_.seed;
+  sp_.sampling = m_.modimizer_sampling;
+  if (m_.index_mode == kMinimizers && m_.k != m_.minimizer_size)
+    sp_.ocm = ocm_params((int)m_.k, (int)m_.minimizer_size);
+  else
+    sp_.ocm = OcmParams{1, (int)m_.minimizer_size, 1};
+  if (sp_.klen > 32) sp_.lk = long_kmer_consts(sp_.klen);
+  check(!m_.homopolymer_compression, kEUnsupported,
+        "homopolymer-compressed indexes are not supported by the GPU query path yet");
+
+  // Memory admission: banks (padded rows) + recovery directory.
+  uint64_t need = 0;
+  for (auto& b : m_.banks) need += b.slots * round_up(b.row_bytes(), 16);
+  need += m_.abandoned_recovery ? m_.abandoned_hashes * 8 * 4 + m_.abandoned_origins * 4 : 0;
+  size_t free_b = 0, total_b = 0;
+  cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+  uint64_t budget = options.hbm_budget
+                        ? options.hbm_budget
+                        : (free_b > (4ull << 30) ? free_b - (4ull << 30) : free_b / 2);
+  if (need > budget)
+    raise(kENoMem, "index needs " + std::to_string(need) + " bytes of HBM, budget is " +
+                       std::to_string(budget));
+
+  const int threads = options.threads > 0 ? options.threads
+                                          : (int)std::max(1u, std::thread::hardware_concurrency());
+  const int b = m_.fingerprint_bits;
+  host_ix_ = DevIndex{};
+  host_ix_.seed = m_.seed;
+  host_ix_.classes = (uint32_t)m_.classes.size();
+  host_ix_.colors = (uint32_t)m_.colors.size();
+  host_ix_.hashes = m_.hashes;
+  host_ix_.bits = b;
+
+  // Staging for bank uploads.
+  const uint64_t stage_bytes = 256ull << 20;
+  uint8_t* d_stage = nullptr;
+  dev_alloc(&d_stage, stage_bytes, "bank staging");
+  std::vector<uint8_t> payload;
+  for (size_t ci = 0; ci < m_.classes.size(); ++ci) {
+    const auto& banks = m_.classes[ci];
+    const BankMeta& first = m_.banks[banks[0]];
+    const uint64_t G = first.groups.size(), row_bytes = first.row_bytes();
+    const uint32_t stride = (uint32_t)round_up(row_bytes, 16);
+    DevClass& C = host_ix_.cls[ci];
+    C.slots = first.slots;
+    C.seg = m_.segment_for(first.slots);
+    C.partitions = (uint32_t)banks.size();
+    C.groups = (uint32_t)G;
+    C.row_stride = stride;
+    C.fp_chunks = (uint32_t)((first.lookup_bytes(b) + 15) / 16);
+    uint8_t* data = nullptr;
+    dev_alloc(&data, (uint64_t)banks.size() * first.slots * stride, "bank payload");
+    allocations_.push_back(data);
+    resident_bytes_ += (uint64_t)banks.size() * first.slots * stride;
+    for (size_t pi = 0; pi < banks.size(); ++pi) {
+      const BankMeta& bm = m_.banks[banks[pi]];
+      const uint64_t bytes = bm.slots * row_bytes;
+      payload.resize(bytes);
+      uint8_t header[40];
+      read_bank_stream(dir + "/" + bm.file, header, payload.data(), bytes, threads);
+      check_format(!memcmp(header, "ZORPOW3\0", 8), "invalid bank magic");
+      check_format(le64(header + 8) == bm.slots && le64(header + 16) == bm.row_bits &&
+                       le64(header + 24) == bm.groups.size() && le64(header + 32) == bytes,
+                   "bank header differs from manifest");
+      uint8_t* dst = data + pi * bm.slots * stride;
+      const uint64_t rows_per_chunk = std::max<uint64_t>(1, stage_bytes / row_bytes);
+      for (uint64_t r0 = 0; r0 < bm.slots; r0 += rows_per_chunk) {
+        uint64_t rows = std::min(rows_per_chunk, bm.slots - r0);
+        cuda_check(cudaMemcpy(d_stage, payload.data() + r0 * row_bytes, rows * row_bytes,
+                              cudaMemcpyHostToDevice),
+                   "bank upload");
+        repack_rows_kernel<<<sms_ * 8, 256>>>(d_stage, rows, (uint32_t)row_bytes, stride,
+                                              dst + r0 * stride);
+        cuda_check(cudaGetLastError(), "repack_rows_kernel");
+      }
+    }
+    // Group -> colour table, multi-member decode table.
+    std::vector<uint32_t> gc(G), multi, members;
+    for (uint64_t g = 0; g < G; ++g) {
+      const GroupMeta& gm = first.groups[g];
+      if (gm.members.size() == 1) {
+        gc[g] = gm.members[0];
+        continue;
+      }
+      check(gm.members.size() <= 63, kEFormat, "invalid membership width");
+      gc[g] = kMultiGroup | (uint32_t)(multi.size() / 3);
+      multi.push_back((uint32_t)(G * b + gm.offset - g * b));
+      multi.push_back((uint32_t)gm.members.size());
+      multi.push_back((uint32_t)members.size());
+      members.insert(members.end(), gm.members.begin(), gm.members.end());
+    }
+    uint32_t *d_gc, *d_multi, *d_members;
+    dev_alloc(&d_gc, gc.size(), "group table");
+    dev_alloc(&d_multi, multi.size(), "multi table");
+    dev_alloc(&d_members, members.size(), "member table");
+    allocations_.push_back(d_gc);
+    allocations_.push_back(d_multi);
+    allocations_.push_back(d_members);
+    cuda_check(cudaMemcpy(d_gc, gc.data(), gc.size() * 4, cudaMemcpyHostToDevice), "upload");
+    if (!multi.empty()) {
+      cuda_check(cudaMemcpy(d_multi, multi.data(), multi.size() * 4, cudaMemcpyHostToDevice),
+                 "upload");
+      cuda_check(cudaMemcpy(d_members, members.data(), members.size() * 4, cudaMemcpyHostToDevice),
+                 "upload");
+    }
+    C.data = data;
+    C.group_color = d_gc;
+    C.multi = d_multi;
+    C.members = d_members;
+  }
+  cuda_check(cudaDeviceSynchronize(), "bank upload");
+  cudaFree(d_stage);
+
+  // Recovery directory.
+  if (m_.abandoned_recovery && m_.abandoned_hashes) {
+    RecoveryRecords rr = read_recovery(dir, m_);
+    const uint64_t n = rr.hashes.size();
+    check(n < (1ull << 31), kEUnsupported, "too many abandoned hashes for the device directory");
+    check(rr.origins.size() < (1ull << 32), kEUnsupported, "too many abandoned origins");
+    uint64_t cap = 4;
+    while (cap < 2 * n) cap <<= 1;
+    uint32_t bits = 0;
+    while ((1ull << bits) < cap) ++bits;
+    std::vector<uint64_t> dir_entries(cap, (uint64_t)kRecEmpty);
+    std::vector<uint2> ranges;
+    for (uint64_t i = 0; i < n; ++i) {
+      uint32_t h = rr.hashes[i];
+      uint64_t len = rr.starts[i + 1] - rr.starts[i];
+      uint32_t value;
+      if (len == 1 && rr.origins[rr.starts[i]] < kRecMultiple) {
+        value = rr.origins[rr.starts[i]];
+      } else {
+        value = kRecMultiple | (uint32_t)ranges.size();
+        ranges.push_back(make_uint2((uint32_t)rr.starts[i], (uint32_t)len));
+      }
+      uint64_t slot = h >> (32 - bits), mask = cap - 1;
+      while ((uint32_t)dir_entries[slot] != kRecEmpty) slot = (slot + 1) & mask;
+      dir_entries[slot] = ((uint64_t)h << 32) | value;
+    }
+    uint64_t* d_dir;
+    uint2* d_ranges;
+    uint32_t* d_origins;
+    dev_alloc(&d_dir, cap, "recovery directory");
+    dev_alloc(&d_ranges, ranges.size(), "recovery ranges");
+    dev_alloc(&d_origins, rr.origins.size(), "recovery origins");
+    allocations_.push_back(d_dir);
+    allocations_.push_back(d_ranges);
+    allocations_.push_back(d_origins);
+    resident_bytes_ += cap * 8 + ranges.size() * 8 + rr.origins.size() * 4;
+    cuda_check(cudaMemcpy(d_dir, dir_entries.data(), cap * 8, cudaMemcpyHostToDevice), "upload");
+    if (!ranges.empty())
+      cuda_check(cudaMemcpy(d_ranges, ranges.data(), ranges.size() * 8, cudaMemcpyHostToDevice),
+                 "upload");
+    cuda_check(cudaMemcpy(d_origins, rr.origins.data(), rr.origins.size() * 4,
+                          cudaMemcpyHostToDevice),
+               "upload");
+    host_ix_.rec = DevRecovery{d_dir, d_ranges, d_origins, bits};
+  }
+  dev_alloc(&d_ix_rec_, 1, "index table");
+  dev_alloc(&d_ix_norec_, 1, "index table");
+  cuda_check(cudaMemcpy(d_ix_rec_, &host_ix_, sizeof(DevIndex), cudaMemcpyHostToDevice), "upload");
+  DevIndex norec = host_ix_;
+  norec.rec = DevRecovery{nullptr, nullptr, nullptr, 0};
+  cuda_check(cudaMemcpy(d_ix_norec_, &norec, sizeof(DevIndex), cudaMemcpyHostToDevice), "upload");
+  launch_ = default_launch();
+  ws_ = make_workspace();
+}
+
+uint64_t Engine::gather_bytes_per_seed() const {
+  uint64_t s = 0;
+  for (auto& cls : m_.classes) s += (uint64_t)m_.hashes * m_.banks[cls[0]].lookup_bytes(m_.fingerprint_bits);
+  return s;
+}
+
+QueryLaunch Engine::default_launch() const {
+  uint32_t chunks = 1;
+  for (uint32_t c = 0; c < host_ix_.classes; ++c) chunks = std::max(chunks, host_ix_.cls[c].fp_chunks);
+  int team = 1;
+  while (team < 32 && (uint32_t)team < chunks) team <<= 1;
+  QueryLaunch l;
+  l.team = team;
+  l.warps = 4;
+  l.smem_counters = m_.colors.size() <= 16384 ? 1 : 0;
+  l.blocks = 0;  // 0: fill the device (occupancy-derived)
+  return l;
+}
+
+size_t Engine::fused_smem_bytes(const QueryLaunch& l) const {
+  return FusedSmem::total(sp_.mode, sp_.k, (uint32_t)m_.colors.size(), l.smem_counters, l.warps);
+}
+
+int Engine::max_blocks(const QueryLaunch& l) const {
+  int per_sm = 0;
+  size_t smem = fused_smem_bytes(l);
+  cudaFuncSetAttribute(fused_query_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_query_kernel,
+                                                           l.warps * 32, smem),
+             "occupancy");
+  return std::max(1, per_sm) * sms_;
+}
+
+void Engine::set_launch(const QueryLaunch& l) {
+  check(l.team >= 1 && l.team <= 32 && (l.team & (l.team - 1)) == 0, kEInval,
+        "team size must be a power of two in 1..32");
+  check(l.warps >= 1 && l.warps <= 16, kEInval, "warps per block must be in 1..16");
+  check(l.smem_counters == 0 || m_.colors.size() <= 16384, kEInval,
+        "shared-memory counters support at most 16384 colours");
+  check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
+  std::lock_guard<std::mutex> lock(mu_);
+  launch_ = l;
+  ws_->release_graphs();
+}
+
+std::unique_ptr<Workspace> Engine::make_workspace() {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  auto ws = std::make_unique<Workspace>();
+  ws->device = device_;
+  cuda_check(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  return ws;
+}
+
+void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
+  const uint64_t colors = m_.colors.size();
+  if (nbases > ws.cap_bases) {
+    uint64_t cap = std::max<uint64_t>(nbases, ws.cap_bases * 3 / 2);
+    cap = round_up(cap, 4096);
+    if (ws.bases) cudaFree(ws.bases);
+    if (ws.packed) cudaFree(ws.packed);
+    if (ws.invalid) cudaFree(ws.invalid);
+    dev_alloc(&ws.bases, cap + 64, "batch bases");
+    dev_alloc(&ws.packed, cap / 32 + 8, "packed bases");
+    dev_alloc(&ws.invalid, cap / 32 + 8, "invalid masks");
+    ws.cap_bases = cap;
+    ws.cap_tiles = 0;
+    ws.release_graphs();
+  }
+  if (records > ws.cap_records || !ws.offsets) {
+    uint64_t cap = std::max<uint64_t>({records, ws.cap_records * 3 / 2, 1024});
+    if (ws.offsets) cudaFree(ws.offsets);
+    if (ws.tile_counts) cudaFree(ws.tile_counts);
+    if (ws.tile_first) cudaFree(ws.tile_first);
+    if (ws.scan_tmp) cudaFree(ws.scan_tmp);
+    dev_alloc(&ws.offsets, cap + 1, "record offsets");
+    dev_alloc(&ws.tile_counts, cap + 1, "tile counts");
+    dev_alloc(&ws.tile_first, cap + 1, "tile offsets");
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, ws.tile_counts, ws.tile_first, (int)(cap + 1));
+    dev_alloc((uint8_t**)&ws.scan_tmp, tmp, "scan scratch");
+    ws.scan_tmp_bytes = tmp;
+    ws.cap_records = cap;
+    ws.cap_tiles = 0;
+    ws.release_graphs();
+  }
+  uint64_t tiles = ws.cap_bases / kTileWindows + ws.cap_bases / kFindereTask + ws.cap_records + 16;
+  if (tiles > ws.cap_tiles) {
+    if (ws.tiles) cudaFree(ws.tiles);
+    dev_alloc(&ws.tiles, tiles, "tiles");
+    ws.cap_tiles = tiles;
+    ws.release_graphs();
+  }
+  uint64_t partial = (uint64_t)max_blocks(launch_) * colors;
+  if (partial > ws.cap_partial) {
+    if (ws.partial) cudaFree(ws.partial);
+    dev_alloc(&ws.partial, partial, "block counters");
+    ws.cap_partial = partial;
+    ws.release_graphs();
+  }
+  if (colors > ws.cap_colors || !ws.counts) {
+    if (ws.counts) cudaFree(ws.counts);
+    if (ws.total) cudaFree(ws.total);
+    dev_alloc(&ws.counts, colors, "counts");
+    dev_alloc(&ws.total, 1, "total");
+    ws.cap_colors = colors;
+    ws.release_graphs();
+  }
+}
+
+void Engine::ensure_host_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
+  if (nbases > ws.cap_h_bases) {
+    if (ws.h_bases) cudaFreeHost(ws.h_bases);
+    uint64_t cap = round_up(std::max<uint64_t>(nbases, ws.cap_h_bases * 3 / 2), 4096);
+    host_alloc(&ws.h_bases, cap);
+    ws.cap_h_bases = cap;
+  }
+  if (records + 1 > ws.cap_h_records || !ws.h_offsets) {
+    if (ws.h_offsets) cudaFreeHost(ws.h_offsets);
+    uint64_t cap = std::max<uint64_t>({records + 1, ws.cap_h_records * 3 / 2, 1024});
+    host_alloc(&ws.h_offsets, cap);
+    ws.cap_h_records = cap;
+  }
+  if (!ws.h_counts) {
+    host_alloc(&ws.h_counts, std::max<uint64_t>(m_.colors.size(), 1));
+    host_alloc(&ws.h_total, 1);
+  }
+}
+
+void Engine::plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records,
+                        cudaStream_t s) {
+  const int findere = m_.index_mode == kFindere;
+  int grid = (int)std::min<uint64_t>((records + 255) / 256, (uint64_t)sms_ * 16);
+  grid = std::max(grid, 1);
+  cuda_check(cudaMemsetAsync(ws.tile_counts + records, 0, 4, s), "memset");
+  if (records) {
+    count_tiles_kernel<<<grid, 256, 0, s>>>(offsets, records, span(), findere, ws.tile_counts);
+    cuda_check(cudaGetLastError(), "count_tiles_kernel");
+  }
+  size_t tmp = ws.scan_tmp_bytes;
+  cuda_check(cub::DeviceScan::ExclusiveSum(ws.scan_tmp, tmp, ws.tile_counts, ws.tile_first,
+                                           (int)(records + 1), s),
+             "tile scan");
+  if (records) {
+    fill_tiles_kernel<<<grid, 256, 0, s>>>(offsets, records, span(), ws.tile_first, ws.tiles);
+    cuda_check(cudaGetLastError(), "fill_tiles_kernel");
+  }
+}
+
+void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                     const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
+                     unsigned long long* total, cudaStream_t s) {
+  const uint64_t words = nbases / 32 + 2;
+  {
+    int grid = (int)std::min<uint64_t>((words + 255) / 256, (uint64_t)sms_ * 16);
+    pack_kernel<<<std::max(grid, 1), 256, 0, s>>>(bases, nbases, ws.packed, ws.invalid, words);
+    cuda_check(cudaGetLastError(), "pack_kernel");
+  }
+  plan_tiles(ws, offsets, records, s);
+  QueryLaunch l = launch_;
+  const size_t smem = fused_smem_bytes(l);
+  const int blocks_cap = max_blocks(l);
+  uint64_t tiles_bound = nbases / kTileWindows + records + nbases / kFindereTask + 1;
+  uint64_t want = (tiles_bound + l.warps - 1) / l.warps;
+  int blocks = l.blocks > 0 ? std::min(l.blocks, blocks_cap)
+                            : (int)std::min<uint64_t>((uint64_t)blocks_cap, std::max<uint64_t>(want, 1));
+  l.blocks = blocks;
+  BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records};
+  fused_query_kernel<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l,
+                                                        ws.partial, counts, total);
+  cuda_check(cudaGetLastError(), "fused_query_kernel");
+  if (l.smem_counters) {
+    const uint32_t colors = (uint32_t)m_.colors.size();
+    reduce_counters_kernel<<<std::max(1u, (colors + 255) / 256), 256, 0, s>>>(ws.partial, blocks,
+                                                                               colors, counts);
+    cuda_check(cudaGetLastError(), "reduce_counters_kernel");
+  }
+}
+
+void Engine::query_device(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                          const uint64_t* offsets, uint64_t records, bool recover,
+                          uint64_t* counts, unsigned long long* total, cudaStream_t s,
+                          bool use_graph) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  ensure_capacity(ws, nbases, records);
+  if (!use_graph) {
+    enqueue(ws, bases, nbases, offsets, records, recover, counts, total, s);
+    return;
+  }
+  auto key = std::make_tuple((const void*)bases, nbases, (const void*)offsets, records,
+                             (void*)counts, (void*)total, (int)recover);
+  auto it = ws.graphs.find(key);
+  if (it == ws.graphs.end()) {
+    cudaStream_t cap;
+    cuda_check(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaGraph_t graph;
+    cuda_check(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      enqueue(ws, bases, nbases, offsets, records, recover, counts, total, cap);
+    } catch (...) {
+      cudaStreamEndCapture(cap, &graph);
+      cudaStreamDestroy(cap);
+      throw;
+    }
+    cuda_check(cudaStreamEndCapture(cap, &graph), "end capture");
+    cudaGraphExec_t exec;
+    cuda_check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+    cudaGraphDestroy(graph);
+    cudaStreamDestroy(cap);
+    it = ws.graphs.emplace(key, exec).first;
+  }
+  cuda_check(cudaGraphLaunch(it->second, s), "graph launch");
+}
+
+void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                        const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
+                        uint64_t* total) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
+  for (uint64_t r = 0; r < records; ++r)
+    check(offsets[r] <= offsets[r + 1], kEInval, "offsets must be non-decreasing");
+  ensure_capacity(ws, nbases, records);
+  ensure_host_capacity(ws, nbases, records);
+  const uint64_t colors = m_.colors.size();
+  cudaStream_t s = ws.stream;
+  memcpy(ws.h_bases, bases, nbases);
+  memcpy(ws.h_offsets, offsets, (records + 1) * 8);
+  cuda_check(cudaMemcpyAsync(ws.bases, ws.h_bases, nbases, cudaMemcpyHostToDevice, s), "H2D");
+  cuda_check(cudaMemcpyAsync(ws.offsets, ws.h_offsets, (records + 1) * 8, cudaMemcpyHostToDevice, s),
+             "H2D");
+  cuda_check(cudaMemsetAsync(ws.counts, 0, colors * 8, s), "memset");
+  cuda_check(cudaMemsetAsync(ws.total, 0, 8, s), "memset");
+  enqueue(ws, ws.bases, nbases, ws.offsets, records, recover, ws.counts, ws.total, s);
+  cuda_check(cudaMemcpyAsync(ws.h_counts, ws.counts, colors * 8, cudaMemcpyDeviceToHost, s), "D2H");
+  cuda_check(cudaMemcpyAsync(ws.h_total, ws.total, 8, cudaMemcpyDeviceToHost, s), "D2H");
+  cuda_check(cudaStreamSynchronize(s), "query");
+  memcpy(counts, ws.h_counts, colors * 8);
+  *total = *ws.h_total;
+}
+
+void Engine::query_host_plain(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                              const uint64_t* offsets, uint64_t records, bool recover,
+                              uint64_t* counts, uint64_t* total) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
+  ensure_capacity(ws, nbases, records);
+  ensure_host_capacity(ws, nbases, records);
+  const uint64_t colors = m_.colors.size();
+  cudaStream_t s = ws.stream;
+  memcpy(ws.h_bases, bases, nbases);
+  cuda_check(cudaMemcpyAsync(ws.bases, ws.h_bases, nbases, cudaMemcpyHostToDevice, s), "H2D");
+  cuda_check(cudaMemsetAsync(ws.counts, 0, colors * 8, s), "memset");
+  cuda_check(cudaMemsetAsync(ws.total, 0, 8, s), "memset");
+  // One record per launch sequence, default tiles: each record is its own batch.
+  for (uint64_t r = 0; r < records; ++r) {
+    ws.h_offsets[2 * (r % 2)] = 0;
+    ws.h_offsets[2 * (r % 2) + 1] = offsets[r + 1] - offsets[r];
+    uint64_t* d_off = ws.offsets + 2 * (r % 2);
+    cuda_check(cudaMemcpyAsync(d_off, ws.h_offsets + 2 * (r % 2), 16, cudaMemcpyHostToDevice, s),
+               "H2D");
+    enqueue(ws, ws.bases + offsets[r], offsets[r + 1] - offsets[r], d_off, 1, recover, ws.counts,
+            ws.total, s);
+    if (r % 2 == 1) cuda_check(cudaStreamSynchronize(s), "plain query");
+  }
+  cuda_check(cudaMemcpyAsync(ws.h_counts, ws.counts, colors * 8, cudaMemcpyDeviceToHost, s), "D2H");
+  cuda_check(cudaMemcpyAsync(ws.h_total, ws.total, 8, cudaMemcpyDeviceToHost, s), "D2H");
+  cuda_check(cudaStreamSynchronize(s), "plain query");
+  memcpy(counts, ws.h_counts, colors * 8);
+  *total = *ws.h_total;
+}
+
+void Engine::extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                          const uint64_t* offsets, uint64_t records, std::vector<uint64_t>& keys) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
+  ensure_capacity(ws, nbases, records);
+  ensure_host_capacity(ws, nbases, records);
+  cudaStream_t s = ws.stream;
+  memcpy(ws.h_bases, bases, nbases);
+  memcpy(ws.h_offsets, offsets, (records + 1) * 8);
+  cuda_check(cudaMemcpyAsync(ws.bases, ws.h_bases, nbases, cudaMemcpyHostToDevice, s), "H2D");
+  cuda_check(cudaMemcpyAsync(ws.offsets, ws.h_offsets, (records + 1) * 8, cudaMemcpyHostToDevice, s),
+             "H2D");
+  const uint64_t words = nbases / 32 + 2;
+  pack_kernel<<<std::max<int>(1, (int)std::min<uint64_t>((words + 255) / 256, sms_ * 16ull)), 256, 0, s>>>(
+      ws.bases, nbases, ws.packed, ws.invalid, words);
+  cuda_check(cudaGetLastError(), "pack_kernel");
+  plan_tiles(ws, ws.offsets, records, s);
+  uint32_t ntiles = 0;
+  cuda_check(cudaMemcpyAsync(&ntiles, ws.tile_first + records, 4, cudaMemcpyDeviceToHost, s), "D2H");
+  cuda_check(cudaStreamSynchronize(s), "tiles");
+  if (ntiles == 0) {
+    keys.clear();
+    return;
+  }
+  uint64_t need = (uint64_t)ntiles * kTileWindows;
+  if (need > ws.cap_keys) {
+    if (ws.keys_out) cudaFree(ws.keys_out);
+    if (ws.keys_count) cudaFree(ws.keys_count);
+    dev_alloc(&ws.keys_out, need, "extracted keys");
+    dev_alloc(&ws.keys_count, ntiles, "extracted counts");
+    ws.cap_keys = need;
+  }
+  const int warps = 4;
+  size_t smem = 256 * 8 + warps * FusedSmem::warp_bytes(sp_.mode, sp_.k);
+  cudaFuncSetAttribute(extract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  BatchView bv{PackedView{ws.packed, ws.invalid}, ws.offsets, ws.tiles, ws.tile_first + records};
+  int grid = (int)std::min<uint64_t>((ntiles + warps - 1) / warps, (uint64_t)sms_ * 8);
+  extract_kernel<<<grid, warps * 32, smem, s>>>(bv, sp_, ws.keys_out, ws.keys_count, warps);
+  cuda_check(cudaGetLastError(), "extract_kernel");
+  std::vector<uint64_t> all(need);
+  std::vector<uint32_t> cnt(ntiles);
+  cuda_check(cudaMemcpyAsync(all.data(), ws.keys_out, need * 8, cudaMemcpyDeviceToHost, s), "D2H");
+  cuda_check(cudaMemcpyAsync(cnt.data(), ws.keys_count, ntiles * 4ull, cudaMemcpyDeviceToHost, s),
+             "D2H");
+  cuda_check(cudaStreamSynchronize(s), "extract");
+  keys.clear();
+  for (uint32_t t = 0; t < ntiles; ++t)
+    keys.insert(keys.end(), all.begin() + (uint64_t)t * kTileWindows,
+                all.begin() + (uint64_t)t * kTileWindows + cnt[t]);
+}
+
+}  // namespace zx

@@ -1,0 +1,127 @@
+// Host runtime of the GPU query path: loads an index directory into HBM and
+// runs batched queries on one device.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "host/manifest.h"
+#include "kernels/device_index.cuh"
+#include "kernels/types.cuh"
+
+namespace zx {
+
+struct OpenOptions {
+  int device = 0;
+  uint64_t hbm_budget = 0;  // bytes the resident index may take; 0 = free memory - 4 GiB
+  int threads = 0;          // host threads for decompression; 0 = hardware concurrency
+};
+
+// Device buffers of one in-flight batch. One workspace serves one stream at a
+// time; the serving loop keeps one per slot.
+struct Workspace {
+  int device = 0;
+  uint8_t* bases = nullptr;
+  uint64_t* offsets = nullptr;
+  uint64_t* packed = nullptr;
+  uint32_t* invalid = nullptr;
+  uint32_t* tile_counts = nullptr;  // records + 1
+  uint32_t* tile_first = nullptr;   // records + 1 (last entry = tile total)
+  Tile* tiles = nullptr;
+  void* scan_tmp = nullptr;
+  size_t scan_tmp_bytes = 0;
+  uint32_t* partial = nullptr;
+  uint64_t* counts = nullptr;
+  unsigned long long* total = nullptr;
+  uint64_t* keys_out = nullptr;     // extraction-only output
+  uint32_t* keys_count = nullptr;
+  // Pinned host staging.
+  uint8_t* h_bases = nullptr;
+  uint64_t* h_offsets = nullptr;
+  uint64_t* h_counts = nullptr;
+  unsigned long long* h_total = nullptr;
+  uint64_t cap_bases = 0, cap_records = 0, cap_tiles = 0, cap_partial = 0, cap_colors = 0,
+           cap_keys = 0, cap_h_bases = 0, cap_h_records = 0;
+  cudaStream_t stream = nullptr;
+  // Graph cache: one instantiated graph per (input pointers, sizes, recover).
+  std::map<std::tuple<const void*, uint64_t, const void*, uint64_t, void*, void*, int>,
+           cudaGraphExec_t>
+      graphs;
+  ~Workspace();
+  void release_graphs();
+};
+
+class Engine {
+ public:
+  Engine(const std::string& dir, const OpenOptions& options);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  const Manifest& manifest() const { return m_; }
+  int device() const { return device_; }
+  uint64_t resident_bytes() const { return resident_bytes_; }
+  int span() const;  // k-window span of the index mode
+  const SeedParams& seed_params() const { return sp_; }
+  // Launch configuration used by the batched kernels (tunable).
+  QueryLaunch launch() const { return launch_; }
+  void set_launch(const QueryLaunch& l);
+  QueryLaunch default_launch() const;
+  size_t fused_smem_bytes(const QueryLaunch& l) const;
+  int max_blocks(const QueryLaunch& l) const;
+  // Bytes of fingerprint planes gathered per seed, summed over classes.
+  uint64_t gather_bytes_per_seed() const;
+
+  std::unique_ptr<Workspace> make_workspace();
+  Workspace& default_workspace() { return *ws_; }
+
+  // Asynchronous query of a batch resident on the device. counts (colors
+  // entries) and total are accumulated, not cleared. use_graph replays a
+  // captured CUDA graph when the same batch shape was seen before.
+  void query_device(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
+                    uint64_t records, bool recover, uint64_t* counts, unsigned long long* total,
+                    cudaStream_t stream, bool use_graph);
+  // Synchronous query of host buffers (bases, records + 1 offsets).
+  void query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
+                  uint64_t records, bool recover, uint64_t* counts, uint64_t* total);
+  // One record per launch (the plain form), host buffers, synchronous.
+  void query_host_plain(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                        const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
+                        uint64_t* total);
+  // Seeds of host records in record/window order (extraction only).
+  void extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
+                    uint64_t records, std::vector<uint64_t>& keys);
+
+ private:
+  void load(const std::string& dir, const OpenOptions& options);
+  void ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records);
+  void ensure_host_capacity(Workspace& ws, uint64_t nbases, uint64_t records);
+  void enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
+               uint64_t records, bool recover, uint64_t* counts, unsigned long long* total,
+               cudaStream_t stream);
+  void plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records, cudaStream_t stream);
+
+  Manifest m_;
+  int device_ = 0;
+  int sms_ = 0;
+  SeedParams sp_{};
+  QueryLaunch launch_{};
+  DevIndex host_ix_{};
+  DevIndex* d_ix_rec_ = nullptr;    // with recovery
+  DevIndex* d_ix_norec_ = nullptr;  // recovery disabled
+  std::vector<void*> allocations_;
+  uint64_t resident_bytes_ = 0;
+  std::unique_ptr<Workspace> ws_;
+  std::mutex mu_;
+};
+
+// CUDA error check that throws zx::Error(kECuda).
+void cuda_check(cudaError_t e, const char* what);
+
+}  // namespace zx

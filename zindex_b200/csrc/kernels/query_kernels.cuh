@@ -1,0 +1,218 @@
+// Batched query kernels: tile planning, the fused seed-extraction + probe
+// kernel and the per-colour counter reduction.
+//
+// A batch is many records of uneven length (bases concatenated, offsets[r]
+// .. offsets[r+1]). Records are cut into tiles of at most kTileWindows
+// windows (a device work list built by plan_tiles); one warp extracts the
+// seeds of a tile into shared memory and then probes them with teams of T
+// lanes. Counters live in shared memory per block and are reduced at the end
+// (the aggregate matches[] of query_ordinary, query_stream.rs:280-300, and
+// flush, storage.rs:3545-3598).
+#pragma once
+#include <stdint.h>
+
+#include "device_index.cuh"
+#include "probe.cuh"
+#include "seeds.cuh"
+
+namespace zx {
+
+constexpr uint32_t kTileWindows = 256;
+constexpr uint32_t kFindereTask = 16384;  // src/findere.rs:13-16
+
+// Windows of record r: k-windows fully inside the record.
+__device__ __forceinline__ uint32_t record_windows(const uint64_t* offsets, uint64_t r, int span) {
+  uint64_t len = offsets[r + 1] - offsets[r];
+  return len >= (uint64_t)span ? (uint32_t)(len - span + 1) : 0u;
+}
+
+// Tiles per record. Findere tiles never cross a 16,384-window task.
+__global__ void count_tiles_kernel(const uint64_t* __restrict__ offsets, uint64_t records,
+                                   int span, int findere, uint32_t* __restrict__ counts) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < records;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t w = record_windows(offsets, r, span);
+    uint32_t n;
+    if (!findere) {
+      n = (w + kTileWindows - 1) / kTileWindows;
+    } else {
+      uint32_t full = w / kFindereTask, rest = w % kFindereTask;
+      n = full * (kFindereTask / kTileWindows) + (rest + kTileWindows - 1) / kTileWindows;
+    }
+    counts[r] = n;
+  }
+}
+
+__global__ void fill_tiles_kernel(const uint64_t* __restrict__ offsets, uint64_t records, int span,
+                                  const uint32_t* __restrict__ first, Tile* __restrict__ tiles) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < records;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t w = record_windows(offsets, r, span);
+    uint32_t t = first[r];
+    for (uint32_t w0 = 0; w0 < w;) {
+      uint32_t task = (w0 / kFindereTask) * kFindereTask;
+      uint32_t end = min(w, min(w0 + kTileWindows, task + kFindereTask));
+      tiles[t++] = Tile{(uint32_t)r, w0, end - w0, task};
+      w0 = end;
+    }
+  }
+}
+
+struct BatchView {
+  PackedView pv;
+  const uint64_t* offsets;
+  const Tile* tiles;
+  const uint32_t* ntiles;  // device scalar
+};
+
+// Shared memory of the fused kernel, in order: DevIndex copy, counters,
+// inner hash table (minimizers), then per warp: keys[2 * kTileWindows],
+// minimizer scratch (pre, suf, pos).
+struct FusedSmem {
+  static constexpr size_t ix_bytes = (sizeof(DevIndex) + 15) / 16 * 16;
+  static __host__ __device__ size_t counter_bytes(uint32_t colors, int smem_counters) {
+    return smem_counters ? ((size_t)colors * 4 + 15) / 16 * 16 : 0;
+  }
+  static __host__ __device__ size_t ocm_entries(int k) { return kTileWindows + (size_t)k + 1; }
+  static __host__ __device__ size_t warp_bytes(int mode, int k) {
+    size_t b = 2 * kTileWindows * 8;
+    if (mode == 1) b += 2 * ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
+    return (b + 15) / 16 * 16;
+  }
+  static __host__ __device__ size_t total(int mode, int k, uint32_t colors, int smem_counters,
+                                          int warps) {
+    return ix_bytes + counter_bytes(colors, smem_counters) + (mode == 1 ? 256 * 8 : 0) +
+           (size_t)warps * warp_bytes(mode, k);
+  }
+};
+
+// Extracts the seeds of one tile into `keys`; returns their number.
+__device__ __forceinline__ uint32_t extract_tile(const BatchView& bv, const SeedParams& sp,
+                                                 const Tile& t, uint64_t* keys, uint8_t* ocm,
+                                                 const uint64_t* inner, int lane) {
+  const uint64_t rb = bv.offsets[t.record];
+  switch (sp.mode) {
+    case 1:
+      if (sp.k == sp.m) return tile_ocm_full(bv.pv, rb, t.w0, t.nw, sp.m, keys, lane);
+      {
+        Rank16* pre = reinterpret_cast<Rank16*>(ocm);
+        Rank16* suf = pre + FusedSmem::ocm_entries(sp.k);
+        uint32_t* pos = reinterpret_cast<uint32_t*>(suf + FusedSmem::ocm_entries(sp.k));
+        return tile_ocm(bv.pv, rb, t.w0, t.nw, sp, inner, pre, suf, pos, keys, lane);
+      }
+    case 0:
+    case 2: {
+      bool modi = sp.mode == 2;
+      if (sp.klen <= 32)
+        return tile_kmers_short(bv.pv, rb, t.w0, t.nw, sp.klen, modi, sp.seed, sp.sampling, keys,
+                                lane);
+      return tile_kmers_long(bv.pv, rb, t.w0, t.nw, sp.klen, sp.lk, modi, sp.seed, sp.sampling,
+                             keys, keys + kTileWindows, lane);
+    }
+    default:
+      return 0;
+  }
+}
+
+__device__ __forceinline__ void load_index_smem(const DevIndex* __restrict__ gix, DevIndex* six) {
+  const uint4* src = reinterpret_cast<const uint4*>(gix);
+  uint4* dst = reinterpret_cast<uint4*>(six);
+  for (uint32_t i = threadIdx.x; i < sizeof(DevIndex) / 16; i += blockDim.x) dst[i] = src[i];
+}
+
+__device__ __forceinline__ void build_inner_table(const SeedParams& sp, uint64_t* inner) {
+  if (sp.mode != 1) return;
+  const int s = sp.ocm.s;
+  for (uint32_t v = threadIdx.x; v < (1u << (2 * s)); v += blockDim.x)
+    inner[v] = mixsplit(canonical_encoded(v, s), sp.seed ^ kInnerHashSeed);
+}
+
+// Fused extraction + probe over the tile list. partial: gridDim.x x colors
+// block counters (smem_counters) or null; counts: global counters (used
+// directly when smem_counters == 0). total: seeds processed.
+__global__ void __launch_bounds__(512) fused_query_kernel(const DevIndex* __restrict__ gix,
+                                                          BatchView bv, SeedParams sp,
+                                                          QueryLaunch lc,
+                                                          uint32_t* __restrict__ partial,
+                                                          uint64_t* __restrict__ counts,
+                                                          unsigned long long* __restrict__ total) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  DevIndex* six = reinterpret_cast<DevIndex*>(smem);
+  uint8_t* p = smem + FusedSmem::ix_bytes;
+  uint32_t* scount = nullptr;
+  if (lc.smem_counters) {
+    scount = reinterpret_cast<uint32_t*>(p);
+    p += FusedSmem::counter_bytes(gix->colors, 1);
+  }
+  uint64_t* inner = nullptr;
+  if (sp.mode == 1) {
+    inner = reinterpret_cast<uint64_t*>(p);
+    p += 256 * 8;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(sp.mode, sp.k);
+  uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
+  uint8_t* ocm = wbase + 2 * kTileWindows * 8;
+
+  load_index_smem(gix, six);
+  build_inner_table(sp, inner);
+  const uint32_t colors = gix->colors;
+  if (scount)
+    for (uint32_t c = threadIdx.x; c < colors; c += blockDim.x) scount[c] = 0;
+  __syncthreads();
+  const DevIndex& ix = *six;
+  const Counters cnt{scount, counts};
+  const int T = lc.team, team = lane / T, tl = lane % T, nteams = 32 / T;
+  const uint32_t ntiles = *bv.ntiles;
+  const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
+  unsigned long long seeds = 0;
+  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + warp; t < ntiles; t += warps_total) {
+    const Tile tile = bv.tiles[t];
+    uint32_t n = extract_tile(bv, sp, tile, keys, ocm, inner, lane);
+    __syncwarp();
+    seeds += n;
+    for (uint32_t i = team; i < n; i += nteams) probe_seed(ix, keys[i], tl, T, cnt);
+    __syncwarp();
+  }
+  if (lane == 0 && seeds) atomicAdd(total, seeds);
+  __syncthreads();
+  if (scount)
+    for (uint32_t c = threadIdx.x; c < colors; c += blockDim.x)
+      partial[(uint64_t)blockIdx.x * colors + c] = scount[c];
+}
+
+// counts[c] += sum over blocks of partial[block][c].
+__global__ void reduce_counters_kernel(const uint32_t* __restrict__ partial, uint32_t blocks,
+                                       uint32_t colors, uint64_t* __restrict__ counts) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < colors; c += gridDim.x * blockDim.x) {
+    uint64_t s = 0;
+    for (uint32_t b = 0; b < blocks; ++b) s += partial[(uint64_t)b * colors + c];
+    counts[c] += s;
+  }
+}
+
+// Extraction only (testing and inspection): tile t's keys go to
+// out[t * kTileWindows ...], their number to out_count[t].
+__global__ void extract_kernel(BatchView bv, SeedParams sp, uint64_t* __restrict__ out,
+                               uint32_t* __restrict__ out_count, int warps_per_block) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint64_t* inner = reinterpret_cast<uint64_t*>(smem);
+  uint8_t* p = smem + 256 * 8;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(sp.mode, sp.k);
+  uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
+  uint8_t* ocm = wbase + 2 * kTileWindows * 8;
+  build_inner_table(sp, inner);
+  __syncthreads();
+  const uint32_t ntiles = *bv.ntiles;
+  const uint32_t warps_total = gridDim.x * warps_per_block;
+  for (uint32_t t = blockIdx.x * warps_per_block + warp; t < ntiles; t += warps_total) {
+    uint32_t n = extract_tile(bv, sp, bv.tiles[t], keys, ocm, inner, lane);
+    __syncwarp();
+    for (uint32_t i = lane; i < n; i += 32) out[(uint64_t)t * kTileWindows + i] = keys[i];
+    if (lane == 0) out_count[t] = n;
+    __syncwarp();
+  }
+}
+
+}  // namespace zx

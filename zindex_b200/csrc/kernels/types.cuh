@@ -1,0 +1,35 @@
+// Plain parameter structs shared by the host runtime and the query kernels.
+#pragma once
+#include <stdint.h>
+
+#include "../zx_hash.h"
+#include "device_index.cuh"
+
+namespace zx {
+
+struct SeedParams {
+  int mode;        // 0 kmers, 1 minimizers, 2 modimizers, 3 findere
+  int k;           // window span (k-mer length, minimizer window, findere k)
+  int m;           // minimizer length
+  int klen;        // length of the hashed k-mer: k, or k - z for findere s-mers
+  uint64_t seed;
+  uint64_t sampling;
+  OcmParams ocm;
+  LongKmerConsts lk;
+};
+
+struct Tile {
+  uint32_t record;  // record index in the batch
+  uint32_t w0;      // first window start (record coordinates)
+  uint32_t nw;      // windows in this tile
+  uint32_t task;    // findere: first window of the enclosing 16,384-window task
+};
+
+struct QueryLaunch {
+  int team;           // lanes per seed (1..32, power of two)
+  int warps;          // warps per block
+  int blocks;         // grid size
+  int smem_counters;  // 1: per-block shared counters; 0: global atomics
+};
+
+}  // namespace zx
