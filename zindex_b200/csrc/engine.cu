@@ -420,8 +420,8 @@ std::unique_ptr<Workspace> Engine::make_workspace() {
 
 void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
   const uint64_t colors = m_.colors.size();
-  if (nbases > ws.cap_bases) {
-    uint64_t cap = std::max<uint64_t>(nbases, ws.cap_bases * 3 / 2);
+  if (nbases > ws.cap_bases || !ws.bases) {
+    uint64_t cap = std::max<uint64_t>({nbases, ws.cap_bases * 3 / 2, 4096});
     cap = round_up(cap, 4096);
     if (ws.bases) cudaFree(ws.bases);
     if (ws.packed) cudaFree(ws.packed);
@@ -475,9 +475,9 @@ void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
 }
 
 void Engine::ensure_host_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
-  if (nbases > ws.cap_h_bases) {
+  if (nbases > ws.cap_h_bases || !ws.h_bases) {
     if (ws.h_bases) cudaFreeHost(ws.h_bases);
-    uint64_t cap = round_up(std::max<uint64_t>(nbases, ws.cap_h_bases * 3 / 2), 4096);
+    uint64_t cap = round_up(std::max<uint64_t>({nbases, ws.cap_h_bases * 3 / 2, 4096}), 4096);
     host_alloc(&ws.h_bases, cap);
     ws.cap_h_bases = cap;
   }
