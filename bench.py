@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark of the Zindex query hot path on B200.
+
+Workload (the batched k-mer query): 256 colours with genome lengths
+log-uniform in 1-10 Mbp, each genome 70% i.i.d. uniform ACGT and 30% copied
+from 50 seeded 100 kbp core segments; index k=31, H=4, b=8 built by the host
+builder; query 1,000,000 reads of 150 bp (70% sampled from random colours with
+0.5% substitutions, 30% uniform random). Seeded synthetic data stand in for
+real collections (there is no network).
+
+One step = one aggregate query pass over the whole read batch:
+  value : batch resident in HBM, one CUDA-graph replay per step (pack, tile
+          plan, fused extraction+probe kernel, counter reduction).
+  e2e   : the same query through the C ABI with host buffers (pinned), H2D of
+          bases + offsets and D2H of the per-colour counts inside each step.
+Both report query seeds/s (whole job, all GPUs). With --gpus N each rank holds
+a full index replica and queries its own read batch (weak scaling, no
+collective on the data path).
+
+--impl reference times the CPU restatement of the reference query (the
+reference is Rust and cannot be built here) on all host cores, on a bounded
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import fcntl
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = {
+    "workload": "batched-kmer-query",
+    "colors": 256, "genome_len_bp": [1_000_000, 10_000_000], "genome_model": "70% iid + 30% core-pool",
+    "k": 31, "hashes": 4, "fingerprint_bits": 8, "index_mode": "kmers",
+    "reads": 1_000_000, "read_len_bp": 150, "sourced": 0.7, "substitutions": 0.005,
+    "genome_seed": 1, "read_seed": 7,
+}
+SYNTH = "pool:256:1000000:10000000:1"
+METRIC = "query seeds/s"
+LIB = ROOT / "zindex_b200" / "_lib"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def build_native():
+    from zindex_b200.build import build
+
+    build()
+    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
+
+
+def prepare(cache: Path, rank: int):
+    """Index (built once per cache dir, file-locked) and this rank's reads."""
+    cache.mkdir(parents=True, exist_ok=True)
+    index = cache / "index-c2-k31-H4-b8"
+    with open(cache / ".lock", "w") as lk:
+        fcntl.flock(lk, fcntl.LOCK_EX)
+        if not (index / "manifest.json").exists():
+            t0 = time.time()
+            subprocess.run([str(LIB / "zx_build"), "--synth", SYNTH, "-o", str(index), "-k", "31",
+                            "-H", "4", "-b", "8", "-q"], check=True)
+            log(f"built index in {time.time() - t0:.1f}s")
+        reads = cache / f"reads-c2-r{rank}"
+        if not Path(str(reads) + ".offsets").exists():
+            subprocess.run([str(LIB / "zx_synth"), "reads", "--kind", "short", "--genome-kind", "pool",
+                            "--colors", "256", "--min-len", "1000000", "--max-len", "10000000",
+                            "--seed", "1", "--read-seed", str(7 + rank), "--reads", "1000000",
+                            "--length", "150", "--sourced", "0.7", "--subst", "0.005",
+                            "--format", "raw", "--out", str(reads)], check=True)
+    bases = np.fromfile(str(reads) + ".bases", dtype=np.uint8)
+    offsets = np.fromfile(str(reads) + ".offsets", dtype=np.uint64)
+    return index, bases, offsets
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            out, _ = self.proc.communicate(timeout=10)
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    try:
+        p = json.loads(PEAKS.read_text())
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class CpuOracle:
+    """The oracle (CPU restatement of the reference query) with its index
+    resident in host memory, timed on all host cores."""
+
+    def __init__(self, index):
+        import ctypes
+        from ctypes import POINTER, c_char_p, c_double, c_int, c_size_t, c_uint64, c_void_p
+
+        self.ct = ctypes
+        lib = ctypes.CDLL(str(ROOT / "oracle" / "_build" / "liboracle.so"))
+        lib.oracle_open.argtypes = [c_char_p, c_int, POINTER(c_void_p)]
+        lib.oracle_open.restype = c_int
+        lib.oracle_close.argtypes = [c_void_p]
+        lib.oracle_query_handle.argtypes = [c_void_p, c_void_p, POINTER(c_uint64), c_size_t, c_int,
+                                            POINTER(c_uint64), c_size_t, POINTER(c_uint64),
+                                            POINTER(c_double)]
+        lib.oracle_query_handle.restype = c_int
+        lib.oracle_last_error.restype = c_char_p
+        self.lib = lib
+        self.h = c_void_p()
+        if lib.oracle_open(str(index).encode(), 1, ctypes.byref(self.h)):
+            raise RuntimeError(lib.oracle_last_error().decode())
+        self.cores = os.cpu_count() or 1
+
+    def run(self, bases, offsets, n, colors):
+        ct = self.ct
+        off = np.ascontiguousarray(offsets[: n + 1])
+        counts = np.zeros(colors, dtype=np.uint64)
+        total, secs = ct.c_uint64(), ct.c_double()
+        rc = self.lib.oracle_query_handle(self.h, bases.ctypes.data_as(ct.c_void_p),
+                                          off.ctypes.data_as(ct.POINTER(ct.c_uint64)), n, self.cores,
+                                          counts.ctypes.data_as(ct.POINTER(ct.c_uint64)), colors,
+                                          ct.byref(total), ct.byref(secs))
+        if rc:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        return total.value, secs.value, counts
+
+    def sized(self, bases, offsets, colors, target_s):
+        n = 20000
+        seeds, secs, _ = self.run(bases, offsets, n, colors)
+        n = int(min(len(offsets) - 1, max(n, n * target_s / max(secs, 1e-3))))
+        seeds, secs, counts = self.run(bases, offsets, n, colors)
+        return seeds, secs, counts, n
+
+    def close(self):
+        self.lib.oracle_close(self.h)
+
+
+def cpu_baseline(index, bases, offsets, colors, target_s=15.0):
+    """seeds/s of the oracle on a bounded prefix of the read batch."""
+    orc = CpuOracle(index)
+    seeds, secs, counts, n = orc.sized(bases, offsets, colors, target_s)
+    orc.close()
+    return {"value": seeds / secs, "unit": "seeds/s", "cores": orc.cores, "kind": "port",
+            "sample": f"first {n} of the 1,000,000 reads ({seeds} seeds), query only "
+                      f"(index load excluded), {secs:.2f}s"}, n, counts
+
+
+def reference_arm(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    build_native()
+    index, bases, offsets = prepare(Path(args.cache), 0)
+    orc = CpuOracle(index)
+    per_step = max(1.0, 60.0 / max(1, args.steps + args.warmup))
+    n = None
+    vals = []
+    for i in range(args.warmup + args.steps):
+        if n is None:
+            seeds, secs, _, n = orc.sized(bases, offsets, 256, per_step)
+        else:
+            seeds, secs, _ = orc.run(bases, offsets, n, 256)
+        if i >= args.warmup:
+            vals.append(seeds / secs)
+    orc.close()
+    base = {"unit": "seeds/s", "cores": orc.cores, "kind": "port",
+            "sample": f"first {n} of the 1,000,000 reads per step, query only (index load excluded)"}
+    value = statistics.median(vals)
+    base = dict(base, value=value)
+    line = {"metric": METRIC, "value": value, "unit": "seeds/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
+            "config": dict(WORKLOAD, l2="index 1.4+ GB and reads 150 MB exceed the 126 MB L2"),
+            "cpu_baseline": base,
+            "e2e": {"value": value, "unit": "seeds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    if rank == 0 or world == 1:
+        build_native()
+    if world > 1:
+        dist.barrier()
+    import zindex_b200 as zx
+
+    index_dir, bases, offsets = prepare(Path(args.cache), rank)
+    if args.reads:
+        offsets = offsets[: args.reads + 1].copy()
+        bases = bases[: int(offsets[-1])].copy()
+        WORKLOAD["reads"] = args.reads
+    records = len(offsets) - 1
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ix = zx.Index(index_dir, device=local)
+    info = ix.info
+    # Device-resident batch.
+    d_bases = torch.from_numpy(bases).to(dev)
+    d_off = torch.from_numpy(offsets.view(np.int64)).to(dev)
+    d_counts = torch.zeros(ix.colors, dtype=torch.int64, device=dev)
+    d_total = torch.zeros(1, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(graph=True):
+        d_counts.zero_()
+        d_total.zero_()
+        ix.query_device(d_bases.data_ptr(), len(bases), d_off.data_ptr(), records,
+                        d_counts.data_ptr(), d_total.data_ptr(), stream=stream.cuda_stream,
+                        use_graph=graph)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    seeds = int(d_total.item())
+    counts_dev = d_counts.cpu().numpy().astype(np.uint64)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * seeds / (ms / 1e3)
+    launches = 5 * args.steps  # pack, count_tiles, fill_tiles, fused query, reduce per step
+
+    # Dominant kernel (fused extraction + probe) timed alone with CUDA events
+    # on its launch stream.
+    ix.set_timing(True)
+    kms = []
+    for _ in range(max(3, min(args.steps, 10))):
+        step(graph=False)
+        kms.append(ix.last_kernel_ms())
+    ix.set_timing(False)
+    kernel_ms = statistics.median(kms)
+    gather = info.gather_bytes_per_seed
+    rec_bytes = 8 if info.abandoned_hashes else 0
+    alg_bytes = seeds * (gather + rec_bytes) + len(bases) * 3 // 8
+    peak, peak_kind = hbm_peak()
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+
+    # End to end through the C ABI with pinned host buffers.
+    h_bases = torch.from_numpy(bases).pin_memory()
+    h_off = torch.from_numpy(offsets.view(np.int64)).pin_memory()
+    hb, ho = h_bases.numpy(), h_off.numpy().view(np.uint64)
+    for _ in range(2):
+        c_e2e, t_e2e = ix.query_records(hb, ho)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        c_e2e, t_e2e = ix.query_records(hb, ho)
+        times.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(times)
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    assert t_e2e == seeds and np.array_equal(c_e2e, counts_dev), "e2e and device paths disagree"
+
+    # Plain form: one record per launch, on a prefix.
+    n_plain = 4000
+    pb = bases[: int(offsets[n_plain])]
+    po = offsets[: n_plain + 1]
+    t0 = time.perf_counter()
+    _, plain_seeds = ix.query_records(pb, po, plain=True)
+    plain_rate = plain_seeds / (time.perf_counter() - t0)
+
+    if rank == 0:
+        cb = None
+        parity = None
+        if world == 1 and not args.no_cpu_baseline:
+            cb, n_cpu, cpu_counts = cpu_baseline(index_dir, bases, offsets, ix.colors)
+            c_part, _ = ix.query_records(bases[: int(offsets[n_cpu])], offsets[: n_cpu + 1])
+            parity = bool(np.array_equal(c_part, cpu_counts))
+        line = {
+            "metric": METRIC, "value": value, "unit": "seeds/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic",
+            "config": dict(WORKLOAD, seeds_per_step=seeds, bases_per_step=int(len(bases)),
+                           parallelism=f"replicas{world}",
+                           l2="no flush: index and reads exceed the 126 MB L2",
+                           launch=ix.launch()),
+            "bases_per_s": world * len(bases) / (ms / 1e3),
+            "e2e": {"value": world * seeds / e2e_s, "unit": "seeds/s",
+                    "h2d_bytes_per_step": int(len(bases) + 8 * (records + 1)),
+                    "d2h_bytes_per_step": int(8 * ix.colors + 8)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "fused_query_kernel", "kernel_ms": kernel_ms,
+                         "algorithmic_bytes_per_launch": int(alg_bytes),
+                         "gather_bytes_per_seed": int(gather)},
+            "forms": {"plain_seeds_per_s": plain_rate, "batched_seeds_per_s": value / world},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cb,
+            "parity_vs_oracle_sample": parity,
+        }
+        print(json.dumps(line), flush=True)
+    ix.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cache", default=os.environ.get("ZX_BENCH_CACHE", "/tmp/zx_bench"))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reads", type=int, default=None,
+                    help="query only the first N reads (smaller case for profiler captures)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

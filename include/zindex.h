@@ -125,6 +125,13 @@ int zx_get_launch(const zx_index* index, zx_launch* out);
 int zx_set_launch(zx_index* index, const zx_launch* launch);
 int zx_default_launch(const zx_index* index, zx_launch* out);
 
+/* Measurement hook: with timing on, zx_query_device calls made with
+ * use_graph == 0 record CUDA events around the fused extraction+probe kernel
+ * on the launch stream; zx_last_kernel_ms waits for the last such kernel and
+ * returns its duration in milliseconds. */
+int zx_set_timing(zx_index* index, int on);
+int zx_last_kernel_ms(zx_index* index, float* ms);
+
 /* Write the aggregate report exactly as print_aggregate does
  * (storage.rs:3817-3844): stdout-style TSV
  * "color\tmatches\tratio\tunique_kmers" with rows whose ratio >= min_ratio to

@@ -1235,6 +1235,38 @@ int oracle_query_timed(const char* index_dir, const uint8_t* bases, const uint64
   });
 }
 
+struct oracle_index {
+  std::unique_ptr<Index> ix;
+};
+
+int oracle_open(const char* index_dir, int recover, oracle_index** out) {
+  return guarded([&] {
+    auto h = std::make_unique<oracle_index>();
+    h->ix = load_index(index_dir, recover != 0);
+    *out = h.release();
+  });
+}
+
+void oracle_close(oracle_index* index) { delete index; }
+
+int oracle_query_handle(oracle_index* h, const uint8_t* bases, const uint64_t* offsets,
+                        size_t records, int threads, uint64_t* counts, size_t colors,
+                        uint64_t* total, double* seconds) {
+  return guarded([&] {
+    const Index& ix = *h->ix;
+    ensure(colors == ix.colors.size(), "colour count differs from the index");
+    auto t0 = std::chrono::steady_clock::now();
+    Work w;
+    for (size_t r = 0; r < records; ++r)
+      prepare_record(ix.f, bases + offsets[r], offsets[r + 1] - offsets[r], w);
+    std::vector<uint64_t> out;
+    run_query(ix, w, threads, out);
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    memcpy(counts, out.data(), colors * 8);
+    *total = w.total;
+  });
+}
+
 }  // extern "C"
 
 #ifdef ZX_ORACLE_MAIN

@@ -47,6 +47,16 @@ int oracle_index_colors(const char* index_dir, size_t* colors);
 int oracle_format_aggregate(const char* index_dir, const uint64_t* counts, uint64_t total,
                             double min_ratio, char* buf, size_t cap, size_t* written);
 
+// Resident index handle for repeated timed queries (the CPU baseline).
+typedef struct oracle_index oracle_index;
+int oracle_open(const char* index_dir, int recover, oracle_index** out);
+void oracle_close(oracle_index* index);
+// Query of in-memory records with `threads` workers; *seconds receives the
+// query time (parsing of records into seeds + lookup), index load excluded.
+int oracle_query_handle(oracle_index* index, const uint8_t* bases, const uint64_t* offsets,
+                        size_t records, int threads, uint64_t* counts, size_t colors,
+                        uint64_t* total, double* seconds);
+
 const char* oracle_last_error(void);
 
 #ifdef __cplusplus

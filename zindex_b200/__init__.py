@@ -127,6 +127,15 @@ class Index:
                                         len(offsets) - 1, _p64(out), len(out), byref(count)))
         return out[: count.value]
 
+    # -- measurement ----------------------------------------------------------
+    def set_timing(self, on: bool = True) -> None:
+        _lib.check(_lib.load().zx_set_timing(self._h, int(on)))
+
+    def last_kernel_ms(self) -> float:
+        ms = ctypes.c_float()
+        _lib.check(_lib.load().zx_last_kernel_ms(self._h, byref(ms)))
+        return float(ms.value)
+
     # -- launch configuration -------------------------------------------------
     def launch(self) -> dict:
         l = ZxLaunch()

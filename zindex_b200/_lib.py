@@ -27,7 +27,7 @@ EXPORTED = (
     "zx_last_error", "zx_open", "zx_close", "zx_index_info", "zx_color_name",
     "zx_color_unique_kmers", "zx_query_file", "zx_query_host", "zx_query_host_plain",
     "zx_query_device", "zx_extract_seeds", "zx_get_launch", "zx_set_launch",
-    "zx_default_launch", "zx_write_aggregate",
+    "zx_default_launch", "zx_write_aggregate", "zx_set_timing", "zx_last_kernel_ms",
 )
 
 
@@ -81,6 +81,8 @@ def load() -> ctypes.CDLL:
         "zx_get_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
         "zx_set_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
         "zx_default_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
+        "zx_set_timing": (c_int, [c_void_p, c_int]),
+        "zx_last_kernel_ms": (c_int, [c_void_p, POINTER(ctypes.c_float)]),
         "zx_write_aggregate": (c_int, [c_void_p, c_char_p, P64, c_uint64, c_uint64, c_double,
                                        c_double, c_char_p, c_int]),
     }

@@ -182,6 +182,22 @@ int zx_set_launch(zx_index* index, const zx_launch* l) {
   });
 }
 
+int zx_set_timing(zx_index* index, int on) {
+  return guarded([&] {
+    zx::check(index, zx::kEInval, "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    index->engine->set_timing(on != 0);
+  });
+}
+
+int zx_last_kernel_ms(zx_index* index, float* ms) {
+  return guarded([&] {
+    zx::check(index && ms, zx::kEInval, "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    *ms = index->engine->last_fused_ms();
+  });
+}
+
 int zx_write_aggregate(const zx_index* index, const char* query_label, const uint64_t* counts,
                        uint64_t total, uint64_t probes, double min_ratio, double seconds,
                        const char* out_path, int stats) {

@@ -131,6 +131,7 @@ int build(int argc, char** argv, int threads) {
     else if (a == "-X" || a == "--max-subindex-size") o.max_subindex_size = parse_size(val());
     else if (a == "-R" || a == "--drop-abandoned") o.drop_abandoned = true;
     else if (a == "--groups") o.groups = val();
+    else if (a == "--synth") o.synth = val();
     else return usage();
   }
   if (mode == "kmers") o.features.mode = 0;
@@ -138,7 +139,7 @@ int build(int argc, char** argv, int threads) {
   else if (mode == "modimizers") o.features.mode = 2;
   else if (mode == "findere") o.features.mode = 3;
   else return usage();
-  if (o.fof.empty() || o.output.empty()) return usage();
+  if ((o.fof.empty() && o.synth.empty()) || o.output.empty()) return usage();
   try {
     zx::build_index(o);
   } catch (const std::exception& e) {

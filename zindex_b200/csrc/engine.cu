@@ -171,6 +171,8 @@ Engine::Engine(const std::string& dir, const OpenOptions& options) { load(dir, o
 Engine::~Engine() {
   ws_.reset();
   cudaSetDevice(device_);
+  if (ev_begin_) cudaEventDestroy(ev_begin_);
+  if (ev_end_) cudaEventDestroy(ev_end_);
   for (void* p : allocations_) cudaFree(p);
   if (d_ix_rec_) cudaFree(d_ix_rec_);
   if (d_ix_norec_) cudaFree(d_ix_norec_);
@@ -389,13 +391,35 @@ size_t Engine::fused_smem_bytes(const QueryLaunch& l) const {
 }
 
 int Engine::max_blocks(const QueryLaunch& l) const {
+  if (cached_blocks_ && cached_for_.team == l.team && cached_for_.warps == l.warps &&
+      cached_for_.smem_counters == l.smem_counters)
+    return cached_blocks_;
   int per_sm = 0;
   size_t smem = fused_smem_bytes(l);
   cudaFuncSetAttribute(fused_query_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_query_kernel,
                                                            l.warps * 32, smem),
              "occupancy");
-  return std::max(1, per_sm) * sms_;
+  const_cast<Engine*>(this)->cached_blocks_ = std::max(1, per_sm) * sms_;
+  const_cast<Engine*>(this)->cached_for_ = l;
+  return cached_blocks_;
+}
+
+void Engine::set_timing(bool on) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  if (on && !ev_begin_) {
+    cuda_check(cudaEventCreate(&ev_begin_), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&ev_end_), "cudaEventCreate");
+  }
+  timing_ = on;
+}
+
+float Engine::last_fused_ms() {
+  check(ev_end_ != nullptr, kEInval, "kernel timing is not enabled");
+  cuda_check(cudaEventSynchronize(ev_end_), "timing");
+  float ms = 0;
+  cuda_check(cudaEventElapsedTime(&ms, ev_begin_, ev_end_), "timing");
+  return ms;
 }
 
 void Engine::set_launch(const QueryLaunch& l) {
@@ -532,9 +556,14 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                             : (int)std::min<uint64_t>((uint64_t)blocks_cap, std::max<uint64_t>(want, 1));
   l.blocks = blocks;
   BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records};
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  cuda_check(cudaStreamIsCapturing(s, &capturing), "cudaStreamIsCapturing");
+  const bool timed = timing_ && capturing == cudaStreamCaptureStatusNone;
+  if (timed) cuda_check(cudaEventRecord(ev_begin_, s), "cudaEventRecord");
   fused_query_kernel<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l,
                                                         ws.partial, counts, total);
   cuda_check(cudaGetLastError(), "fused_query_kernel");
+  if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
   if (l.smem_counters) {
     const uint32_t colors = (uint32_t)m_.colors.size();
     reduce_counters_kernel<<<std::max(1u, (colors + 255) / 256), 256, 0, s>>>(ws.partial, blocks,
@@ -589,10 +618,28 @@ void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   ensure_host_capacity(ws, nbases, records);
   const uint64_t colors = m_.colors.size();
   cudaStream_t s = ws.stream;
-  memcpy(ws.h_bases, bases, nbases);
-  memcpy(ws.h_offsets, offsets, (records + 1) * 8);
-  cuda_check(cudaMemcpyAsync(ws.bases, ws.h_bases, nbases, cudaMemcpyHostToDevice, s), "H2D");
-  cuda_check(cudaMemcpyAsync(ws.offsets, ws.h_offsets, (records + 1) * 8, cudaMemcpyHostToDevice, s),
+  // Page-locked caller buffers are copied directly; pageable ones through the
+  // workspace's pinned staging.
+  auto pinned = [](const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+  };
+  const uint8_t* src_bases = bases;
+  const uint64_t* src_offsets = offsets;
+  if (nbases && !pinned(bases)) {
+    memcpy(ws.h_bases, bases, nbases);
+    src_bases = ws.h_bases;
+  }
+  if (!pinned(offsets)) {
+    memcpy(ws.h_offsets, offsets, (records + 1) * 8);
+    src_offsets = ws.h_offsets;
+  }
+  cuda_check(cudaMemcpyAsync(ws.bases, src_bases, nbases, cudaMemcpyHostToDevice, s), "H2D");
+  cuda_check(cudaMemcpyAsync(ws.offsets, src_offsets, (records + 1) * 8, cudaMemcpyHostToDevice, s),
              "H2D");
   cuda_check(cudaMemsetAsync(ws.counts, 0, colors * 8, s), "memset");
   cuda_check(cudaMemsetAsync(ws.total, 0, 8, s), "memset");

@@ -94,6 +94,11 @@ class Engine {
   void query_host_plain(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                         const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
                         uint64_t* total);
+  // Kernel timing: when enabled, non-graph launches record CUDA events around
+  // the fused query kernel on its stream; last_fused_ms() waits for and
+  // returns the most recent interval.
+  void set_timing(bool on);
+  float last_fused_ms();
   // Seeds of host records in record/window order (extraction only).
   void extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
                     uint64_t records, std::vector<uint64_t>& keys);
@@ -119,6 +124,10 @@ class Engine {
   uint64_t resident_bytes_ = 0;
   std::unique_ptr<Workspace> ws_;
   std::mutex mu_;
+  bool timing_ = false;
+  cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
+  int cached_blocks_ = 0;
+  QueryLaunch cached_for_{};
 };
 
 // CUDA error check that throws zx::Error(kECuda).
