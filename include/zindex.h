@@ -54,10 +54,12 @@ typedef struct zx_info {
 } zx_info;
 
 typedef struct zx_launch {
-  int team;           /* lanes sharing one seed: 1, 2, 4, 8, 16 or 32 */
-  int warps;          /* warps per block, 1..16 */
+  int team;           /* register gather: lanes sharing one seed, 1..32 (power of two) */
+  int warps;          /* warps per block, 1..8 */
   int blocks;         /* grid size; 0 = fill the device */
   int smem_counters;  /* 1 = per-block shared colour counters, 0 = global atomics */
+  int stage_bytes;    /* > 0: staged bulk-copy gather, bytes per ring stage (multiple of 16) */
+  int stages;         /* stages per warp ring for the staged gather, 1..8 */
 } zx_launch;
 
 /* Thread-local message of the last failed call on this thread. */
@@ -124,6 +126,11 @@ int zx_extract_seeds(zx_index* index, const uint8_t* bases, const uint64_t* offs
 int zx_get_launch(const zx_index* index, zx_launch* out);
 int zx_set_launch(zx_index* index, const zx_launch* launch);
 int zx_default_launch(const zx_index* index, zx_launch* out);
+
+/* Status of the last asynchronous zx_query_device calls of this index: ZX_OK,
+ * or ZX_ETIMEOUT when a bounded device wait expired (counts incomplete). The
+ * device error word is cleared. Synchronous calls report it directly. */
+int zx_query_status(zx_index* index);
 
 /* Measurement hook: with timing on, zx_query_device calls made with
  * use_graph == 0 record CUDA events around the fused extraction+probe kernel

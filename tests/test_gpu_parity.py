@@ -218,8 +218,18 @@ def test_device_api_with_graph_replay(gpu, oracle, tmp_path_factory):
             assert int(d_total.item()) == want_total
 
 
-@pytest.mark.parametrize("team,warps", [(1, 4), (2, 2), (8, 8), (32, 1), (4, 16)])
-def test_launch_configurations_do_not_change_results(gpu, oracle, tmp_path_factory, team, warps):
+LAUNCHES = [
+    dict(team=1, warps=4, stage_bytes=0), dict(team=2, warps=2, stage_bytes=0),
+    dict(team=8, warps=8, stage_bytes=0), dict(team=32, warps=1, stage_bytes=0),
+    dict(team=16, warps=3, stage_bytes=0),
+    dict(warps=4, stage_bytes=8192, stages=2), dict(warps=8, stage_bytes=4096, stages=3),
+    dict(warps=2, stage_bytes=64, stages=1), dict(warps=4, stage_bytes=128, stages=4),
+    dict(warps=1, stage_bytes=16384, stages=8),
+]
+
+
+@pytest.mark.parametrize("launch", LAUNCHES, ids=lambda l: "-".join(f"{k}{v}" for k, v in l.items()))
+def test_launch_configurations_do_not_change_results(gpu, oracle, tmp_path_factory, launch):
     import zindex_b200 as zx
 
     ix, genomes = index_for(tmp_path_factory, colors=40, length=4000, mode="kmers", k=31, H=4, b=8)
@@ -228,7 +238,36 @@ def test_launch_configurations_do_not_change_results(gpu, oracle, tmp_path_facto
     want, want_total = oracle.query_records(ix, bases, offsets)
     with zx.Index(ix) as index:
         for smem in (0, 1):
-            index.set_launch(team, warps, 0, smem)
+            index.set_launch(smem_counters=smem, **launch)
             got, total = index.query_records(bases, offsets)
             np.testing.assert_array_equal(got, want)
             assert total == want_total
+
+
+@pytest.mark.parametrize("stage_bytes,stages", [(0, 0), (8192, 2), (256, 3), (64, 2)])
+def test_staged_gather_on_wide_partitioned_multiclass_index(gpu, oracle, tmp_path_factory,
+                                                            stage_bytes, stages):
+    import zindex_b200 as zx
+
+    d = tmp_path_factory.mktemp("wide")
+    lengths = [2000 + 37 * i for i in range(300)] + [40000 + 1000 * i for i in range(12)]
+    lines = []
+    genomes = []
+    for i, n in enumerate(lengths):
+        g = dna(n, 500 + i)
+        genomes.append(g)
+        p = d / f"g{i}.fa"
+        helpers.write_fasta(p, [g])
+        lines.append(f"g{i}\t{p}")
+    (d / "fof.tsv").write_text("\n".join(lines) + "\n")
+    ix = build_index(d / "fof.tsv", d / "index", k=31, H=4, b=16, min_docs=1, max_size="256KiB",
+                     groups="3,4,5,6;10,11")
+    reads = reads_for(genomes, n=400)
+    bases, offsets = zx.pack_records(reads)
+    want, want_total = oracle.query_records(ix, bases, offsets)
+    with zx.Index(ix) as index:
+        assert index.info.classes >= 2
+        index.set_launch(stage_bytes=stage_bytes, stages=stages or 1)
+        got, total = index.query_records(bases, offsets)
+    np.testing.assert_array_equal(got, want)
+    assert total == want_total

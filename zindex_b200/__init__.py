@@ -137,21 +137,37 @@ class Index:
         return float(ms.value)
 
     # -- launch configuration -------------------------------------------------
+    @staticmethod
+    def _launch_dict(l: ZxLaunch) -> dict:
+        return {"team": l.team, "warps": l.warps, "blocks": l.blocks,
+                "smem_counters": l.smem_counters, "stage_bytes": l.stage_bytes,
+                "stages": l.stages}
+
     def launch(self) -> dict:
         l = ZxLaunch()
         _lib.check(_lib.load().zx_get_launch(self._h, byref(l)))
-        return {"team": l.team, "warps": l.warps, "blocks": l.blocks, "smem_counters": l.smem_counters}
+        return self._launch_dict(l)
 
     def default_launch(self) -> dict:
         l = ZxLaunch()
         _lib.check(_lib.load().zx_default_launch(self._h, byref(l)))
-        return {"team": l.team, "warps": l.warps, "blocks": l.blocks, "smem_counters": l.smem_counters}
+        return self._launch_dict(l)
 
-    def set_launch(self, team: int, warps: int, blocks: int = 0, smem_counters: Optional[int] = None):
-        if smem_counters is None:
-            smem_counters = self.default_launch()["smem_counters"]
-        l = ZxLaunch(int(team), int(warps), int(blocks), int(smem_counters))
+    def set_launch(self, team: int = None, warps: int = None, blocks: int = 0,
+                   smem_counters: Optional[int] = None, stage_bytes: Optional[int] = None,
+                   stages: Optional[int] = None, **_ignored):
+        """Change the launch configuration (never changes results); unset
+        fields keep their default values."""
+        d = self.default_launch()
+        l = ZxLaunch(int(d["team"] if team is None else team), int(d["warps"] if warps is None else warps),
+                     int(blocks), int(d["smem_counters"] if smem_counters is None else smem_counters),
+                     int(d["stage_bytes"] if stage_bytes is None else stage_bytes),
+                     int(d["stages"] if stages is None else stages))
         _lib.check(_lib.load().zx_set_launch(self._h, byref(l)))
+
+    def query_status(self) -> None:
+        """Raise if a bounded device wait expired in an asynchronous query."""
+        _lib.check(_lib.load().zx_query_status(self._h))
 
     # -- output ---------------------------------------------------------------
     def format_aggregate(self, counts, total: int, min_ratio: float = 0.0) -> str:

@@ -28,6 +28,7 @@ EXPORTED = (
     "zx_color_unique_kmers", "zx_query_file", "zx_query_host", "zx_query_host_plain",
     "zx_query_device", "zx_extract_seeds", "zx_get_launch", "zx_set_launch",
     "zx_default_launch", "zx_write_aggregate", "zx_set_timing", "zx_last_kernel_ms",
+    "zx_query_status",
 )
 
 
@@ -42,7 +43,8 @@ class ZxInfo(ctypes.Structure):
 
 
 class ZxLaunch(ctypes.Structure):
-    _fields_ = [("team", c_int), ("warps", c_int), ("blocks", c_int), ("smem_counters", c_int)]
+    _fields_ = [("team", c_int), ("warps", c_int), ("blocks", c_int), ("smem_counters", c_int),
+                ("stage_bytes", c_int), ("stages", c_int)]
 
 
 class ZxError(RuntimeError):
@@ -82,6 +84,7 @@ def load() -> ctypes.CDLL:
         "zx_set_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
         "zx_default_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
         "zx_set_timing": (c_int, [c_void_p, c_int]),
+        "zx_query_status": (c_int, [c_void_p]),
         "zx_last_kernel_ms": (c_int, [c_void_p, POINTER(ctypes.c_float)]),
         "zx_write_aggregate": (c_int, [c_void_p, c_char_p, P64, c_uint64, c_uint64, c_double,
                                        c_double, c_char_p, c_int]),

@@ -42,6 +42,8 @@ void fill_launch(const zx::QueryLaunch& l, zx_launch* out) {
   out->warps = l.warps;
   out->blocks = l.blocks;
   out->smem_counters = l.smem_counters;
+  out->stage_bytes = l.stage_bytes;
+  out->stages = l.stages;
 }
 
 }  // namespace
@@ -178,7 +180,18 @@ int zx_set_launch(zx_index* index, const zx_launch* l) {
   return guarded([&] {
     zx::check(index && l, zx::kEInval, "null argument");
     std::lock_guard<std::mutex> lock(index->mu);
-    index->engine->set_launch(zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters});
+    index->engine->set_launch(
+        zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters, l->stage_bytes, l->stages});
+  });
+}
+
+int zx_query_status(zx_index* index) {
+  return guarded([&] {
+    zx::check(index, zx::kEInval, "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    auto& e = *index->engine;
+    if (e.take_error(e.default_workspace()))
+      zx::raise(zx::kETimeout, "a bounded device wait expired during a query");
   });
 }
 

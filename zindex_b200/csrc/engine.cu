@@ -61,6 +61,26 @@ __global__ void repack_rows_kernel(const uint8_t* __restrict__ src, uint64_t row
   }
 }
 
+using FusedFn = void (*)(const DevIndex*, BatchView, SeedParams, QueryLaunch, uint32_t*, uint64_t*,
+                        unsigned long long*, uint32_t*);
+using ExtractFn = void (*)(BatchView, SeedParams, uint64_t*, uint32_t*, int);
+
+FusedFn fused_for(int mode) {
+  switch (mode) {
+    case 1: return fused_query_kernel<1>;
+    case 2: return fused_query_kernel<2>;
+    default: return fused_query_kernel<0>;
+  }
+}
+
+ExtractFn extract_for(int mode) {
+  switch (mode) {
+    case 1: return extract_kernel<1>;
+    case 2: return extract_kernel<2>;
+    default: return extract_kernel<0>;
+  }
+}
+
 uint64_t le64(const uint8_t* p) {
   uint64_t v = 0;
   for (int i = 7; i >= 0; --i) v = (v << 8) | p[i];
@@ -152,7 +172,7 @@ RecoveryRecords read_recovery(const std::string& dir, const Manifest& m) {
 Workspace::~Workspace() {
   release_graphs();
   void* dev[] = {bases, offsets, packed, invalid, tile_counts, tile_first, tiles,
-                 scan_tmp, partial, counts, total, keys_out, keys_count};
+                 scan_tmp, partial, counts, total, keys_out, keys_count, error};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total};
@@ -383,21 +403,27 @@ QueryLaunch Engine::default_launch() const {
   l.warps = 4;
   l.smem_counters = m_.colors.size() <= 16384 ? 1 : 0;
   l.blocks = 0;  // 0: fill the device (occupancy-derived)
+  l.stage_bytes = 8192;
+  l.stages = 2;
+  // Widest class row slice must fit a stage at least H times 16 bytes.
+  if ((uint64_t)m_.hashes * 16 > (uint64_t)l.stage_bytes) l.stage_bytes = 0;
   return l;
 }
 
 size_t Engine::fused_smem_bytes(const QueryLaunch& l) const {
-  return FusedSmem::total(sp_.mode, sp_.k, (uint32_t)m_.colors.size(), l.smem_counters, l.warps);
+  return FusedSmem::total(sp_.mode, sp_.k, (uint32_t)m_.colors.size(), host_ix_.classes, l);
 }
 
 int Engine::max_blocks(const QueryLaunch& l) const {
   if (cached_blocks_ && cached_for_.team == l.team && cached_for_.warps == l.warps &&
-      cached_for_.smem_counters == l.smem_counters)
+      cached_for_.smem_counters == l.smem_counters && cached_for_.stage_bytes == l.stage_bytes &&
+      cached_for_.stages == l.stages)
     return cached_blocks_;
   int per_sm = 0;
   size_t smem = fused_smem_bytes(l);
-  cudaFuncSetAttribute(fused_query_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_query_kernel,
+  FusedFn fn = fused_for(sp_.mode);
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
                                                            l.warps * 32, smem),
              "occupancy");
   const_cast<Engine*>(this)->cached_blocks_ = std::max(1, per_sm) * sms_;
@@ -425,9 +451,12 @@ float Engine::last_fused_ms() {
 void Engine::set_launch(const QueryLaunch& l) {
   check(l.team >= 1 && l.team <= 32 && (l.team & (l.team - 1)) == 0, kEInval,
         "team size must be a power of two in 1..32");
-  check(l.warps >= 1 && l.warps <= 16, kEInval, "warps per block must be in 1..16");
+  check(l.warps >= 1 && l.warps <= 8, kEInval, "warps per block must be in 1..8");
   check(l.smem_counters == 0 || m_.colors.size() <= 16384, kEInval,
         "shared-memory counters support at most 16384 colours");
+  check(l.stage_bytes == 0 || (l.stage_bytes % 16 == 0 && l.stage_bytes >= 16 * m_.hashes &&
+                                l.stage_bytes <= 65536 && l.stages >= 1 && l.stages <= 8),
+        kEInval, "staged gather needs 16-byte multiple stages of at least 16*H bytes, 1..8 stages");
   check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
   std::lock_guard<std::mutex> lock(mu_);
   launch_ = l;
@@ -493,6 +522,10 @@ void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
     if (ws.total) cudaFree(ws.total);
     dev_alloc(&ws.counts, colors, "counts");
     dev_alloc(&ws.total, 1, "total");
+    if (!ws.error) {
+      dev_alloc(&ws.error, 1, "error word");
+      cuda_check(cudaMemset(ws.error, 0, 4), "memset");
+    }
     ws.cap_colors = colors;
     ws.release_graphs();
   }
@@ -560,8 +593,9 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   cuda_check(cudaStreamIsCapturing(s, &capturing), "cudaStreamIsCapturing");
   const bool timed = timing_ && capturing == cudaStreamCaptureStatusNone;
   if (timed) cuda_check(cudaEventRecord(ev_begin_, s), "cudaEventRecord");
-  fused_query_kernel<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l,
-                                                        ws.partial, counts, total);
+  FusedFn fn = fused_for(sp_.mode);
+  fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, ws.partial,
+                                        counts, total, ws.error);
   cuda_check(cudaGetLastError(), "fused_query_kernel");
   if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
   if (l.smem_counters) {
@@ -570,6 +604,24 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                                                                                colors, counts);
     cuda_check(cudaGetLastError(), "reduce_counters_kernel");
   }
+}
+
+void Engine::check_error_word(Workspace& ws) {
+  uint32_t err = 0;
+  cuda_check(cudaMemcpy(&err, ws.error, 4, cudaMemcpyDeviceToHost), "error word");
+  if (err) {
+    cuda_check(cudaMemset(ws.error, 0, 4), "memset");
+    raise(kETimeout, "a bounded device wait expired during the query");
+  }
+}
+
+uint32_t Engine::take_error(Workspace& ws) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  uint32_t err = 0;
+  if (!ws.error) return 0;
+  cuda_check(cudaMemcpy(&err, ws.error, 4, cudaMemcpyDeviceToHost), "error word");
+  if (err) cuda_check(cudaMemset(ws.error, 0, 4), "memset");
+  return err;
 }
 
 void Engine::query_device(Workspace& ws, const uint8_t* bases, uint64_t nbases,
@@ -647,6 +699,7 @@ void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   cuda_check(cudaMemcpyAsync(ws.h_counts, ws.counts, colors * 8, cudaMemcpyDeviceToHost, s), "D2H");
   cuda_check(cudaMemcpyAsync(ws.h_total, ws.total, 8, cudaMemcpyDeviceToHost, s), "D2H");
   cuda_check(cudaStreamSynchronize(s), "query");
+  check_error_word(ws);
   memcpy(counts, ws.h_counts, colors * 8);
   *total = *ws.h_total;
 }
@@ -678,6 +731,7 @@ void Engine::query_host_plain(Workspace& ws, const uint8_t* bases, uint64_t nbas
   cuda_check(cudaMemcpyAsync(ws.h_counts, ws.counts, colors * 8, cudaMemcpyDeviceToHost, s), "D2H");
   cuda_check(cudaMemcpyAsync(ws.h_total, ws.total, 8, cudaMemcpyDeviceToHost, s), "D2H");
   cuda_check(cudaStreamSynchronize(s), "plain query");
+  check_error_word(ws);
   memcpy(counts, ws.h_counts, colors * 8);
   *total = *ws.h_total;
 }
@@ -715,11 +769,12 @@ void Engine::extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     ws.cap_keys = need;
   }
   const int warps = 4;
-  size_t smem = 256 * 8 + warps * FusedSmem::warp_bytes(sp_.mode, sp_.k);
-  cudaFuncSetAttribute(extract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  size_t smem = 256 * 8 + warps * FusedSmem::warp_bytes(sp_.mode, sp_.k, 0);
+  ExtractFn efn = extract_for(sp_.mode);
+  cudaFuncSetAttribute(efn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   BatchView bv{PackedView{ws.packed, ws.invalid}, ws.offsets, ws.tiles, ws.tile_first + records};
   int grid = (int)std::min<uint64_t>((ntiles + warps - 1) / warps, (uint64_t)sms_ * 8);
-  extract_kernel<<<grid, warps * 32, smem, s>>>(bv, sp_, ws.keys_out, ws.keys_count, warps);
+  efn<<<grid, warps * 32, smem, s>>>(bv, sp_, ws.keys_out, ws.keys_count, warps);
   cuda_check(cudaGetLastError(), "extract_kernel");
   std::vector<uint64_t> all(need);
   std::vector<uint32_t> cnt(ntiles);

@@ -39,6 +39,7 @@ struct Workspace {
   uint32_t* partial = nullptr;
   uint64_t* counts = nullptr;
   unsigned long long* total = nullptr;
+  uint32_t* error = nullptr;        // bit 0: a bounded device wait expired
   uint64_t* keys_out = nullptr;     // extraction-only output
   uint32_t* keys_count = nullptr;
   // Pinned host staging.
@@ -99,6 +100,9 @@ class Engine {
   // returns the most recent interval.
   void set_timing(bool on);
   float last_fused_ms();
+  // Device error word of a workspace (read and cleared); nonzero means a
+  // bounded wait expired and the query's counts are incomplete.
+  uint32_t take_error(Workspace& ws);
   // Seeds of host records in record/window order (extraction only).
   void extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
                     uint64_t records, std::vector<uint64_t>& keys);
@@ -111,6 +115,7 @@ class Engine {
                uint64_t records, bool recover, uint64_t* counts, unsigned long long* total,
                cudaStream_t stream);
   void plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records, cudaStream_t stream);
+  void check_error_word(Workspace& ws);
 
   Manifest m_;
   int device_ = 0;

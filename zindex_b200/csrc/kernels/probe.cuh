@@ -204,4 +204,334 @@ __device__ __forceinline__ void probe_seed(const DevIndex& ix, uint64_t key, int
     for (uint32_t i = 0; i < rec.len; ++i) cnt.add(rec.at(i));
 }
 
+// ---- warp-cooperative probe of a batch of seeds -----------------------------
+// The scalar part of each seed (fingerprint, position hash, partition choice,
+// recovery probe) is computed once by an owner lane into a shared-memory
+// descriptor; teams of T lanes then gather the fingerprint-plane chunks of two
+// seeds at a time so each lane keeps 2 * H 16-byte loads in flight.
+struct SeedDesc {
+  uint64_t first, step;
+  const uint32_t* rec_list;
+  uint32_t pattern;  // fingerprint replicated over every b-bit field of a word
+  uint32_t rec_len, rec_single, pad;
+};
+
+__device__ __forceinline__ bool desc_rec_contains(const SeedDesc& d, uint32_t c) {
+  RecHit r{d.rec_list, d.rec_len, d.rec_single};
+  return rec_contains(r, c);
+}
+
+// Row-address offset (within the class allocation) of row i of a seed.
+__device__ __forceinline__ uint64_t row_offset(uint64_t row0, uint64_t h, int i, uint64_t seg,
+                                               uint32_t stride) {
+  uint32_t low = ((uint32_t)h ^ (uint32_t)(h >> 33)) & (uint32_t)(seg - 1);
+  return row0 + ((uint64_t)i * seg + low) * stride;
+}
+
+// Fields of one XORed 16-byte chunk equal to the fingerprint -> on_hit(group).
+template <class OnGroup>
+__device__ __forceinline__ void chunk_hits(const uint4& acc, uint32_t chunk, uint32_t groups, int b,
+                                           uint32_t ones, uint32_t pattern, OnGroup&& on_group) {
+  const int fpw = 32 / b;
+  const uint32_t words[4] = {acc.x, acc.y, acc.z, acc.w};
+#pragma unroll
+  for (int wi = 0; wi < 4; ++wi) {
+    uint32_t field0 = chunk * (uint32_t)(4 * fpw) + (uint32_t)(wi * fpw);
+    if (field0 >= groups) break;
+    uint32_t hits = zero_fields(words[wi] ^ pattern, b, ones);
+    uint32_t valid = groups - field0;
+    if (valid < (uint32_t)fpw) hits &= (1u << (valid * b)) - 1u;
+    while (hits) {
+      uint32_t bit = __ffs(hits) - 1;
+      hits &= hits - 1;
+      on_group(field0 + bit / b);
+    }
+  }
+}
+
+// Colours of a hit group (singleton, or XOR-decoded members).
+template <class OnHit>
+__device__ __forceinline__ void group_hit(const DevClass& C, uint32_t group, const SeedDesc& d,
+                                          uint64_t row0, int H, OnHit&& on_hit) {
+  uint32_t gc = __ldg(C.group_color + group);
+  if (!(gc & kMultiGroup)) {
+    on_hit(gc);
+    return;
+  }
+  const uint32_t* mg = C.multi + 3 * (gc & ~kMultiGroup);
+  uint32_t off = __ldg(mg), cnt = __ldg(mg + 1), firstm = __ldg(mg + 2);
+  uint64_t mask = 0, h = d.first;
+  for (int i = 0; i < H; ++i, h += d.step)
+    mask ^= row_bits(C.data + row_offset(row0, h, i, C.seg, C.row_stride), off, cnt);
+  while (mask) {
+    uint32_t mb = __ffsll((long long)mask) - 1;
+    mask &= mask - 1;
+    on_hit(__ldg(C.members + firstm + mb));
+  }
+}
+
+// Probes keys[0..n) (shared memory) with the whole warp. desc: 32 entries;
+// row0: 32 * ix.classes entries (row offset of position 0 per seed and class).
+__device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n, SeedDesc* desc,
+                            uint64_t* row0s, int T, const Counters& cnt, int lane) {
+  const int H = ix.hashes, b = ix.bits;
+  const uint32_t ones = field_ones(b);
+  const uint32_t classes = ix.classes;
+  const int team = lane / T, tl = lane % T, nteams = 32 / T;
+  for (uint32_t r0 = 0; r0 < n; r0 += 32) {
+    const uint32_t m = min(32u, n - r0);
+    if ((uint32_t)lane < m) {
+      const uint64_t key = keys[r0 + lane];
+      SeedDesc d;
+      d.first = mixsplit(key, ix.seed);
+      d.step = splitmix64(d.first);
+      d.pattern = (uint32_t)fingerprint(key, ix.seed, b) * ones;
+      RecHit r = recovery_lookup(ix.rec, recovery_hash(key, ix.seed));
+      d.rec_list = r.list;
+      d.rec_len = r.len;
+      d.rec_single = r.single;
+      d.pad = 0;
+      desc[lane] = d;
+      for (uint32_t ci = 0; ci < classes; ++ci) {
+        const DevClass& C = ix.cls[ci];
+        const uint32_t part = C.partitions > 1 ? partition_id(key, ix.seed, C.partitions) : 0;
+        const uint64_t count = C.slots / C.seg - (uint64_t)H + 1;
+        const uint64_t base = mulhi64(d.first, count) * C.seg;
+        row0s[lane * classes + ci] = ((uint64_t)part * C.slots + base) * C.row_stride;
+      }
+      for (uint32_t i = 0; i < r.len; ++i) cnt.add(r.at(i));
+    }
+    __syncwarp();
+    for (uint32_t ci = 0; ci < classes; ++ci) {
+      const DevClass& C = ix.cls[ci];
+      if ((uint32_t)tl >= C.fp_chunks) continue;
+      const uint64_t seg = C.seg;
+      const uint32_t stride = C.row_stride;
+      for (uint32_t s = team; s < m; s += 2 * nteams) {
+        const uint32_t s2 = s + nteams;
+        const bool two = s2 < m;
+        const SeedDesc& da = desc[s];
+        const SeedDesc& db = desc[two ? s2 : s];
+        const uint64_t ra = row0s[s * classes + ci];
+        const uint64_t rb = row0s[(two ? s2 : s) * classes + ci];
+        for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T) {
+          uint4 aa = make_uint4(0, 0, 0, 0), ab = make_uint4(0, 0, 0, 0);
+          uint64_t ha = da.first, hb = db.first;
+          for (int i0 = 0; i0 < H; i0 += 4) {
+            uint4 va[4], vb[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int i = i0 + j;
+              va[j] = vb[j] = make_uint4(0, 0, 0, 0);
+              if (i < H) {
+                va[j] = ld_row_chunk(C.data + row_offset(ra, ha, i, seg, stride) + chunk * 16u);
+                if (two) vb[j] = ld_row_chunk(C.data + row_offset(rb, hb, i, seg, stride) + chunk * 16u);
+                ha += da.step;
+                hb += db.step;
+              }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              aa.x ^= va[j].x; aa.y ^= va[j].y; aa.z ^= va[j].z; aa.w ^= va[j].w;
+              ab.x ^= vb[j].x; ab.y ^= vb[j].y; ab.z ^= vb[j].z; ab.w ^= vb[j].w;
+            }
+          }
+          chunk_hits(aa, chunk, C.groups, b, ones, da.pattern, [&](uint32_t g) {
+            group_hit(C, g, da, ra, H, [&](uint32_t c) {
+              if (da.rec_len && desc_rec_contains(da, c)) return;
+              cnt.add(c);
+            });
+          });
+          if (two)
+            chunk_hits(ab, chunk, C.groups, b, ones, db.pattern, [&](uint32_t g) {
+              group_hit(C, g, db, rb, H, [&](uint32_t c) {
+                if (db.rec_len && desc_rec_contains(db, c)) return;
+                cnt.add(c);
+              });
+            });
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---- asynchronous staged gather (cp.async.bulk + mbarrier) ------------------
+// One lane arms a stage's mbarrier with the byte count, all lanes issue 1-D
+// bulk copies of fingerprint-plane row slices (16-byte aligned, multiples of
+// 16 bytes) into a per-warp shared-memory ring, and the warp XORs and compares
+// the landed slices while the next stages are in flight. Waits are bounded:
+// on expiry the warp raises bit 0 of *err and stops probing.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t* bar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+          smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the completion of the phase with the given parity.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < (1u << 22); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+struct StageRing {
+  uint8_t* mem;       // stages * stage_bytes
+  uint64_t* bars;     // stages mbarriers
+  uint32_t stage_bytes, stages;
+  uint32_t phases;    // parity bit per stage
+  uint32_t pending;   // stage bits with copies in flight
+};
+
+// Probes keys[0..n) with staged bulk gathers. desc/row0s hold 64 seeds.
+__device__ bool probe_batch_async(const DevIndex& ix, const uint64_t* keys, uint32_t n,
+                                  SeedDesc* desc, uint64_t* row0s, StageRing& ring,
+                                  const Counters& cnt, int lane, uint32_t* err) {
+  const int H = ix.hashes, b = ix.bits;
+  const uint32_t ones = field_ones(b);
+  const uint32_t classes = ix.classes;
+  for (uint32_t r0 = 0; r0 < n; r0 += 64) {
+    const uint32_t m = min(64u, n - r0);
+    for (uint32_t q = lane; q < m; q += 32) {
+      const uint64_t key = keys[r0 + q];
+      SeedDesc d;
+      d.first = mixsplit(key, ix.seed);
+      d.step = splitmix64(d.first);
+      d.pattern = (uint32_t)fingerprint(key, ix.seed, b) * ones;
+      RecHit r = recovery_lookup(ix.rec, recovery_hash(key, ix.seed));
+      d.rec_list = r.list;
+      d.rec_len = r.len;
+      d.rec_single = r.single;
+      d.pad = 0;
+      desc[q] = d;
+      for (uint32_t ci = 0; ci < classes; ++ci) {
+        const DevClass& C = ix.cls[ci];
+        const uint32_t part = C.partitions > 1 ? partition_id(key, ix.seed, C.partitions) : 0;
+        const uint64_t count = C.slots / C.seg - (uint64_t)H + 1;
+        const uint64_t base = mulhi64(d.first, count) * C.seg;
+        row0s[q * classes + ci] = ((uint64_t)part * C.slots + base) * C.row_stride;
+      }
+      for (uint32_t i = 0; i < r.len; ++i) cnt.add(r.at(i));
+    }
+    __syncwarp();
+    for (uint32_t ci = 0; ci < classes; ++ci) {
+      const DevClass& C = ix.cls[ci];
+      const uint32_t rb = C.fp_chunks * 16u;                      // bytes gathered per row
+      uint32_t cw = (ring.stage_bytes / (uint32_t)H) & ~15u;      // column tile width
+      if (cw > rb) cw = rb;
+      const uint32_t tiles = (rb + cw - 1) / cw;                  // column tiles per seed
+      const uint32_t items = m * tiles;
+      const uint32_t per_stage = ring.stage_bytes / ((uint32_t)H * cw);
+      const uint32_t batches = (items + per_stage - 1) / per_stage;
+      const uint32_t cpi = cw / 16;                               // chunks per item slot
+      auto issue = [&](uint32_t bi) {
+        const uint32_t st = bi % ring.stages;
+        const uint32_t i0 = bi * per_stage, ni = min(per_stage, items - i0);
+        uint8_t* smem = ring.mem + (size_t)st * ring.stage_bytes;
+        // Order this lane's earlier generic reads of the stage before the
+        // async-proxy writes that will overwrite it.
+        fence_proxy_async_smem();
+        if (lane == 0) {
+          uint32_t bytes = 0;
+          for (uint32_t it = i0; it < i0 + ni; ++it) {
+            uint32_t col0 = (it % tiles) * cw;
+            bytes += (uint32_t)H * min(cw, rb - col0);
+          }
+          mbar_arrive_expect(ring.bars + st, bytes);
+        }
+        __syncwarp();
+        for (uint32_t li = lane; li < ni; li += 32) {
+          const uint32_t it = i0 + li, s = it / tiles, col0 = (it % tiles) * cw;
+          const uint32_t w = min(cw, rb - col0);
+          const SeedDesc& d = desc[s];
+          const uint64_t row0 = row0s[s * classes + ci];
+          uint64_t h = d.first;
+          for (int i = 0; i < H; ++i, h += d.step)
+            bulk_copy_g2s(smem + ((size_t)li * H + i) * cw,
+                          C.data + row_offset(row0, h, i, C.seg, C.row_stride) + col0, w,
+                          ring.bars + st);
+        }
+        ring.pending |= 1u << st;
+      };
+      const uint32_t prologue = min(ring.stages, batches);
+      for (uint32_t bi = 0; bi < prologue; ++bi) issue(bi);
+      for (uint32_t bi = 0; bi < batches; ++bi) {
+        const uint32_t st = bi % ring.stages;
+        const bool ok = mbar_wait(ring.bars + st, (ring.phases >> st) & 1u);
+        if (__any_sync(0xFFFFFFFFu, !ok)) {
+          if (lane == 0) atomicOr(err, 1u);
+          return false;
+        }
+        ring.phases ^= 1u << st;
+        ring.pending &= ~(1u << st);
+        const uint32_t i0 = bi * per_stage, ni = min(per_stage, items - i0);
+        const uint8_t* smem = ring.mem + (size_t)st * ring.stage_bytes;
+        for (uint32_t pair = lane; pair < ni * cpi; pair += 32) {
+          const uint32_t li = pair / cpi, c = pair % cpi;
+          const uint32_t it = i0 + li, s = it / tiles, col0 = (it % tiles) * cw;
+          if (col0 + c * 16 >= rb) continue;
+          uint4 acc = make_uint4(0, 0, 0, 0);
+          for (int i = 0; i < H; ++i) {
+            const uint4 v = *reinterpret_cast<const uint4*>(smem + ((size_t)li * H + i) * cw + c * 16);
+            acc.x ^= v.x; acc.y ^= v.y; acc.z ^= v.z; acc.w ^= v.w;
+          }
+          const SeedDesc& d = desc[s];
+          const uint64_t row0 = row0s[s * classes + ci];
+          chunk_hits(acc, col0 / 16 + c, C.groups, b, ones, d.pattern, [&](uint32_t g) {
+            group_hit(C, g, d, row0, H, [&](uint32_t col) {
+              if (d.rec_len && desc_rec_contains(d, col)) return;
+              cnt.add(col);
+            });
+          });
+        }
+        __syncwarp();
+        if (bi + ring.stages < batches) issue(bi + ring.stages);
+      }
+    }
+    __syncwarp();
+  }
+  return true;
+}
+
+// Bounded drain of stages still in flight (after an error).
+__device__ __forceinline__ void ring_drain(StageRing& ring) {
+  for (uint32_t st = 0; st < ring.stages; ++st)
+    if (ring.pending & (1u << st)) {
+      mbar_wait(ring.bars + st, (ring.phases >> st) & 1u);
+      ring.phases ^= 1u << st;
+    }
+  ring.pending = 0;
+}
+
 }  // namespace zx

@@ -66,52 +66,52 @@ struct BatchView {
 };
 
 // Shared memory of the fused kernel, in order: DevIndex copy, counters,
-// inner hash table (minimizers), then per warp: keys[2 * kTileWindows],
-// minimizer scratch (pre, suf, pos).
+// inner hash table (minimizers), then per warp: keys[2 * kTileWindows], 32
+// seed descriptors, 32 x classes row offsets, minimizer scratch (pre, suf,
+// pos).
 struct FusedSmem {
   static constexpr size_t ix_bytes = (sizeof(DevIndex) + 15) / 16 * 16;
   static __host__ __device__ size_t counter_bytes(uint32_t colors, int smem_counters) {
     return smem_counters ? ((size_t)colors * 4 + 15) / 16 * 16 : 0;
   }
   static __host__ __device__ size_t ocm_entries(int k) { return kTileWindows + (size_t)k + 1; }
-  static __host__ __device__ size_t warp_bytes(int mode, int k) {
-    size_t b = 2 * kTileWindows * 8;
+  static __host__ __device__ size_t probe_bytes(uint32_t classes) {
+    return 64 * sizeof(SeedDesc) + 64 * 8 * (size_t)classes;
+  }
+  static __host__ __device__ size_t ring_bytes(int stage_bytes, int stages) {
+    return stage_bytes > 0 ? (size_t)stage_bytes * stages + 8 * 8 : 0;
+  }
+  static __host__ __device__ size_t warp_bytes(int mode, int k, uint32_t classes, int stage_bytes = 0,
+                                               int stages = 0) {
+    size_t b = 2 * kTileWindows * 8 + probe_bytes(classes) + ring_bytes(stage_bytes, stages);
     if (mode == 1) b += 2 * ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
     return (b + 15) / 16 * 16;
   }
-  static __host__ __device__ size_t total(int mode, int k, uint32_t colors, int smem_counters,
-                                          int warps) {
-    return ix_bytes + counter_bytes(colors, smem_counters) + (mode == 1 ? 256 * 8 : 0) +
-           (size_t)warps * warp_bytes(mode, k);
+  static __host__ __device__ size_t total(int mode, int k, uint32_t colors, uint32_t classes,
+                                          const QueryLaunch& l) {
+    return ix_bytes + counter_bytes(colors, l.smem_counters) + (mode == 1 ? 256 * 8 : 0) +
+           (size_t)l.warps * warp_bytes(mode, k, classes, l.stage_bytes, l.stages);
   }
 };
 
 // Extracts the seeds of one tile into `keys`; returns their number.
+template <int MODE>
 __device__ __forceinline__ uint32_t extract_tile(const BatchView& bv, const SeedParams& sp,
                                                  const Tile& t, uint64_t* keys, uint8_t* ocm,
                                                  const uint64_t* inner, int lane) {
   const uint64_t rb = bv.offsets[t.record];
-  switch (sp.mode) {
-    case 1:
-      if (sp.k == sp.m) return tile_ocm_full(bv.pv, rb, t.w0, t.nw, sp.m, keys, lane);
-      {
-        Rank16* pre = reinterpret_cast<Rank16*>(ocm);
-        Rank16* suf = pre + FusedSmem::ocm_entries(sp.k);
-        uint32_t* pos = reinterpret_cast<uint32_t*>(suf + FusedSmem::ocm_entries(sp.k));
-        return tile_ocm(bv.pv, rb, t.w0, t.nw, sp, inner, pre, suf, pos, keys, lane);
-      }
-    case 0:
-    case 2: {
-      bool modi = sp.mode == 2;
-      if (sp.klen <= 32)
-        return tile_kmers_short(bv.pv, rb, t.w0, t.nw, sp.klen, modi, sp.seed, sp.sampling, keys,
-                                lane);
-      return tile_kmers_long(bv.pv, rb, t.w0, t.nw, sp.klen, sp.lk, modi, sp.seed, sp.sampling,
-                             keys, keys + kTileWindows, lane);
-    }
-    default:
-      return 0;
+  if (MODE == 1) {
+    if (sp.k == sp.m) return tile_ocm_full(bv.pv, rb, t.w0, t.nw, sp.m, keys, lane);
+    Rank16* pre = reinterpret_cast<Rank16*>(ocm);
+    Rank16* suf = pre + FusedSmem::ocm_entries(sp.k);
+    uint32_t* pos = reinterpret_cast<uint32_t*>(suf + FusedSmem::ocm_entries(sp.k));
+    return tile_ocm(bv.pv, rb, t.w0, t.nw, sp, inner, pre, suf, pos, keys, lane);
   }
+  const bool modi = MODE == 2;
+  if (sp.klen <= 32)
+    return tile_kmers_short(bv.pv, rb, t.w0, t.nw, sp.klen, modi, sp.seed, sp.sampling, keys, lane);
+  return tile_kmers_long(bv.pv, rb, t.w0, t.nw, sp.klen, sp.lk, modi, sp.seed, sp.sampling, keys,
+                         keys + kTileWindows, lane);
 }
 
 __device__ __forceinline__ void load_index_smem(const DevIndex* __restrict__ gix, DevIndex* six) {
@@ -127,52 +127,72 @@ __device__ __forceinline__ void build_inner_table(const SeedParams& sp, uint64_t
     inner[v] = mixsplit(canonical_encoded(v, s), sp.seed ^ kInnerHashSeed);
 }
 
-// Fused extraction + probe over the tile list. partial: gridDim.x x colors
-// block counters (smem_counters) or null; counts: global counters (used
-// directly when smem_counters == 0). total: seeds processed.
-__global__ void __launch_bounds__(512) fused_query_kernel(const DevIndex* __restrict__ gix,
+// Fused extraction + probe over the tile list (one instantiation per seed
+// mode). partial: gridDim.x x colors block counters (smem_counters); counts:
+// global counters (used directly when smem_counters == 0). total: seeds.
+template <int MODE>
+__global__ void __launch_bounds__(256) fused_query_kernel(const DevIndex* __restrict__ gix,
                                                           BatchView bv, SeedParams sp,
                                                           QueryLaunch lc,
                                                           uint32_t* __restrict__ partial,
                                                           uint64_t* __restrict__ counts,
-                                                          unsigned long long* __restrict__ total) {
+                                                          unsigned long long* __restrict__ total,
+                                                          uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) uint8_t smem[];
   DevIndex* six = reinterpret_cast<DevIndex*>(smem);
   uint8_t* p = smem + FusedSmem::ix_bytes;
   uint32_t* scount = nullptr;
+  const uint32_t colors = gix->colors, classes = gix->classes;
   if (lc.smem_counters) {
     scount = reinterpret_cast<uint32_t*>(p);
-    p += FusedSmem::counter_bytes(gix->colors, 1);
+    p += FusedSmem::counter_bytes(colors, 1);
   }
   uint64_t* inner = nullptr;
-  if (sp.mode == 1) {
+  if (MODE == 1) {
     inner = reinterpret_cast<uint64_t*>(p);
     p += 256 * 8;
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(sp.mode, sp.k);
+  uint8_t* wbase =
+      p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, classes, lc.stage_bytes, lc.stages);
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
-  uint8_t* ocm = wbase + 2 * kTileWindows * 8;
+  SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + 2 * kTileWindows * 8);
+  uint64_t* row0s = reinterpret_cast<uint64_t*>(desc + 64);
+  uint8_t* ring_base = wbase + 2 * kTileWindows * 8 + FusedSmem::probe_bytes(classes);
+  uint8_t* ocm = ring_base + FusedSmem::ring_bytes(lc.stage_bytes, lc.stages);
+  StageRing ring{ring_base + 64, reinterpret_cast<uint64_t*>(ring_base), (uint32_t)lc.stage_bytes,
+                 (uint32_t)lc.stages, 0u, 0u};
+  if (lc.stage_bytes > 0) {
+    if (lane == 0) {
+      for (int st = 0; st < lc.stages; ++st) mbar_init(ring.bars + st, 1);
+      mbar_fence_init();
+    }
+    __syncwarp();
+  }
 
   load_index_smem(gix, six);
   build_inner_table(sp, inner);
-  const uint32_t colors = gix->colors;
   if (scount)
     for (uint32_t c = threadIdx.x; c < colors; c += blockDim.x) scount[c] = 0;
   __syncthreads();
   const DevIndex& ix = *six;
   const Counters cnt{scount, counts};
-  const int T = lc.team, team = lane / T, tl = lane % T, nteams = 32 / T;
   const uint32_t ntiles = *bv.ntiles;
   const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
   unsigned long long seeds = 0;
   for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + warp; t < ntiles; t += warps_total) {
     const Tile tile = bv.tiles[t];
-    uint32_t n = extract_tile(bv, sp, tile, keys, ocm, inner, lane);
+    uint32_t n = extract_tile<MODE>(bv, sp, tile, keys, ocm, inner, lane);
     __syncwarp();
     seeds += n;
-    for (uint32_t i = team; i < n; i += nteams) probe_seed(ix, keys[i], tl, T, cnt);
-    __syncwarp();
+    if (lc.stage_bytes > 0) {
+      if (!probe_batch_async(ix, keys, n, desc, row0s, ring, cnt, lane, err)) {
+        ring_drain(ring);
+        break;
+      }
+    } else {
+      probe_batch(ix, keys, n, desc, row0s, lc.team, cnt, lane);
+    }
   }
   if (lane == 0 && seeds) atomicAdd(total, seeds);
   __syncthreads();
@@ -193,21 +213,22 @@ __global__ void reduce_counters_kernel(const uint32_t* __restrict__ partial, uin
 
 // Extraction only (testing and inspection): tile t's keys go to
 // out[t * kTileWindows ...], their number to out_count[t].
+template <int MODE>
 __global__ void extract_kernel(BatchView bv, SeedParams sp, uint64_t* __restrict__ out,
                                uint32_t* __restrict__ out_count, int warps_per_block) {
   extern __shared__ __align__(16) uint8_t smem[];
   uint64_t* inner = reinterpret_cast<uint64_t*>(smem);
   uint8_t* p = smem + 256 * 8;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(sp.mode, sp.k);
+  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, 0);
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
-  uint8_t* ocm = wbase + 2 * kTileWindows * 8;
+  uint8_t* ocm = wbase + 2 * kTileWindows * 8 + FusedSmem::probe_bytes(0);
   build_inner_table(sp, inner);
   __syncthreads();
   const uint32_t ntiles = *bv.ntiles;
   const uint32_t warps_total = gridDim.x * warps_per_block;
   for (uint32_t t = blockIdx.x * warps_per_block + warp; t < ntiles; t += warps_total) {
-    uint32_t n = extract_tile(bv, sp, bv.tiles[t], keys, ocm, inner, lane);
+    uint32_t n = extract_tile<MODE>(bv, sp, bv.tiles[t], keys, ocm, inner, lane);
     __syncwarp();
     for (uint32_t i = lane; i < n; i += 32) out[(uint64_t)t * kTileWindows + i] = keys[i];
     if (lane == 0) out_count[t] = n;

@@ -26,10 +26,12 @@ struct Tile {
 };
 
 struct QueryLaunch {
-  int team;           // lanes per seed (1..32, power of two)
+  int team;           // lanes per seed (1..32, power of two), register gather
   int warps;          // warps per block
   int blocks;         // grid size
   int smem_counters;  // 1: per-block shared counters; 0: global atomics
+  int stage_bytes;    // > 0: staged bulk-copy gather with this stage size per warp
+  int stages;         // stages in each warp's ring (staged gather)
 };
 
 }  // namespace zx
