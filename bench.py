@@ -387,6 +387,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cache", default=os.environ.get("ZX_BENCH_CACHE", "/tmp/zx_bench"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", action="store_true",
+                    help="autotune the launch configuration on the workload before timing")
     ap.add_argument("--reads", type=int, default=None,
                     help="query only the first N reads (smaller case for profiler captures)")
     args = ap.parse_args()

@@ -58,8 +58,10 @@ typedef struct zx_launch {
   int warps;          /* warps per block, 1..8 */
   int blocks;         /* grid size; 0 = fill the device */
   int smem_counters;  /* 1 = per-block shared colour counters, 0 = global atomics */
-  int stage_bytes;    /* > 0: staged bulk-copy gather, bytes per ring stage (multiple of 16) */
+  int stage_bytes;    /* > 0: staged gather, bytes per ring stage (multiple of 16) */
   int stages;         /* stages per warp ring for the staged gather, 1..8 */
+  int bulk;           /* staged gather: 1 = cp.async.bulk per row slice, 0 = 16-byte cp.async */
+  int min_blocks;     /* kernel variant register budget: 2, 3 or 4 resident 256-thread blocks */
 } zx_launch;
 
 /* Thread-local message of the last failed call on this thread. */

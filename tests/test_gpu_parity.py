@@ -222,9 +222,12 @@ LAUNCHES = [
     dict(team=1, warps=4, stage_bytes=0), dict(team=2, warps=2, stage_bytes=0),
     dict(team=8, warps=8, stage_bytes=0), dict(team=32, warps=1, stage_bytes=0),
     dict(team=16, warps=3, stage_bytes=0),
-    dict(warps=4, stage_bytes=8192, stages=2), dict(warps=8, stage_bytes=4096, stages=3),
-    dict(warps=2, stage_bytes=64, stages=1), dict(warps=4, stage_bytes=128, stages=4),
-    dict(warps=1, stage_bytes=16384, stages=8),
+    dict(warps=4, stage_bytes=8192, stages=2, bulk=1), dict(warps=8, stage_bytes=4096, stages=3, bulk=1),
+    dict(warps=2, stage_bytes=64, stages=1, bulk=1), dict(warps=4, stage_bytes=128, stages=4, bulk=1),
+    dict(warps=1, stage_bytes=16384, stages=8, bulk=1),
+    dict(warps=4, stage_bytes=8192, stages=2, bulk=0), dict(warps=8, stage_bytes=4096, stages=3, bulk=0),
+    dict(warps=2, stage_bytes=64, stages=1, bulk=0), dict(warps=4, stage_bytes=128, stages=4, bulk=0),
+    dict(warps=1, stage_bytes=16384, stages=8, bulk=0),
 ]
 
 
@@ -244,9 +247,11 @@ def test_launch_configurations_do_not_change_results(gpu, oracle, tmp_path_facto
             assert total == want_total
 
 
-@pytest.mark.parametrize("stage_bytes,stages", [(0, 0), (8192, 2), (256, 3), (64, 2)])
+@pytest.mark.parametrize("stage_bytes,stages,bulk", [(0, 0, 0), (8192, 2, 1), (256, 3, 1),
+                                                    (64, 2, 1), (8192, 2, 0), (256, 3, 0),
+                                                    (64, 2, 0)])
 def test_staged_gather_on_wide_partitioned_multiclass_index(gpu, oracle, tmp_path_factory,
-                                                            stage_bytes, stages):
+                                                            stage_bytes, stages, bulk):
     import zindex_b200 as zx
 
     d = tmp_path_factory.mktemp("wide")
@@ -267,7 +272,7 @@ def test_staged_gather_on_wide_partitioned_multiclass_index(gpu, oracle, tmp_pat
     want, want_total = oracle.query_records(ix, bases, offsets)
     with zx.Index(ix) as index:
         assert index.info.classes >= 2
-        index.set_launch(stage_bytes=stage_bytes, stages=stages or 1)
+        index.set_launch(stage_bytes=stage_bytes, stages=stages or 1, bulk=bulk)
         got, total = index.query_records(bases, offsets)
     np.testing.assert_array_equal(got, want)
     assert total == want_total

@@ -141,7 +141,7 @@ class Index:
     def _launch_dict(l: ZxLaunch) -> dict:
         return {"team": l.team, "warps": l.warps, "blocks": l.blocks,
                 "smem_counters": l.smem_counters, "stage_bytes": l.stage_bytes,
-                "stages": l.stages}
+                "stages": l.stages, "bulk": l.bulk, "min_blocks": l.min_blocks}
 
     def launch(self) -> dict:
         l = ZxLaunch()
@@ -155,14 +155,17 @@ class Index:
 
     def set_launch(self, team: int = None, warps: int = None, blocks: int = 0,
                    smem_counters: Optional[int] = None, stage_bytes: Optional[int] = None,
-                   stages: Optional[int] = None, **_ignored):
+                   stages: Optional[int] = None, bulk: Optional[int] = None,
+                   min_blocks: Optional[int] = None, **_ignored):
         """Change the launch configuration (never changes results); unset
         fields keep their default values."""
         d = self.default_launch()
         l = ZxLaunch(int(d["team"] if team is None else team), int(d["warps"] if warps is None else warps),
                      int(blocks), int(d["smem_counters"] if smem_counters is None else smem_counters),
                      int(d["stage_bytes"] if stage_bytes is None else stage_bytes),
-                     int(d["stages"] if stages is None else stages))
+                     int(d["stages"] if stages is None else stages),
+                     int(d["bulk"] if bulk is None else bulk),
+                     int(d["min_blocks"] if min_blocks is None else min_blocks))
         _lib.check(_lib.load().zx_set_launch(self._h, byref(l)))
 
     def query_status(self) -> None:

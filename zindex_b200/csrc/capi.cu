@@ -44,6 +44,8 @@ void fill_launch(const zx::QueryLaunch& l, zx_launch* out) {
   out->smem_counters = l.smem_counters;
   out->stage_bytes = l.stage_bytes;
   out->stages = l.stages;
+  out->bulk = l.bulk;
+  out->min_blocks = l.min_blocks;
 }
 
 }  // namespace
@@ -181,7 +183,8 @@ int zx_set_launch(zx_index* index, const zx_launch* l) {
     zx::check(index && l, zx::kEInval, "null argument");
     std::lock_guard<std::mutex> lock(index->mu);
     index->engine->set_launch(
-        zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters, l->stage_bytes, l->stages});
+        zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters, l->stage_bytes, l->stages,
+                        l->bulk, l->min_blocks});
   });
 }
 

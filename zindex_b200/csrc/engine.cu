@@ -65,11 +65,20 @@ using FusedFn = void (*)(const DevIndex*, BatchView, SeedParams, QueryLaunch, ui
                         unsigned long long*, uint32_t*);
 using ExtractFn = void (*)(BatchView, SeedParams, uint64_t*, uint32_t*, int);
 
-FusedFn fused_for(int mode) {
+template <int MINB>
+FusedFn fused_mode(int mode) {
   switch (mode) {
-    case 1: return fused_query_kernel<1>;
-    case 2: return fused_query_kernel<2>;
-    default: return fused_query_kernel<0>;
+    case 1: return fused_query_kernel<1, MINB>;
+    case 2: return fused_query_kernel<2, MINB>;
+    default: return fused_query_kernel<0, MINB>;
+  }
+}
+
+FusedFn fused_for(int mode, int min_blocks) {
+  switch (min_blocks) {
+    case 3: return fused_mode<3>(mode);
+    case 4: return fused_mode<4>(mode);
+    default: return fused_mode<2>(mode);
   }
 }
 
@@ -269,6 +278,9 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
     C.groups = (uint32_t)G;
     C.row_stride = stride;
     C.fp_chunks = (uint32_t)((first.lookup_bytes(b) + 15) / 16);
+    // Row offsets are kept as 32-bit counts of 16-byte units by the kernels.
+    check((uint64_t)banks.size() * first.slots * stride < (1ull << 36), kEUnsupported,
+          "a source class larger than 64 GiB is not supported by the device layout");
     uint8_t* data = nullptr;
     dev_alloc(&data, (uint64_t)banks.size() * first.slots * stride, "bank payload");
     allocations_.push_back(data);
@@ -398,30 +410,34 @@ QueryLaunch Engine::default_launch() const {
   for (uint32_t c = 0; c < host_ix_.classes; ++c) chunks = std::max(chunks, host_ix_.cls[c].fp_chunks);
   int team = 1;
   while (team < 32 && (uint32_t)team < chunks) team <<= 1;
+  // Teams of 8 lanes, 8 warps per block measured fastest on B200 for 64-256 B
+  // fingerprint rows; narrower rows use teams of one 16-byte chunk each.
   QueryLaunch l;
-  l.team = team;
-  l.warps = 4;
+  l.team = std::min(team, 8);
+  l.warps = 8;
   l.smem_counters = m_.colors.size() <= 16384 ? 1 : 0;
   l.blocks = 0;  // 0: fill the device (occupancy-derived)
-  l.stage_bytes = 8192;
+  l.stage_bytes = 0;  // register gather by default (fastest measured on B200 for small rows)
   l.stages = 2;
-  // Widest class row slice must fit a stage at least H times 16 bytes.
-  if ((uint64_t)m_.hashes * 16 > (uint64_t)l.stage_bytes) l.stage_bytes = 0;
+  l.bulk = 0;
+  l.min_blocks = 3;
   return l;
 }
 
 size_t Engine::fused_smem_bytes(const QueryLaunch& l) const {
-  return FusedSmem::total(sp_.mode, sp_.k, (uint32_t)m_.colors.size(), host_ix_.classes, l);
+  return FusedSmem::total(sp_.mode, sp_.k, (uint32_t)m_.colors.size(), host_ix_.classes,
+                          m_.hashes, l);
 }
 
 int Engine::max_blocks(const QueryLaunch& l) const {
   if (cached_blocks_ && cached_for_.team == l.team && cached_for_.warps == l.warps &&
       cached_for_.smem_counters == l.smem_counters && cached_for_.stage_bytes == l.stage_bytes &&
-      cached_for_.stages == l.stages)
+      cached_for_.stages == l.stages && cached_for_.bulk == l.bulk &&
+      cached_for_.min_blocks == l.min_blocks)
     return cached_blocks_;
   int per_sm = 0;
   size_t smem = fused_smem_bytes(l);
-  FusedFn fn = fused_for(sp_.mode);
+  FusedFn fn = fused_for(sp_.mode, l.min_blocks);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
                                                            l.warps * 32, smem),
@@ -457,6 +473,8 @@ void Engine::set_launch(const QueryLaunch& l) {
   check(l.stage_bytes == 0 || (l.stage_bytes % 16 == 0 && l.stage_bytes >= 16 * m_.hashes &&
                                 l.stage_bytes <= 65536 && l.stages >= 1 && l.stages <= 8),
         kEInval, "staged gather needs 16-byte multiple stages of at least 16*H bytes, 1..8 stages");
+  check(l.min_blocks >= 2 && l.min_blocks <= 4, kEInval, "min_blocks must be 2, 3 or 4");
+  check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
   check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
   std::lock_guard<std::mutex> lock(mu_);
   launch_ = l;
@@ -593,7 +611,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   cuda_check(cudaStreamIsCapturing(s, &capturing), "cudaStreamIsCapturing");
   const bool timed = timing_ && capturing == cudaStreamCaptureStatusNone;
   if (timed) cuda_check(cudaEventRecord(ev_begin_, s), "cudaEventRecord");
-  FusedFn fn = fused_for(sp_.mode);
+  FusedFn fn = fused_for(sp_.mode, l.min_blocks);
   fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, ws.partial,
                                         counts, total, ws.error);
   cuda_check(cudaGetLastError(), "fused_query_kernel");

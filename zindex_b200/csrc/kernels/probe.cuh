@@ -34,6 +34,16 @@ __device__ __forceinline__ uint32_t zero_fields(uint32_t x, int b, uint32_t ones
   return ~x & ones;
 }
 
+// Bit set at the top bit of each b-bit field of `x` that is zero, for any
+// b in {1,2,4,8,16,32}: adding the low-bits mask carries into a field's top
+// bit exactly when the field's low bits are nonzero (no carry crosses a
+// field); hi = ones << (b - 1).
+__device__ __forceinline__ uint32_t zero_fields_hi(uint32_t x, uint32_t hi) {
+  const uint32_t lo = ~hi;
+  const uint32_t t = (x & lo) + lo;
+  return ~(t | x) & hi;
+}
+
 __device__ __forceinline__ uint4 ld_row_chunk(const uint8_t* p) {
   return __ldg(reinterpret_cast<const uint4*>(p));
 }
@@ -270,13 +280,69 @@ __device__ __forceinline__ void group_hit(const DevClass& C, uint32_t group, con
   }
 }
 
-// Probes keys[0..n) (shared memory) with the whole warp. desc: 32 entries;
-// row0: 32 * ix.classes entries (row offset of position 0 per seed and class).
+// Colours of a hit group given the H row offsets (16-byte units) of the seed.
+template <class OnHit>
+__device__ __noinline__ void group_hit_rows(const DevClass& C, uint32_t group,
+                                            const uint32_t* rows, int H, OnHit on_hit) {
+  uint32_t gc = __ldg(C.group_color + group);
+  if (!(gc & kMultiGroup)) {
+    on_hit(gc);
+    return;
+  }
+  const uint32_t* mg = C.multi + 3 * (gc & ~kMultiGroup);
+  uint32_t off = __ldg(mg), cnt = __ldg(mg + 1), firstm = __ldg(mg + 2);
+  uint64_t mask = 0;
+  for (int i = 0; i < H; ++i) mask ^= row_bits(C.data + (uint64_t)rows[i] * 16u, off, cnt);
+  while (mask) {
+    uint32_t mb = __ffsll((long long)mask) - 1;
+    mask &= mask - 1;
+    on_hit(__ldg(C.members + firstm + mb));
+  }
+}
+
+struct CountUnlessRecovered {
+  const Counters* cnt;
+  const SeedDesc* d;
+  __device__ __forceinline__ void operator()(uint32_t c) const {
+    if (d->rec_len && desc_rec_contains(*d, c)) return;
+    cnt->add(c);
+  }
+};
+
+// Hits of one XORed chunk; returns quickly when no field matches.
+__device__ __forceinline__ void chunk_hits_fast(const uint4& acc, uint32_t chunk, const DevClass& C,
+                                                int b, uint32_t hi, const SeedDesc& d,
+                                                const uint32_t* rows, int H, const Counters& cnt) {
+  const uint32_t p = d.pattern;
+  uint32_t w0 = zero_fields_hi(acc.x ^ p, hi), w1 = zero_fields_hi(acc.y ^ p, hi);
+  uint32_t w2 = zero_fields_hi(acc.z ^ p, hi), w3 = zero_fields_hi(acc.w ^ p, hi);
+  if (!(w0 | w1 | w2 | w3)) return;
+  const uint32_t fpw = 32 / b;
+  const uint32_t words[4] = {w0, w1, w2, w3};
+#pragma unroll
+  for (int wi = 0; wi < 4; ++wi) {
+    uint32_t hits = words[wi];
+    const uint32_t field0 = chunk * 4 * fpw + wi * fpw;
+    while (hits) {
+      const uint32_t bit = __ffs(hits) - 1;
+      hits &= hits - 1;
+      const uint32_t group = field0 + bit / b;
+      if (group >= C.groups) break;  // padding or membership bits past the last field
+      group_hit_rows(C, group, rows, H, CountUnlessRecovered{&cnt, &d});
+    }
+  }
+}
+
+// Probes keys[0..n) (shared memory) with the whole warp. Per round of 32
+// seeds each lane fills one SeedDesc and the H row offsets of its seed for
+// every class (rows: 32 x classes x H, 16-byte units); teams of T lanes then
+// gather two seeds at a time.
 __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n, SeedDesc* desc,
-                            uint64_t* row0s, int T, const Counters& cnt, int lane) {
+                            uint32_t* rows, int T, const Counters& cnt, int lane) {
   const int H = ix.hashes, b = ix.bits;
-  const uint32_t ones = field_ones(b);
+  const uint32_t ones = field_ones(b), hi = ones << (b - 1);
   const uint32_t classes = ix.classes;
+  const uint32_t per_seed = classes * (uint32_t)H;
   const int team = lane / T, tl = lane % T, nteams = 32 / T;
   for (uint32_t r0 = 0; r0 < n; r0 += 32) {
     const uint32_t m = min(32u, n - r0);
@@ -292,12 +358,20 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
       d.rec_single = r.single;
       d.pad = 0;
       desc[lane] = d;
+      uint32_t* myrows = rows + lane * per_seed;
       for (uint32_t ci = 0; ci < classes; ++ci) {
         const DevClass& C = ix.cls[ci];
         const uint32_t part = C.partitions > 1 ? partition_id(key, ix.seed, C.partitions) : 0;
         const uint64_t count = C.slots / C.seg - (uint64_t)H + 1;
         const uint64_t base = mulhi64(d.first, count) * C.seg;
-        row0s[lane * classes + ci] = ((uint64_t)part * C.slots + base) * C.row_stride;
+        const uint32_t stride16 = C.row_stride >> 4;
+        const uint32_t seg = (uint32_t)C.seg;
+        uint64_t h = d.first;
+        uint32_t slot0 = (uint32_t)((uint64_t)part * C.slots + base);
+        for (int i = 0; i < H; ++i, h += d.step) {
+          uint32_t low = ((uint32_t)h ^ (uint32_t)(h >> 33)) & (seg - 1);
+          myrows[ci * H + i] = (slot0 + (uint32_t)i * seg + low) * stride16;
+        }
       }
       for (uint32_t i = 0; i < r.len; ++i) cnt.add(r.at(i));
     }
@@ -305,18 +379,14 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
     for (uint32_t ci = 0; ci < classes; ++ci) {
       const DevClass& C = ix.cls[ci];
       if ((uint32_t)tl >= C.fp_chunks) continue;
-      const uint64_t seg = C.seg;
-      const uint32_t stride = C.row_stride;
+      const uint4* data = reinterpret_cast<const uint4*>(C.data);
       for (uint32_t s = team; s < m; s += 2 * nteams) {
         const uint32_t s2 = s + nteams;
         const bool two = s2 < m;
-        const SeedDesc& da = desc[s];
-        const SeedDesc& db = desc[two ? s2 : s];
-        const uint64_t ra = row0s[s * classes + ci];
-        const uint64_t rb = row0s[(two ? s2 : s) * classes + ci];
+        const uint32_t* ra = rows + s * per_seed + ci * H;
+        const uint32_t* rb = rows + (two ? s2 : s) * per_seed + ci * H;
         for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T) {
           uint4 aa = make_uint4(0, 0, 0, 0), ab = make_uint4(0, 0, 0, 0);
-          uint64_t ha = da.first, hb = db.first;
           for (int i0 = 0; i0 < H; i0 += 4) {
             uint4 va[4], vb[4];
 #pragma unroll
@@ -324,10 +394,8 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
               const int i = i0 + j;
               va[j] = vb[j] = make_uint4(0, 0, 0, 0);
               if (i < H) {
-                va[j] = ld_row_chunk(C.data + row_offset(ra, ha, i, seg, stride) + chunk * 16u);
-                if (two) vb[j] = ld_row_chunk(C.data + row_offset(rb, hb, i, seg, stride) + chunk * 16u);
-                ha += da.step;
-                hb += db.step;
+                va[j] = __ldg(data + ra[i] + chunk);
+                if (two) vb[j] = __ldg(data + rb[i] + chunk);
               }
             }
 #pragma unroll
@@ -336,19 +404,8 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
               ab.x ^= vb[j].x; ab.y ^= vb[j].y; ab.z ^= vb[j].z; ab.w ^= vb[j].w;
             }
           }
-          chunk_hits(aa, chunk, C.groups, b, ones, da.pattern, [&](uint32_t g) {
-            group_hit(C, g, da, ra, H, [&](uint32_t c) {
-              if (da.rec_len && desc_rec_contains(da, c)) return;
-              cnt.add(c);
-            });
-          });
-          if (two)
-            chunk_hits(ab, chunk, C.groups, b, ones, db.pattern, [&](uint32_t g) {
-              group_hit(C, g, db, rb, H, [&](uint32_t c) {
-                if (db.rec_len && desc_rec_contains(db, c)) return;
-                cnt.add(c);
-              });
-            });
+          chunk_hits_fast(aa, chunk, C, b, hi, desc[s], ra, H, cnt);
+          if (two) chunk_hits_fast(ab, chunk, C, b, hi, desc[s2], rb, H, cnt);
         }
       }
     }
@@ -406,12 +463,33 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// Waits until at most n of this thread's committed groups are pending.
+__device__ __forceinline__ void cp_async_wait(uint32_t n) {
+  switch (n) {
+    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+    case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+    case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+    case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+    case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
+    default: asm volatile("cp.async.wait_group 7;" ::: "memory"); break;
+  }
+}
+
 struct StageRing {
   uint8_t* mem;       // stages * stage_bytes
   uint64_t* bars;     // stages mbarriers
   uint32_t stage_bytes, stages;
   uint32_t phases;    // parity bit per stage
   uint32_t pending;   // stage bits with copies in flight
+  bool bulk;          // true: one bulk copy per row slice; false: 16-byte cp.async per lane
 };
 
 // Probes keys[0..n) with staged bulk gathers. desc/row0s hold 64 seeds.
@@ -459,6 +537,22 @@ __device__ bool probe_batch_async(const DevIndex& ix, const uint64_t* keys, uint
         const uint32_t st = bi % ring.stages;
         const uint32_t i0 = bi * per_stage, ni = min(per_stage, items - i0);
         uint8_t* smem = ring.mem + (size_t)st * ring.stage_bytes;
+        if (!ring.bulk) {
+          // Per-lane 16-byte copies: triple t = (item, row, chunk).
+          const uint32_t triples = ni * (uint32_t)H * cpi;
+          for (uint32_t t = lane; t < triples; t += 32) {
+            const uint32_t c = t % cpi, ri = t / cpi, i = ri % (uint32_t)H, li = ri / (uint32_t)H;
+            const uint32_t it = i0 + li, sd = it / tiles, col0 = (it % tiles) * cw;
+            if (col0 + c * 16 >= rb) continue;
+            const SeedDesc& d = desc[sd];
+            const uint64_t h = d.first + (uint64_t)i * d.step;
+            cp_async16(smem + ((size_t)li * H + i) * cw + c * 16,
+                       C.data + row_offset(row0s[sd * classes + ci], h, (int)i, C.seg,
+                                           C.row_stride) + col0 + c * 16);
+          }
+          cp_async_commit();
+          return;
+        }
         // Order this lane's earlier generic reads of the stage before the
         // async-proxy writes that will overwrite it.
         fence_proxy_async_smem();
@@ -488,13 +582,20 @@ __device__ bool probe_batch_async(const DevIndex& ix, const uint64_t* keys, uint
       for (uint32_t bi = 0; bi < prologue; ++bi) issue(bi);
       for (uint32_t bi = 0; bi < batches; ++bi) {
         const uint32_t st = bi % ring.stages;
-        const bool ok = mbar_wait(ring.bars + st, (ring.phases >> st) & 1u);
-        if (__any_sync(0xFFFFFFFFu, !ok)) {
-          if (lane == 0) atomicOr(err, 1u);
-          return false;
+        if (ring.bulk) {
+          const bool ok = mbar_wait(ring.bars + st, (ring.phases >> st) & 1u);
+          if (__any_sync(0xFFFFFFFFu, !ok)) {
+            if (lane == 0) atomicOr(err, 1u);
+            return false;
+          }
+          ring.phases ^= 1u << st;
+          ring.pending &= ~(1u << st);
+        } else {
+          // Batches bi .. min(bi + stages, batches) - 1 are committed; keep
+          // all but the oldest in flight.
+          cp_async_wait(min(ring.stages, batches - bi) - 1);
+          __syncwarp();
         }
-        ring.phases ^= 1u << st;
-        ring.pending &= ~(1u << st);
         const uint32_t i0 = bi * per_stage, ni = min(per_stage, items - i0);
         const uint8_t* smem = ring.mem + (size_t)st * ring.stage_bytes;
         for (uint32_t pair = lane; pair < ni * cpi; pair += 32) {

@@ -30,8 +30,10 @@ struct QueryLaunch {
   int warps;          // warps per block
   int blocks;         // grid size
   int smem_counters;  // 1: per-block shared counters; 0: global atomics
-  int stage_bytes;    // > 0: staged bulk-copy gather with this stage size per warp
+  int stage_bytes;    // > 0: staged gather with this stage size per warp
   int stages;         // stages in each warp's ring (staged gather)
+  int bulk;           // staged gather: 1 = bulk copy per row slice, 0 = 16-byte cp.async
+  int min_blocks;     // kernel variant compiled for 2, 3 or 4 resident 256-thread blocks/SM
 };
 
 }  // namespace zx

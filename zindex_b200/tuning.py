@@ -24,8 +24,11 @@ from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
-TEAMS = (1, 2, 4, 8, 16, 32)
+TEAMS = (2, 4, 8, 16, 32)
 WARPS = (2, 4, 8)
+STAGE_BYTES = (4096, 8192, 16384)
+STAGES = (2, 3, 4)
+MIN_BLOCKS = (2, 3, 4)
 
 
 @dataclass
@@ -42,11 +45,23 @@ class Autotuner:
     rows: List[Measurement] = field(default_factory=list)
 
     @staticmethod
-    def candidates(ix) -> List[dict]:
-        smem_opts = (1, 0) if ix.colors <= 16384 else (0,)
+    def candidates(ix, register_gather: bool = True, staged: bool = True) -> List[dict]:
+        """Register-gather teams and staged bulk-copy rings, shared-memory
+        counters whenever the colours fit (global atomics only otherwise)."""
+        smem = 1 if ix.colors <= 16384 else 0
         out = []
-        for team, warps, smem in itertools.product(TEAMS, WARPS, smem_opts):
-            out.append({"team": team, "warps": warps, "blocks": 0, "smem_counters": smem})
+        if register_gather:
+            for team, warps, minb in itertools.product(TEAMS, WARPS, MIN_BLOCKS):
+                out.append({"team": team, "warps": warps, "blocks": 0, "smem_counters": smem,
+                            "stage_bytes": 0, "stages": 1, "bulk": 0, "min_blocks": minb})
+        if staged:
+            for bulk, stage_bytes, stages, warps in itertools.product(
+                    (0, 1), STAGE_BYTES, STAGES, WARPS):
+                if stage_bytes < 16 * ix.info.hashes:
+                    continue
+                out.append({"team": 8, "warps": warps, "blocks": 0, "smem_counters": smem,
+                            "stage_bytes": stage_bytes, "stages": stages, "bulk": bulk,
+                            "min_blocks": 2})
         return out
 
     @staticmethod
@@ -66,7 +81,10 @@ class Autotuner:
         """Median milliseconds of one batch query under `launch`."""
         import torch
 
-        ix.set_launch(launch["team"], launch["warps"], launch["blocks"], launch["smem_counters"])
+        try:
+            ix.set_launch(**launch)
+        except Exception:
+            return float("inf")  # e.g. more shared memory than a block may use
         stream = torch.cuda.current_stream()
         batch.run(ix, stream)  # captures the graph for this configuration
         torch.cuda.synchronize()
@@ -89,7 +107,7 @@ class Autotuner:
             self.rows.append(Measurement(feats, dict(launch), ms, int(feats["seeds"])))
             if ms < best_ms:
                 best, best_ms = dict(launch), ms
-        ix.set_launch(best["team"], best["warps"], best["blocks"], best["smem_counters"])
+        ix.set_launch(**best)
         return {"launch": best, "ms": best_ms}
 
     def save(self, path: Path) -> None:
