@@ -61,7 +61,7 @@ typedef struct zx_launch {
   int stage_bytes;    /* > 0: staged gather, bytes per ring stage (multiple of 16) */
   int stages;         /* stages per warp ring for the staged gather, 1..8 */
   int bulk;           /* staged gather: 1 = cp.async.bulk per row slice, 0 = 16-byte cp.async */
-  int min_blocks;     /* kernel variant register budget: 2, 3 or 4 resident 256-thread blocks */
+  int min_blocks;     /* kernel variant register budget: 2 or 3 resident 256-thread blocks */
 } zx_launch;
 
 /* Thread-local message of the last failed call on this thread. */

@@ -65,21 +65,20 @@ using FusedFn = void (*)(const DevIndex*, BatchView, SeedParams, QueryLaunch, ui
                         unsigned long long*, uint32_t*);
 using ExtractFn = void (*)(BatchView, SeedParams, uint64_t*, uint32_t*, int);
 
-template <int MINB>
+template <int MINB, int STAGED>
 FusedFn fused_mode(int mode) {
   switch (mode) {
-    case 1: return fused_query_kernel<1, MINB>;
-    case 2: return fused_query_kernel<2, MINB>;
-    default: return fused_query_kernel<0, MINB>;
+    case 1: return fused_query_kernel<1, MINB, STAGED>;
+    case 2: return fused_query_kernel<2, MINB, STAGED>;
+    default: return fused_query_kernel<0, MINB, STAGED>;
   }
 }
 
-FusedFn fused_for(int mode, int min_blocks) {
-  switch (min_blocks) {
-    case 3: return fused_mode<3>(mode);
-    case 4: return fused_mode<4>(mode);
-    default: return fused_mode<2>(mode);
-  }
+// Kernel variant: seed mode x register budget (2 or 3 resident 256-thread
+// blocks per SM) x gather (register teams or staged ring).
+FusedFn fused_for(int mode, int min_blocks, bool staged) {
+  if (staged) return min_blocks == 3 ? fused_mode<3, 1>(mode) : fused_mode<2, 1>(mode);
+  return min_blocks == 3 ? fused_mode<3, 0>(mode) : fused_mode<2, 0>(mode);
 }
 
 ExtractFn extract_for(int mode) {
@@ -437,7 +436,7 @@ int Engine::max_blocks(const QueryLaunch& l) const {
     return cached_blocks_;
   int per_sm = 0;
   size_t smem = fused_smem_bytes(l);
-  FusedFn fn = fused_for(sp_.mode, l.min_blocks);
+  FusedFn fn = fused_for(sp_.mode, l.min_blocks, l.stage_bytes > 0);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
                                                            l.warps * 32, smem),
@@ -473,7 +472,7 @@ void Engine::set_launch(const QueryLaunch& l) {
   check(l.stage_bytes == 0 || (l.stage_bytes % 16 == 0 && l.stage_bytes >= 16 * m_.hashes &&
                                 l.stage_bytes <= 65536 && l.stages >= 1 && l.stages <= 8),
         kEInval, "staged gather needs 16-byte multiple stages of at least 16*H bytes, 1..8 stages");
-  check(l.min_blocks >= 2 && l.min_blocks <= 4, kEInval, "min_blocks must be 2, 3 or 4");
+  check(l.min_blocks >= 2 && l.min_blocks <= 3, kEInval, "min_blocks must be 2 or 3");
   check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
   check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
   std::lock_guard<std::mutex> lock(mu_);
@@ -611,7 +610,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   cuda_check(cudaStreamIsCapturing(s, &capturing), "cudaStreamIsCapturing");
   const bool timed = timing_ && capturing == cudaStreamCaptureStatusNone;
   if (timed) cuda_check(cudaEventRecord(ev_begin_, s), "cudaEventRecord");
-  FusedFn fn = fused_for(sp_.mode, l.min_blocks);
+  FusedFn fn = fused_for(sp_.mode, l.min_blocks, l.stage_bytes > 0);
   fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, ws.partial,
                                         counts, total, ws.error);
   cuda_check(cudaGetLastError(), "fused_query_kernel");

@@ -280,34 +280,21 @@ __device__ __forceinline__ void group_hit(const DevClass& C, uint32_t group, con
   }
 }
 
-// Colours of a hit group given the H row offsets (16-byte units) of the seed.
-template <class OnHit>
-__device__ __noinline__ void group_hit_rows(const DevClass& C, uint32_t group,
-                                            const uint32_t* rows, int H, OnHit on_hit) {
-  uint32_t gc = __ldg(C.group_color + group);
-  if (!(gc & kMultiGroup)) {
-    on_hit(gc);
-    return;
-  }
+// Members of a multi-member hit group: XOR of the H membership fields.
+__device__ __noinline__ void multi_group_hit(const DevClass& C, uint32_t gc, const uint32_t* rows,
+                                             int H, const SeedDesc& d, const Counters& cnt) {
   const uint32_t* mg = C.multi + 3 * (gc & ~kMultiGroup);
-  uint32_t off = __ldg(mg), cnt = __ldg(mg + 1), firstm = __ldg(mg + 2);
+  uint32_t off = __ldg(mg), n = __ldg(mg + 1), firstm = __ldg(mg + 2);
   uint64_t mask = 0;
-  for (int i = 0; i < H; ++i) mask ^= row_bits(C.data + (uint64_t)rows[i] * 16u, off, cnt);
+  for (int i = 0; i < H; ++i) mask ^= row_bits(C.data + (uint64_t)rows[i] * 16u, off, n);
   while (mask) {
     uint32_t mb = __ffsll((long long)mask) - 1;
     mask &= mask - 1;
-    on_hit(__ldg(C.members + firstm + mb));
+    uint32_t c = __ldg(C.members + firstm + mb);
+    if (d.rec_len && desc_rec_contains(d, c)) continue;
+    cnt.add(c);
   }
 }
-
-struct CountUnlessRecovered {
-  const Counters* cnt;
-  const SeedDesc* d;
-  __device__ __forceinline__ void operator()(uint32_t c) const {
-    if (d->rec_len && desc_rec_contains(*d, c)) return;
-    cnt->add(c);
-  }
-};
 
 // Hits of one XORed chunk; returns quickly when no field matches.
 __device__ __forceinline__ void chunk_hits_fast(const uint4& acc, uint32_t chunk, const DevClass& C,
@@ -328,7 +315,12 @@ __device__ __forceinline__ void chunk_hits_fast(const uint4& acc, uint32_t chunk
       hits &= hits - 1;
       const uint32_t group = field0 + bit / b;
       if (group >= C.groups) break;  // padding or membership bits past the last field
-      group_hit_rows(C, group, rows, H, CountUnlessRecovered{&cnt, &d});
+      const uint32_t gc = __ldg(C.group_color + group);
+      if (gc & kMultiGroup) {
+        multi_group_hit(C, gc, rows, H, d, cnt);
+      } else if (!d.rec_len || !desc_rec_contains(d, gc)) {
+        cnt.add(gc);
+      }
     }
   }
 }

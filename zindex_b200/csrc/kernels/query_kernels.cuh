@@ -135,7 +135,7 @@ __device__ __forceinline__ void build_inner_table(const SeedParams& sp, uint64_t
 // Fused extraction + probe over the tile list (one instantiation per seed
 // mode). partial: gridDim.x x colors block counters (smem_counters); counts:
 // global counters (used directly when smem_counters == 0). total: seeds.
-template <int MODE, int MINB>
+template <int MODE, int MINB, int STAGED>
 __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* __restrict__ gix,
                                                           BatchView bv, SeedParams sp,
                                                           QueryLaunch lc,
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   uint8_t* ocm = ring_base + FusedSmem::ring_bytes(lc.stage_bytes, lc.stages);
   StageRing ring{ring_base + 64, reinterpret_cast<uint64_t*>(ring_base), (uint32_t)lc.stage_bytes,
                  (uint32_t)lc.stages, 0u, 0u, lc.bulk != 0};
-  if (lc.stage_bytes > 0 && lc.bulk) {
+  if (STAGED && lc.bulk) {
     if (lane == 0) {
       for (int st = 0; st < lc.stages; ++st) mbar_init(ring.bars + st, 1);
       mbar_fence_init();
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
     uint32_t n = extract_tile<MODE>(bv, sp, tile, keys, ocm, inner, lane);
     __syncwarp();
     seeds += n;
-    if (lc.stage_bytes > 0) {
+    if (STAGED) {
       if (!probe_batch_async(ix, keys, n, desc, row0s, ring, cnt, lane, err)) {
         ring_drain(ring);
         break;

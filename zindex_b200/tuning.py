@@ -28,7 +28,7 @@ TEAMS = (2, 4, 8, 16, 32)
 WARPS = (2, 4, 8)
 STAGE_BYTES = (4096, 8192, 16384)
 STAGES = (2, 3, 4)
-MIN_BLOCKS = (2, 3, 4)
+MIN_BLOCKS = (2, 3)
 
 
 @dataclass
