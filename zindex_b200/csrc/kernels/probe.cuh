@@ -281,12 +281,13 @@ __device__ __forceinline__ void group_hit(const DevClass& C, uint32_t group, con
 }
 
 // Members of a multi-member hit group: XOR of the H membership fields.
-__device__ __noinline__ void multi_group_hit(const DevClass& C, uint32_t gc, const uint32_t* rows,
+__device__ __noinline__ void multi_group_hit(const DevClass& C, uint32_t gc, uint64_t row0,
                                              int H, const SeedDesc& d, const Counters& cnt) {
   const uint32_t* mg = C.multi + 3 * (gc & ~kMultiGroup);
   uint32_t off = __ldg(mg), n = __ldg(mg + 1), firstm = __ldg(mg + 2);
-  uint64_t mask = 0;
-  for (int i = 0; i < H; ++i) mask ^= row_bits(C.data + (uint64_t)rows[i] * 16u, off, n);
+  uint64_t mask = 0, h = d.first;
+  for (int i = 0; i < H; ++i, h += d.step)
+    mask ^= row_bits(C.data + row_offset(row0, h, i, C.seg, C.row_stride), off, n);
   while (mask) {
     uint32_t mb = __ffsll((long long)mask) - 1;
     mask &= mask - 1;
@@ -299,7 +300,7 @@ __device__ __noinline__ void multi_group_hit(const DevClass& C, uint32_t gc, con
 // Hits of one XORed chunk; returns quickly when no field matches.
 __device__ __forceinline__ void chunk_hits_fast(const uint4& acc, uint32_t chunk, const DevClass& C,
                                                 int b, uint32_t hi, const SeedDesc& d,
-                                                const uint32_t* rows, int H, const Counters& cnt) {
+                                                uint64_t row0, int H, const Counters& cnt) {
   const uint32_t p = d.pattern;
   uint32_t w0 = zero_fields_hi(acc.x ^ p, hi), w1 = zero_fields_hi(acc.y ^ p, hi);
   uint32_t w2 = zero_fields_hi(acc.z ^ p, hi), w3 = zero_fields_hi(acc.w ^ p, hi);
@@ -317,7 +318,7 @@ __device__ __forceinline__ void chunk_hits_fast(const uint4& acc, uint32_t chunk
       if (group >= C.groups) break;  // padding or membership bits past the last field
       const uint32_t gc = __ldg(C.group_color + group);
       if (gc & kMultiGroup) {
-        multi_group_hit(C, gc, rows, H, d, cnt);
+        multi_group_hit(C, gc, row0, H, d, cnt);
       } else if (!d.rec_len || !desc_rec_contains(d, gc)) {
         cnt.add(gc);
       }
@@ -326,15 +327,14 @@ __device__ __forceinline__ void chunk_hits_fast(const uint4& acc, uint32_t chunk
 }
 
 // Probes keys[0..n) (shared memory) with the whole warp. Per round of 32
-// seeds each lane fills one SeedDesc and the H row offsets of its seed for
-// every class (rows: 32 x classes x H, 16-byte units); teams of T lanes then
-// gather two seeds at a time.
+// seeds each lane fills the descriptor of one seed (and its per-class row
+// offset of position 0); teams of T lanes then gather two seeds at a time,
+// computing row addresses in registers.
 __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n, SeedDesc* desc,
-                            uint32_t* rows, int T, const Counters& cnt, int lane) {
+                            uint64_t* row0s, int T, const Counters& cnt, int lane) {
   const int H = ix.hashes, b = ix.bits;
   const uint32_t ones = field_ones(b), hi = ones << (b - 1);
   const uint32_t classes = ix.classes;
-  const uint32_t per_seed = classes * (uint32_t)H;
   const int team = lane / T, tl = lane % T, nteams = 32 / T;
   for (uint32_t r0 = 0; r0 < n; r0 += 32) {
     const uint32_t m = min(32u, n - r0);
@@ -350,20 +350,12 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
       d.rec_single = r.single;
       d.pad = 0;
       desc[lane] = d;
-      uint32_t* myrows = rows + lane * per_seed;
       for (uint32_t ci = 0; ci < classes; ++ci) {
         const DevClass& C = ix.cls[ci];
         const uint32_t part = C.partitions > 1 ? partition_id(key, ix.seed, C.partitions) : 0;
         const uint64_t count = C.slots / C.seg - (uint64_t)H + 1;
         const uint64_t base = mulhi64(d.first, count) * C.seg;
-        const uint32_t stride16 = C.row_stride >> 4;
-        const uint32_t seg = (uint32_t)C.seg;
-        uint64_t h = d.first;
-        uint32_t slot0 = (uint32_t)((uint64_t)part * C.slots + base);
-        for (int i = 0; i < H; ++i, h += d.step) {
-          uint32_t low = ((uint32_t)h ^ (uint32_t)(h >> 33)) & (seg - 1);
-          myrows[ci * H + i] = (slot0 + (uint32_t)i * seg + low) * stride16;
-        }
+        row0s[lane * classes + ci] = ((uint64_t)part * C.slots + base) * C.row_stride;
       }
       for (uint32_t i = 0; i < r.len; ++i) cnt.add(r.at(i));
     }
@@ -371,14 +363,18 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
     for (uint32_t ci = 0; ci < classes; ++ci) {
       const DevClass& C = ix.cls[ci];
       if ((uint32_t)tl >= C.fp_chunks) continue;
-      const uint4* data = reinterpret_cast<const uint4*>(C.data);
+      const uint64_t seg = C.seg;
+      const uint32_t stride = C.row_stride;
       for (uint32_t s = team; s < m; s += 2 * nteams) {
         const uint32_t s2 = s + nteams;
         const bool two = s2 < m;
-        const uint32_t* ra = rows + s * per_seed + ci * H;
-        const uint32_t* rb = rows + (two ? s2 : s) * per_seed + ci * H;
+        const SeedDesc& da = desc[s];
+        const SeedDesc& db = desc[two ? s2 : s];
+        const uint64_t ra = row0s[s * classes + ci];
+        const uint64_t rb = row0s[(two ? s2 : s) * classes + ci];
         for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T) {
           uint4 aa = make_uint4(0, 0, 0, 0), ab = make_uint4(0, 0, 0, 0);
+          uint64_t ha = da.first, hb = db.first;
           for (int i0 = 0; i0 < H; i0 += 4) {
             uint4 va[4], vb[4];
 #pragma unroll
@@ -386,8 +382,10 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
               const int i = i0 + j;
               va[j] = vb[j] = make_uint4(0, 0, 0, 0);
               if (i < H) {
-                va[j] = __ldg(data + ra[i] + chunk);
-                if (two) vb[j] = __ldg(data + rb[i] + chunk);
+                va[j] = ld_row_chunk(C.data + row_offset(ra, ha, i, seg, stride) + chunk * 16u);
+                if (two) vb[j] = ld_row_chunk(C.data + row_offset(rb, hb, i, seg, stride) + chunk * 16u);
+                ha += da.step;
+                hb += db.step;
               }
             }
 #pragma unroll
@@ -396,8 +394,8 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
               ab.x ^= vb[j].x; ab.y ^= vb[j].y; ab.z ^= vb[j].z; ab.w ^= vb[j].w;
             }
           }
-          chunk_hits_fast(aa, chunk, C, b, hi, desc[s], ra, H, cnt);
-          if (two) chunk_hits_fast(ab, chunk, C, b, hi, desc[s2], rb, H, cnt);
+          chunk_hits_fast(aa, chunk, C, b, hi, da, ra, H, cnt);
+          if (two) chunk_hits_fast(ab, chunk, C, b, hi, db, rb, H, cnt);
         }
       }
     }

@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
         break;
       }
     } else {
-      probe_batch(ix, keys, n, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, cnt, lane);
+      probe_batch(ix, keys, n, desc, row0s, lc.team, cnt, lane);
     }
   }
   if (lane == 0 && seeds) atomicAdd(total, seeds);
