@@ -74,16 +74,16 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         _run([nvcc, *ARCH, "-shared", "-o", so, *cuda_objs, *host_objs, *LIBS], verbose)
     cli = LIB / "zorindex"
     cli_src = CSRC / "cli" / "zorindex.cpp"
-    build_src = [CSRC / "build" / "builder.cpp"]
+    build_src = [CSRC / "builder" / "builder.cpp"]
     if force or _stale(cli, [cli_src, so] + build_src + heads):
         _run(["g++", "-O3", "-std=c++17", "-Wall", "-o", cli, cli_src, *build_src, *host_objs,
               f"-L{LIB}", "-lzindex_b200", f"-Wl,-rpath,$ORIGIN", *LIBS], verbose)
     zb = LIB / "zx_build"
-    zb_src = [CSRC / "build" / "zx_build_main.cpp", CSRC / "build" / "builder.cpp"]
+    zb_src = [CSRC / "builder" / "zx_build_main.cpp", CSRC / "builder" / "builder.cpp"]
     if force or _stale(zb, zb_src + heads + host_objs):
         _run(["g++", "-O3", "-std=c++17", "-Wall", "-o", zb, *zb_src, *host_objs, *LIBS], verbose)
     zs = LIB / "zx_synth"
-    zs_src = CSRC / "build" / "zx_synth.cpp"
+    zs_src = CSRC / "builder" / "zx_synth.cpp"
     if force or _stale(zs, [zs_src] + heads):
         _run(["g++", "-O3", "-std=c++17", "-Wall", "-o", zs, zs_src, "-lpthread"], verbose)
     return so

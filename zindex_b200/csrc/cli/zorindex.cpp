@@ -15,7 +15,7 @@
 #include <vector>
 
 #include "../../../include/zindex.h"
-#include "../build/builder.h"
+#include "../builder/builder.h"
 #include "../host/error.h"
 
 namespace {
