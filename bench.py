@@ -334,7 +334,7 @@ def ours(args):
     assert t_e2e == seeds and np.array_equal(c_e2e, counts_dev), "e2e and device paths disagree"
 
     # Plain form: one record per launch, on a prefix.
-    n_plain = 4000
+    n_plain = min(4000, records)
     pb = bases[: int(offsets[n_plain])]
     po = offsets[: n_plain + 1]
     t0 = time.perf_counter()

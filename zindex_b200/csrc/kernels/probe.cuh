@@ -280,52 +280,6 @@ __device__ __forceinline__ void group_hit(const DevClass& C, uint32_t group, con
   }
 }
 
-// Members of a multi-member hit group: XOR of the H membership fields.
-__device__ __noinline__ void multi_group_hit(const DevClass& C, uint32_t gc, uint64_t row0,
-                                             int H, const SeedDesc& d, const Counters& cnt) {
-  const uint32_t* mg = C.multi + 3 * (gc & ~kMultiGroup);
-  uint32_t off = __ldg(mg), n = __ldg(mg + 1), firstm = __ldg(mg + 2);
-  uint64_t mask = 0, h = d.first;
-  for (int i = 0; i < H; ++i, h += d.step)
-    mask ^= row_bits(C.data + row_offset(row0, h, i, C.seg, C.row_stride), off, n);
-  while (mask) {
-    uint32_t mb = __ffsll((long long)mask) - 1;
-    mask &= mask - 1;
-    uint32_t c = __ldg(C.members + firstm + mb);
-    if (d.rec_len && desc_rec_contains(d, c)) continue;
-    cnt.add(c);
-  }
-}
-
-// Hits of one XORed chunk; returns quickly when no field matches.
-__device__ __forceinline__ void chunk_hits_fast(const uint4& acc, uint32_t chunk, const DevClass& C,
-                                                int b, uint32_t hi, const SeedDesc& d,
-                                                uint64_t row0, int H, const Counters& cnt) {
-  const uint32_t p = d.pattern;
-  uint32_t w0 = zero_fields_hi(acc.x ^ p, hi), w1 = zero_fields_hi(acc.y ^ p, hi);
-  uint32_t w2 = zero_fields_hi(acc.z ^ p, hi), w3 = zero_fields_hi(acc.w ^ p, hi);
-  if (!(w0 | w1 | w2 | w3)) return;
-  const uint32_t fpw = 32 / b;
-  const uint32_t words[4] = {w0, w1, w2, w3};
-#pragma unroll
-  for (int wi = 0; wi < 4; ++wi) {
-    uint32_t hits = words[wi];
-    const uint32_t field0 = chunk * 4 * fpw + wi * fpw;
-    while (hits) {
-      const uint32_t bit = __ffs(hits) - 1;
-      hits &= hits - 1;
-      const uint32_t group = field0 + bit / b;
-      if (group >= C.groups) break;  // padding or membership bits past the last field
-      const uint32_t gc = __ldg(C.group_color + group);
-      if (gc & kMultiGroup) {
-        multi_group_hit(C, gc, row0, H, d, cnt);
-      } else if (!d.rec_len || !desc_rec_contains(d, gc)) {
-        cnt.add(gc);
-      }
-    }
-  }
-}
-
 // Probes keys[0..n) (shared memory) with the whole warp. Per round of 32
 // seeds each lane fills the descriptor of one seed (and its per-class row
 // offset of position 0); teams of T lanes then gather two seeds at a time,
@@ -333,7 +287,7 @@ __device__ __forceinline__ void chunk_hits_fast(const uint4& acc, uint32_t chunk
 __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n, SeedDesc* desc,
                             uint64_t* row0s, int T, const Counters& cnt, int lane) {
   const int H = ix.hashes, b = ix.bits;
-  const uint32_t ones = field_ones(b), hi = ones << (b - 1);
+  const uint32_t ones = field_ones(b);
   const uint32_t classes = ix.classes;
   const int team = lane / T, tl = lane % T, nteams = 32 / T;
   for (uint32_t r0 = 0; r0 < n; r0 += 32) {
@@ -394,8 +348,19 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
               ab.x ^= vb[j].x; ab.y ^= vb[j].y; ab.z ^= vb[j].z; ab.w ^= vb[j].w;
             }
           }
-          chunk_hits_fast(aa, chunk, C, b, hi, da, ra, H, cnt);
-          if (two) chunk_hits_fast(ab, chunk, C, b, hi, db, rb, H, cnt);
+          chunk_hits(aa, chunk, C.groups, b, ones, da.pattern, [&](uint32_t g) {
+            group_hit(C, g, da, ra, H, [&](uint32_t c) {
+              if (da.rec_len && desc_rec_contains(da, c)) return;
+              cnt.add(c);
+            });
+          });
+          if (two)
+            chunk_hits(ab, chunk, C.groups, b, ones, db.pattern, [&](uint32_t g) {
+              group_hit(C, g, db, rb, H, [&](uint32_t c) {
+                if (db.rec_len && desc_rec_contains(db, c)) return;
+                cnt.add(c);
+              });
+            });
         }
       }
     }
