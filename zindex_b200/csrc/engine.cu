@@ -611,6 +611,10 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   const bool timed = timing_ && capturing == cudaStreamCaptureStatusNone;
   if (timed) cuda_check(cudaEventRecord(ev_begin_, s), "cudaEventRecord");
   FusedFn fn = fused_for(sp_.mode, l.min_blocks, l.stage_bytes > 0);
+  // The dynamic shared-memory limit is a property of the kernel function, shared by
+  // every engine in the process: set it for this launch's size every time.
+  cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
   fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, ws.partial,
                                         counts, total, ws.error);
   cuda_check(cudaGetLastError(), "fused_query_kernel");
