@@ -117,6 +117,27 @@ int zx_query_device(zx_index* index, const uint8_t* d_bases, uint64_t nbases,
                     const uint64_t* d_offsets, uint64_t records, int recover,
                     uint64_t* d_counts, uint64_t* d_total, void* stream, int use_graph);
 
+/* Allocation-free variant of zx_query_device. No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory while
+ * querying, such as a host process whose HBM is already fully reserved by its
+ * own allocator or by resident indexes, or latency-critical loops that must
+ * not enter the driver's allocator (cudaMalloc / cudaFree can synchronise the
+ * device). It performs no cudaMalloc, cudaFree or allocating library call:
+ * its scratch (packed bases, tile plan, scan workspace) lives in one
+ * file-scope device array of 64 MiB per GPU that loads the library, held
+ * until process exit. The first call on a device resolves that array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. Limit: about 0.4 byte per base plus 28 bytes per record must fit in
+ * 64 MiB (for example 150 Mbp cannot, 100 Mbp of short reads can); larger
+ * batches return ZX_EINVAL with the needed size. Colour counts are added into
+ * d_counts / d_total (caller-zeroed) with global atomics. Every call shares
+ * the one array, so calls that overlap on the GPU (different streams, or
+ * different indexes on the same GPU) race: serialise them. Asynchronous on
+ * `stream` (a cudaStream_t; NULL = legacy default stream). */
+int zx_query_device_noalloc(zx_index* index, const uint8_t* d_bases, uint64_t nbases,
+                            const uint64_t* d_offsets, uint64_t records, int recover,
+                            uint64_t* d_counts, uint64_t* d_total, void* stream);
+
 /* Seeds of host records, in record and window order, as the reference's
  * scan_index_features emits them (src/lib.rs:574-642). *count receives the
  * total number of seeds; at most cap are written. */

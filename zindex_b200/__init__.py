@@ -114,6 +114,17 @@ class Index:
                                               c_void_p(d_counts), c_void_p(d_total),
                                               c_void_p(stream), int(use_graph)))
 
+    def query_device_noalloc(self, d_bases: int, nbases: int, d_offsets: int, records: int,
+                             d_counts: int, d_total: int, stream: int = 0,
+                             recover: bool = True) -> None:
+        """Enqueue a query of a device-resident batch without allocating any
+        device memory (scratch in a static 64 MiB array per GPU; calls must not
+        overlap on the GPU). For callers that cannot allocate while querying."""
+        _lib.check(_lib.load().zx_query_device_noalloc(self._h, c_void_p(d_bases), nbases,
+                                                      c_void_p(d_offsets), records, int(recover),
+                                                      c_void_p(d_counts), c_void_p(d_total),
+                                                      c_void_p(stream)))
+
     def extract_seeds(self, bases: np.ndarray, offsets: np.ndarray) -> np.ndarray:
         """Seeds of the records in record/window order (extraction only)."""
         bases = np.ascontiguousarray(bases, dtype=np.uint8)

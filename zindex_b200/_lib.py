@@ -28,7 +28,7 @@ EXPORTED = (
     "zx_color_unique_kmers", "zx_query_file", "zx_query_host", "zx_query_host_plain",
     "zx_query_device", "zx_extract_seeds", "zx_get_launch", "zx_set_launch",
     "zx_default_launch", "zx_write_aggregate", "zx_set_timing", "zx_last_kernel_ms",
-    "zx_query_status",
+    "zx_query_status", "zx_query_device_noalloc",
 )
 
 
@@ -79,6 +79,8 @@ def load() -> ctypes.CDLL:
         "zx_query_host_plain": (c_int, [c_void_p, c_void_p, P64, c_uint64, c_int, P64, P64]),
         "zx_query_device": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_int,
                                     c_void_p, c_void_p, c_void_p, c_int]),
+        "zx_query_device_noalloc": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64,
+                                            c_int, c_void_p, c_void_p, c_void_p]),
         "zx_extract_seeds": (c_int, [c_void_p, c_void_p, P64, c_uint64, P64, c_uint64, P64]),
         "zx_get_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
         "zx_set_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),

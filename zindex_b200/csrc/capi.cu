@@ -151,6 +151,18 @@ int zx_query_device(zx_index* index, const uint8_t* d_bases, uint64_t nbases,
   });
 }
 
+int zx_query_device_noalloc(zx_index* index, const uint8_t* d_bases, uint64_t nbases,
+                            const uint64_t* d_offsets, uint64_t records, int recover,
+                            uint64_t* d_counts, uint64_t* d_total, void* stream) {
+  return guarded([&] {
+    zx::check(index && d_offsets && d_counts && d_total, zx::kEInval, "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    index->engine->query_device_noalloc(d_bases, nbases, d_offsets, records, recover != 0,
+                                        d_counts, reinterpret_cast<unsigned long long*>(d_total),
+                                        static_cast<cudaStream_t>(stream));
+  });
+}
+
 int zx_extract_seeds(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
                      uint64_t records, uint64_t* out, uint64_t cap, uint64_t* count) {
   return guarded([&] {

@@ -177,6 +177,102 @@ RecoveryRecords read_recovery(const std::string& dir, const Manifest& m) {
 
 }  // namespace
 
+// ---- allocation-free query: scratch in a static device array ---------------
+// For callers that cannot allocate device memory (see zx_query_device_noalloc
+// in include/zindex.h). One 64 MiB array per GPU that loads the library, held
+// until process exit; its device address is resolved once per device.
+constexpr uint64_t kNoAllocScratchBytes = 64ull << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[256] = {};
+
+// Device address of the static scratch on the current device (set-up on first
+// use per device; this device must be current).
+void* noalloc_scratch(int device) {
+  check(device >= 0 && device < 256, kEInval, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+    g_noalloc_ptr[device] = p;
+  }
+  return g_noalloc_ptr[device];
+}
+}  // namespace
+
+void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
+                                  uint64_t records, bool recover, uint64_t* counts,
+                                  unsigned long long* total, cudaStream_t s) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  check(records < (1ull << 31), kEInval, "too many records for one query");
+  uint8_t* base = static_cast<uint8_t*>(noalloc_scratch(device_));
+  // Scratch layout, every region 256-byte aligned.
+  const uint64_t words = nbases / 32 + 2;
+  const uint64_t tiles = nbases / kTileWindows + nbases / kFindereTask + records + 16;
+  size_t scan_bytes = 0;
+  cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr,
+                                           (uint32_t*)nullptr, (int)(records + 1)),
+             "scan size");
+  uint64_t at = 0;
+  auto carve = [&](uint64_t bytes) {
+    uint64_t off = at;
+    at = round_up(at + bytes, 256);
+    return base + off;
+  };
+  uint32_t* err = reinterpret_cast<uint32_t*>(carve(4));
+  uint64_t* packed = reinterpret_cast<uint64_t*>(carve(words * 8));
+  uint32_t* invalid = reinterpret_cast<uint32_t*>(carve(words * 4));
+  uint32_t* tile_counts = reinterpret_cast<uint32_t*>(carve((records + 1) * 4));
+  uint32_t* tile_first = reinterpret_cast<uint32_t*>(carve((records + 1) * 4));
+  Tile* tile_list = reinterpret_cast<Tile*>(carve(tiles * sizeof(Tile)));
+  void* scan_tmp = carve(scan_bytes);
+  if (at > kNoAllocScratchBytes)
+    raise(kEInval, "batch needs " + std::to_string(at) + " bytes of scratch; the allocation-free "
+                   "query holds at most " + std::to_string(kNoAllocScratchBytes) +
+                   " bytes (about 0.4 byte per base + 28 bytes per record): split the batch");
+  // The array keeps the previous call's contents: reset what must start at zero.
+  cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+  cuda_check(cudaMemsetAsync(tile_counts + records, 0, 4, s), "memset");
+  int grid = (int)std::min<uint64_t>((words + 255) / 256, (uint64_t)sms_ * 16);
+  pack_kernel<<<std::max(grid, 1), 256, 0, s>>>(bases, nbases, packed, invalid, words);
+  cuda_check(cudaGetLastError(), "pack_kernel");
+  const int findere = m_.index_mode == kFindere;
+  int rgrid = std::max(1, (int)std::min<uint64_t>((records + 255) / 256, (uint64_t)sms_ * 16));
+  if (records) {
+    count_tiles_kernel<<<rgrid, 256, 0, s>>>(offsets, records, span(), findere, tile_counts);
+    cuda_check(cudaGetLastError(), "count_tiles_kernel");
+  }
+  size_t tmp = scan_bytes;
+  cuda_check(cub::DeviceScan::ExclusiveSum(scan_tmp, tmp, tile_counts, tile_first,
+                                           (int)(records + 1), s),
+             "tile scan");
+  if (records) {
+    fill_tiles_kernel<<<rgrid, 256, 0, s>>>(offsets, records, span(), tile_first, tile_list);
+    cuda_check(cudaGetLastError(), "fill_tiles_kernel");
+  }
+  // Register gather, colour counts added straight into the caller's counters.
+  QueryLaunch l = launch_;
+  l.smem_counters = 0;
+  l.stage_bytes = 0;
+  l.blocks = 0;
+  const size_t smem = fused_smem_bytes(l);
+  FusedFn fn = fused_for(sp_.mode, l.min_blocks, false);
+  cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  int per_sm = 0;
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, l.warps * 32, smem),
+             "occupancy");
+  uint64_t want = (tiles + l.warps - 1) / l.warps;
+  int blocks = (int)std::min<uint64_t>((uint64_t)std::max(1, per_sm) * sms_, std::max<uint64_t>(want, 1));
+  l.blocks = blocks;
+  BatchView bv{PackedView{packed, invalid}, offsets, tile_list, tile_first + records};
+  fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, nullptr,
+                                        counts, total, err);
+  cuda_check(cudaGetLastError(), "fused_query_kernel");
+}
+
 Workspace::~Workspace() {
   release_graphs();
   void* dev[] = {bases, offsets, packed, invalid, tile_counts, tile_first, tiles,

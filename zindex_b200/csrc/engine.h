@@ -88,6 +88,11 @@ class Engine {
   void query_device(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
                     uint64_t records, bool recover, uint64_t* counts, unsigned long long* total,
                     cudaStream_t stream, bool use_graph);
+  // As query_device, but every scratch buffer comes from one static device
+  // array (no device allocation at all); see zx_query_device_noalloc.
+  void query_device_noalloc(const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
+                            uint64_t records, bool recover, uint64_t* counts,
+                            unsigned long long* total, cudaStream_t stream);
   // Synchronous query of host buffers (bases, records + 1 offsets).
   void query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
                   uint64_t records, bool recover, uint64_t* counts, uint64_t* total);
