@@ -62,6 +62,8 @@ typedef struct zx_launch {
   int stages;         /* stages per warp ring for the staged gather, 1..8 */
   int bulk;           /* staged gather: 1 = cp.async.bulk per row slice, 0 = 16-byte cp.async */
   int min_blocks;     /* kernel variant register budget: 2 or 3 resident 256-thread blocks */
+  int planes;         /* register gather: 1 = per-seed row indices and per-lane bit-plane colour
+                         counters, 0 = per-seed descriptors and one counter update per hit */
 } zx_launch;
 
 /* Thread-local message of the last failed call on this thread. */

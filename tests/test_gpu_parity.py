@@ -37,11 +37,14 @@ def gpu_vs_oracle(oracle, index_dir, records, recover=True, plain=False):
     import zindex_b200 as zx
 
     bases, offsets = zx.pack_records(records)
-    with zx.Index(index_dir) as ix:
-        got, total = ix.query_records(bases, offsets, recover=recover, plain=plain)
     want, want_total = oracle.query_records(index_dir, bases, offsets, recover=recover)
-    assert total == want_total
-    np.testing.assert_array_equal(got, want)
+    with zx.Index(index_dir) as ix:
+        # Both register-gather forms: per-hit counter updates and bit-plane counters.
+        for planes in ((0,) if plain else (0, 1)):
+            ix.set_launch(planes=planes)
+            got, total = ix.query_records(bases, offsets, recover=recover, plain=plain)
+            assert total == want_total
+            np.testing.assert_array_equal(got, want)
     return got, total
 
 
@@ -222,6 +225,9 @@ LAUNCHES = [
     dict(team=1, warps=4, stage_bytes=0), dict(team=2, warps=2, stage_bytes=0),
     dict(team=8, warps=8, stage_bytes=0), dict(team=32, warps=1, stage_bytes=0),
     dict(team=16, warps=3, stage_bytes=0),
+    dict(team=1, warps=4, planes=1), dict(team=2, warps=3, planes=1),
+    dict(team=8, warps=8, planes=1, min_blocks=2), dict(team=32, warps=1, planes=1),
+    dict(team=4, warps=8, planes=1, min_blocks=2), dict(team=16, warps=8, planes=1),
     dict(warps=4, stage_bytes=8192, stages=2, bulk=1), dict(warps=8, stage_bytes=4096, stages=3, bulk=1),
     dict(warps=2, stage_bytes=64, stages=1, bulk=1), dict(warps=4, stage_bytes=128, stages=4, bulk=1),
     dict(warps=1, stage_bytes=16384, stages=8, bulk=1),
@@ -247,11 +253,11 @@ def test_launch_configurations_do_not_change_results(gpu, oracle, tmp_path_facto
             assert total == want_total
 
 
-@pytest.mark.parametrize("stage_bytes,stages,bulk", [(0, 0, 0), (8192, 2, 1), (256, 3, 1),
-                                                    (64, 2, 1), (8192, 2, 0), (256, 3, 0),
-                                                    (64, 2, 0)])
-def test_staged_gather_on_wide_partitioned_multiclass_index(gpu, oracle, tmp_path_factory,
-                                                            stage_bytes, stages, bulk):
+@pytest.mark.parametrize("stage_bytes,stages,bulk,planes", [
+    (0, 0, 0, 0), (0, 0, 0, 1), (8192, 2, 1, 0), (256, 3, 1, 0), (64, 2, 1, 0), (8192, 2, 0, 0),
+    (256, 3, 0, 0), (64, 2, 0, 0)])
+def test_gathers_on_wide_partitioned_multiclass_index(gpu, oracle, tmp_path_factory,
+                                                      stage_bytes, stages, bulk, planes):
     import zindex_b200 as zx
 
     d = tmp_path_factory.mktemp("wide")
@@ -272,7 +278,7 @@ def test_staged_gather_on_wide_partitioned_multiclass_index(gpu, oracle, tmp_pat
     want, want_total = oracle.query_records(ix, bases, offsets)
     with zx.Index(ix) as index:
         assert index.info.classes >= 2
-        index.set_launch(stage_bytes=stage_bytes, stages=stages or 1, bulk=bulk)
+        index.set_launch(stage_bytes=stage_bytes, stages=stages or 1, bulk=bulk, planes=planes)
         got, total = index.query_records(bases, offsets)
     np.testing.assert_array_equal(got, want)
     assert total == want_total

@@ -152,7 +152,8 @@ class Index:
     def _launch_dict(l: ZxLaunch) -> dict:
         return {"team": l.team, "warps": l.warps, "blocks": l.blocks,
                 "smem_counters": l.smem_counters, "stage_bytes": l.stage_bytes,
-                "stages": l.stages, "bulk": l.bulk, "min_blocks": l.min_blocks}
+                "stages": l.stages, "bulk": l.bulk, "min_blocks": l.min_blocks,
+                "planes": l.planes}
 
     def launch(self) -> dict:
         l = ZxLaunch()
@@ -167,7 +168,7 @@ class Index:
     def set_launch(self, team: int = None, warps: int = None, blocks: int = 0,
                    smem_counters: Optional[int] = None, stage_bytes: Optional[int] = None,
                    stages: Optional[int] = None, bulk: Optional[int] = None,
-                   min_blocks: Optional[int] = None, **_ignored):
+                   min_blocks: Optional[int] = None, planes: Optional[int] = None, **_ignored):
         """Change the launch configuration (never changes results); unset
         fields keep their default values."""
         d = self.default_launch()
@@ -176,7 +177,8 @@ class Index:
                      int(d["stage_bytes"] if stage_bytes is None else stage_bytes),
                      int(d["stages"] if stages is None else stages),
                      int(d["bulk"] if bulk is None else bulk),
-                     int(d["min_blocks"] if min_blocks is None else min_blocks))
+                     int(d["min_blocks"] if min_blocks is None else min_blocks),
+                     int(d["planes"] if planes is None else planes))
         _lib.check(_lib.load().zx_set_launch(self._h, byref(l)))
 
     def query_status(self) -> None:

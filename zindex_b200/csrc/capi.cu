@@ -46,6 +46,7 @@ void fill_launch(const zx::QueryLaunch& l, zx_launch* out) {
   out->stages = l.stages;
   out->bulk = l.bulk;
   out->min_blocks = l.min_blocks;
+  out->planes = l.planes;
 }
 
 }  // namespace
@@ -196,7 +197,7 @@ int zx_set_launch(zx_index* index, const zx_launch* l) {
     std::lock_guard<std::mutex> lock(index->mu);
     index->engine->set_launch(
         zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters, l->stage_bytes, l->stages,
-                        l->bulk, l->min_blocks});
+                        l->bulk, l->min_blocks, l->planes});
   });
 }
 

@@ -65,20 +65,26 @@ using FusedFn = void (*)(const DevIndex*, BatchView, SeedParams, QueryLaunch, ui
                         unsigned long long*, uint32_t*);
 using ExtractFn = void (*)(BatchView, SeedParams, uint64_t*, uint32_t*, int);
 
-template <int MINB, int STAGED>
+template <int MINB, int VARIANT>
 FusedFn fused_mode(int mode) {
   switch (mode) {
-    case 1: return fused_query_kernel<1, MINB, STAGED>;
-    case 2: return fused_query_kernel<2, MINB, STAGED>;
-    default: return fused_query_kernel<0, MINB, STAGED>;
+    case 1: return fused_query_kernel<1, MINB, VARIANT>;
+    case 2: return fused_query_kernel<2, MINB, VARIANT>;
+    default: return fused_query_kernel<0, MINB, VARIANT>;
   }
 }
 
 // Kernel variant: seed mode x register budget (2 or 3 resident 256-thread
-// blocks per SM) x gather (register teams or staged ring).
-FusedFn fused_for(int mode, int min_blocks, bool staged) {
-  if (staged) return min_blocks == 3 ? fused_mode<3, 1>(mode) : fused_mode<2, 1>(mode);
-  return min_blocks == 3 ? fused_mode<3, 0>(mode) : fused_mode<2, 0>(mode);
+// blocks per SM) x gather (register teams with per-hit counter updates,
+// staged ring, or register teams with bit-plane counters).
+FusedFn fused_for(int mode, const QueryLaunch& l) {
+  const int v = l.stage_bytes > 0 ? 1 : (l.planes ? 2 : 0);
+  if (l.min_blocks == 3) {
+    if (v == 1) return fused_mode<3, 1>(mode);
+    return v == 2 ? fused_mode<3, 2>(mode) : fused_mode<3, 0>(mode);
+  }
+  if (v == 1) return fused_mode<2, 1>(mode);
+  return v == 2 ? fused_mode<2, 2>(mode) : fused_mode<2, 0>(mode);
 }
 
 ExtractFn extract_for(int mode) {
@@ -258,7 +264,7 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
   l.stage_bytes = 0;
   l.blocks = 0;
   const size_t smem = fused_smem_bytes(l);
-  FusedFn fn = fused_for(sp_.mode, l.min_blocks, false);
+  FusedFn fn = fused_for(sp_.mode, l);
   cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "cudaFuncSetAttribute");
   int per_sm = 0;
@@ -505,17 +511,26 @@ QueryLaunch Engine::default_launch() const {
   for (uint32_t c = 0; c < host_ix_.classes; ++c) chunks = std::max(chunks, host_ix_.cls[c].fp_chunks);
   int team = 1;
   while (team < 32 && (uint32_t)team < chunks) team <<= 1;
-  // Teams of 8 lanes, 8 warps per block measured fastest on B200 for 64-256 B
-  // fingerprint rows; narrower rows use teams of one 16-byte chunk each.
+  // Row-index gather with bit-plane counters, teams of up to 16 lanes (one
+  // 16-byte chunk each) and 2 resident 8-warp blocks per SM measured fastest
+  // on B200 for 256-byte fingerprint rows (22.8 ms against 40.6 ms for the
+  // per-hit form with teams of 8 on 1.2e8 seeds). The per-hit form stays the
+  // fallback when the per-seed row indices do not fit shared memory.
   QueryLaunch l;
-  l.team = std::min(team, 8);
+  l.team = std::min(team, 16);
   l.warps = 8;
   l.smem_counters = m_.colors.size() <= 16384 ? 1 : 0;
   l.blocks = 0;  // 0: fill the device (occupancy-derived)
   l.stage_bytes = 0;  // register gather by default (fastest measured on B200 for small rows)
   l.stages = 2;
   l.bulk = 0;
-  l.min_blocks = 3;
+  l.min_blocks = 2;
+  l.planes = 1;
+  if (fused_smem_bytes(l) > 110 * 1024) {
+    l.planes = 0;
+    l.team = std::min(team, 8);
+    l.min_blocks = 3;
+  }
   return l;
 }
 
@@ -528,11 +543,11 @@ int Engine::max_blocks(const QueryLaunch& l) const {
   if (cached_blocks_ && cached_for_.team == l.team && cached_for_.warps == l.warps &&
       cached_for_.smem_counters == l.smem_counters && cached_for_.stage_bytes == l.stage_bytes &&
       cached_for_.stages == l.stages && cached_for_.bulk == l.bulk &&
-      cached_for_.min_blocks == l.min_blocks)
+      cached_for_.min_blocks == l.min_blocks && cached_for_.planes == l.planes)
     return cached_blocks_;
   int per_sm = 0;
   size_t smem = fused_smem_bytes(l);
-  FusedFn fn = fused_for(sp_.mode, l.min_blocks, l.stage_bytes > 0);
+  FusedFn fn = fused_for(sp_.mode, l);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
                                                            l.warps * 32, smem),
@@ -569,6 +584,7 @@ void Engine::set_launch(const QueryLaunch& l) {
                                 l.stage_bytes <= 65536 && l.stages >= 1 && l.stages <= 8),
         kEInval, "staged gather needs 16-byte multiple stages of at least 16*H bytes, 1..8 stages");
   check(l.min_blocks >= 2 && l.min_blocks <= 3, kEInval, "min_blocks must be 2 or 3");
+  check(l.planes == 0 || l.planes == 1, kEInval, "planes must be 0 or 1");
   check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
   check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
   std::lock_guard<std::mutex> lock(mu_);
@@ -706,7 +722,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   cuda_check(cudaStreamIsCapturing(s, &capturing), "cudaStreamIsCapturing");
   const bool timed = timing_ && capturing == cudaStreamCaptureStatusNone;
   if (timed) cuda_check(cudaEventRecord(ev_begin_, s), "cudaEventRecord");
-  FusedFn fn = fused_for(sp_.mode, l.min_blocks, l.stage_bytes > 0);
+  FusedFn fn = fused_for(sp_.mode, l);
   // The dynamic shared-memory limit is a property of the kernel function, shared by
   // every engine in the process: set it for this launch's size every time.
   cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),

@@ -117,9 +117,9 @@ __device__ __forceinline__ bool rec_contains(const RecHit& r, uint32_t c) {
 struct Counters {
   uint32_t* smem;   // colours entries, or nullptr
   uint64_t* gmem;   // used when smem is null
-  __device__ __forceinline__ void add(uint32_t c) const {
-    if (smem) atomicAdd(smem + c, 1u);
-    else atomicAdd(reinterpret_cast<unsigned long long*>(gmem + c), 1ull);
+  __device__ __forceinline__ void add(uint32_t c, uint32_t n = 1) const {
+    if (smem) atomicAdd(smem + c, n);
+    else atomicAdd(reinterpret_cast<unsigned long long*>(gmem + c), (unsigned long long)n);
   }
 };
 
@@ -363,6 +363,258 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
             });
         }
       }
+    }
+    __syncwarp();
+  }
+}
+
+// ---- row-index probe with bit-plane colour counters -------------------------
+// The owner lane of each seed writes, besides the descriptor, the row index
+// (partition * slots + cell; below 2^32 because a class holds at most 64 GiB
+// of rows of at least 16 bytes) of each of its H cells per class, so a team
+// gathers with one multiply-add per row. A lane always covers the same
+// fingerprint fields of a class (chunks tl, tl + T, ...), so its hits are
+// counted per field in vertical binary counters held in registers (bit p of
+// plane k is bit k of the count of field p) and added to the colour counters
+// only every few dozen seeds, instead of one shared-memory atomic per hit.
+// One class per lane is counted this way: the first whose fields of the lane
+// fit one 32-bit dense word (4 * chunks per lane <= b). Hits on multi-member
+// groups, every hit of a seed with recovered origins, and hits in the other
+// classes take the per-hit path (membership decode, recovered-origin
+// exclusion).
+constexpr int kPlanes = 6;            // counts up to 63 per field
+constexpr uint32_t kPlaneFlush = 31;  // team steps (two seeds each) between flushes
+
+__device__ __forceinline__ int log2_bits(int b) { return 31 - __clz(b); }
+
+// Dense layout of a lane's fields in a class: word q of the lane (its chunk
+// q / 4, 32-bit word q % 4 of that chunk) has its field-match flags at bits
+// f * b + b - 1 (zero_fields_hi); they move to dense word q / b, bits
+// f * b + q % b. Returns the group of dense word d, bit `bit`.
+__device__ __forceinline__ uint32_t dense_group(uint32_t bit, uint32_t d, int b, int lb, int tl, int T) {
+  const uint32_t r = bit & (uint32_t)(b - 1), f = bit >> lb;
+  const uint32_t q = d * (uint32_t)b + r;
+  const uint32_t chunk = (uint32_t)tl + (q >> 2) * (uint32_t)T;
+  return chunk * (128u >> lb) + (q & 3u) * (32u >> lb) + f;
+}
+
+struct LanePlanes {
+  uint32_t c[kPlanes];
+  uint32_t valid;  // dense positions that are fields of the lane
+  uint32_t multi;  // dense positions whose group has several members
+  int cls;         // class counted in the planes (-1: none)
+  uint32_t steps;
+};
+
+__device__ __forceinline__ void plane_add(uint32_t (&c)[kPlanes], uint32_t m) {
+#pragma unroll
+  for (int k = 0; k < kPlanes; ++k) {
+    const uint32_t t = c[k] & m;
+    c[k] ^= m;
+    m = t;
+  }
+}
+
+// Dense words a lane needs for class C.
+__device__ __forceinline__ uint32_t plane_words(const DevClass& C, int b, int T) {
+  const uint32_t jmax = (C.fp_chunks + (uint32_t)T - 1) / (uint32_t)T;
+  return (4u * jmax + (uint32_t)b - 1) / (uint32_t)b;
+}
+
+__device__ __forceinline__ void planes_init(LanePlanes& P, const DevIndex& ix, int tl, int T) {
+#pragma unroll
+  for (int k = 0; k < kPlanes; ++k) P.c[k] = 0;
+  P.cls = -1;
+  P.valid = P.multi = 0;
+  P.steps = 0;
+  const int b = ix.bits, lb = log2_bits(b);
+  for (uint32_t ci = 0; ci < ix.classes; ++ci) {
+    const DevClass& C = ix.cls[ci];
+    if ((uint32_t)tl >= C.fp_chunks || plane_words(C, b, T) != 1) continue;
+    P.cls = (int)ci;
+    for (uint32_t bit = 0; bit < 32; ++bit) {
+      const uint32_t q = bit & (uint32_t)(b - 1);
+      if ((uint32_t)tl + (q >> 2) * (uint32_t)T >= C.fp_chunks) continue;
+      const uint32_t g = dense_group(bit, 0, b, lb, tl, T);
+      if (g >= C.groups) continue;
+      P.valid |= 1u << bit;
+      if (__ldg(C.group_color + g) & kMultiGroup) P.multi |= 1u << bit;
+    }
+    return;
+  }
+}
+
+__device__ __forceinline__ void planes_flush(LanePlanes& P, const DevIndex& ix, int tl, int T,
+                                             const Counters& cnt) {
+  P.steps = 0;
+  uint32_t any = 0;
+#pragma unroll
+  for (int k = 0; k < kPlanes; ++k) any |= P.c[k];
+  if (!any) return;
+  const DevClass& C = ix.cls[P.cls];
+  const int b = ix.bits, lb = log2_bits(b);
+  while (any) {
+    const uint32_t bit = __ffs(any) - 1;
+    any &= any - 1;
+    uint32_t v = 0;
+#pragma unroll
+    for (int k = 0; k < kPlanes; ++k) v |= ((P.c[k] >> bit) & 1u) << k;
+    cnt.add(__ldg(C.group_color + dense_group(bit, 0, b, lb, tl, T)), v);
+  }
+#pragma unroll
+  for (int k = 0; k < kPlanes; ++k) P.c[k] = 0;
+}
+
+// Colours of a hit group given the seed's H row indices (singleton, or
+// XOR-decoded members).
+template <class OnHit>
+__device__ __forceinline__ void group_hit_rows(const DevClass& C, uint32_t group, const uint32_t* rows,
+                                               int H, OnHit&& on_hit) {
+  const uint32_t gc = __ldg(C.group_color + group);
+  if (!(gc & kMultiGroup)) {
+    on_hit(gc);
+    return;
+  }
+  const uint32_t* mg = C.multi + 3 * (gc & ~kMultiGroup);
+  const uint32_t off = __ldg(mg), n = __ldg(mg + 1), firstm = __ldg(mg + 2);
+  uint64_t mask = 0;
+  for (int i = 0; i < H; ++i) mask ^= row_bits(C.data + (uint64_t)rows[i] * C.row_stride, off, n);
+  while (mask) {
+    const uint32_t mb = __ffsll((long long)mask) - 1;
+    mask &= mask - 1;
+    on_hit(__ldg(C.members + firstm + mb));
+  }
+}
+
+// XOR of the H rows' 16-byte chunk at `col` for two seeds (row indices in
+// shared memory, 4 per seed at a time; all 8 loads issue before any XOR).
+__device__ __forceinline__ void gather_xor2(const uint8_t* col, uint32_t stride, const uint32_t* ra,
+                                            const uint32_t* rb, int H, bool two, uint4& aa, uint4& ab) {
+  aa = ab = make_uint4(0, 0, 0, 0);
+  for (int i0 = 0; i0 < H; i0 += 4) {
+    const uint4 x = *reinterpret_cast<const uint4*>(ra + i0);
+    const uint4 y = *reinterpret_cast<const uint4*>(rb + i0);
+    const uint32_t xi[4] = {x.x, x.y, x.z, x.w}, yi[4] = {y.x, y.y, y.z, y.w};
+    uint4 va[4], vb[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      va[j] = vb[j] = make_uint4(0, 0, 0, 0);
+      if (i0 + j < H) {
+        va[j] = ld_row_chunk(col + (uint64_t)xi[j] * stride);
+        if (two) vb[j] = ld_row_chunk(col + (uint64_t)yi[j] * stride);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      aa.x ^= va[j].x; aa.y ^= va[j].y; aa.z ^= va[j].z; aa.w ^= va[j].w;
+      ab.x ^= vb[j].x; ab.y ^= vb[j].y; ab.z ^= vb[j].z; ab.w ^= vb[j].w;
+    }
+  }
+}
+
+// Rows per seed and class in shared memory: H rounded up to 4.
+__device__ __forceinline__ int padded_hashes(int H) { return (H + 3) & ~3; }
+
+__device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n, SeedDesc* desc,
+                           uint32_t* rows, int T, LanePlanes& P, const Counters& cnt, int lane) {
+  const int H = ix.hashes, Hp = padded_hashes(H), b = ix.bits, lb = log2_bits(b);
+  const uint32_t ones = field_ones(b), hi = ones << (b - 1);
+  const uint32_t classes = ix.classes;
+  const uint32_t per_seed = classes * (uint32_t)Hp;
+  const int team = lane / T, tl = lane % T, nteams = 32 / T;
+  for (uint32_t r0 = 0; r0 < n; r0 += 32) {
+    const uint32_t m = min(32u, n - r0);
+    if ((uint32_t)lane < m) {
+      const uint64_t key = keys[r0 + lane];
+      SeedDesc d;
+      d.first = mixsplit(key, ix.seed);
+      d.step = splitmix64(d.first);
+      d.pattern = (uint32_t)fingerprint(key, ix.seed, b) * ones;
+      const RecHit r = recovery_lookup(ix.rec, recovery_hash(key, ix.seed));
+      d.rec_list = r.list;
+      d.rec_len = r.len;
+      d.rec_single = r.single;
+      d.pad = 0;
+      desc[lane] = d;
+      uint32_t* my = rows + lane * per_seed;
+      for (uint32_t ci = 0; ci < classes; ++ci) {
+        const DevClass& C = ix.cls[ci];
+        const uint32_t part = C.partitions > 1 ? partition_id(key, ix.seed, C.partitions) : 0;
+        const uint64_t count = C.slots / C.seg - (uint64_t)H + 1;
+        const uint32_t seg = (uint32_t)C.seg;
+        const uint32_t row0 = (uint32_t)((uint64_t)part * C.slots + mulhi64(d.first, count) * C.seg);
+        uint64_t h = d.first;
+        for (int i = 0; i < H; ++i, h += d.step)
+          my[ci * Hp + i] = row0 + (uint32_t)i * seg + (((uint32_t)h ^ (uint32_t)(h >> 33)) & (seg - 1));
+      }
+      for (uint32_t i = 0; i < r.len; ++i) cnt.add(r.at(i));
+    }
+    __syncwarp();
+    for (uint32_t s = team; s < m; s += 2 * nteams) {
+      const uint32_t s2 = s + nteams;
+      const bool two = s2 < m;
+      const SeedDesc& da = desc[s];
+      const SeedDesc& db = desc[two ? s2 : s];
+      const uint32_t pa = da.pattern, pb = db.pattern;
+      const bool slow_a = da.rec_len != 0, slow_b = two && db.rec_len != 0;
+      for (uint32_t ci = 0; ci < classes; ++ci) {
+        const DevClass& C = ix.cls[ci];
+        if ((uint32_t)tl >= C.fp_chunks) continue;
+        const uint32_t stride = C.row_stride;
+        const uint32_t* ra = rows + s * per_seed + ci * Hp;
+        const uint32_t* rb = rows + (two ? s2 : s) * per_seed + ci * Hp;
+        if ((int)ci == P.cls) {
+          // Plane class: this lane's fields fit one dense word.
+          uint32_t xa = 0, xb = 0;
+          uint32_t q0 = 0;
+          for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T, q0 += 4) {
+            uint4 aa, ab;
+            gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, two, aa, ab);
+            const uint32_t wa[4] = {aa.x, aa.y, aa.z, aa.w}, wb[4] = {ab.x, ab.y, ab.z, ab.w};
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+              const uint32_t sh = (uint32_t)(b - 1) - ((q0 + (uint32_t)w) & (uint32_t)(b - 1));
+              xa |= zero_fields_hi(wa[w] ^ pa, hi) >> sh;
+              xb |= zero_fields_hi(wb[w] ^ pb, hi) >> sh;
+            }
+          }
+          xa &= P.valid;
+          xb = two ? (xb & P.valid) : 0u;
+          const uint32_t slowa = slow_a ? xa : (xa & P.multi);
+          const uint32_t slowb = slow_b ? xb : (xb & P.multi);
+          plane_add(P.c, xa & ~slowa);
+          plane_add(P.c, xb & ~slowb);
+          for (uint32_t x = slowa; x; x &= x - 1)
+            group_hit_rows(C, dense_group(__ffs(x) - 1, 0, b, lb, tl, T), ra, H, [&](uint32_t c) {
+              if (da.rec_len && desc_rec_contains(da, c)) return;
+              cnt.add(c);
+            });
+          for (uint32_t x = slowb; x; x &= x - 1)
+            group_hit_rows(C, dense_group(__ffs(x) - 1, 0, b, lb, tl, T), rb, H, [&](uint32_t c) {
+              if (db.rec_len && desc_rec_contains(db, c)) return;
+              cnt.add(c);
+            });
+          continue;
+        }
+        for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T) {
+          uint4 aa, ab;
+          gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, two, aa, ab);
+          chunk_hits(aa, chunk, C.groups, b, ones, pa, [&](uint32_t g) {
+            group_hit_rows(C, g, ra, H, [&](uint32_t c) {
+              if (da.rec_len && desc_rec_contains(da, c)) return;
+              cnt.add(c);
+            });
+          });
+          if (two)
+            chunk_hits(ab, chunk, C.groups, b, ones, pb, [&](uint32_t g) {
+              group_hit_rows(C, g, rb, H, [&](uint32_t c) {
+                if (db.rec_len && desc_rec_contains(db, c)) return;
+                cnt.add(c);
+              });
+            });
+        }
+      }
+      if (P.cls >= 0 && ++P.steps == kPlaneFlush) planes_flush(P, ix, tl, T, cnt);
     }
     __syncwarp();
   }

@@ -75,27 +75,29 @@ struct FusedSmem {
     return smem_counters ? ((size_t)colors * 4 + 15) / 16 * 16 : 0;
   }
   static __host__ __device__ size_t ocm_entries(int k) { return kTileWindows + (size_t)k + 1; }
-  // Seed descriptors plus row offsets: 64 x classes x 8 bytes (staged
-  // gather) or 32 x classes x H x 4 bytes (register gather), whichever is
-  // larger.
-  static __host__ __device__ size_t probe_bytes(uint32_t classes, int hashes = 4) {
-    size_t rows = 64 * 8 * (size_t)classes;
-    size_t r2 = 32 * 4 * (size_t)classes * (size_t)hashes;
-    return 64 * sizeof(SeedDesc) + (rows > r2 ? rows : r2);
+  // Seed descriptors plus, per gather form: row offsets of position 0 for
+  // 64 seeds x classes (8 bytes each; descriptor and staged gathers) or the
+  // row indices of 32 seeds x classes x H rounded up to 4 (4 bytes each;
+  // row-index gather with bit-plane counters).
+  static __host__ __device__ size_t probe_bytes(uint32_t classes, int hashes = 4, int planes = 0) {
+    const size_t rows = planes ? 32 * 4 * (size_t)classes * (size_t)((hashes + 3) & ~3)
+                               : 64 * 8 * (size_t)classes;
+    return 64 * sizeof(SeedDesc) + rows;
   }
   static __host__ __device__ size_t ring_bytes(int stage_bytes, int stages) {
     return stage_bytes > 0 ? (size_t)stage_bytes * stages + 8 * 8 : 0;
   }
   static __host__ __device__ size_t warp_bytes(int mode, int k, uint32_t classes, int stage_bytes = 0,
-                                               int stages = 0, int hashes = 4) {
-    size_t b = 2 * kTileWindows * 8 + probe_bytes(classes, hashes) + ring_bytes(stage_bytes, stages);
+                                               int stages = 0, int hashes = 4, int planes = 0) {
+    size_t b = 2 * kTileWindows * 8 + probe_bytes(classes, hashes, planes) +
+               ring_bytes(stage_bytes, stages);
     if (mode == 1) b += 2 * ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
     return (b + 15) / 16 * 16;
   }
   static __host__ __device__ size_t total(int mode, int k, uint32_t colors, uint32_t classes,
                                           int hashes, const QueryLaunch& l) {
     return ix_bytes + counter_bytes(colors, l.smem_counters) + (mode == 1 ? 256 * 8 : 0) +
-           (size_t)l.warps * warp_bytes(mode, k, classes, l.stage_bytes, l.stages, hashes);
+           (size_t)l.warps * warp_bytes(mode, k, classes, l.stage_bytes, l.stages, hashes, l.planes);
   }
 };
 
@@ -135,7 +137,7 @@ __device__ __forceinline__ void build_inner_table(const SeedParams& sp, uint64_t
 // Fused extraction + probe over the tile list (one instantiation per seed
 // mode). partial: gridDim.x x colors block counters (smem_counters); counts:
 // global counters (used directly when smem_counters == 0). total: seeds.
-template <int MODE, int MINB, int STAGED>
+template <int MODE, int MINB, int VARIANT>
 __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* __restrict__ gix,
                                                           BatchView bv, SeedParams sp,
                                                           QueryLaunch lc,
@@ -160,14 +162,16 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int hashes = gix->hashes;
   uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, classes, lc.stage_bytes,
-                                                            lc.stages, hashes);
+                                                            lc.stages, hashes, VARIANT == 2);
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
   SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + 2 * kTileWindows * 8);
   uint64_t* row0s = reinterpret_cast<uint64_t*>(desc + 64);
-  uint8_t* ring_base = wbase + 2 * kTileWindows * 8 + FusedSmem::probe_bytes(classes, hashes);
+  uint8_t* ring_base =
+      wbase + 2 * kTileWindows * 8 + FusedSmem::probe_bytes(classes, hashes, VARIANT == 2);
   uint8_t* ocm = ring_base + FusedSmem::ring_bytes(lc.stage_bytes, lc.stages);
   StageRing ring{ring_base + 64, reinterpret_cast<uint64_t*>(ring_base), (uint32_t)lc.stage_bytes,
                  (uint32_t)lc.stages, 0u, 0u, lc.bulk != 0};
+  constexpr bool STAGED = VARIANT == 1;
   if (STAGED && lc.bulk) {
     if (lane == 0) {
       for (int st = 0; st < lc.stages; ++st) mbar_init(ring.bars + st, 1);
@@ -183,6 +187,8 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   __syncthreads();
   const DevIndex& ix = *six;
   const Counters cnt{scount, counts};
+  LanePlanes planes;
+  if (VARIANT == 2) planes_init(planes, ix, lane % lc.team, lc.team);
   const uint32_t ntiles = *bv.ntiles;
   const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
   unsigned long long seeds = 0;
@@ -196,10 +202,13 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
         ring_drain(ring);
         break;
       }
+    } else if (VARIANT == 2) {
+      probe_rows(ix, keys, n, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes, cnt, lane);
     } else {
       probe_batch(ix, keys, n, desc, row0s, lc.team, cnt, lane);
     }
   }
+  if (VARIANT == 2 && planes.cls >= 0) planes_flush(planes, ix, lane % lc.team, lc.team, cnt);
   if (lane == 0 && seeds) atomicAdd(total, seeds);
   __syncthreads();
   if (scount)

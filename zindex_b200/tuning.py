@@ -29,6 +29,7 @@ WARPS = (2, 4, 8)
 STAGE_BYTES = (4096, 8192, 16384)
 STAGES = (2, 3, 4)
 MIN_BLOCKS = (2, 3)
+PLANES = (0, 1)
 
 
 @dataclass
@@ -51,9 +52,10 @@ class Autotuner:
         smem = 1 if ix.colors <= 16384 else 0
         out = []
         if register_gather:
-            for team, warps, minb in itertools.product(TEAMS, WARPS, MIN_BLOCKS):
+            for team, warps, minb, planes in itertools.product(TEAMS, WARPS, MIN_BLOCKS, PLANES):
                 out.append({"team": team, "warps": warps, "blocks": 0, "smem_counters": smem,
-                            "stage_bytes": 0, "stages": 1, "bulk": 0, "min_blocks": minb})
+                            "stage_bytes": 0, "stages": 1, "bulk": 0, "min_blocks": minb,
+                            "planes": planes})
         if staged:
             for bulk, stage_bytes, stages, warps in itertools.product(
                     (0, 1), STAGE_BYTES, STAGES, WARPS):
@@ -61,7 +63,7 @@ class Autotuner:
                     continue
                 out.append({"team": 8, "warps": warps, "blocks": 0, "smem_counters": smem,
                             "stage_bytes": stage_bytes, "stages": stages, "bulk": bulk,
-                            "min_blocks": 2})
+                            "min_blocks": 2, "planes": 0})
         return out
 
     @staticmethod
