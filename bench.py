@@ -48,6 +48,10 @@ WORKLOAD = {
 }
 SYNTH = "pool:256:1000000:10000000:1"
 METRIC = "query seeds/s"
+# DRAM bytes (read + write) per seed of the fused kernel on this workload, from one ncu
+# capture of a 1.2e7-seed slice (profiles/fused_query_kernel-c2-batched.md:
+# 12.034 GB read + 7.0 MB written); scaled by the seeds of a launch.
+TRAFFIC_BYTES_PER_SEED = 12.041e9 / 1.2e7
 LIB = ROOT / "zindex_b200" / "_lib"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
@@ -362,7 +366,9 @@ def ours(args):
                     "h2d_bytes_per_step": int(len(bases) + 8 * (records + 1)),
                     "d2h_bytes_per_step": int(8 * ix.colors + 8)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak,
+                         "traffic": TRAFFIC_BYTES_PER_SEED * seeds / 1e9, "traffic_unit": "GB",
+                         "peak_kind": peak_kind,
                          "kernel": "fused_query_kernel", "kernel_ms": kernel_ms,
                          "algorithmic_bytes_per_launch": int(alg_bytes),
                          "gather_bytes_per_seed": int(gather)},
