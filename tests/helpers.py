@@ -195,6 +195,10 @@ def build_index(fof: Path, out: Path, **opts) -> Path:
             if val:
                 args.append("-R")
             continue
+        if key == "homopolymer":
+            if val:
+                args.append("-c")
+            continue
         args += [flag[key], str(val)]
     subprocess.run(args, check=True)
     return out

@@ -95,6 +95,85 @@ def test_modimizers_match_oracle(gpu, oracle, tmp_path_factory, case):
     gpu_vs_oracle(oracle, ix, reads_for(genomes, length=400, n=150, n_runs=0.1))
 
 
+FINDERE_CASES = [
+    dict(k=31, z=10, H=4, b=8),
+    dict(k=25, z=3, H=3, b=4),
+    dict(k=21, z=1, H=2, b=16),
+    dict(k=45, z=8, H=4, b=8),   # s = 37: polynomial hash of long s-mers
+    dict(k=31, z=30, H=8, b=1),  # s = 1
+]
+
+
+@pytest.mark.parametrize("case", FINDERE_CASES, ids=lambda c: "k{k}-z{z}-H{H}-b{b}".format(**c))
+def test_findere_matches_oracle(gpu, oracle, tmp_path_factory, case):
+    ix, genomes = index_for(tmp_path_factory, colors=6, length=20000, mode="findere", **case)
+    reads = reads_for(genomes, n=150, length=300, n_runs=0.2, lower=0.05)
+    g = genomes[1]
+    # Records across a 16,384-window findere task, shorter than k, exactly k, with N.
+    reads += [g[:18000], g[100:100 + case["k"] - 1], g[200:200 + case["k"]], b"",
+              g[300:600] + b"N" + g[600:900], b"ACGT" * 50]
+    gpu_vs_oracle(oracle, ix, reads)
+
+
+def test_findere_groups_and_recovery(gpu, oracle, tmp_path_factory):
+    ix, genomes = index_for(tmp_path_factory, colors=8, length=15000, seed=31, mode="findere",
+                            k=31, z=6, H=4, b=4, groups="0,1,2;3,5;6,7")
+    reads = reads_for(genomes, n=300, length=250)
+    gpu_vs_oracle(oracle, ix, reads, recover=True)
+    gpu_vs_oracle(oracle, ix, reads, recover=False)
+
+
+def test_findere_noalloc_equals_device_query(gpu, oracle, tmp_path_factory):
+    import torch
+
+    import zindex_b200 as zx
+
+    ix, genomes = index_for(tmp_path_factory, colors=6, length=20000, mode="findere", k=31, z=10,
+                            H=4, b=8)
+    reads = reads_for(genomes, n=200, length=200)
+    bases, offsets = zx.pack_records(reads)
+    want, want_total = oracle.query_records(ix, bases, offsets)
+    dev = torch.device("cuda", 0)
+    d_bases = torch.from_numpy(bases).to(dev)
+    d_off = torch.from_numpy(offsets.view(np.int64)).to(dev)
+    with zx.Index(ix) as index:
+        for _ in range(2):
+            counts = torch.zeros(index.colors, dtype=torch.int64, device=dev)
+            total = torch.zeros(1, dtype=torch.int64, device=dev)
+            index.query_device_noalloc(d_bases.data_ptr(), len(bases), d_off.data_ptr(), len(reads),
+                                       counts.data_ptr(), total.data_ptr())
+            torch.cuda.synchronize(dev)
+            assert int(total.item()) == want_total
+            np.testing.assert_array_equal(counts.cpu().numpy().astype(np.uint64), want)
+
+
+@pytest.mark.parametrize("mode,opts", [
+    ("kmers", dict(k=21, H=4, b=8)),
+    ("kmers", dict(k=41, H=3, b=8)),
+    ("minimizers", dict(k=31, m=21, H=4, b=8)),
+    ("modimizers", dict(k=25, d=4, H=4, b=8)),
+    ("findere", dict(k=31, z=10, H=4, b=8)),
+], ids=lambda v: v if isinstance(v, str) else "-".join(f"{a}{b}" for a, b in v.items()))
+def test_homopolymer_compression(gpu, oracle, tmp_path_factory, mode, opts):
+    ix, genomes = index_for(tmp_path_factory, colors=5, length=15000, seed=41, mode=mode,
+                            homopolymer=True, **opts)
+    reads = reads_for(genomes, n=200, length=300, n_runs=0.3, lower=0.1)
+    g = genomes[0]
+    reads += [b"AAAAAAAAAAAACCCCCCCCGGGGGTTTT" * 8, g[:400].replace(b"A", b"AAA"),
+              b"acgtNNNNaaaaccccggggtttt" * 10, b"", b"A" * 300]
+    gpu_vs_oracle(oracle, ix, reads)
+    if mode != "findere":
+        import zindex_b200 as zx
+
+        bases, offsets = zx.pack_records(reads)
+        with zx.Index(ix) as index:
+            got = index.extract_seeds(bases, offsets)
+        want = np.concatenate([oracle.features(r, mode=mode, k=opts["k"], m=opts.get("m", 21),
+                                               sampling=opts.get("d", 16), homopolymer=True)
+                               for r in reads])
+        np.testing.assert_array_equal(got, want)
+
+
 def test_multi_member_groups(gpu, oracle, tmp_path_factory):
     ix, genomes = index_for(tmp_path_factory, colors=8, mode="kmers", k=31, H=4, b=4,
                             groups="0,1,2;3,5;6,7")

@@ -78,6 +78,8 @@ FusedFn fused_mode(int mode) {
 // blocks per SM) x gather (register teams with per-hit counter updates,
 // staged ring, or register teams with bit-plane counters).
 FusedFn fused_for(int mode, const QueryLaunch& l) {
+  // Findere has one form: the row-index probe with per-colour position masks.
+  if (mode == 3) return l.min_blocks == 3 ? fused_query_kernel<3, 3, 2> : fused_query_kernel<3, 2, 2>;
   const int v = l.stage_bytes > 0 ? 1 : (l.planes ? 2 : 0);
   if (l.min_blocks == 3) {
     if (v == 1) return fused_mode<3, 1>(mode);
@@ -93,6 +95,46 @@ ExtractFn extract_for(int mode) {
     case 2: return extract_kernel<2>;
     default: return extract_kernel<0>;
   }
+}
+
+// ---- homopolymer compression of a batch (lib.rs:211-222, applied per ACGT
+// run by scan_index_features, lib.rs:574-589): inside a run of A/C/G/T a base
+// equal to the one before it is dropped; other bytes are kept as separators.
+__global__ void hp_mark_starts_kernel(const uint64_t* __restrict__ offsets, uint64_t records,
+                                      uint32_t* __restrict__ starts) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < records;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t p = offsets[r];
+    atomicOr(starts + (p >> 5), 1u << (p & 31));
+  }
+}
+
+__global__ void hp_keep_kernel(const uint8_t* __restrict__ bases, uint64_t nbases,
+                               const uint32_t* __restrict__ starts, uint32_t* __restrict__ keep) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= nbases;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t k = 0;
+    if (i < nbases) {
+      const uint32_t c = encode_base(bases[i]);
+      const bool start = (starts[i >> 5] >> (i & 31)) & 1u;
+      k = c > 3 || start || i == 0 || encode_base(bases[i - 1]) != c;
+    }
+    keep[i] = k;
+  }
+}
+
+__global__ void hp_compact_kernel(const uint8_t* __restrict__ bases, uint64_t nbases,
+                                  const uint32_t* __restrict__ pos, uint8_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nbases;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    if (pos[i + 1] != pos[i]) out[pos[i]] = bases[i];
+}
+
+__global__ void hp_offsets_kernel(const uint64_t* __restrict__ offsets, uint64_t records,
+                                  const uint32_t* __restrict__ pos, uint64_t* __restrict__ out) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r <= records;
+       r += (uint64_t)gridDim.x * blockDim.x)
+    out[r] = pos[offsets[r]];
 }
 
 uint64_t le64(const uint8_t* p) {
@@ -213,10 +255,30 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
                                   unsigned long long* total, cudaStream_t s) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   check(records < (1ull << 31), kEInval, "too many records for one query");
+  check(!m_.homopolymer_compression, kEUnsupported,
+        "the allocation-free query does not run homopolymer compression (the compressed batch "
+        "needs scratch of its own): use zx_query_device");
   uint8_t* base = static_cast<uint8_t*>(noalloc_scratch(device_));
-  // Scratch layout, every region 256-byte aligned.
   const uint64_t words = nbases / 32 + 2;
   const uint64_t tiles = nbases / kTileWindows + nbases / kFindereTask + records + 16;
+  // Register gather, colour counts added straight into the caller's counters.
+  QueryLaunch l = launch_;
+  l.smem_counters = 0;
+  l.stage_bytes = 0;
+  l.blocks = 0;
+  const size_t smem = fused_smem_bytes(l);
+  FusedFn fn = fused_for(sp_.mode, l);
+  cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  int per_sm = 0;
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, l.warps * 32, smem),
+             "occupancy");
+  uint64_t want = (tiles + l.warps - 1) / l.warps;
+  int blocks = (int)std::min<uint64_t>((uint64_t)std::max(1, per_sm) * sms_, std::max<uint64_t>(want, 1));
+  l.blocks = blocks;
+  const uint64_t fstate_bytes =
+      m_.index_mode == kFindere ? (uint64_t)blocks * l.warps * 2 * m_.colors.size() * 4 : 0;
+  // Scratch layout, every region 256-byte aligned.
   size_t scan_bytes = 0;
   cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr,
                                            (uint32_t*)nullptr, (int)(records + 1)),
@@ -234,12 +296,14 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
   uint32_t* tile_first = reinterpret_cast<uint32_t*>(carve((records + 1) * 4));
   Tile* tile_list = reinterpret_cast<Tile*>(carve(tiles * sizeof(Tile)));
   void* scan_tmp = carve(scan_bytes);
+  uint32_t* fstate = fstate_bytes ? reinterpret_cast<uint32_t*>(carve(fstate_bytes)) : nullptr;
   if (at > kNoAllocScratchBytes)
     raise(kEInval, "batch needs " + std::to_string(at) + " bytes of scratch; the allocation-free "
                    "query holds at most " + std::to_string(kNoAllocScratchBytes) +
                    " bytes (about 0.4 byte per base + 28 bytes per record): split the batch");
   // The array keeps the previous call's contents: reset what must start at zero.
   cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
+  if (fstate) cuda_check(cudaMemsetAsync(fstate, 0, fstate_bytes, s), "memset");
   cuda_check(cudaMemsetAsync(tile_counts + records, 0, 4, s), "memset");
   int grid = (int)std::min<uint64_t>((words + 255) / 256, (uint64_t)sms_ * 16);
   pack_kernel<<<std::max(grid, 1), 256, 0, s>>>(bases, nbases, packed, invalid, words);
@@ -258,22 +322,7 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
     fill_tiles_kernel<<<rgrid, 256, 0, s>>>(offsets, records, span(), tile_first, tile_list);
     cuda_check(cudaGetLastError(), "fill_tiles_kernel");
   }
-  // Register gather, colour counts added straight into the caller's counters.
-  QueryLaunch l = launch_;
-  l.smem_counters = 0;
-  l.stage_bytes = 0;
-  l.blocks = 0;
-  const size_t smem = fused_smem_bytes(l);
-  FusedFn fn = fused_for(sp_.mode, l);
-  cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-             "cudaFuncSetAttribute");
-  int per_sm = 0;
-  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, l.warps * 32, smem),
-             "occupancy");
-  uint64_t want = (tiles + l.warps - 1) / l.warps;
-  int blocks = (int)std::min<uint64_t>((uint64_t)std::max(1, per_sm) * sms_, std::max<uint64_t>(want, 1));
-  l.blocks = blocks;
-  BatchView bv{PackedView{packed, invalid}, offsets, tile_list, tile_first + records};
+  BatchView bv{PackedView{packed, invalid}, offsets, tile_list, tile_first + records, fstate};
   fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, nullptr,
                                         counts, total, err);
   cuda_check(cudaGetLastError(), "fused_query_kernel");
@@ -281,8 +330,10 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
 
 Workspace::~Workspace() {
   release_graphs();
-  void* dev[] = {bases, offsets, packed, invalid, tile_counts, tile_first, tiles,
-                 scan_tmp, partial, counts, total, keys_out, keys_count, error};
+  void* dev[] = {bases,      offsets,  packed,    invalid,  tile_counts, tile_first,
+                 tiles,      scan_tmp, partial,   counts,   total,       keys_out,
+                 keys_count, error,    fstate,    hp_starts, hp_keep,    hp_pos,
+                 hp_bases,   hp_offsets, hp_scan_tmp};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total};
@@ -318,8 +369,8 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
   cuda_check(cudaGetDeviceProperties(&prop, device_), "cudaGetDeviceProperties");
   sms_ = prop.multiProcessorCount;
   check(m_.classes.size() <= (size_t)kMaxClasses, kEUnsupported, "too many source classes");
-  check(m_.index_mode != kFindere, kEUnsupported,
-        "findere indexes are not supported by the GPU query path yet");
+  check(m_.index_mode != kFindere || m_.findere_z <= 224, kEUnsupported,
+        "findere z above 224 is not supported by the GPU query path");
   for (auto& b : m_.banks)
     check(b.fingerprint_first, kEUnsupported,
           "legacy interleaved (non fingerprint-first) banks are not supported; rebuild the index");
@@ -336,8 +387,6 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
   else
     sp_.ocm = OcmParams{1, (int)m_.minimizer_size, 1};
   if (sp_.klen > 32) sp_.lk = long_kmer_consts(sp_.klen);
-  check(!m_.homopolymer_compression, kEUnsupported,
-        "homopolymer-compressed indexes are not supported by the GPU query path yet");
 
   // Memory admission: banks (padded rows) + recovery directory.
   uint64_t need = 0;
@@ -583,6 +632,8 @@ void Engine::set_launch(const QueryLaunch& l) {
   check(l.stage_bytes == 0 || (l.stage_bytes % 16 == 0 && l.stage_bytes >= 16 * m_.hashes &&
                                 l.stage_bytes <= 65536 && l.stages >= 1 && l.stages <= 8),
         kEInval, "staged gather needs 16-byte multiple stages of at least 16*H bytes, 1..8 stages");
+  check(m_.index_mode != kFindere || l.stage_bytes == 0, kEInval,
+        "findere indexes use the register gather only");
   check(l.min_blocks >= 2 && l.min_blocks <= 3, kEInval, "min_blocks must be 2 or 3");
   check(l.planes == 0 || l.planes == 1, kEInval, "planes must be 0 or 1");
   check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
@@ -639,6 +690,15 @@ void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
     ws.cap_tiles = tiles;
     ws.release_graphs();
   }
+  if (m_.index_mode == kFindere) {
+    const uint64_t need = (uint64_t)max_blocks(launch_) * launch_.warps * 2 * std::max<uint64_t>(colors, 1);
+    if (need > ws.cap_fstate) {
+      if (ws.fstate) cudaFree(ws.fstate);
+      dev_alloc(&ws.fstate, need, "findere colour state");
+      ws.cap_fstate = need;
+      ws.release_graphs();
+    }
+  }
   uint64_t partial = (uint64_t)max_blocks(launch_) * colors;
   if (partial > ws.cap_partial) {
     if (ws.partial) cudaFree(ws.partial);
@@ -679,6 +739,51 @@ void Engine::ensure_host_capacity(Workspace& ws, uint64_t nbases, uint64_t recor
   }
 }
 
+void Engine::compress_homopolymers(Workspace& ws, const uint8_t*& bases, uint64_t nbases,
+                                   const uint64_t*& offsets, uint64_t records, cudaStream_t s) {
+  check(nbases < (1ull << 31) - 1, kEInval,
+        "homopolymer-compressed queries take batches below 2^31 bases: split the batch");
+  if (nbases > ws.cap_hp_bases || !ws.hp_bases) {
+    const uint64_t cap = round_up(std::max<uint64_t>({nbases, ws.cap_hp_bases * 3 / 2, 4096}), 4096);
+    for (void* p : {(void*)ws.hp_starts, (void*)ws.hp_keep, (void*)ws.hp_pos, (void*)ws.hp_bases,
+                    ws.hp_scan_tmp})
+      if (p) cudaFree(p);
+    dev_alloc(&ws.hp_starts, cap / 32 + 2, "homopolymer record starts");
+    dev_alloc(&ws.hp_keep, cap + 1, "homopolymer flags");
+    dev_alloc(&ws.hp_pos, cap + 1, "homopolymer positions");
+    dev_alloc(&ws.hp_bases, cap + 64, "compressed bases");
+    size_t tmp = 0;
+    cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, tmp, ws.hp_keep, ws.hp_pos, (int)(cap + 1)),
+               "scan size");
+    dev_alloc((uint8_t**)&ws.hp_scan_tmp, tmp, "homopolymer scan scratch");
+    ws.hp_scan_bytes = tmp;
+    ws.cap_hp_bases = cap;
+    ws.release_graphs();
+  }
+  if (records + 1 > ws.cap_hp_records || !ws.hp_offsets) {
+    const uint64_t cap = std::max<uint64_t>({records + 1, ws.cap_hp_records * 3 / 2, 1024});
+    if (ws.hp_offsets) cudaFree(ws.hp_offsets);
+    dev_alloc(&ws.hp_offsets, cap, "compressed offsets");
+    ws.cap_hp_records = cap;
+    ws.release_graphs();
+  }
+  const int bgrid = std::max(1, (int)std::min<uint64_t>((nbases + 256) / 256, (uint64_t)sms_ * 16));
+  const int rgrid = std::max(1, (int)std::min<uint64_t>((records + 256) / 256, (uint64_t)sms_ * 16));
+  cuda_check(cudaMemsetAsync(ws.hp_starts, 0, (nbases / 32 + 2) * 4, s), "memset");
+  if (records) hp_mark_starts_kernel<<<rgrid, 256, 0, s>>>(offsets, records, ws.hp_starts);
+  hp_keep_kernel<<<bgrid, 256, 0, s>>>(bases, nbases, ws.hp_starts, ws.hp_keep);
+  cuda_check(cudaGetLastError(), "hp_keep_kernel");
+  size_t tmp = ws.hp_scan_bytes;
+  cuda_check(cub::DeviceScan::ExclusiveSum(ws.hp_scan_tmp, tmp, ws.hp_keep, ws.hp_pos,
+                                           (int)(nbases + 1), s),
+             "homopolymer scan");
+  hp_compact_kernel<<<bgrid, 256, 0, s>>>(bases, nbases, ws.hp_pos, ws.hp_bases);
+  hp_offsets_kernel<<<rgrid, 256, 0, s>>>(offsets, records, ws.hp_pos, ws.hp_offsets);
+  cuda_check(cudaGetLastError(), "hp_offsets_kernel");
+  bases = ws.hp_bases;
+  offsets = ws.hp_offsets;
+}
+
 void Engine::plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records,
                         cudaStream_t s) {
   const int findere = m_.index_mode == kFindere;
@@ -702,6 +807,7 @@ void Engine::plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records
 void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                      const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
                      unsigned long long* total, cudaStream_t s) {
+  if (m_.homopolymer_compression) compress_homopolymers(ws, bases, nbases, offsets, records, s);
   const uint64_t words = nbases / 32 + 2;
   {
     int grid = (int)std::min<uint64_t>((words + 255) / 256, (uint64_t)sms_ * 16);
@@ -717,7 +823,12 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   int blocks = l.blocks > 0 ? std::min(l.blocks, blocks_cap)
                             : (int)std::min<uint64_t>((uint64_t)blocks_cap, std::max<uint64_t>(want, 1));
   l.blocks = blocks;
-  BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records};
+  BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records,
+               ws.fstate};
+  if (m_.index_mode == kFindere)
+    cuda_check(cudaMemsetAsync(ws.fstate, 0,
+                               (uint64_t)blocks * l.warps * 2 * m_.colors.size() * 4, s),
+               "memset");
   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
   cuda_check(cudaStreamIsCapturing(s, &capturing), "cudaStreamIsCapturing");
   const bool timed = timing_ && capturing == cudaStreamCaptureStatusNone;
@@ -873,6 +984,8 @@ void Engine::extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                           const uint64_t* offsets, uint64_t records, std::vector<uint64_t>& keys) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
+  check(m_.index_mode != kFindere, kEUnsupported,
+        "seed extraction output is defined for k-mer, minimizer and modimizer indexes");
   ensure_capacity(ws, nbases, records);
   ensure_host_capacity(ws, nbases, records);
   cudaStream_t s = ws.stream;
@@ -881,11 +994,14 @@ void Engine::extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   cuda_check(cudaMemcpyAsync(ws.bases, ws.h_bases, nbases, cudaMemcpyHostToDevice, s), "H2D");
   cuda_check(cudaMemcpyAsync(ws.offsets, ws.h_offsets, (records + 1) * 8, cudaMemcpyHostToDevice, s),
              "H2D");
+  const uint8_t* d_bases = ws.bases;
+  const uint64_t* d_offsets = ws.offsets;
+  if (m_.homopolymer_compression) compress_homopolymers(ws, d_bases, nbases, d_offsets, records, s);
   const uint64_t words = nbases / 32 + 2;
   pack_kernel<<<std::max<int>(1, (int)std::min<uint64_t>((words + 255) / 256, sms_ * 16ull)), 256, 0, s>>>(
-      ws.bases, nbases, ws.packed, ws.invalid, words);
+      d_bases, nbases, ws.packed, ws.invalid, words);
   cuda_check(cudaGetLastError(), "pack_kernel");
-  plan_tiles(ws, ws.offsets, records, s);
+  plan_tiles(ws, d_offsets, records, s);
   uint32_t ntiles = 0;
   cuda_check(cudaMemcpyAsync(&ntiles, ws.tile_first + records, 4, cudaMemcpyDeviceToHost, s), "D2H");
   cuda_check(cudaStreamSynchronize(s), "tiles");
@@ -905,7 +1021,8 @@ void Engine::extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   size_t smem = 256 * 8 + warps * FusedSmem::warp_bytes(sp_.mode, sp_.k, 0);
   ExtractFn efn = extract_for(sp_.mode);
   cudaFuncSetAttribute(efn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  BatchView bv{PackedView{ws.packed, ws.invalid}, ws.offsets, ws.tiles, ws.tile_first + records};
+  BatchView bv{PackedView{ws.packed, ws.invalid}, d_offsets, ws.tiles, ws.tile_first + records,
+               nullptr};
   int grid = (int)std::min<uint64_t>((ntiles + warps - 1) / warps, (uint64_t)sms_ * 8);
   efn<<<grid, warps * 32, smem, s>>>(bv, sp_, ws.keys_out, ws.keys_count, warps);
   cuda_check(cudaGetLastError(), "extract_kernel");

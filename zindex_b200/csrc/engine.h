@@ -42,6 +42,16 @@ struct Workspace {
   uint32_t* error = nullptr;        // bit 0: a bounded device wait expired
   uint64_t* keys_out = nullptr;     // extraction-only output
   uint32_t* keys_count = nullptr;
+  uint32_t* fstate = nullptr;       // findere: per grid warp, colour round masks + run lengths
+  // Homopolymer compression of the batch (indexes built with it).
+  uint32_t* hp_starts = nullptr;    // record-start bits
+  uint32_t* hp_keep = nullptr;      // keep flag per base (+1)
+  uint32_t* hp_pos = nullptr;       // exclusive scan of the flags
+  uint8_t* hp_bases = nullptr;      // compressed bases
+  uint64_t* hp_offsets = nullptr;   // compressed record offsets
+  void* hp_scan_tmp = nullptr;
+  size_t hp_scan_bytes = 0;
+  uint64_t cap_fstate = 0, cap_hp_bases = 0, cap_hp_records = 0;
   // Pinned host staging.
   uint8_t* h_bases = nullptr;
   uint64_t* h_offsets = nullptr;
@@ -115,6 +125,10 @@ class Engine {
  private:
   void load(const std::string& dir, const OpenOptions& options);
   void ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records);
+  // Homopolymer compression on the device (lib.rs:211-222 per ACGT run):
+  // replaces (bases, offsets) by the compressed batch in the workspace.
+  void compress_homopolymers(Workspace& ws, const uint8_t*& bases, uint64_t nbases,
+                             const uint64_t*& offsets, uint64_t records, cudaStream_t s);
   void ensure_host_capacity(Workspace& ws, uint64_t nbases, uint64_t records);
   void enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
                uint64_t records, bool recover, uint64_t* counts, unsigned long long* total,

@@ -223,7 +223,8 @@ struct SeedDesc {
   uint64_t first, step;
   const uint32_t* rec_list;
   uint32_t pattern;  // fingerprint replicated over every b-bit field of a word
-  uint32_t rec_len, rec_single, pad;
+  uint32_t rec_len, rec_single;
+  uint32_t live;  // row-index probe: 1 when the seed is probed (findere skips invalid s-mers)
 };
 
 __device__ __forceinline__ bool desc_rec_contains(const SeedDesc& d, uint32_t c) {
@@ -302,7 +303,7 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
       d.rec_list = r.list;
       d.rec_len = r.len;
       d.rec_single = r.single;
-      d.pad = 0;
+      d.live = 1;
       desc[lane] = d;
       for (uint32_t ci = 0; ci < classes; ++ci) {
         const DevClass& C = ix.cls[ci];
@@ -444,8 +445,9 @@ __device__ __forceinline__ void planes_init(LanePlanes& P, const DevIndex& ix, i
   }
 }
 
+template <class Sink>
 __device__ __forceinline__ void planes_flush(LanePlanes& P, const DevIndex& ix, int tl, int T,
-                                             const Counters& cnt) {
+                                             const Sink& cnt) {
   P.steps = 0;
   uint32_t any = 0;
 #pragma unroll
@@ -489,7 +491,8 @@ __device__ __forceinline__ void group_hit_rows(const DevClass& C, uint32_t group
 // XOR of the H rows' 16-byte chunk at `col` for two seeds (row indices in
 // shared memory, 4 per seed at a time; all 8 loads issue before any XOR).
 __device__ __forceinline__ void gather_xor2(const uint8_t* col, uint32_t stride, const uint32_t* ra,
-                                            const uint32_t* rb, int H, bool two, uint4& aa, uint4& ab) {
+                                            const uint32_t* rb, int H, bool va_, bool vb_, uint4& aa,
+                                            uint4& ab) {
   aa = ab = make_uint4(0, 0, 0, 0);
   for (int i0 = 0; i0 < H; i0 += 4) {
     const uint4 x = *reinterpret_cast<const uint4*>(ra + i0);
@@ -500,8 +503,8 @@ __device__ __forceinline__ void gather_xor2(const uint8_t* col, uint32_t stride,
     for (int j = 0; j < 4; ++j) {
       va[j] = vb[j] = make_uint4(0, 0, 0, 0);
       if (i0 + j < H) {
-        va[j] = ld_row_chunk(col + (uint64_t)xi[j] * stride);
-        if (two) vb[j] = ld_row_chunk(col + (uint64_t)yi[j] * stride);
+        if (va_) va[j] = ld_row_chunk(col + (uint64_t)xi[j] * stride);
+        if (vb_) vb[j] = ld_row_chunk(col + (uint64_t)yi[j] * stride);
       }
     }
 #pragma unroll
@@ -515,8 +518,16 @@ __device__ __forceinline__ void gather_xor2(const uint8_t* col, uint32_t stride,
 // Rows per seed and class in shared memory: H rounded up to 4.
 __device__ __forceinline__ int padded_hashes(int H) { return (H + 3) & ~3; }
 
-__device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n, SeedDesc* desc,
-                           uint32_t* rows, int T, LanePlanes& P, const Counters& cnt, int lane) {
+// Probes keys[0..n) in rounds of 32 (seed s of a round is keys[r0 + s]).
+// kvalid (nullptr: all valid) marks the keys to probe, bit i of word i / 32.
+// Every colour a seed hits (filter hit or recovered origin) goes to
+// sink.hit(colour, s), except singleton hits counted in the lane's bit planes
+// (flushed through sink.add(colour, count)); on_round(r0, m) runs after each
+// round with the warp converged.
+template <class Sink, class OnRound>
+__device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
+                           const uint32_t* kvalid, SeedDesc* desc, uint32_t* rows, int T,
+                           LanePlanes& P, const Sink& sink, int lane, OnRound&& on_round) {
   const int H = ix.hashes, Hp = padded_hashes(H), b = ix.bits, lb = log2_bits(b);
   const uint32_t ones = field_ones(b), hi = ones << (b - 1);
   const uint32_t classes = ix.classes;
@@ -524,30 +535,38 @@ __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
   const int team = lane / T, tl = lane % T, nteams = 32 / T;
   for (uint32_t r0 = 0; r0 < n; r0 += 32) {
     const uint32_t m = min(32u, n - r0);
+    const uint32_t round_valid = kvalid ? kvalid[r0 >> 5] : 0xFFFFFFFFu;
     if ((uint32_t)lane < m) {
-      const uint64_t key = keys[r0 + lane];
       SeedDesc d;
-      d.first = mixsplit(key, ix.seed);
-      d.step = splitmix64(d.first);
-      d.pattern = (uint32_t)fingerprint(key, ix.seed, b) * ones;
-      const RecHit r = recovery_lookup(ix.rec, recovery_hash(key, ix.seed));
-      d.rec_list = r.list;
-      d.rec_len = r.len;
-      d.rec_single = r.single;
-      d.pad = 0;
-      desc[lane] = d;
-      uint32_t* my = rows + lane * per_seed;
-      for (uint32_t ci = 0; ci < classes; ++ci) {
-        const DevClass& C = ix.cls[ci];
-        const uint32_t part = C.partitions > 1 ? partition_id(key, ix.seed, C.partitions) : 0;
-        const uint64_t count = C.slots / C.seg - (uint64_t)H + 1;
-        const uint32_t seg = (uint32_t)C.seg;
-        const uint32_t row0 = (uint32_t)((uint64_t)part * C.slots + mulhi64(d.first, count) * C.seg);
-        uint64_t h = d.first;
-        for (int i = 0; i < H; ++i, h += d.step)
-          my[ci * Hp + i] = row0 + (uint32_t)i * seg + (((uint32_t)h ^ (uint32_t)(h >> 33)) & (seg - 1));
+      d.live = (round_valid >> lane) & 1u;
+      d.rec_list = nullptr;
+      d.rec_len = d.rec_single = 0;
+      d.pattern = 0;
+      if (d.live) {
+        const uint64_t key = keys[r0 + lane];
+        d.first = mixsplit(key, ix.seed);
+        d.step = splitmix64(d.first);
+        d.pattern = (uint32_t)fingerprint(key, ix.seed, b) * ones;
+        const RecHit r = recovery_lookup(ix.rec, recovery_hash(key, ix.seed));
+        d.rec_list = r.list;
+        d.rec_len = r.len;
+        d.rec_single = r.single;
+        uint32_t* my = rows + lane * per_seed;
+        for (uint32_t ci = 0; ci < classes; ++ci) {
+          const DevClass& C = ix.cls[ci];
+          const uint32_t part = C.partitions > 1 ? partition_id(key, ix.seed, C.partitions) : 0;
+          const uint64_t count = C.slots / C.seg - (uint64_t)H + 1;
+          const uint32_t seg = (uint32_t)C.seg;
+          const uint32_t row0 =
+              (uint32_t)((uint64_t)part * C.slots + mulhi64(d.first, count) * C.seg);
+          uint64_t h = d.first;
+          for (int i = 0; i < H; ++i, h += d.step)
+            my[ci * Hp + i] =
+                row0 + (uint32_t)i * seg + (((uint32_t)h ^ (uint32_t)(h >> 33)) & (seg - 1));
+        }
+        for (uint32_t i = 0; i < r.len; ++i) sink.hit(r.at(i), (uint32_t)lane);
       }
-      for (uint32_t i = 0; i < r.len; ++i) cnt.add(r.at(i));
+      desc[lane] = d;
     }
     __syncwarp();
     for (uint32_t s = team; s < m; s += 2 * nteams) {
@@ -555,8 +574,9 @@ __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
       const bool two = s2 < m;
       const SeedDesc& da = desc[s];
       const SeedDesc& db = desc[two ? s2 : s];
+      const bool va = da.live != 0, vb = two && db.live != 0;
       const uint32_t pa = da.pattern, pb = db.pattern;
-      const bool slow_a = da.rec_len != 0, slow_b = two && db.rec_len != 0;
+      const bool slow_a = da.rec_len != 0, slow_b = vb && db.rec_len != 0;
       for (uint32_t ci = 0; ci < classes; ++ci) {
         const DevClass& C = ix.cls[ci];
         if ((uint32_t)tl >= C.fp_chunks) continue;
@@ -569,7 +589,7 @@ __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
           uint32_t q0 = 0;
           for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T, q0 += 4) {
             uint4 aa, ab;
-            gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, two, aa, ab);
+            gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, va, vb, aa, ab);
             const uint32_t wa[4] = {aa.x, aa.y, aa.z, aa.w}, wb[4] = {ab.x, ab.y, ab.z, ab.w};
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
@@ -578,8 +598,8 @@ __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
               xb |= zero_fields_hi(wb[w] ^ pb, hi) >> sh;
             }
           }
-          xa &= P.valid;
-          xb = two ? (xb & P.valid) : 0u;
+          xa = va ? (xa & P.valid) : 0u;
+          xb = vb ? (xb & P.valid) : 0u;
           const uint32_t slowa = slow_a ? xa : (xa & P.multi);
           const uint32_t slowb = slow_b ? xb : (xb & P.multi);
           plane_add(P.c, xa & ~slowa);
@@ -587,36 +607,96 @@ __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
           for (uint32_t x = slowa; x; x &= x - 1)
             group_hit_rows(C, dense_group(__ffs(x) - 1, 0, b, lb, tl, T), ra, H, [&](uint32_t c) {
               if (da.rec_len && desc_rec_contains(da, c)) return;
-              cnt.add(c);
+              sink.hit(c, s);
             });
           for (uint32_t x = slowb; x; x &= x - 1)
             group_hit_rows(C, dense_group(__ffs(x) - 1, 0, b, lb, tl, T), rb, H, [&](uint32_t c) {
               if (db.rec_len && desc_rec_contains(db, c)) return;
-              cnt.add(c);
+              sink.hit(c, s2);
             });
           continue;
         }
         for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T) {
           uint4 aa, ab;
-          gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, two, aa, ab);
-          chunk_hits(aa, chunk, C.groups, b, ones, pa, [&](uint32_t g) {
-            group_hit_rows(C, g, ra, H, [&](uint32_t c) {
-              if (da.rec_len && desc_rec_contains(da, c)) return;
-              cnt.add(c);
+          gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, va, vb, aa, ab);
+          if (va)
+            chunk_hits(aa, chunk, C.groups, b, ones, pa, [&](uint32_t g) {
+              group_hit_rows(C, g, ra, H, [&](uint32_t c) {
+                if (da.rec_len && desc_rec_contains(da, c)) return;
+                sink.hit(c, s);
+              });
             });
-          });
-          if (two)
+          if (vb)
             chunk_hits(ab, chunk, C.groups, b, ones, pb, [&](uint32_t g) {
               group_hit_rows(C, g, rb, H, [&](uint32_t c) {
                 if (db.rec_len && desc_rec_contains(db, c)) return;
-                cnt.add(c);
+                sink.hit(c, s2);
               });
             });
         }
       }
-      if (P.cls >= 0 && ++P.steps == kPlaneFlush) planes_flush(P, ix, tl, T, cnt);
+      if (P.cls >= 0 && ++P.steps == kPlaneFlush) planes_flush(P, ix, tl, T, sink);
     }
     __syncwarp();
+    on_round(r0, m);
+  }
+}
+
+// Colour counting sink of the ordinary modes.
+struct CountSink {
+  Counters cnt;
+  __device__ __forceinline__ void hit(uint32_t c, uint32_t) const { cnt.add(c); }
+  __device__ __forceinline__ void add(uint32_t c, uint32_t n) const { cnt.add(c, n); }
+};
+
+// ---- findere ----------------------------------------------------------------
+// Scores::score, findere branch (query_stream.rs:670-689; findere.rs:74-105): a
+// colour scores a k-window when all z + 1 s-mers of the window hit it. A warp
+// probes the s-mers of a tile's windows w0 .. w0 + nw - 1 (positions 0 .. nw +
+// z - 1, s-mer i starting at base w0 + i) in rounds of 32; each hit sets bit s
+// of the colour's round mask (an OR, so a colour hit by the filter and by
+// recovery counts once, the union of lookup_selected). After each round a
+// sweep counts, per colour, the positions that end a run of at least z + 1
+// consecutive hits, carrying the run length (saturated at z) into the next
+// round. Windows are the features: total = valid k-windows.
+struct FindereSink {
+  uint32_t* mask;  // colours round masks of this warp
+  __device__ __forceinline__ void hit(uint32_t c, uint32_t s) const { atomicOr(mask + c, 1u << s); }
+  __device__ __forceinline__ void add(uint32_t, uint32_t) const {}
+};
+
+// Sweeps the round masks of positions r0 .. r0 + len - 1 (bit i = r0 + i):
+// counts the positions whose run of consecutive hits is at least z + 1 long
+// and clears the masks; run[c] carries the run length at the round's end (0
+// after the tile's last round).
+__device__ __forceinline__ void findere_sweep(uint32_t* mask, uint32_t* run, uint32_t colors, int z,
+                                              uint32_t len, bool last, const Counters& cnt,
+                                              int lane) {
+  // The masks are set by L2 atomics of every lane: read them past L1 and
+  // clear them atomically. run[c] belongs to lane c % 32.
+  for (uint32_t c = (uint32_t)lane; c < colors; c += 32) {
+    uint32_t m = __ldcg(mask + c);
+    const uint32_t r = run[c];
+    if (!m) {
+      if (r) run[c] = 0;
+      continue;
+    }
+    m = atomicExch(mask + c, 0u);
+    uint32_t y = m;
+    for (int t = 1; t <= z && y; ++t) y &= t < 32 ? (m << t) : 0u;
+    uint32_t n = __popc(y);
+    const uint32_t lead = m == 0xFFFFFFFFu ? 32u : (uint32_t)(__ffs(~m) - 1);
+    const int lo = max(0, z - (int)r), hi2 = min(z, (int)lead);
+    if (hi2 > lo) n += (uint32_t)(hi2 - lo);
+    uint32_t nr;
+    if (lead >= len) {
+      nr = min((uint32_t)z, r + len);
+    } else {
+      const uint32_t mm = len == 32 ? m : (m << (32 - len));
+      nr = min((uint32_t)z, (uint32_t)__clz(~mm));
+    }
+    run[c] = last ? 0u : nr;
+    if (n) cnt.add(c, n);
   }
 }
 
@@ -718,7 +798,7 @@ __device__ bool probe_batch_async(const DevIndex& ix, const uint64_t* keys, uint
       d.rec_list = r.list;
       d.rec_len = r.len;
       d.rec_single = r.single;
-      d.pad = 0;
+      d.live = 1;
       desc[q] = d;
       for (uint32_t ci = 0; ci < classes; ++ci) {
         const DevClass& C = ix.cls[ci];

@@ -63,6 +63,7 @@ struct BatchView {
   const uint64_t* offsets;
   const Tile* tiles;
   const uint32_t* ntiles;  // device scalar
+  uint32_t* fstate;        // findere: per warp of the grid, colours round masks then run lengths
 };
 
 // Shared memory of the fused kernel, in order: DevIndex copy, counters,
@@ -92,12 +93,16 @@ struct FusedSmem {
     size_t b = 2 * kTileWindows * 8 + probe_bytes(classes, hashes, planes) +
                ring_bytes(stage_bytes, stages);
     if (mode == 1) b += 2 * ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
+    if (mode == 3) b += 64;  // findere: valid bits of up to 512 s-mer positions
     return (b + 15) / 16 * 16;
   }
+  // Findere always runs the row-index probe without a staged ring.
   static __host__ __device__ size_t total(int mode, int k, uint32_t colors, uint32_t classes,
                                           int hashes, const QueryLaunch& l) {
+    const bool fin = mode == 3;
     return ix_bytes + counter_bytes(colors, l.smem_counters) + (mode == 1 ? 256 * 8 : 0) +
-           (size_t)l.warps * warp_bytes(mode, k, classes, l.stage_bytes, l.stages, hashes, l.planes);
+           (size_t)l.warps * warp_bytes(mode, k, classes, fin ? 0 : l.stage_bytes, l.stages, hashes,
+                                        fin ? 1 : l.planes);
   }
 };
 
@@ -161,14 +166,16 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int hashes = gix->hashes;
-  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, classes, lc.stage_bytes,
-                                                            lc.stages, hashes, VARIANT == 2);
+  // Findere always runs the row-index probe (VARIANT 2) without a ring.
+  constexpr bool ROWS = VARIANT == 2 || MODE == 3;
+  const int stage_bytes = MODE == 3 ? 0 : lc.stage_bytes;
+  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, classes, stage_bytes,
+                                                            lc.stages, hashes, ROWS);
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
   SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + 2 * kTileWindows * 8);
   uint64_t* row0s = reinterpret_cast<uint64_t*>(desc + 64);
-  uint8_t* ring_base =
-      wbase + 2 * kTileWindows * 8 + FusedSmem::probe_bytes(classes, hashes, VARIANT == 2);
-  uint8_t* ocm = ring_base + FusedSmem::ring_bytes(lc.stage_bytes, lc.stages);
+  uint8_t* ring_base = wbase + 2 * kTileWindows * 8 + FusedSmem::probe_bytes(classes, hashes, ROWS);
+  uint8_t* ocm = ring_base + FusedSmem::ring_bytes(stage_bytes, lc.stages);
   StageRing ring{ring_base + 64, reinterpret_cast<uint64_t*>(ring_base), (uint32_t)lc.stage_bytes,
                  (uint32_t)lc.stages, 0u, 0u, lc.bulk != 0};
   constexpr bool STAGED = VARIANT == 1;
@@ -188,12 +195,37 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   const DevIndex& ix = *six;
   const Counters cnt{scount, counts};
   LanePlanes planes;
-  if (VARIANT == 2) planes_init(planes, ix, lane % lc.team, lc.team);
+  if (ROWS) planes_init(planes, ix, lane % lc.team, lc.team);
+  if (MODE == 3) planes.cls = -1;  // findere: every hit goes to the position masks
   const uint32_t ntiles = *bv.ntiles;
   const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
+  const uint32_t gwarp = blockIdx.x * (blockDim.x >> 5) + warp;
   unsigned long long seeds = 0;
-  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + warp; t < ntiles; t += warps_total) {
+  for (uint32_t t = gwarp; t < ntiles; t += warps_total) {
     const Tile tile = bv.tiles[t];
+    if constexpr (MODE == 3) {
+      // Findere: s-mers of positions 0 .. nw + z - 1, windows are the features.
+      const int z = sp.k - sp.klen;
+      const uint32_t npos = tile.nw + (uint32_t)z;
+      const uint64_t rb = bv.offsets[tile.record];
+      uint32_t* kvalid = reinterpret_cast<uint32_t*>(ocm);
+      tile_smers(bv.pv, rb, tile.w0, npos, sp.klen, sp.lk, keys, kvalid, lane);
+      for (uint32_t i0 = 0; i0 < tile.nw; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool ok = i < tile.nw && bv.pv.valid(rb + tile.w0 + i, (uint32_t)sp.k);
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, ok);
+        if (lane == 0) seeds += __popc(bal);
+      }
+      uint32_t* fmask = bv.fstate + (uint64_t)gwarp * 2 * colors;
+      uint32_t* frun = fmask + colors;
+      const FindereSink fs{fmask};
+      probe_rows(ix, keys, npos, kvalid, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
+                 fs, lane, [&](uint32_t r0, uint32_t m) {
+                   findere_sweep(fmask, frun, colors, z, m, r0 + m >= npos, cnt, lane);
+                   __syncwarp();
+                 });
+      continue;
+    } else {
     uint32_t n = extract_tile<MODE>(bv, sp, tile, keys, ocm, inner, lane);
     __syncwarp();
     seeds += n;
@@ -203,12 +235,15 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
         break;
       }
     } else if (VARIANT == 2) {
-      probe_rows(ix, keys, n, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes, cnt, lane);
+      probe_rows(ix, keys, n, nullptr, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
+                 CountSink{cnt}, lane, [](uint32_t, uint32_t) {});
     } else {
       probe_batch(ix, keys, n, desc, row0s, lc.team, cnt, lane);
     }
+    }
   }
-  if (VARIANT == 2 && planes.cls >= 0) planes_flush(planes, ix, lane % lc.team, lc.team, cnt);
+  if (ROWS && planes.cls >= 0)
+    planes_flush(planes, ix, lane % lc.team, lc.team, CountSink{cnt});
   if (lane == 0 && seeds) atomicAdd(total, seeds);
   __syncthreads();
   if (scount)

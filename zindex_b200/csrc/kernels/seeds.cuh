@@ -196,6 +196,65 @@ __device__ __forceinline__ uint32_t tile_kmers_long(const PackedView& pv, uint64
   return total;
 }
 
+// ---- findere s-mers ----------------------------------------------------------
+// The canonical s-mer (s = klen bases) at every position w0 + i, i < npos, of
+// the record starting at global base rb, by position: keys[i], and bit i % 32
+// of valid[i / 32] set when its s bases are all A/C/G/T (scan_canonical_kmers
+// per ACGT run, lib.rs:645-731, as findere scans them, findere.rs:178-233).
+// k > 32 uses the polynomial hash, each lane rolling over a contiguous range.
+__device__ __forceinline__ void tile_smers(const PackedView& pv, uint64_t rb, uint32_t w0,
+                                           uint32_t npos, int s, const LongKmerConsts& lk,
+                                           uint64_t* keys, uint32_t* valid, int lane) {
+  if (s <= 32) {
+    for (uint32_t i0 = 0; i0 < npos; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      bool ok = false;
+      if (i < npos) {
+        const uint64_t p = rb + w0 + i;
+        ok = pv.valid(p, s);
+        if (ok) keys[i] = canonical_at(pv, p, s);
+      }
+      const uint32_t bits = __ballot_sync(0xFFFFFFFFu, ok);
+      if (lane == 0) valid[i0 >> 5] = bits;
+    }
+    __syncwarp();
+    return;
+  }
+  for (uint32_t w = lane; w < (npos + 31) / 32; w += 32) valid[w] = 0;
+  __syncwarp();
+  const uint32_t per = (npos + 31) / 32;
+  const uint32_t a = min(npos, per * lane), e = min(npos, a + per);
+  bool live = false;
+  uint64_t f = 0, r = 0;
+  for (uint32_t i = a; i < e; ++i) {
+    const uint64_t p = rb + w0 + i;
+    if (live) {
+      if (pv.inv32(p + s - 1) & 1) {
+        live = false;
+        continue;
+      }
+      const uint64_t o = pv.code(p - 1), c = pv.code(p + s - 1);
+      f = (f - (o + 1) * lk.power) * kLongKmerBase + (c + 1);
+      r = (r - (4 - o)) * lk.inverse + (4 - c) * lk.power;
+    } else {
+      if (!pv.valid(p, s)) continue;
+      live = true;
+      f = 0;
+      r = 0;
+      uint64_t wgt = 1;
+      for (int q = 0; q < s; ++q) {
+        const uint64_t c = pv.code(p + q);
+        f = f * kLongKmerBase + (c + 1);
+        r += (4 - c) * wgt;
+        wgt *= kLongKmerBase;
+      }
+    }
+    keys[i] = splitmix64((f < r ? f : r) ^ lk.domain);
+    atomicOr(valid + (i >> 5), 1u << (i & 31));
+  }
+  __syncwarp();
+}
+
 // ---- open-closed mod-minimizers -------------------------------------------
 struct Rank16 {
   uint64_t hash;
