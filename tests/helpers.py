@@ -199,6 +199,10 @@ def build_index(fof: Path, out: Path, **opts) -> Path:
             if val:
                 args.append("-c")
             continue
+        if key == "legacy":
+            if val:
+                args.append("--legacy-layout")
+            continue
         args += [flag[key], str(val)]
     subprocess.run(args, check=True)
     return out

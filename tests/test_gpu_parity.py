@@ -174,6 +174,24 @@ def test_homopolymer_compression(gpu, oracle, tmp_path_factory, mode, opts):
         np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.parametrize("opts", [
+    dict(mode="kmers", k=31, H=4, b=8, groups="0,1,2;3,5"),
+    dict(mode="kmers", k=25, H=3, b=1, groups="1,2"),
+    dict(mode="kmers", k=31, H=4, b=16, max_size="64KiB"),
+    dict(mode="minimizers", k=31, m=21, H=4, b=4, groups="0,4"),
+    dict(mode="findere", k=31, z=10, H=4, b=8, groups="2,3,4"),
+], ids=lambda o: "-".join(f"{a}{b}" for a, b in o.items()).replace(",", "_").replace(";", "+"))
+def test_legacy_interleaved_banks(gpu, oracle, tmp_path_factory, opts):
+    """Legacy ZORPOW1 banks are permuted into fingerprint-first rows at load;
+    the counts must equal the oracle's, which reads the legacy layout as is."""
+    ix, genomes = index_for(tmp_path_factory, colors=7, length=30000, seed=13, legacy=True, **opts)
+    import json
+
+    manifest = json.loads((ix / "manifest.json").read_text())
+    assert all(not b.get("fingerprint_first", False) for b in manifest["banks"])
+    gpu_vs_oracle(oracle, ix, reads_for(genomes, n=300, length=200, n_runs=0.1))
+
+
 def test_multi_member_groups(gpu, oracle, tmp_path_factory):
     ix, genomes = index_for(tmp_path_factory, colors=8, mode="kmers", k=31, H=4, b=4,
                             groups="0,1,2;3,5;6,7")

@@ -583,7 +583,8 @@ void build_index(const BuildOptions& opt) {
       for (uint32_t e : lost)
         dropped[ji].push_back(Abandoned{recovery_hash(k[e], fp.seed), (uint32_t)job.group,
                                         g.members.size() == 1 ? 1 : v[e] >> b});
-    // Fingerprint-first packing into this partition's rows.
+    // Fingerprint-first packing into this partition's rows (legacy: the
+    // group's whole field, fingerprint in its low bits, at its offset).
     const uint64_t G = cl.groups.size(), row_bytes = (cl.row_bits + 7) / 8;
     const uint64_t mem_off = G * (uint64_t)b + g.offset - g.column * (uint64_t)b;
     uint64_t* words = cl.rows[job.partition].data();
@@ -591,6 +592,11 @@ void build_index(const BuildOptions& opt) {
       uint64_t cell = cells[s];
       if (!cell) continue;
       uint64_t base = s * row_bytes * 8;
+      if (opt.legacy_layout) {
+        or_bits(words, base + g.offset, (uint64_t)b, cell & fp_mask);
+        if (g.width > (uint64_t)b) or_bits(words, base + g.offset + b, g.width - b, cell >> b);
+        continue;
+      }
       or_bits(words, base + g.column * (uint64_t)b, (uint64_t)b, cell & fp_mask);
       if (g.width > (uint64_t)b) or_bits(words, base + mem_off, g.width - b, cell >> b);
     }
@@ -625,7 +631,7 @@ void build_index(const BuildOptions& opt) {
     const uint64_t row_bytes = (cl.row_bits + 7) / 8, payload = cl.local_slots * row_bytes;
     FramedWriter w(stage + "/" + banks[bi].file, opt.zstd_level);
     uint8_t header[40];
-    memcpy(header, "ZORPOW3\0", 8);
+    memcpy(header, opt.legacy_layout ? "ZORPOW1\0" : "ZORPOW3\0", 8);
     uint64_t fields[4] = {cl.local_slots, cl.row_bits, cl.groups.size(), payload};
     for (int i = 0; i < 4; ++i)
       for (int j = 0; j < 8; ++j) header[8 + 8 * i + j] = (uint8_t)(fields[i] >> (8 * j));
@@ -767,7 +773,7 @@ void build_index(const BuildOptions& opt) {
       gl.arr.push_back(std::move(gj));
     }
     bj.set("groups", std::move(gl));
-    bj.set("fingerprint_first", JsonValue::boolean(true));
+    bj.set("fingerprint_first", JsonValue::boolean(!opt.legacy_layout));
     if (cl.partitions > 1) {
       JsonValue rt = JsonValue::object();
       rt.set("source_slots", JsonValue::uint(cl.source_slots));

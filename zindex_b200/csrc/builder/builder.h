@@ -33,6 +33,10 @@ struct BuildOptions {
   std::string synth;
   int zstd_level = 1;
   bool quiet = false;
+  // Write banks in the legacy interleaved layout ("ZORPOW1", group fields
+  // fingerprint then membership at each group's offset) instead of
+  // fingerprint-first ("ZORPOW3").
+  bool legacy_layout = false;
 };
 
 // Builds the index; throws zx::Error.

@@ -47,6 +47,7 @@ int main(int argc, char** argv) {
     else if (a == "-z" || a == "--findere-z") o.features.z = std::stoi(val());
     else if (a == "-d" || a == "--modimizer-sampling") o.features.sampling = std::stoull(val());
     else if (a == "-c" || a == "--homopolymer-compression") o.features.homopolymer = true;
+    else if (a == "--legacy-layout") o.legacy_layout = true;
     else if (a == "-S" || a == "--slot-scale") o.slot_scale = std::stod(val());
     else if (a == "-L" || a == "--segment-length") o.segment_length = std::stoull(val());
     else if (a == "-D" || a == "--min-subindex-documents") o.min_subindex_documents = std::stoull(val());

@@ -61,6 +61,45 @@ __global__ void repack_rows_kernel(const uint8_t* __restrict__ src, uint64_t row
   }
 }
 
+// Legacy interleaved rows (ZORPOW1: group g's fingerprint in the low b bits of
+// its field at offset_g, membership bits after it; storage.rs:2864-2914) moved
+// into the device's fingerprint-first rows (fingerprint at g*b, membership at
+// G*b + offset_g - g*b; storage.rs:1721-1754). The move is a fixed bit
+// permutation of the row, and XOR commutes with it, so the query kernels read
+// legacy indexes unchanged. One warp per row; fields are ORed into the
+// zeroed destination row.
+__global__ void repack_legacy_kernel(const uint8_t* __restrict__ src, uint64_t rows,
+                                     uint32_t row_bytes, uint32_t stride,
+                                     const uint2* __restrict__ fields, uint32_t groups, int b,
+                                     uint8_t* __restrict__ dst) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t r = blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); r < rows;
+       r += warps) {
+    const uint8_t* in = src + r * row_bytes;
+    uint32_t* out = reinterpret_cast<uint32_t*>(dst + r * stride);
+    for (uint32_t w = lane; w < stride / 4; w += 32) out[w] = 0;
+    __syncwarp();
+    auto put = [&](uint64_t bit, uint32_t width, uint64_t v) {
+      while (width) {
+        const uint32_t sh = (uint32_t)(bit & 31), n = min(width, 32 - sh);
+        const uint32_t part = (uint32_t)(v & ((1ull << n) - 1));
+        if (part) atomicOr(out + (bit >> 5), part << sh);
+        v >>= n;
+        bit += n;
+        width -= n;
+      }
+    };
+    for (uint32_t g = lane; g < groups; g += 32) {
+      const uint2 f = fields[g];  // {offset, width}
+      put((uint64_t)g * b, (uint32_t)b, row_bits(in, f.x, (uint32_t)b));
+      if (f.y > (uint32_t)b)
+        put((uint64_t)groups * b + f.x - (uint64_t)g * b, f.y - b, row_bits(in, f.x + b, f.y - b));
+    }
+    __syncwarp();
+  }
+}
+
 using FusedFn = void (*)(const DevIndex*, BatchView, SeedParams, QueryLaunch, uint32_t*, uint64_t*,
                         unsigned long long*, uint32_t*);
 using ExtractFn = void (*)(BatchView, SeedParams, uint64_t*, uint32_t*, int);
@@ -371,9 +410,6 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
   check(m_.classes.size() <= (size_t)kMaxClasses, kEUnsupported, "too many source classes");
   check(m_.index_mode != kFindere || m_.findere_z <= 224, kEUnsupported,
         "findere z above 224 is not supported by the GPU query path");
-  for (auto& b : m_.banks)
-    check(b.fingerprint_first, kEUnsupported,
-          "legacy interleaved (non fingerprint-first) banks are not supported; rebuild the index");
 
   // Seed parameters from the manifest (the query takes every setting from it).
   sp_.mode = m_.index_mode;
@@ -428,9 +464,27 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
     C.groups = (uint32_t)G;
     C.row_stride = stride;
     C.fp_chunks = (uint32_t)((first.lookup_bytes(b) + 15) / 16);
-    // Row offsets are kept as 32-bit counts of 16-byte units by the kernels.
+    // The kernels address rows by 32-bit row index (partition * slots + cell):
+    // at least 16 bytes per row, so at most 64 GiB per class.
     check((uint64_t)banks.size() * first.slots * stride < (1ull << 36), kEUnsupported,
           "a source class larger than 64 GiB is not supported by the device layout");
+    // Legacy banks: each group's {offset, width} for the row permutation.
+    uint2* d_fields = nullptr;
+    bool any_legacy = false;
+    for (size_t bi : banks) any_legacy |= !m_.banks[bi].fingerprint_first;
+    if (any_legacy) {
+      std::vector<uint2> fields(G);
+      for (uint64_t g = 0; g < G; ++g) {
+        const GroupMeta& gm = first.groups[g];
+        check_format(gm.width >= (uint64_t)b && gm.width - b <= 63 &&
+                         gm.offset + gm.width <= first.row_bits,
+                     "invalid group field in a legacy bank");
+        fields[g] = make_uint2((uint32_t)gm.offset, (uint32_t)gm.width);
+      }
+      dev_alloc(&d_fields, G, "legacy field table");
+      cuda_check(cudaMemcpy(d_fields, fields.data(), G * sizeof(uint2), cudaMemcpyHostToDevice),
+                 "upload");
+    }
     uint8_t* data = nullptr;
     dev_alloc(&data, (uint64_t)banks.size() * first.slots * stride, "bank payload");
     allocations_.push_back(data);
@@ -441,7 +495,8 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
       payload.resize(bytes);
       uint8_t header[40];
       read_bank_stream(dir + "/" + bm.file, header, payload.data(), bytes, threads);
-      check_format(!memcmp(header, "ZORPOW3\0", 8), "invalid bank magic");
+      check_format(!memcmp(header, bm.fingerprint_first ? "ZORPOW3\0" : "ZORPOW1\0", 8),
+                   "invalid bank magic");
       check_format(le64(header + 8) == bm.slots && le64(header + 16) == bm.row_bits &&
                        le64(header + 24) == bm.groups.size() && le64(header + 32) == bytes,
                    "bank header differs from manifest");
@@ -452,10 +507,18 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
         cuda_check(cudaMemcpy(d_stage, payload.data() + r0 * row_bytes, rows * row_bytes,
                               cudaMemcpyHostToDevice),
                    "bank upload");
-        repack_rows_kernel<<<sms_ * 8, 256>>>(d_stage, rows, (uint32_t)row_bytes, stride,
-                                              dst + r0 * stride);
-        cuda_check(cudaGetLastError(), "repack_rows_kernel");
+        if (bm.fingerprint_first)
+          repack_rows_kernel<<<sms_ * 8, 256>>>(d_stage, rows, (uint32_t)row_bytes, stride,
+                                                dst + r0 * stride);
+        else
+          repack_legacy_kernel<<<sms_ * 8, 256>>>(d_stage, rows, (uint32_t)row_bytes, stride,
+                                                  d_fields, (uint32_t)G, b, dst + r0 * stride);
+        cuda_check(cudaGetLastError(), "repack kernel");
       }
+    }
+    if (d_fields) {
+      cuda_check(cudaDeviceSynchronize(), "legacy repack");
+      cudaFree(d_fields);
     }
     // Group -> colour table, multi-member decode table.
     std::vector<uint32_t> gc(G), multi, members;
