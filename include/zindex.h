@@ -164,6 +164,59 @@ int zx_query_status(zx_index* index);
 int zx_set_timing(zx_index* index, int on);
 int zx_last_kernel_ms(zx_index* index, float* ms);
 
+/* Several requests coalesced into one asynchronous launch on `stream`, each
+ * with its own counters: the batch's records are the requests' records back
+ * to back, request s owning records seg_records[s] .. seg_records[s+1]-1
+ * (host array of segments + 1 entries, seg_records[segments] == records).
+ * counts (device, segments x colours, request-major) and totals (device,
+ * segments) are accumulated, not cleared. Each request's counts equal those
+ * of querying it alone (query_stream.rs:280-300 per request). Replaces one
+ * query_command_with_memory call per query file (storage.rs:3731) when many
+ * files are answered by one resident index. */
+int zx_query_segments(zx_index* index, const uint8_t* bases, uint64_t nbases,
+                      const uint64_t* offsets, uint64_t records, const uint64_t* seg_records,
+                      uint32_t segments, int recover, uint64_t* counts, uint64_t* totals,
+                      void* stream);
+
+/* Request server over a resident index (no reference counterpart: the
+ * reference answers one query file per process run, zorindex.rs:341-343).
+ * Requests from any thread are copied at submit, queued, admitted into a
+ * batch when one of `slots` batch slots is free and the batch still has room
+ * in the slot's device buffers (slot_bases bases, slot_records records,
+ * slot_requests requests, sized at start), and answered by one segmented
+ * launch per batch; slots run on their own streams, so batches overlap.
+ * Results are those of each request queried alone. The index must outlive
+ * the server; other calls on the index serialise with its launches. */
+typedef struct zx_server zx_server;
+
+typedef struct zx_server_options {
+  int slots;              /* batches in flight, 1..16 (0 = 3) */
+  uint64_t slot_bases;    /* bases per batch (0 = 64 Mi) */
+  uint64_t slot_records;  /* records per batch (0 = 1 Mi) */
+  uint32_t slot_requests; /* requests per batch (0 = 512) */
+} zx_server_options;
+
+typedef struct zx_server_report {
+  uint64_t submitted, completed, failed, batches, seeds, bases;
+  double p50_s, p99_s, mean_s, max_s; /* submit-to-completion latency */
+  double elapsed_s;                   /* since start or the last reset */
+  uint64_t device_bytes;              /* device memory held by the slots */
+} zx_server_report;
+
+int zx_server_start(zx_index* index, const zx_server_options* options, zx_server** out);
+/* Queue one request (host buffers, copied before returning); ZX_EINVAL if it
+ * does not fit one batch slot. */
+int zx_server_submit(zx_server* server, const uint8_t* bases, const uint64_t* offsets,
+                     uint64_t records, int recover, uint64_t* ticket);
+/* Wait up to timeout_ms (< 0: forever); ZX_ETIMEOUT if not done yet (the
+ * ticket stays valid). On success the counts (colours entries), total and
+ * latency are written and the ticket is released. */
+int zx_server_wait(zx_server* server, uint64_t ticket, int timeout_ms, uint64_t* counts,
+                   uint64_t* total, double* latency_s);
+int zx_server_stats(zx_server* server, int reset, zx_server_report* out);
+/* Finish every queued request, then stop (pending results are dropped). */
+void zx_server_stop(zx_server* server);
+
 /* Write the aggregate report exactly as print_aggregate does
  * (storage.rs:3817-3844): stdout-style TSV
  * "color\tmatches\tratio\tunique_kmers" with rows whose ratio >= min_ratio to

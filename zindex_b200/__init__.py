@@ -9,6 +9,8 @@ Host-side mirror of the reference's query interface:
   ``print_aggregate`` (storage.rs:3817-3844).
 * ``query_command(index_dir, query, min_ratio, recover)`` prints the aggregate
   TSV like ``query_command_with_recovery`` (storage.rs:3722-3744).
+* ``Server(index)`` answers many query requests from a resident index with
+  continuous batching (one segmented launch per batch, per-request counts).
 
 All compute runs in the CUDA kernels of libzindex_b200.so; this module only
 moves buffers across the C ABI (include/zindex.h).
@@ -26,7 +28,7 @@ import numpy as np
 from . import _lib
 from ._lib import ZxError, ZxInfo, ZxLaunch
 
-__all__ = ["Index", "ZxError", "query_command", "pack_records", "LIB_DIR"]
+__all__ = ["Index", "Server", "ZxError", "query_command", "pack_records", "LIB_DIR"]
 
 LIB_DIR = _lib.LIB_DIR
 INDEX_MODES = ("kmers", "minimizers", "modimizers", "findere")
@@ -125,6 +127,18 @@ class Index:
                                                       c_void_p(d_counts), c_void_p(d_total),
                                                       c_void_p(stream)))
 
+    def query_segments(self, d_bases: int, nbases: int, d_offsets: int, records: int,
+                       seg_records: np.ndarray, d_counts: int, d_totals: int, stream: int = 0,
+                       recover: bool = True) -> None:
+        """Enqueue several requests coalesced into one launch: request s owns
+        records seg_records[s] .. seg_records[s+1]-1 of the device batch; its
+        counts go to row s of d_counts (segments x colours, uint64) and its
+        total to d_totals[s]. Each row equals the request queried alone."""
+        seg = np.ascontiguousarray(seg_records, dtype=np.uint64)
+        _lib.check(_lib.load().zx_query_segments(
+            self._h, c_void_p(d_bases), nbases, c_void_p(d_offsets), records, _p64(seg),
+            len(seg) - 1, int(recover), c_void_p(d_counts), c_void_p(d_totals), c_void_p(stream)))
+
     def extract_seeds(self, bases: np.ndarray, offsets: np.ndarray) -> np.ndarray:
         """Seeds of the records in record/window order (extraction only)."""
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
@@ -201,6 +215,63 @@ class Index:
         _lib.check(_lib.load().zx_write_aggregate(
             self._h, label.encode(), _p64(counts), int(total), int(probes), float(min_ratio),
             float(seconds), out_path.encode() if out_path else None, int(stats)))
+
+
+class Server:
+    """Request server over a resident Index (see zx_server_start in include/zindex.h).
+
+    submit() copies a request and returns a ticket; wait() returns its
+    (counts, total, latency_s). Requests are admitted into batches as batch
+    slots free up (continuous batching) and answered by segmented launches on
+    per-slot streams. The Index must stay open while the server runs.
+    """
+
+    def __init__(self, index: Index, slots: int = 0, slot_bases: int = 0, slot_records: int = 0,
+                 slot_requests: int = 0):
+        self.index = index
+        opts = _lib.ZxServerOptions(int(slots), int(slot_bases), int(slot_records),
+                                    int(slot_requests))
+        handle = c_void_p()
+        _lib.check(_lib.load().zx_server_start(index._h, byref(opts), byref(handle)))
+        self._h = handle
+
+    def submit(self, bases: np.ndarray, offsets: np.ndarray, recover: bool = True) -> int:
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        ticket = c_uint64()
+        _lib.check(_lib.load().zx_server_submit(self._h, bases.ctypes.data_as(c_void_p),
+                                               _p64(offsets), len(offsets) - 1, int(recover),
+                                               byref(ticket)))
+        return int(ticket.value)
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        counts = np.zeros(self.index.colors, dtype=np.uint64)
+        total, latency = c_uint64(), ctypes.c_double()
+        _lib.check(_lib.load().zx_server_wait(self._h, int(ticket), int(timeout_ms), _p64(counts),
+                                             byref(total), byref(latency)))
+        return counts, int(total.value), float(latency.value)
+
+    def stats(self, reset: bool = False) -> dict:
+        st = _lib.ZxServerStats()
+        _lib.check(_lib.load().zx_server_stats(self._h, int(reset), byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().zx_server_stop(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def query_command(index_dir, query, min_ratio: float = 0.0, recover: bool = True,

@@ -28,7 +28,8 @@ EXPORTED = (
     "zx_color_unique_kmers", "zx_query_file", "zx_query_host", "zx_query_host_plain",
     "zx_query_device", "zx_extract_seeds", "zx_get_launch", "zx_set_launch",
     "zx_default_launch", "zx_write_aggregate", "zx_set_timing", "zx_last_kernel_ms",
-    "zx_query_status", "zx_query_device_noalloc",
+    "zx_query_status", "zx_query_device_noalloc", "zx_query_segments", "zx_server_start",
+    "zx_server_submit", "zx_server_wait", "zx_server_stats", "zx_server_stop",
 )
 
 
@@ -46,6 +47,18 @@ class ZxLaunch(ctypes.Structure):
     _fields_ = [("team", c_int), ("warps", c_int), ("blocks", c_int), ("smem_counters", c_int),
                 ("stage_bytes", c_int), ("stages", c_int), ("bulk", c_int), ("min_blocks", c_int),
                 ("planes", c_int)]
+
+
+class ZxServerOptions(ctypes.Structure):
+    _fields_ = [("slots", c_int), ("slot_bases", c_uint64), ("slot_records", c_uint64),
+                ("slot_requests", c_uint32)]
+
+
+class ZxServerStats(ctypes.Structure):
+    _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("failed", c_uint64),
+                ("batches", c_uint64), ("seeds", c_uint64), ("bases", c_uint64),
+                ("p50_s", c_double), ("p99_s", c_double), ("mean_s", c_double),
+                ("max_s", c_double), ("elapsed_s", c_double), ("device_bytes", c_uint64)]
 
 
 class ZxError(RuntimeError):
@@ -91,6 +104,13 @@ def load() -> ctypes.CDLL:
         "zx_last_kernel_ms": (c_int, [c_void_p, POINTER(ctypes.c_float)]),
         "zx_write_aggregate": (c_int, [c_void_p, c_char_p, P64, c_uint64, c_uint64, c_double,
                                        c_double, c_char_p, c_int]),
+        "zx_query_segments": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, P64,
+                                      c_uint32, c_int, c_void_p, c_void_p, c_void_p]),
+        "zx_server_start": (c_int, [c_void_p, POINTER(ZxServerOptions), POINTER(c_void_p)]),
+        "zx_server_submit": (c_int, [c_void_p, c_void_p, P64, c_uint64, c_int, P64]),
+        "zx_server_wait": (c_int, [c_void_p, c_uint64, c_int, P64, P64, POINTER(c_double)]),
+        "zx_server_stats": (c_int, [c_void_p, c_int, POINTER(ZxServerStats)]),
+        "zx_server_stop": (None, [c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

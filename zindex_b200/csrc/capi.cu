@@ -8,11 +8,17 @@
 #include "../../include/zindex.h"
 #include "engine.h"
 #include "host/error.h"
+#include "server.h"
 #include "host/fastx.h"
 
 struct zx_index {
   std::unique_ptr<zx::Engine> engine;
   std::mutex mu;  // guards the shared workspace
+  std::unique_ptr<zx::Workspace> seg_ws;  // zx_query_segments
+};
+
+struct zx_server {
+  std::unique_ptr<zx::Server> server;
 };
 
 namespace {
@@ -226,6 +232,80 @@ int zx_last_kernel_ms(zx_index* index, float* ms) {
     *ms = index->engine->last_fused_ms();
   });
 }
+
+int zx_query_segments(zx_index* index, const uint8_t* bases, uint64_t nbases,
+                      const uint64_t* offsets, uint64_t records, const uint64_t* seg_records,
+                      uint32_t segments, int recover, uint64_t* counts, uint64_t* totals,
+                      void* stream) {
+  return guarded([&] {
+    zx::check(index && offsets && seg_records && counts && totals && (bases || nbases == 0),
+              zx::kEInval, "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    auto& e = *index->engine;
+    if (!index->seg_ws) index->seg_ws = e.make_workspace();
+    // Grid shares from the record counts (the lengths stay on the device).
+    std::vector<uint64_t> est(segments);
+    for (uint32_t s = 0; s < segments; ++s) est[s] = seg_records[s + 1] - seg_records[s] + 1;
+    e.query_segments(*index->seg_ws, bases, nbases, offsets, records, seg_records, est.data(),
+                     segments, recover != 0, counts, reinterpret_cast<unsigned long long*>(totals),
+                     static_cast<cudaStream_t>(stream));
+  });
+}
+
+int zx_server_start(zx_index* index, const zx_server_options* options, zx_server** out) {
+  return guarded([&] {
+    zx::check(index && out, zx::kEInval, "null argument");
+    *out = nullptr;
+    zx::ServerOptions o;
+    if (options) {
+      if (options->slots) o.slots = options->slots;
+      if (options->slot_bases) o.slot_bases = options->slot_bases;
+      if (options->slot_records) o.slot_records = options->slot_records;
+      if (options->slot_requests) o.slot_requests = options->slot_requests;
+    }
+    auto sv = std::make_unique<zx_server>();
+    sv->server = std::make_unique<zx::Server>(*index->engine, index->mu, o);
+    *out = sv.release();
+  });
+}
+
+int zx_server_submit(zx_server* server, const uint8_t* bases, const uint64_t* offsets,
+                     uint64_t records, int recover, uint64_t* ticket) {
+  return guarded([&] {
+    zx::check(server && offsets && ticket, zx::kEInval, "null argument");
+    *ticket = server->server->submit(bases, offsets[records], offsets, records, recover != 0);
+  });
+}
+
+int zx_server_wait(zx_server* server, uint64_t ticket, int timeout_ms, uint64_t* counts,
+                   uint64_t* total, double* latency_s) {
+  return guarded([&] {
+    zx::check(server, zx::kEInval, "null argument");
+    if (!server->server->wait(ticket, timeout_ms, counts, total, latency_s))
+      zx::raise(zx::kETimeout, "request not finished yet");
+  });
+}
+
+int zx_server_stats(zx_server* server, int reset, zx_server_report* out) {
+  return guarded([&] {
+    zx::check(server && out, zx::kEInval, "null argument");
+    const zx::ServerStats st = server->server->stats(reset != 0);
+    out->submitted = st.submitted;
+    out->completed = st.completed;
+    out->failed = st.failed;
+    out->batches = st.batches;
+    out->seeds = st.seeds;
+    out->bases = st.bases;
+    out->p50_s = st.p50_s;
+    out->p99_s = st.p99_s;
+    out->mean_s = st.mean_s;
+    out->max_s = st.max_s;
+    out->elapsed_s = st.elapsed_s;
+    out->device_bytes = st.device_bytes;
+  });
+}
+
+void zx_server_stop(zx_server* server) { delete server; }
 
 int zx_write_aggregate(const zx_index* index, const char* query_label, const uint64_t* counts,
                        uint64_t total, uint64_t probes, double min_ratio, double seconds,

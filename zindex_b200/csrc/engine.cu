@@ -372,12 +372,13 @@ Workspace::~Workspace() {
   void* dev[] = {bases,      offsets,  packed,    invalid,  tile_counts, tile_first,
                  tiles,      scan_tmp, partial,   counts,   total,       keys_out,
                  keys_count, error,    fstate,    hp_starts, hp_keep,    hp_pos,
-                 hp_bases,   hp_offsets, hp_scan_tmp};
+                 hp_bases,   hp_offsets, hp_scan_tmp, seg_blocks, seg_tiles, seg_records};
   for (void* p : dev)
     if (p) cudaFree(p);
-  void* host[] = {h_bases, h_offsets, h_counts, h_total};
+  void* host[] = {h_bases, h_offsets, h_counts, h_total, h_seg_blocks, h_seg_records};
   for (void* p : host)
     if (p) cudaFreeHost(p);
+  if (seg_staged) cudaEventDestroy(seg_staged);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -910,6 +911,110 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     reduce_counters_kernel<<<std::max(1u, (colors + 255) / 256), 256, 0, s>>>(ws.partial, blocks,
                                                                                colors, counts);
     cuda_check(cudaGetLastError(), "reduce_counters_kernel");
+  }
+}
+
+uint64_t Engine::tiles_for_length(uint64_t len) const {
+  const uint64_t span = (uint64_t)this->span();
+  if (len < span) return 0;
+  const uint64_t w = len - span + 1;
+  if (m_.index_mode != kFindere) return (w + kTileWindows - 1) / kTileWindows;
+  return (w / kFindereTask) * (kFindereTask / kTileWindows) +
+         (w % kFindereTask + kTileWindows - 1) / kTileWindows;
+}
+
+void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                            const uint64_t* offsets, uint64_t records, const uint64_t* seg_records,
+                            const uint64_t* est_tiles, uint32_t segments, bool recover,
+                            uint64_t* counts, unsigned long long* totals, cudaStream_t s) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  check(segments > 0, kEInval, "a segmented query needs at least one segment");
+  check(seg_records[0] == 0 && seg_records[segments] == records, kEInval,
+        "segments must span the records");
+  ensure_capacity(ws, nbases, records);
+  QueryLaunch l = launch_;
+  const int cap = max_blocks(l);
+  const uint32_t wpb = (uint32_t)l.warps;
+  // Grid shares: proportional to the estimated tiles, at least one block,
+  // at most one warp per tile.
+  uint64_t est_total = 0;
+  for (uint32_t i = 0; i < segments; ++i) est_total += est_tiles[i];
+  if (segments + 1 > ws.cap_segments || !ws.seg_blocks) {
+    const uint64_t c = std::max<uint64_t>(segments + 1, 256);
+    for (void* p : {(void*)ws.seg_blocks, (void*)ws.seg_tiles, (void*)ws.seg_records})
+      if (p) cudaFree(p);
+    for (void* p : {(void*)ws.h_seg_blocks, (void*)ws.h_seg_records})
+      if (p) cudaFreeHost(p);
+    dev_alloc(&ws.seg_blocks, c, "segment blocks");
+    dev_alloc(&ws.seg_tiles, c, "segment tiles");
+    dev_alloc(&ws.seg_records, c, "segment records");
+    host_alloc(&ws.h_seg_blocks, c);
+    host_alloc(&ws.h_seg_records, c);
+    ws.cap_segments = c;
+  }
+  // The pinned staging is reused: wait until the previous call's copies ran.
+  if (!ws.seg_staged)
+    cuda_check(cudaEventCreateWithFlags(&ws.seg_staged, cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaEventSynchronize(ws.seg_staged), "segment staging");
+  uint32_t blocks = 0;
+  for (uint32_t i = 0; i < segments; ++i) {
+    ws.h_seg_blocks[i] = blocks;
+    uint64_t share = est_total ? est_tiles[i] * (uint64_t)cap / est_total : 1;
+    share = std::min<uint64_t>(share, (est_tiles[i] + wpb - 1) / wpb);
+    blocks += (uint32_t)std::max<uint64_t>(share, 1);
+    ws.h_seg_records[i] = seg_records[i];
+  }
+  ws.h_seg_blocks[segments] = blocks;
+  ws.h_seg_records[segments] = seg_records[segments];
+  const uint64_t colors = m_.colors.size();
+  if ((uint64_t)blocks * colors > ws.cap_partial) {
+    if (ws.partial) cudaFree(ws.partial);
+    dev_alloc(&ws.partial, (uint64_t)blocks * colors, "block counters");
+    ws.cap_partial = (uint64_t)blocks * colors;
+    ws.release_graphs();
+  }
+  if (m_.index_mode == kFindere && (uint64_t)blocks * wpb * 2 * colors > ws.cap_fstate) {
+    if (ws.fstate) cudaFree(ws.fstate);
+    dev_alloc(&ws.fstate, (uint64_t)blocks * wpb * 2 * colors, "findere colour state");
+    ws.cap_fstate = (uint64_t)blocks * wpb * 2 * colors;
+    ws.release_graphs();
+  }
+  cuda_check(cudaMemcpyAsync(ws.seg_blocks, ws.h_seg_blocks, (segments + 1) * 4ull,
+                             cudaMemcpyHostToDevice, s),
+             "H2D");
+  cuda_check(cudaMemcpyAsync(ws.seg_records, ws.h_seg_records, (segments + 1) * 8ull,
+                             cudaMemcpyHostToDevice, s),
+             "H2D");
+  cuda_check(cudaEventRecord(ws.seg_staged, s), "cudaEventRecord");
+  if (m_.homopolymer_compression) compress_homopolymers(ws, bases, nbases, offsets, records, s);
+  const uint64_t words = nbases / 32 + 2;
+  {
+    int grid = (int)std::min<uint64_t>((words + 255) / 256, (uint64_t)sms_ * 16);
+    pack_kernel<<<std::max(grid, 1), 256, 0, s>>>(bases, nbases, ws.packed, ws.invalid, words);
+    cuda_check(cudaGetLastError(), "pack_kernel");
+  }
+  plan_tiles(ws, offsets, records, s);
+  segment_tiles_kernel<<<(segments + 256) / 256, 256, 0, s>>>(ws.tile_first, ws.seg_records,
+                                                              segments, ws.seg_tiles);
+  cuda_check(cudaGetLastError(), "segment_tiles_kernel");
+  l.blocks = (int)blocks;
+  const size_t smem = fused_smem_bytes(l);
+  BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records,
+               ws.fstate, segments, ws.seg_blocks, ws.seg_tiles};
+  if (m_.index_mode == kFindere)
+    cuda_check(cudaMemsetAsync(ws.fstate, 0, (uint64_t)blocks * wpb * 2 * colors * 4, s), "memset");
+  FusedFn fn = fused_for(sp_.mode, l);
+  cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, ws.partial,
+                                        counts, totals, ws.error);
+  cuda_check(cudaGetLastError(), "fused_query_kernel");
+  if (l.smem_counters) {
+    const uint64_t n = (uint64_t)segments * colors;
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, sms_ * 8ull));
+    reduce_segments_kernel<<<grid, 256, 0, s>>>(ws.partial, ws.seg_blocks, segments,
+                                                (uint32_t)colors, counts);
+    cuda_check(cudaGetLastError(), "reduce_segments_kernel");
   }
 }
 

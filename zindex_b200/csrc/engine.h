@@ -52,6 +52,14 @@ struct Workspace {
   void* hp_scan_tmp = nullptr;
   size_t hp_scan_bytes = 0;
   uint64_t cap_fstate = 0, cap_hp_bases = 0, cap_hp_records = 0;
+  // Segmented launches (several requests per launch).
+  uint32_t* seg_blocks = nullptr;   // segments + 1
+  uint32_t* seg_tiles = nullptr;    // segments + 1
+  uint64_t* seg_records = nullptr;  // segments + 1
+  uint32_t* h_seg_blocks = nullptr;   // pinned staging
+  uint64_t* h_seg_records = nullptr;  // pinned staging
+  uint64_t cap_segments = 0;
+  cudaEvent_t seg_staged = nullptr;   // the last segmented call's staging copies are done
   // Pinned host staging.
   uint8_t* h_bases = nullptr;
   uint64_t* h_offsets = nullptr;
@@ -90,6 +98,10 @@ class Engine {
   uint64_t gather_bytes_per_seed() const;
 
   std::unique_ptr<Workspace> make_workspace();
+  // Sizes a workspace's device buffers for batches up to these sizes.
+  void reserve(Workspace& ws, uint64_t nbases, uint64_t records) {
+    ensure_capacity(ws, nbases, records);
+  }
   Workspace& default_workspace() { return *ws_; }
 
   // Asynchronous query of a batch resident on the device. counts (colors
@@ -118,6 +130,18 @@ class Engine {
   // Device error word of a workspace (read and cleared); nonzero means a
   // bounded wait expired and the query's counts are incomplete.
   uint32_t take_error(Workspace& ws);
+  // Asynchronous query of several requests coalesced into one launch: the
+  // batch's records are the requests' records back to back, request s owning
+  // records seg_records[s] .. seg_records[s+1]-1 (host array, segments + 1
+  // entries). counts (segments x colours) and totals (segments) are
+  // accumulated, not cleared. est_tiles[s] (host) sizes each request's share
+  // of the grid; any positive estimate gives exact results.
+  void query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
+                      uint64_t records, const uint64_t* seg_records, const uint64_t* est_tiles,
+                      uint32_t segments, bool recover, uint64_t* counts,
+                      unsigned long long* totals, cudaStream_t stream);
+  // Upper bound of the tiles of one record of `len` bases.
+  uint64_t tiles_for_length(uint64_t len) const;
   // Seeds of host records in record/window order (extraction only).
   void extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
                     uint64_t records, std::vector<uint64_t>& keys);

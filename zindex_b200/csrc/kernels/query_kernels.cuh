@@ -64,6 +64,12 @@ struct BatchView {
   const Tile* tiles;
   const uint32_t* ntiles;  // device scalar
   uint32_t* fstate;        // findere: per warp of the grid, colours round masks then run lengths
+  // Segmented launch (several requests in one launch, each with its own
+  // counters): 0, or the number of segments; segment s owns blocks
+  // seg_blocks[s] .. seg_blocks[s+1]-1 and tiles seg_tiles[s] .. seg_tiles[s+1]-1.
+  uint32_t segments;
+  const uint32_t* seg_blocks;
+  const uint32_t* seg_tiles;
 };
 
 // Shared memory of the fused kernel, in order: DevIndex copy, counters,
@@ -193,15 +199,28 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
     for (uint32_t c = threadIdx.x; c < colors; c += blockDim.x) scount[c] = 0;
   __syncthreads();
   const DevIndex& ix = *six;
-  const Counters cnt{scount, counts};
   LanePlanes planes;
   if (ROWS) planes_init(planes, ix, lane % lc.team, lc.team);
   if (MODE == 3) planes.cls = -1;  // findere: every hit goes to the position masks
-  const uint32_t ntiles = *bv.ntiles;
-  const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
-  const uint32_t gwarp = blockIdx.x * (blockDim.x >> 5) + warp;
+  const uint32_t wpb = blockDim.x >> 5;
+  const uint32_t gwarp = blockIdx.x * wpb + warp;
+  // Tile range of this warp: the whole list, or its block's segment.
+  uint32_t t_first = gwarp, t_end = *bv.ntiles, t_stride = gridDim.x * wpb, seg = 0;
+  if (bv.segments) {
+    uint32_t lo = 0, hi = bv.segments;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (bv.seg_blocks[mid] <= blockIdx.x) lo = mid;
+      else hi = mid;
+    }
+    seg = lo;
+    t_first = bv.seg_tiles[seg] + (blockIdx.x - bv.seg_blocks[seg]) * wpb + warp;
+    t_end = bv.seg_tiles[seg + 1];
+    t_stride = (bv.seg_blocks[seg + 1] - bv.seg_blocks[seg]) * wpb;
+  }
+  const Counters cnt{scount, counts + (uint64_t)seg * colors};
   unsigned long long seeds = 0;
-  for (uint32_t t = gwarp; t < ntiles; t += warps_total) {
+  for (uint32_t t = t_first; t < t_end; t += t_stride) {
     const Tile tile = bv.tiles[t];
     if constexpr (MODE == 3) {
       // Findere: s-mers of positions 0 .. nw + z - 1, windows are the features.
@@ -244,7 +263,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   }
   if (ROWS && planes.cls >= 0)
     planes_flush(planes, ix, lane % lc.team, lc.team, CountSink{cnt});
-  if (lane == 0 && seeds) atomicAdd(total, seeds);
+  if (lane == 0 && seeds) atomicAdd(total + seg, seeds);
   __syncthreads();
   if (scount)
     for (uint32_t c = threadIdx.x; c < colors; c += blockDim.x)
@@ -259,6 +278,31 @@ __global__ void reduce_counters_kernel(const uint32_t* __restrict__ partial, uin
     for (uint32_t b = 0; b < blocks; ++b) s += partial[(uint64_t)b * colors + c];
     counts[c] += s;
   }
+}
+
+// Segmented launches: counts[s][c] += sum over the blocks of segment s of
+// partial[block][c].
+__global__ void reduce_segments_kernel(const uint32_t* __restrict__ partial,
+                                       const uint32_t* __restrict__ seg_blocks, uint32_t segments,
+                                       uint32_t colors, uint64_t* __restrict__ counts) {
+  const uint64_t n = (uint64_t)segments * colors;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t sgm = (uint32_t)(i / colors), c = (uint32_t)(i % colors);
+    uint64_t sum = 0;
+    for (uint32_t b = seg_blocks[sgm]; b < seg_blocks[sgm + 1]; ++b)
+      sum += partial[(uint64_t)b * colors + c];
+    counts[i] += sum;
+  }
+}
+
+// seg_tiles[s] = tile_first[seg_records[s]] for s <= segments (record-first
+// tile offsets of a planned batch; tile_first[records] is the tile total).
+__global__ void segment_tiles_kernel(const uint32_t* __restrict__ tile_first,
+                                     const uint64_t* __restrict__ seg_records, uint32_t segments,
+                                     uint32_t* __restrict__ seg_tiles) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s <= segments; s += gridDim.x * blockDim.x)
+    seg_tiles[s] = tile_first[seg_records[s]];
 }
 
 // Extraction only (testing and inspection): tile t's keys go to
