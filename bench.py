@@ -91,9 +91,125 @@ def prepare(cache: Path, rank: int):
                             "--seed", "1", "--read-seed", str(7 + rank), "--reads", "1000000",
                             "--length", "150", "--sourced", "0.7", "--subst", "0.005",
                             "--format", "raw", "--out", str(reads)], check=True)
+        long = cache / f"long-c2-r{rank}"
+        if not Path(str(long) + ".offsets").exists():
+            # Long records for the served request mix: lognormal lengths,
+            # median 30 kbp, clipped to 100 bp-100 kbp, 60% sourced.
+            subprocess.run([str(LIB / "zx_synth"), "reads", "--kind", "long", "--genome-kind", "pool",
+                            "--colors", "256", "--min-len", "1000000", "--max-len", "10000000",
+                            "--seed", "1", "--read-seed", str(101 + rank), "--reads", "400",
+                            "--length", "30000", "--sourced", "0.6", "--subst", "0.005",
+                            "--format", "raw", "--out", str(long)], check=True)
     bases = np.fromfile(str(reads) + ".bases", dtype=np.uint8)
     offsets = np.fromfile(str(reads) + ".offsets", dtype=np.uint64)
     return index, bases, offsets
+
+
+def long_pool(cache: Path, rank: int):
+    long = cache / f"long-c2-r{rank}"
+    return (np.fromfile(str(long) + ".bases", dtype=np.uint8),
+            np.fromfile(str(long) + ".offsets", dtype=np.uint64))
+
+
+def make_requests(bases, offsets, lbases, loffsets, n, seed):
+    """Served request mix: half are 1-10,000 reads of 150 bp, half 1-10 long
+    records (lognormal, median 30 kbp), drawn from the read pools."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        if rng.random() < 0.5:
+            b, o, k = bases, offsets, int(rng.integers(1, 10001))
+        else:
+            b, o, k = lbases, loffsets, int(rng.integers(1, 11))
+        r = len(o) - 1
+        st = int(rng.integers(0, max(1, r - k)))
+        oo = o[st: st + k + 1] - o[st]
+        out.append((b[int(o[st]): int(o[st + k])], np.ascontiguousarray(oo)))
+    return out
+
+
+def planned_form(ix, bases, offsets, seeds, step_ms):
+    """The learned planner (trained on the GPU on the committed autotuner rows)
+    picks the launch and the cut for this batch; exhaustive autotuning over the
+    same candidates is timed alongside for its regret, and the default launch
+    for its gain. step_ms(launch) times device steps under a launch."""
+    from zindex_b200 import planner as pl
+    from zindex_b200 import tuning as tn
+
+    rows, _ = pl.load_rows()
+    planner = pl.Planner(seed=1)
+    t0 = time.perf_counter()
+    loss = planner.fit(rows)
+    train_s = time.perf_counter() - t0
+    default = dict(ix.default_launch(), blocks=0)
+    lengths = np.diff(offsets.astype(np.int64))
+    feats = tn.Autotuner.features(ix, lengths, seeds)
+    cands = [dict(default, **l, stage_bytes=0) for l in tn.REGISTER_LAUNCHES]
+    t0 = time.perf_counter()
+    pick = planner.choose(feats, cands, default=default, margin=pl.LAUNCH_MARGIN)
+    pick = planner.choose(feats, [dict(pick, cut=c) for c in tn.CUTS], e2e=True,
+                          default=dict(pick, cut=default["cut"]), margin=pl.CUT_MARGIN)
+    plan_ms = (time.perf_counter() - t0) * 1e3
+    timed = {}
+    for launch in cands + [default, pick]:
+        key = pl.launch_key(dict(launch, cut=1))
+        if key not in timed:
+            timed[key] = step_ms(launch)
+    best_key = min(timed, key=timed.get)
+    t_pick = timed[pl.launch_key(dict(pick, cut=1))]
+    return pick, {
+        "chosen": {k: pick[k] for k in ("team", "warps", "min_blocks", "planes", "cut")},
+        "ms_per_step": t_pick, "default_ms_per_step": timed[pl.launch_key(dict(default, cut=1))],
+        "exhaustive_best_ms_per_step": timed[best_key],
+        "exhaustive_best": dict((k, v) for k, v in best_key if k in ("team", "warps", "min_blocks",
+                                                                      "planes")),
+        "regret": t_pick / timed[best_key] - 1.0,
+        "gain_over_default": timed[pl.launch_key(dict(default, cut=1))] / t_pick,
+        "candidates": len(cands), "train_rows": len(rows), "train_loss": loss,
+        "train_s_on_gpu": train_s, "plan_ms": plan_ms,
+    }
+
+
+def served_form(zx, ix, requests_closed, requests_open, rate):
+    """Closed loop (all requests queued at once: served throughput) and an open
+    Poisson arrival stream at `rate` requests/s (latency percentiles)."""
+    out = {}
+    with zx.Server(ix, slots=3) as server:
+        for b, o in requests_closed[:20]:  # warm-up
+            server.wait(server.submit(b, o))
+        server.stats(reset=True)
+        t0 = time.perf_counter()
+        tickets = [server.submit(b, o) for b, o in requests_closed]
+        seeds = sum(server.wait(t)[1] for t in tickets)
+        dt = time.perf_counter() - t0
+        st = server.stats(reset=True)
+        out["closed_loop"] = {"requests": len(tickets), "seconds": dt, "seeds_per_s": seeds / dt,
+                              "bases_per_s": st["bases"] / dt, "batches": st["batches"],
+                              "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3}
+        rng = np.random.default_rng(5)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(requests_open)))
+        tickets = [None] * len(requests_open)
+        start = time.perf_counter()
+
+        def submitter():
+            for i, (b, o) in enumerate(requests_open):
+                delay = start + arrivals[i] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[i] = server.submit(b, o)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        seeds = sum(server.wait(t)[1] for t in tickets)
+        dt = time.perf_counter() - start
+        st = server.stats(reset=True)
+        out["poisson"] = {"rate_req_per_s": rate, "requests": len(tickets), "seconds": dt,
+                          "seeds_per_s": seeds / dt, "batches": st["batches"],
+                          "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
+                          "max_ms": st["max_s"] * 1e3,
+                          "server_device_bytes": st["device_bytes"]}
+    return out
 
 
 class ClockSampler:
@@ -337,6 +453,37 @@ def ours(args):
         e2e_s = float(t.item())
     assert t_e2e == seeds and np.array_equal(c_e2e, counts_dev), "e2e and device paths disagree"
 
+    # Planned form: launch and cut chosen by the learned planner.
+    def step_ms(launch, reps=5):
+        ix.set_launch(**launch)
+        step()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            step()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / reps
+
+    default_launch = ix.launch()
+    pick, planned = planned_form(ix, bases, offsets, seeds, step_ms)
+    ix.set_launch(**pick)
+    times = []
+    for _ in range(max(3, args.steps // 2)):
+        t0 = time.perf_counter()
+        c_pl, t_pl = ix.query_records(hb, ho)
+        times.append(time.perf_counter() - t0)
+    assert t_pl == seeds and np.array_equal(c_pl, counts_dev), "planned launch changed the counts"
+    planned["seeds_per_s"] = seeds / (planned["ms_per_step"] / 1e3)
+    planned["e2e_seeds_per_s"] = seeds / statistics.median(times)
+    ix.set_launch(**default_launch)
+
+    # Served form: request mix through the continuous-batching server.
+    lb, lo = long_pool(Path(args.cache), rank)
+    served = served_form(zx, ix, make_requests(bases, offsets, lb, lo, 400, 11 + rank),
+                         make_requests(bases, offsets, lb, lo, 1000, 23 + rank), 200.0)
+
     # Plain form: one record per launch, on a prefix.
     n_plain = min(4000, records)
     pb = bases[: int(offsets[n_plain])]
@@ -372,7 +519,10 @@ def ours(args):
                          "kernel": "fused_query_kernel", "kernel_ms": kernel_ms,
                          "algorithmic_bytes_per_launch": int(alg_bytes),
                          "gather_bytes_per_seed": int(gather)},
-            "forms": {"plain_seeds_per_s": plain_rate, "batched_seeds_per_s": value / world},
+            "forms": {"plain_seeds_per_s": plain_rate, "batched_seeds_per_s": value / world,
+                      "served_seeds_per_s": served["closed_loop"]["seeds_per_s"],
+                      "planned_seeds_per_s": world * planned["seeds_per_s"],
+                      "served": served, "planned": planned},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cpu_baseline": cb,

@@ -64,6 +64,9 @@ typedef struct zx_launch {
   int min_blocks;     /* kernel variant register budget: 2 or 3 resident 256-thread blocks */
   int planes;         /* register gather: 1 = per-seed row indices and per-lane bit-plane colour
                          counters, 0 = per-seed descriptors and one counter update per hit */
+  int cut;            /* host-buffer queries: the batch is cut at record boundaries into this many
+                         chunks (1..64) whose host-to-device copies overlap the previous chunk's
+                         kernels; chunks below 1 MiB of bases are merged */
 } zx_launch;
 
 /* Thread-local message of the last failed call on this thread. */
@@ -216,6 +219,26 @@ int zx_server_wait(zx_server* server, uint64_t ticket, int timeout_ms, uint64_t*
 int zx_server_stats(zx_server* server, int reset, zx_server_report* out);
 /* Finish every queued request, then stop (pending results are dropped). */
 void zx_server_stop(zx_server* server);
+
+/* Learned launch planner network (no reference counterpart: the reference
+ * has no launch configuration to choose). A two-layer FP32 perceptron,
+ * y = w2 . relu(W1 x + b1) + b2, trained on the GPU by the library's own
+ * forward, backward and Adam kernels; parameters in the order W1 (hidden x
+ * inputs, row-major), b1, w2, b2. Host arrays: x is n x inputs row-major,
+ * targets and outputs n. Inputs 1..32, hidden units 1..64. */
+typedef struct zx_mlp zx_mlp;
+int zx_mlp_create(int device, int inputs, int hidden, uint64_t seed, zx_mlp** out);
+void zx_mlp_destroy(zx_mlp* mlp);
+uint64_t zx_mlp_param_count(const zx_mlp* mlp);
+int zx_mlp_get_params(zx_mlp* mlp, float* params);
+int zx_mlp_set_params(zx_mlp* mlp, const float* params, uint64_t count);
+/* Loss (1/2n) sum (y - t)^2 and its gradient (param_count entries, may be NULL). */
+int zx_mlp_loss_grad(zx_mlp* mlp, const float* x, const float* targets, uint64_t n, float* loss,
+                     float* grad);
+/* Full-batch Adam steps; *loss receives the loss after the last step. */
+int zx_mlp_train(zx_mlp* mlp, const float* x, const float* targets, uint64_t n, int epochs,
+                 float lr, float* loss);
+int zx_mlp_predict(zx_mlp* mlp, const float* x, uint64_t n, float* out);
 
 /* Write the aggregate report exactly as print_aggregate does
  * (storage.rs:3817-3844): stdout-style TSV

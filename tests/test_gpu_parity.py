@@ -192,6 +192,26 @@ def test_legacy_interleaved_banks(gpu, oracle, tmp_path_factory, opts):
     gpu_vs_oracle(oracle, ix, reads_for(genomes, n=300, length=200, n_runs=0.1))
 
 
+@pytest.mark.parametrize("mode", ["kmers", "findere"])
+def test_pipelined_host_chunks_equal_one_pass(gpu, oracle, tmp_path_factory, mode):
+    """A host batch cut into record-aligned chunks (copies overlapping the
+    previous chunk's kernels) gives the counts of one pass and the oracle's."""
+    import zindex_b200 as zx
+
+    opts = dict(mode=mode, k=31, H=4, b=8) if mode == "kmers" else dict(mode=mode, k=31, z=6,
+                                                                       H=4, b=8)
+    ix, genomes = index_for(tmp_path_factory, colors=6, length=30000, **opts)
+    reads = reads_for(genomes, n=24000, length=150, n_runs=0.05)
+    bases, offsets = zx.pack_records(reads)
+    want, want_total = oracle.query_records(ix, bases, offsets)
+    with zx.Index(ix) as index:
+        for cut in (1, 3, 64):
+            index.set_launch(cut=cut)
+            got, total = index.query_records(bases, offsets)
+            assert total == want_total, cut
+            np.testing.assert_array_equal(got, want)
+
+
 def test_multi_member_groups(gpu, oracle, tmp_path_factory):
     ix, genomes = index_for(tmp_path_factory, colors=8, mode="kmers", k=31, H=4, b=4,
                             groups="0,1,2;3,5;6,7")

@@ -1,0 +1,103 @@
+"""The learned launch planner: its network's CUDA kernels against a CPU
+restatement (gradients, training, prediction), and what the trained planner
+gains over the default launch on measured timings, with its regret against
+exhaustive autotuning."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def cpu_forward_backward(p, x, t, D, H):
+    """float64 restatement: L = (1/2n) sum (y - t)^2, y = w2 . relu(W1 x + b1) + b2."""
+    p = p.astype(np.float64)
+    W1 = p[: H * D].reshape(H, D)
+    b1 = p[H * D: H * D + H]
+    w2 = p[H * D + H: H * D + 2 * H]
+    b2 = p[-1]
+    x = x.astype(np.float64)
+    z = x @ W1.T + b1
+    h = np.maximum(z, 0.0)
+    y = h @ w2 + b2
+    n = len(t)
+    r = y - t
+    loss = 0.5 * np.sum(r * r) / n
+    dy = r / n
+    dz = (dy[:, None] * w2[None, :]) * (z > 0)
+    grad = np.concatenate([(dz.T @ x).ravel(), dz.sum(0), h.T @ dy, [dy.sum()]])
+    return loss, grad, y
+
+
+def test_gradients_match_the_cpu_restatement(gpu):
+    from zindex_b200.planner import Mlp
+
+    rng = np.random.default_rng(0)
+    D, H = 20, 32
+    net = Mlp(D, H, seed=3)
+    p = net.params()
+    assert len(p) == H * D + 2 * H + 1
+    for n in (1, 63, 64, 65, 1000):
+        x = rng.normal(size=(n, D)).astype(np.float32)
+        t = rng.normal(size=n).astype(np.float32)
+        loss, g = net.loss_grad(x, t)
+        want_loss, want_g, _ = cpu_forward_backward(p, x, t, D, H)
+        # FP32 kernels against float64: relative 1e-4 of the gradient scale.
+        np.testing.assert_allclose(loss, want_loss, rtol=1e-5)
+        np.testing.assert_allclose(g, want_g, rtol=1e-4, atol=1e-4 * np.abs(want_g).max())
+    # The CPU restatement itself, by central differences in float64.
+    x = rng.normal(size=(50, D)).astype(np.float32)
+    t = rng.normal(size=50).astype(np.float32)
+    _, g64, _ = cpu_forward_backward(p, x, t, D, H)
+    for q in rng.choice(len(p), 25, replace=False):
+        e = np.zeros(len(p))
+        e[q] = 1e-6
+        lp = cpu_forward_backward(p + e, x, t, D, H)[0]
+        lm = cpu_forward_backward(p - e, x, t, D, H)[0]
+        assert abs((lp - lm) / 2e-6 - g64[q]) <= 1e-6 + 1e-4 * abs(g64[q])
+
+
+def test_training_fits_and_prediction_matches_cpu(gpu):
+    from zindex_b200.planner import Mlp
+
+    rng = np.random.default_rng(1)
+    D, H = 4, 32
+    x = rng.uniform(-1, 1, size=(2000, D)).astype(np.float32)
+    t = (np.sin(2 * x[:, 0]) + x[:, 1] ** 2 - 0.5 * x[:, 2]).astype(np.float32)
+    net = Mlp(D, H, seed=5)
+    start, _ = net.loss_grad(x, t)
+    final = net.train(x, t, epochs=3000, lr=3e-3)
+    assert final < 0.05 * start
+    _, _, y = cpu_forward_backward(net.params(), x, t, D, H)
+    np.testing.assert_allclose(net.predict(x), y, rtol=1e-4, atol=1e-4)
+
+
+def test_planner_gain_over_default_and_regret(gpu):
+    """Leave-one-setting-out on the committed autotuner measurements: for each
+    setting the planner is trained on the others' timings only, chooses among
+    that setting's measured launches (and cuts), and is scored against the
+    exhaustive best (regret) and the default launch (gain)."""
+    from zindex_b200 import planner as pl
+
+    rows, defaults = pl.load_rows()
+    settings = sorted({r.setting for r in rows})
+    assert len(settings) >= 8
+    dev, e2e = [], []
+    for held in settings:
+        p = pl.Planner(seed=7)
+        p.fit([r for r in rows if r.setting != held])
+        test = [r for r in rows if r.setting == held]
+        dev.append(pl.evaluate(p, test, defaults[held]))
+        e2e.append(pl.evaluate(p, test, defaults[held], e2e=True))
+    gm = lambda v: float(np.exp(np.mean(np.log(v))))
+    gain = gm([r["gain_over_default"] for r in dev])
+    regret = gm([1 + r["regret"] for r in dev]) - 1
+    e2e_gain = gm([r["gain_over_default"] for r in e2e])
+    print(f"launch: gain over the default {gain:.3f}, regret {regret:.3f}; "
+          f"cut: gain over the default {e2e_gain:.3f}")
+    # Measured timings are the ground truth: the planner's launches must beat
+    # the default launch on average and stay near the exhaustive best; its cut
+    # decision (little headroom: the default cut was within 2% of the best)
+    # must not lose more than a few percent.
+    assert gain >= 1.0
+    assert regret <= 0.15
+    assert e2e_gain >= 0.95

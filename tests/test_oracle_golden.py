@@ -128,3 +128,13 @@ def test_findere_indexes_smers_of_long_runs(oracle):
     got = oracle.features(seq, mode="findere", k=31, z=10)
     want = oracle.features(dna(100, 4), k=21)
     assert np.array_equal(got, want)  # the 20-base run is shorter than k
+
+
+def test_planner_measurements_and_features():
+    """The committed planner training set loads and encodes (no GPU needed)."""
+    from zindex_b200 import planner as pl
+
+    rows, defaults = pl.load_rows()
+    assert rows and set(defaults) == {r.setting for r in rows}
+    x = pl.encode(rows[0].features, rows[0].launch, rows[0].e2e)
+    assert x.shape == (len(pl.FEATURES),) and np.isfinite(x).all()

@@ -167,7 +167,7 @@ class Index:
         return {"team": l.team, "warps": l.warps, "blocks": l.blocks,
                 "smem_counters": l.smem_counters, "stage_bytes": l.stage_bytes,
                 "stages": l.stages, "bulk": l.bulk, "min_blocks": l.min_blocks,
-                "planes": l.planes}
+                "planes": l.planes, "cut": l.cut}
 
     def launch(self) -> dict:
         l = ZxLaunch()
@@ -182,7 +182,8 @@ class Index:
     def set_launch(self, team: int = None, warps: int = None, blocks: int = 0,
                    smem_counters: Optional[int] = None, stage_bytes: Optional[int] = None,
                    stages: Optional[int] = None, bulk: Optional[int] = None,
-                   min_blocks: Optional[int] = None, planes: Optional[int] = None, **_ignored):
+                   min_blocks: Optional[int] = None, planes: Optional[int] = None,
+                   cut: Optional[int] = None, **_ignored):
         """Change the launch configuration (never changes results); unset
         fields keep their default values."""
         d = self.default_launch()
@@ -192,7 +193,8 @@ class Index:
                      int(d["stages"] if stages is None else stages),
                      int(d["bulk"] if bulk is None else bulk),
                      int(d["min_blocks"] if min_blocks is None else min_blocks),
-                     int(d["planes"] if planes is None else planes))
+                     int(d["planes"] if planes is None else planes),
+                     int(d["cut"] if cut is None else cut))
         _lib.check(_lib.load().zx_set_launch(self._h, byref(l)))
 
     def query_status(self) -> None:

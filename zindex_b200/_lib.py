@@ -29,7 +29,9 @@ EXPORTED = (
     "zx_query_device", "zx_extract_seeds", "zx_get_launch", "zx_set_launch",
     "zx_default_launch", "zx_write_aggregate", "zx_set_timing", "zx_last_kernel_ms",
     "zx_query_status", "zx_query_device_noalloc", "zx_query_segments", "zx_server_start",
-    "zx_server_submit", "zx_server_wait", "zx_server_stats", "zx_server_stop",
+    "zx_server_submit", "zx_server_wait", "zx_server_stats", "zx_server_stop", "zx_mlp_create",
+    "zx_mlp_destroy", "zx_mlp_param_count", "zx_mlp_get_params", "zx_mlp_set_params",
+    "zx_mlp_loss_grad", "zx_mlp_train", "zx_mlp_predict",
 )
 
 
@@ -46,7 +48,7 @@ class ZxInfo(ctypes.Structure):
 class ZxLaunch(ctypes.Structure):
     _fields_ = [("team", c_int), ("warps", c_int), ("blocks", c_int), ("smem_counters", c_int),
                 ("stage_bytes", c_int), ("stages", c_int), ("bulk", c_int), ("min_blocks", c_int),
-                ("planes", c_int)]
+                ("planes", c_int), ("cut", c_int)]
 
 
 class ZxServerOptions(ctypes.Structure):
@@ -81,6 +83,7 @@ def load() -> ctypes.CDLL:
         raise RuntimeError(f"{LIB_PATH} is missing: run `python -m zindex_b200.build`")
     lib = ctypes.CDLL(str(LIB_PATH))
     P64 = POINTER(c_uint64)
+    PF = POINTER(ctypes.c_float)
     sig = {
         "zx_last_error": (c_char_p, []),
         "zx_open": (c_int, [c_char_p, c_int, c_uint64, POINTER(c_void_p)]),
@@ -111,6 +114,14 @@ def load() -> ctypes.CDLL:
         "zx_server_wait": (c_int, [c_void_p, c_uint64, c_int, P64, P64, POINTER(c_double)]),
         "zx_server_stats": (c_int, [c_void_p, c_int, POINTER(ZxServerStats)]),
         "zx_server_stop": (None, [c_void_p]),
+        "zx_mlp_create": (c_int, [c_int, c_int, c_int, c_uint64, POINTER(c_void_p)]),
+        "zx_mlp_destroy": (None, [c_void_p]),
+        "zx_mlp_param_count": (c_uint64, [c_void_p]),
+        "zx_mlp_get_params": (c_int, [c_void_p, PF]),
+        "zx_mlp_set_params": (c_int, [c_void_p, PF, c_uint64]),
+        "zx_mlp_loss_grad": (c_int, [c_void_p, PF, PF, c_uint64, PF, PF]),
+        "zx_mlp_train": (c_int, [c_void_p, PF, PF, c_uint64, c_int, ctypes.c_float, PF]),
+        "zx_mlp_predict": (c_int, [c_void_p, PF, c_uint64, PF]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -8,6 +8,7 @@
 #include "../../include/zindex.h"
 #include "engine.h"
 #include "host/error.h"
+#include "planner.h"
 #include "server.h"
 #include "host/fastx.h"
 
@@ -19,6 +20,10 @@ struct zx_index {
 
 struct zx_server {
   std::unique_ptr<zx::Server> server;
+};
+
+struct zx_mlp {
+  std::unique_ptr<zx::Mlp> net;
 };
 
 namespace {
@@ -53,6 +58,7 @@ void fill_launch(const zx::QueryLaunch& l, zx_launch* out) {
   out->bulk = l.bulk;
   out->min_blocks = l.min_blocks;
   out->planes = l.planes;
+  out->cut = l.cut;
 }
 
 }  // namespace
@@ -203,7 +209,7 @@ int zx_set_launch(zx_index* index, const zx_launch* l) {
     std::lock_guard<std::mutex> lock(index->mu);
     index->engine->set_launch(
         zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters, l->stage_bytes, l->stages,
-                        l->bulk, l->min_blocks, l->planes});
+                        l->bulk, l->min_blocks, l->planes, l->cut});
   });
 }
 
@@ -306,6 +312,58 @@ int zx_server_stats(zx_server* server, int reset, zx_server_report* out) {
 }
 
 void zx_server_stop(zx_server* server) { delete server; }
+
+int zx_mlp_create(int device, int inputs, int hidden, uint64_t seed, zx_mlp** out) {
+  return guarded([&] {
+    zx::check(out != nullptr, zx::kEInval, "null argument");
+    *out = nullptr;
+    auto m = std::make_unique<zx_mlp>();
+    m->net = std::make_unique<zx::Mlp>(device, inputs, hidden, seed);
+    *out = m.release();
+  });
+}
+
+void zx_mlp_destroy(zx_mlp* mlp) { delete mlp; }
+
+uint64_t zx_mlp_param_count(const zx_mlp* mlp) { return mlp ? mlp->net->param_count() : 0; }
+
+int zx_mlp_get_params(zx_mlp* mlp, float* params) {
+  return guarded([&] {
+    zx::check(mlp && params, zx::kEInval, "null argument");
+    const std::vector<float> p = mlp->net->params();
+    std::copy(p.begin(), p.end(), params);
+  });
+}
+
+int zx_mlp_set_params(zx_mlp* mlp, const float* params, uint64_t count) {
+  return guarded([&] {
+    zx::check(mlp && params, zx::kEInval, "null argument");
+    mlp->net->set_params(params, count);
+  });
+}
+
+int zx_mlp_loss_grad(zx_mlp* mlp, const float* x, const float* targets, uint64_t n, float* loss,
+                     float* grad) {
+  return guarded([&] {
+    zx::check(mlp && x && targets && loss, zx::kEInval, "null argument");
+    *loss = mlp->net->loss_grad(x, targets, n, grad);
+  });
+}
+
+int zx_mlp_train(zx_mlp* mlp, const float* x, const float* targets, uint64_t n, int epochs,
+                 float lr, float* loss) {
+  return guarded([&] {
+    zx::check(mlp && x && targets && loss, zx::kEInval, "null argument");
+    *loss = mlp->net->train(x, targets, n, epochs, lr);
+  });
+}
+
+int zx_mlp_predict(zx_mlp* mlp, const float* x, uint64_t n, float* out) {
+  return guarded([&] {
+    zx::check(mlp && x && out, zx::kEInval, "null argument");
+    mlp->net->predict(x, n, out);
+  });
+}
 
 int zx_write_aggregate(const zx_index* index, const char* query_label, const uint64_t* counts,
                        uint64_t total, uint64_t probes, double min_ratio, double seconds,

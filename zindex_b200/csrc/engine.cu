@@ -379,6 +379,8 @@ Workspace::~Workspace() {
   for (void* p : host)
     if (p) cudaFreeHost(p);
   if (seg_staged) cudaEventDestroy(seg_staged);
+  for (cudaEvent_t e : chunk_events) cudaEventDestroy(e);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -639,6 +641,7 @@ QueryLaunch Engine::default_launch() const {
   l.bulk = 0;
   l.min_blocks = 2;
   l.planes = 1;
+  l.cut = 4;
   if (fused_smem_bytes(l) > 110 * 1024) {
     l.planes = 0;
     l.team = std::min(team, 8);
@@ -656,7 +659,8 @@ int Engine::max_blocks(const QueryLaunch& l) const {
   if (cached_blocks_ && cached_for_.team == l.team && cached_for_.warps == l.warps &&
       cached_for_.smem_counters == l.smem_counters && cached_for_.stage_bytes == l.stage_bytes &&
       cached_for_.stages == l.stages && cached_for_.bulk == l.bulk &&
-      cached_for_.min_blocks == l.min_blocks && cached_for_.planes == l.planes)
+      cached_for_.min_blocks == l.min_blocks && cached_for_.planes == l.planes &&
+      cached_for_.cut == l.cut)
     return cached_blocks_;
   int per_sm = 0;
   size_t smem = fused_smem_bytes(l);
@@ -700,6 +704,7 @@ void Engine::set_launch(const QueryLaunch& l) {
         "findere indexes use the register gather only");
   check(l.min_blocks >= 2 && l.min_blocks <= 3, kEInval, "min_blocks must be 2 or 3");
   check(l.planes == 0 || l.planes == 1, kEInval, "planes must be 0 or 1");
+  check(l.cut >= 1 && l.cut <= 64, kEInval, "cut must be in 1..64");
   check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
   check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
   std::lock_guard<std::mutex> lock(mu_);
@@ -1078,12 +1083,35 @@ void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
   for (uint64_t r = 0; r < records; ++r)
     check(offsets[r] <= offsets[r + 1], kEInval, "offsets must be non-decreasing");
-  ensure_capacity(ws, nbases, records);
-  ensure_host_capacity(ws, nbases, records);
+  // Chunks: record-aligned cuts near multiples of nbases / cut, at least
+  // 1 MiB of bases each.
+  const uint64_t min_chunk = 1ull << 20;
+  uint64_t cut = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)launch_.cut,
+                                                          nbases / min_chunk));
+  std::vector<uint64_t> bounds{0};  // record index of each chunk start, then records
+  for (uint64_t c = 1; c < cut; ++c) {
+    const uint64_t target = nbases / cut * c;
+    const uint64_t r = (uint64_t)(std::lower_bound(offsets, offsets + records + 1, target) - offsets);
+    if (r > bounds.back() && r < records) bounds.push_back(r);
+  }
+  bounds.push_back(records);
+  const uint64_t chunks = bounds.size() - 1;
+  ensure_capacity(ws, nbases, records + chunks);
+  ensure_host_capacity(ws, nbases, records + chunks);
   const uint64_t colors = m_.colors.size();
   cudaStream_t s = ws.stream;
-  // Page-locked caller buffers are copied directly; pageable ones through the
-  // workspace's pinned staging.
+  if (!ws.copy_stream)
+    cuda_check(cudaStreamCreateWithFlags(&ws.copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  while (ws.chunk_events.size() < chunks) {
+    cudaEvent_t e;
+    cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    ws.chunk_events.push_back(e);
+  }
+  // The copy stream must not overwrite buffers the previous query still reads.
+  cuda_check(cudaEventRecord(ws.chunk_events[0], s), "cudaEventRecord");
+  cuda_check(cudaStreamWaitEvent(ws.copy_stream, ws.chunk_events[0], 0), "cudaStreamWaitEvent");
+  // Page-locked caller bases are copied directly; pageable ones through the
+  // workspace's pinned staging, chunk by chunk.
   auto pinned = [](const void* p) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -1092,22 +1120,28 @@ void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     }
     return a.type == cudaMemoryTypeHost;
   };
-  const uint8_t* src_bases = bases;
-  const uint64_t* src_offsets = offsets;
-  if (nbases && !pinned(bases)) {
-    memcpy(ws.h_bases, bases, nbases);
-    src_bases = ws.h_bases;
-  }
-  if (!pinned(offsets)) {
-    memcpy(ws.h_offsets, offsets, (records + 1) * 8);
-    src_offsets = ws.h_offsets;
-  }
-  cuda_check(cudaMemcpyAsync(ws.bases, src_bases, nbases, cudaMemcpyHostToDevice, s), "H2D");
-  cuda_check(cudaMemcpyAsync(ws.offsets, src_offsets, (records + 1) * 8, cudaMemcpyHostToDevice, s),
-             "H2D");
+  const bool direct = nbases && pinned(bases);
   cuda_check(cudaMemsetAsync(ws.counts, 0, colors * 8, s), "memset");
   cuda_check(cudaMemsetAsync(ws.total, 0, 8, s), "memset");
-  enqueue(ws, ws.bases, nbases, ws.offsets, records, recover, ws.counts, ws.total, s);
+  for (uint64_t c = 0; c < chunks; ++c) {
+    const uint64_t r0 = bounds[c], r1 = bounds[c + 1], b0 = offsets[r0], nb = offsets[r1] - b0;
+    uint64_t* h_off = ws.h_offsets + r0 + c;  // chunk-relative offsets, records + 1 entries
+    for (uint64_t r = r0; r <= r1; ++r) h_off[r - r0] = offsets[r] - b0;
+    const uint8_t* src = bases + b0;
+    if (!direct && nb) {
+      memcpy(ws.h_bases + b0, bases + b0, nb);
+      src = ws.h_bases + b0;
+    }
+    if (nb)
+      cuda_check(cudaMemcpyAsync(ws.bases + b0, src, nb, cudaMemcpyHostToDevice, ws.copy_stream),
+                 "H2D");
+    cuda_check(cudaMemcpyAsync(ws.offsets + r0 + c, h_off, (r1 - r0 + 1) * 8,
+                               cudaMemcpyHostToDevice, ws.copy_stream),
+               "H2D");
+    cuda_check(cudaEventRecord(ws.chunk_events[c], ws.copy_stream), "cudaEventRecord");
+    cuda_check(cudaStreamWaitEvent(s, ws.chunk_events[c], 0), "cudaStreamWaitEvent");
+    enqueue(ws, ws.bases + b0, nb, ws.offsets + r0 + c, r1 - r0, recover, ws.counts, ws.total, s);
+  }
   cuda_check(cudaMemcpyAsync(ws.h_counts, ws.counts, colors * 8, cudaMemcpyDeviceToHost, s), "D2H");
   cuda_check(cudaMemcpyAsync(ws.h_total, ws.total, 8, cudaMemcpyDeviceToHost, s), "D2H");
   cuda_check(cudaStreamSynchronize(s), "query");

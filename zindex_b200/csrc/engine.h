@@ -68,6 +68,8 @@ struct Workspace {
   uint64_t cap_bases = 0, cap_records = 0, cap_tiles = 0, cap_partial = 0, cap_colors = 0,
            cap_keys = 0, cap_h_bases = 0, cap_h_records = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;       // host-buffer queries: chunk copies
+  std::vector<cudaEvent_t> chunk_events;    // one per pipelined chunk
   // Graph cache: one instantiated graph per (input pointers, sizes, recover).
   std::map<std::tuple<const void*, uint64_t, const void*, uint64_t, void*, void*, int>,
            cudaGraphExec_t>

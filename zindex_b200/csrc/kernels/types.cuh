@@ -35,6 +35,7 @@ struct QueryLaunch {
   int bulk;           // staged gather: 1 = bulk copy per row slice, 0 = 16-byte cp.async
   int min_blocks;     // kernel variant compiled for 2 or 3 resident 256-thread blocks/SM
   int planes;         // register gather: 1 = row indices + bit-plane colour counters, 0 = descriptors
+  int cut;            // host batches: pipelined chunks (copy of chunk i+1 overlaps chunk i), 1..64
 };
 
 }  // namespace zx

@@ -1,0 +1,253 @@
+"""Learned launch planner: a two-layer FP32 perceptron trained on the GPU.
+
+The planner predicts, for an index geometry, a read batch and one candidate
+launch configuration, the log of the query time; it then picks the candidate
+with the lowest prediction. Two decisions are made per incoming batch:
+
+* the launch configuration of the fused kernel (team size, warps per block,
+  register budget, counting form) from device-time measurements, and
+* the batch cut of host-buffer queries (how many pipelined chunks the batch is
+  split into) from end-to-end measurements with the chosen launch.
+
+The network (hidden 32, ReLU) is trained by the library's own CUDA forward,
+backward and Adam kernels (zx_mlp_* in include/zindex.h) on rows measured by
+the autotuner (zindex_b200.tuning). Exhaustive autotuning is the fallback and
+the judge of its regret. The planner never changes results: every launch
+configuration and cut gives the same counts.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import math
+from ctypes import POINTER, byref, c_float, c_uint64, c_void_p
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Dict, Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+
+FEATURES = (
+    "log2_hashes", "log2_bits", "log2_colors", "classes", "mode_kmers", "mode_minimizers",
+    "mode_modimizers", "mode_findere", "log2_gather_bytes", "log2_len_mean", "log2_seeds",
+    "log2_team", "log2_warps", "min_blocks", "planes", "smem_counters", "log2_stage_bytes",
+    "bulk", "log2_cut", "e2e", "log2_chunks", "team_over_chunks", "plane_word_fits",
+    "idle_lanes",
+)
+DATA = Path(__file__).resolve().parent / "data" / "planner_measurements.json"
+
+
+def encode(features: Dict[str, float], launch: Dict[str, int], e2e: bool = False) -> np.ndarray:
+    """Fixed-scale feature vector (each entry roughly in [0, 1]). Besides the
+    raw geometry it carries how a launch meets the rows: 16-byte chunks per
+    fingerprint-plane row, team size against chunks, whether a lane's fields
+    fit one bit-plane word (4 x chunks per lane <= b), idle lanes."""
+    mode = int(features.get("mode", 0))
+    hashes, bits = max(1.0, features["hashes"]), max(1.0, features["bits"])
+    classes = max(1.0, features.get("classes", 1.0))
+    row_bytes = features["gather_bytes"] / (hashes * classes)
+    chunks = max(1.0, math.ceil(row_bytes / 16.0))
+    team = max(1, launch.get("team", 8))
+    per_lane = math.ceil(chunks / team)
+    planes = float(launch.get("planes", 0))
+    return np.array([
+        math.log2(hashes) / 5.0,
+        math.log2(bits) / 5.0,
+        math.log2(max(1.0, features["colors"])) / 14.0,
+        classes / 8.0,
+        float(mode == 0), float(mode == 1), float(mode == 2), float(mode == 3),
+        math.log2(max(1.0, features["gather_bytes"])) / 16.0,
+        math.log2(1.0 + features["len_mean"]) / 17.0,
+        math.log2(1.0 + features["seeds"]) / 30.0,
+        math.log2(team) / 5.0,
+        math.log2(max(1, launch.get("warps", 8))) / 3.0,
+        float(launch.get("min_blocks", 2) - 2),
+        planes,
+        float(launch.get("smem_counters", 1)),
+        math.log2(1 + launch.get("stage_bytes", 0)) / 16.0,
+        float(launch.get("bulk", 0)),
+        math.log2(max(1, launch.get("cut", 1))) / 6.0,
+        float(e2e),
+        math.log2(chunks) / 8.0,
+        max(-5.0, min(5.0, math.log2(team / chunks))) / 5.0,
+        planes * float(4 * per_lane <= bits),
+        max(0.0, 1.0 - chunks / team),
+    ], dtype=np.float32)
+
+
+def _pf(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_float))
+
+
+class Mlp:
+    """The network on the GPU (zx_mlp_*): y = w2 . relu(W1 x + b1) + b2."""
+
+    def __init__(self, inputs: int, hidden: int = 32, seed: int = 1, device: int = 0):
+        lib = _lib.load()
+        h = c_void_p()
+        _lib.check(lib.zx_mlp_create(int(device), int(inputs), int(hidden), int(seed), byref(h)))
+        self._h = h
+        self.inputs, self.hidden = inputs, hidden
+        self.count = int(lib.zx_mlp_param_count(self._h))
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.count, dtype=np.float32)
+        _lib.check(_lib.load().zx_mlp_get_params(self._h, _pf(p)))
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _lib.check(_lib.load().zx_mlp_set_params(self._h, _pf(p), len(p)))
+
+    def loss_grad(self, x: np.ndarray, t: np.ndarray) -> Tuple[float, np.ndarray]:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.zeros(self.count, dtype=np.float32)
+        loss = c_float()
+        _lib.check(_lib.load().zx_mlp_loss_grad(self._h, _pf(x), _pf(t), len(t), byref(loss),
+                                               _pf(g)))
+        return float(loss.value), g
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs: int, lr: float) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = c_float()
+        _lib.check(_lib.load().zx_mlp_train(self._h, _pf(x), _pf(t), len(t), int(epochs),
+                                           float(lr), byref(loss)))
+        return float(loss.value)
+
+    def predict(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros(len(x), dtype=np.float32)
+        _lib.check(_lib.load().zx_mlp_predict(self._h, _pf(x), len(x), _pf(y)))
+        return y
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().zx_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Row:
+    """One measurement: a setting (index + batch features), a launch, e2e or
+    device timing, and its milliseconds."""
+    setting: str
+    features: Dict[str, float]
+    launch: Dict[str, int]
+    e2e: bool
+    ms: float
+
+
+def load_rows(path: Path = DATA) -> Tuple[List[Row], Dict[str, Dict[str, int]]]:
+    """Measured rows and the default launch of each setting."""
+    raw = json.loads(Path(path).read_text())
+    rows = [Row(r["setting"], r["features"], r["launch"], bool(r["e2e"]), float(r["ms"]))
+            for r in raw["rows"] if math.isfinite(r["ms"])]
+    return rows, raw["defaults"]
+
+
+class Planner:
+    """Train on measured rows; choose launch and cut for new batches.
+
+    Targets are relative: for each setting, log(ms) minus the mean log(ms) of
+    that setting's rows of the same kind (device or end-to-end), scaled by the
+    spread over all rows. Only the ranking of candidates within one batch
+    matters for a choice, and relative targets keep the network from spending
+    its capacity on the large differences between settings."""
+
+    def __init__(self, hidden: int = 32, seed: int = 1, device: int = 0):
+        self.net = Mlp(len(FEATURES), hidden, seed, device)
+        self.sigma = 1.0
+
+    def fit(self, rows: Sequence[Row], epochs: int = 3000, lr: float = 3e-3) -> float:
+        x = np.stack([encode(r.features, r.launch, r.e2e) for r in rows])
+        y = np.log(np.array([r.ms for r in rows], dtype=np.float64))
+        groups: Dict[Tuple[str, bool], List[int]] = {}
+        for i, r in enumerate(rows):
+            groups.setdefault((r.setting, r.e2e), []).append(i)
+        rel = np.zeros_like(y)
+        for idx in groups.values():
+            rel[idx] = y[idx] - y[idx].mean()
+        self.sigma = float(rel.std() or 1.0)
+        return self.net.train(x, (rel / self.sigma).astype(np.float32), epochs, lr)
+
+    def predict_cost(self, features: Dict[str, float], launches: Sequence[Dict[str, int]],
+                     e2e: bool = False) -> np.ndarray:
+        """Predicted time of each candidate relative to the batch's typical
+        time (only ratios between candidates of one batch are meaningful)."""
+        x = np.stack([encode(features, l, e2e) for l in launches])
+        return np.exp(self.net.predict(x).astype(np.float64) * self.sigma)
+
+    def choose(self, features: Dict[str, float], launches: Sequence[Dict[str, int]],
+               e2e: bool = False, default: Optional[Dict[str, int]] = None,
+               margin: float = 0.0) -> Dict[str, int]:
+        """The candidate with the lowest predicted time; with `default` given,
+        the default unless the pick is predicted faster by more than `margin`
+        (a fraction)."""
+        cands = list(launches) + ([default] if default is not None else [])
+        pred = self.predict_cost(features, cands, e2e)
+        k = int(np.argmin(pred[: len(launches)]))
+        if default is not None and not pred[k] < pred[-1] * (1.0 - margin):
+            return dict(default)
+        return dict(launches[k])
+
+    def save(self, path: Path) -> None:
+        Path(path).write_text(json.dumps({
+            "features": list(FEATURES), "hidden": self.net.hidden, "sigma": self.sigma,
+            "params": self.net.params().tolist()}))
+
+    @classmethod
+    def load(cls, path: Path, device: int = 0) -> "Planner":
+        d = json.loads(Path(path).read_text())
+        if tuple(d["features"]) != FEATURES:
+            raise ValueError("planner file was trained on other features")
+        p = cls(hidden=int(d["hidden"]), device=device)
+        p.sigma = float(d["sigma"])
+        p.net.set_params(np.array(d["params"], dtype=np.float32))
+        return p
+
+
+# Margins of the two decisions: launches are taken as predicted; the cut of
+# host batches only moves off the default when the network predicts a clear
+# win (the default cut was within 2% of the best in the measured settings).
+LAUNCH_MARGIN = 0.0
+CUT_MARGIN = 0.06
+
+
+def launch_key(l: Dict[str, int]) -> Tuple:
+    return tuple(sorted((k, int(v)) for k, v in l.items() if k != "blocks"))
+
+
+def evaluate(planner: Planner, rows: Sequence[Row], default: Dict[str, int],
+             e2e: bool = False) -> Dict[str, float]:
+    """Per setting of `rows` (device or e2e rows): the planner's choice among
+    the measured candidates against the exhaustive best (regret) and the
+    default launch (gain). Returns geometric means over settings."""
+    by: Dict[str, List[Row]] = {}
+    for r in rows:
+        if r.e2e == e2e:
+            by.setdefault(r.setting, []).append(r)
+    regrets, gains = [], []
+    dkey = launch_key(default)
+    for setting, rs in by.items():
+        table = {launch_key(r.launch): r for r in rs}
+        if dkey not in table:
+            continue
+        best = min(r.ms for r in rs)
+        pick = planner.choose(rs[0].features, [r.launch for r in rs], e2e, default=default,
+                              margin=CUT_MARGIN if e2e else LAUNCH_MARGIN)
+        chosen = table[launch_key(pick)].ms
+        regrets.append(chosen / best)
+        gains.append(table[dkey].ms / chosen)
+    gm = lambda v: float(np.exp(np.mean(np.log(v)))) if v else float("nan")
+    return {"settings": len(gains), "regret": gm(regrets) - 1.0, "gain_over_default": gm(gains),
+            "worst_gain": min(gains) if gains else float("nan")}
