@@ -39,14 +39,58 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-WORKLOAD = {
-    "workload": "batched-kmer-query",
-    "colors": 256, "genome_len_bp": [1_000_000, 10_000_000], "genome_model": "70% iid + 30% core-pool",
-    "k": 31, "hashes": 4, "fingerprint_bits": 8, "index_mode": "kmers",
-    "reads": 1_000_000, "read_len_bp": 150, "sourced": 0.7, "substitutions": 0.005,
-    "genome_seed": 1, "read_seed": 7,
+# Workloads: c2 (the default line) and the other configurations, each as
+# synthetic genomes (zx_build --synth kind:colors:min:max:seed), index options,
+# the query batch (zx_synth reads) and the long records of the served mix.
+CONFIGS = {
+    "c2": {
+        "workload": {"workload": "batched-kmer-query", "colors": 256,
+                     "genome_len_bp": [1_000_000, 10_000_000],
+                     "genome_model": "70% iid + 30% core-pool", "k": 31, "hashes": 4,
+                     "fingerprint_bits": 8, "index_mode": "kmers", "reads": 1_000_000,
+                     "read_len_bp": 150, "sourced": 0.7, "substitutions": 0.005,
+                     "genome_seed": 1, "read_seed": 7},
+        "synth": "pool:256:1000000:10000000:1", "build": ["-k", "31", "-H", "4", "-b", "8"],
+        "reads": ["--kind", "short", "--reads", "1000000", "--length", "150", "--sourced", "0.7",
+                  "--subst", "0.005"],
+    },
+    "c1": {
+        "workload": {"workload": "plain-kmer-small", "colors": 10, "genome_len_bp": [2_000_000, 2_000_000],
+                     "genome_model": "iid uniform", "k": 31, "hashes": 4, "fingerprint_bits": 8,
+                     "index_mode": "kmers", "reads": 100, "read_len_bp": 1000,
+                     "query": "record 0 copied from genome 0, 99 iid records", "genome_seed": 1},
+        "synth": "uniform:10:2000000:2000000:1", "build": ["-k", "31", "-H", "4", "-b", "8"],
+        "reads": ["--kind", "fragment", "--reads", "100", "--length", "1000"],
+    },
+    "c3": {
+        "workload": {"workload": "batched-minimizer-uneven", "colors": 2048,
+                     "genome_len_bp": [500_000, 8_000_000],
+                     "genome_model": "70% iid + 30% core-pool", "k": 49, "m": 31, "hashes": 3,
+                     "fingerprint_bits": 16, "index_mode": "minimizers", "reads": 200_000,
+                     "read_len_bp": "lognormal median 2000, clipped 100-100000", "sourced": 0.8,
+                     "substitutions": 0.01, "n_runs": 0.1},
+        "synth": "pool:2048:500000:8000000:1",
+        "build": ["-i", "minimizers", "-k", "49", "-m", "31", "-H", "3", "-b", "16"],
+        "reads": ["--kind", "long", "--reads", "200000", "--length", "2000", "--sourced", "0.8",
+                  "--subst", "0.01", "--n-runs", "0.1"],
+    },
+    "c4s": {
+        "workload": {"workload": "served-wide-rows-scaled", "colors": 16384,
+                     "genome_len_bp": [20_000, 120_000],
+                     "genome_model": "70% iid + 30% core-pool", "k": 31, "hashes": 8,
+                     "fingerprint_bits": 4, "index_mode": "kmers", "reads": 20_000,
+                     "read_len_bp": 150, "sourced": 0.6, "substitutions": 0.005,
+                     "scaled": "genome lengths 1-6 Mbp scaled down 50x (the host builder cannot "
+                               "build the 64 GB index in a run); rows are the full 8 KiB"},
+        "synth": "pool:16384:20000:120000:1", "build": ["-k", "31", "-H", "8", "-b", "4"],
+        "reads": ["--kind", "short", "--reads", "20000", "--length", "150", "--sourced", "0.6",
+                  "--subst", "0.005"],
+        # 64 KiB of rows per seed: fewer served requests keep the run bounded.
+        "served": {"closed": 100, "open": 300, "rate": 200.0},
+    },
 }
-SYNTH = "pool:256:1000000:10000000:1"
+CONFIG = CONFIGS["c2"]
+WORKLOAD = CONFIG["workload"]
 METRIC = "query seeds/s"
 # DRAM bytes (read + write) per seed of the fused kernel on this workload, from one ncu
 # capture of a 1.2e7-seed slice (profiles/fused_query_kernel-c2-batched.md:
@@ -73,40 +117,44 @@ def build_native():
     subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
 
 
-def prepare(cache: Path, rank: int):
+def _synth_genome_args(cfg):
+    kind, colors, lo, hi, seed = cfg["synth"].split(":")
+    return ["--genome-kind", kind, "--colors", colors, "--min-len", lo, "--max-len", hi,
+            "--seed", seed]
+
+
+def prepare(cache: Path, rank: int, name: str = "c2"):
     """Index (built once per cache dir, file-locked) and this rank's reads."""
+    cfg = CONFIGS[name]
     cache.mkdir(parents=True, exist_ok=True)
-    index = cache / "index-c2-k31-H4-b8"
+    index = cache / f"index-{name}"
     with open(cache / ".lock", "w") as lk:
         fcntl.flock(lk, fcntl.LOCK_EX)
         if not (index / "manifest.json").exists():
             t0 = time.time()
-            subprocess.run([str(LIB / "zx_build"), "--synth", SYNTH, "-o", str(index), "-k", "31",
-                            "-H", "4", "-b", "8", "-q"], check=True)
+            subprocess.run([str(LIB / "zx_build"), "--synth", cfg["synth"], "-o", str(index),
+                            *cfg["build"], "-q"], check=True)
             log(f"built index in {time.time() - t0:.1f}s")
-        reads = cache / f"reads-c2-r{rank}"
+        reads = cache / f"reads-{name}-r{rank}"
         if not Path(str(reads) + ".offsets").exists():
-            subprocess.run([str(LIB / "zx_synth"), "reads", "--kind", "short", "--genome-kind", "pool",
-                            "--colors", "256", "--min-len", "1000000", "--max-len", "10000000",
-                            "--seed", "1", "--read-seed", str(7 + rank), "--reads", "1000000",
-                            "--length", "150", "--sourced", "0.7", "--subst", "0.005",
-                            "--format", "raw", "--out", str(reads)], check=True)
-        long = cache / f"long-c2-r{rank}"
+            subprocess.run([str(LIB / "zx_synth"), "reads", *_synth_genome_args(cfg),
+                            "--read-seed", str(7 + rank), *cfg["reads"], "--format", "raw",
+                            "--out", str(reads)], check=True)
+        long = cache / f"long-{name}-r{rank}"
         if not Path(str(long) + ".offsets").exists():
             # Long records for the served request mix: lognormal lengths,
             # median 30 kbp, clipped to 100 bp-100 kbp, 60% sourced.
-            subprocess.run([str(LIB / "zx_synth"), "reads", "--kind", "long", "--genome-kind", "pool",
-                            "--colors", "256", "--min-len", "1000000", "--max-len", "10000000",
-                            "--seed", "1", "--read-seed", str(101 + rank), "--reads", "400",
-                            "--length", "30000", "--sourced", "0.6", "--subst", "0.005",
+            subprocess.run([str(LIB / "zx_synth"), "reads", "--kind", "long",
+                            *_synth_genome_args(cfg), "--read-seed", str(101 + rank), "--reads",
+                            "400", "--length", "30000", "--sourced", "0.6", "--subst", "0.005",
                             "--format", "raw", "--out", str(long)], check=True)
     bases = np.fromfile(str(reads) + ".bases", dtype=np.uint8)
     offsets = np.fromfile(str(reads) + ".offsets", dtype=np.uint64)
     return index, bases, offsets
 
 
-def long_pool(cache: Path, rank: int):
-    long = cache / f"long-c2-r{rank}"
+def long_pool(cache: Path, rank: int, name: str = "c2"):
+    long = cache / f"long-{name}-r{rank}"
     return (np.fromfile(str(long) + ".bases", dtype=np.uint8),
             np.fromfile(str(long) + ".offsets", dtype=np.uint64))
 
@@ -122,6 +170,7 @@ def make_requests(bases, offsets, lbases, loffsets, n, seed):
         else:
             b, o, k = lbases, loffsets, int(rng.integers(1, 11))
         r = len(o) - 1
+        k = min(k, r)
         st = int(rng.integers(0, max(1, r - k)))
         oo = o[st: st + k + 1] - o[st]
         out.append((b[int(o[st]): int(o[st + k])], np.ascontiguousarray(oo)))
@@ -322,7 +371,7 @@ def cpu_baseline(index, bases, offsets, colors, target_s=15.0):
     seeds, secs, counts, n = orc.sized(bases, offsets, colors, target_s)
     orc.close()
     return {"value": seeds / secs, "unit": "seeds/s", "cores": orc.cores, "kind": "port",
-            "sample": f"first {n} of the 1,000,000 reads ({seeds} seeds), query only "
+            "sample": f"first {n} of the {len(offsets) - 1:,} query records ({seeds} seeds), query only "
                       f"(index load excluded), {secs:.2f}s"}, n, counts
 
 
@@ -331,27 +380,29 @@ def reference_arm(args):
     if rank != 0:
         return
     build_native()
-    index, bases, offsets = prepare(Path(args.cache), 0)
+    index, bases, offsets = prepare(Path(args.cache), 0, args.config)
     orc = CpuOracle(index)
+    colors = json.loads((index / "manifest.json").read_text())["colors"].__len__()
     per_step = max(1.0, 60.0 / max(1, args.steps + args.warmup))
     n = None
     vals = []
     for i in range(args.warmup + args.steps):
         if n is None:
-            seeds, secs, _, n = orc.sized(bases, offsets, 256, per_step)
+            seeds, secs, _, n = orc.sized(bases, offsets, colors, per_step)
         else:
-            seeds, secs, _ = orc.run(bases, offsets, n, 256)
+            seeds, secs, _ = orc.run(bases, offsets, n, colors)
         if i >= args.warmup:
             vals.append(seeds / secs)
     orc.close()
     base = {"unit": "seeds/s", "cores": orc.cores, "kind": "port",
-            "sample": f"first {n} of the 1,000,000 reads per step, query only (index load excluded)"}
+            "sample": f"first {n} of the {len(offsets) - 1:,} query records per step, query only "
+                      f"(index load excluded)"}
     value = statistics.median(vals)
     base = dict(base, value=value)
     line = {"metric": METRIC, "value": value, "unit": "seeds/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
-            "config": dict(WORKLOAD, l2="index 1.4+ GB and reads 150 MB exceed the 126 MB L2"),
+            "config": dict(WORKLOAD, config=args.config),
             "cpu_baseline": base,
             "e2e": {"value": value, "unit": "seeds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -371,7 +422,7 @@ def ours(args):
         dist.barrier()
     import zindex_b200 as zx
 
-    index_dir, bases, offsets = prepare(Path(args.cache), rank)
+    index_dir, bases, offsets = prepare(Path(args.cache), rank, args.config)
     if args.reads:
         offsets = offsets[: args.reads + 1].copy()
         bases = bases[: int(offsets[-1])].copy()
@@ -403,16 +454,31 @@ def ours(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
+    # An index and batch that fit the 126 MB L2 are timed step by step with
+    # the L2 flushed (a 256 MiB write) before each step, outside the events.
+    flush = info.resident_bytes + len(bases) * 2 < (126 << 20)
+    scrub = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if flush else None
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
-        e0.record(stream)
-        for _ in range(args.steps):
-            step()
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
+        if flush:
+            ms = 0.0
+            for _ in range(args.steps):
+                scrub.fill_(1)
+                e0.record(stream)
+                step()
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                ms += e0.elapsed_time(e1)
+            ms /= args.steps
+        else:
+            e0.record(stream)
+            for _ in range(args.steps):
+                step()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1) / args.steps
     if world > 1:
         dist.barrier()
-    ms = e0.elapsed_time(e1) / args.steps
     if world > 1:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -480,9 +546,10 @@ def ours(args):
     ix.set_launch(**default_launch)
 
     # Served form: request mix through the continuous-batching server.
-    lb, lo = long_pool(Path(args.cache), rank)
-    served = served_form(zx, ix, make_requests(bases, offsets, lb, lo, 400, 11 + rank),
-                         make_requests(bases, offsets, lb, lo, 1000, 23 + rank), 200.0)
+    lb, lo = long_pool(Path(args.cache), rank, args.config)
+    sv = CONFIG.get("served", {"closed": 400, "open": 1000, "rate": 200.0})
+    served = served_form(zx, ix, make_requests(bases, offsets, lb, lo, sv["closed"], 11 + rank),
+                         make_requests(bases, offsets, lb, lo, sv["open"], 23 + rank), sv["rate"])
 
     # Plain form: one record per launch, on a prefix.
     n_plain = min(4000, records)
@@ -506,7 +573,9 @@ def ours(args):
             "data": "synthetic",
             "config": dict(WORKLOAD, seeds_per_step=seeds, bases_per_step=int(len(bases)),
                            parallelism=f"replicas{world}",
-                           l2="no flush: index and reads exceed the 126 MB L2",
+                           config=args.config,
+                           l2=("L2 flushed (256 MiB write) before each timed step" if flush else
+                               "no flush: index and reads exceed the 126 MB L2"),
                            launch=ix.launch()),
             "bases_per_s": world * len(bases) / (ms / 1e3),
             "e2e": {"value": world * seeds / e2e_s, "unit": "seeds/s",
@@ -514,7 +583,8 @@ def ours(args):
                     "d2h_bytes_per_step": int(8 * ix.colors + 8)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": TRAFFIC_BYTES_PER_SEED * seeds / 1e9, "traffic_unit": "GB",
+                         "traffic": (TRAFFIC_BYTES_PER_SEED * seeds / 1e9
+                                     if args.config == "c2" else None), "traffic_unit": "GB",
                          "peak_kind": peak_kind,
                          "kernel": "fused_query_kernel", "kernel_ms": kernel_ms,
                          "algorithmic_bytes_per_launch": int(alg_bytes),
@@ -543,11 +613,14 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cache", default=os.environ.get("ZX_BENCH_CACHE", "/tmp/zx_bench"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--tune", action="store_true",
-                    help="autotune the launch configuration on the workload before timing")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c2",
+                    help="workload: c2 (default line) or another configuration")
     ap.add_argument("--reads", type=int, default=None,
                     help="query only the first N reads (smaller case for profiler captures)")
     args = ap.parse_args()
+    global CONFIG, WORKLOAD
+    CONFIG = CONFIGS[args.config]
+    WORKLOAD = dict(CONFIG["workload"])
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
