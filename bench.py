@@ -493,6 +493,7 @@ def ours(args):
     value = world * seeds / (ms / 1e3)
     launches = 5 * args.steps  # pack, count_tiles, fill_tiles, fused query, reduce per step
 
+    log("stage: kernel timing")
     # Dominant kernel (fused extraction + probe) timed alone with CUDA events
     # on its launch stream.
     ix.set_timing(True)
@@ -508,6 +509,7 @@ def ours(args):
     peak, peak_kind = hbm_peak()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
 
+    log("stage: end to end")
     # End to end through the C ABI with pinned host buffers.
     h_bases = torch.from_numpy(bases).pin_memory()
     h_off = torch.from_numpy(offsets.view(np.int64)).pin_memory()
@@ -526,6 +528,7 @@ def ours(args):
         e2e_s = float(t.item())
     assert t_e2e == seeds and np.array_equal(c_e2e, counts_dev), "e2e and device paths disagree"
 
+    log("stage: planned form")
     # Planned form: launch and cut chosen by the learned planner.
     def step_ms(launch, reps=5):
         ix.set_launch(**launch)
@@ -552,12 +555,14 @@ def ours(args):
     planned["e2e_seeds_per_s"] = seeds / statistics.median(times)
     ix.set_launch(**default_launch)
 
+    log("stage: served form")
     # Served form: request mix through the continuous-batching server.
     lb, lo = long_pool(Path(args.cache), rank, args.config)
     sv = CONFIG.get("served", {"closed": 400, "open": 1000, "rate": 200.0})
     served = served_form(zx, ix, make_requests(bases, offsets, lb, lo, sv["closed"], 11 + rank),
                          make_requests(bases, offsets, lb, lo, sv["open"], 23 + rank), sv["rate"])
 
+    log("stage: plain form")
     # Plain form: one record per launch, on a prefix.
     n_plain = min(4000, records)
     pb = bases[: int(offsets[n_plain])]
@@ -570,6 +575,7 @@ def ours(args):
         cb = None
         parity = None
         if world == 1 and not args.no_cpu_baseline:
+            log("stage: cpu baseline")
             cb, n_cpu, cpu_counts = cpu_baseline(index_dir, bases, offsets, ix.colors)
             c_part, _ = ix.query_records(bases[: int(offsets[n_cpu])], offsets[: n_cpu + 1])
             parity = bool(np.array_equal(c_part, cpu_counts))
