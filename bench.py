@@ -153,6 +153,23 @@ def prepare(cache: Path, rank: int, name: str = "c2"):
     return index, bases, offsets
 
 
+def over_ranks(dist, device, value: float, op: str) -> float:
+    """`value` reduced over the ranks ("max" or "sum"); itself on one process."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def job_rate(dist, device, units: float, seconds: float) -> float:
+    """Whole-job throughput: the units of every rank over the slowest rank's
+    time (the timed region ends when the last rank ends)."""
+    return over_ranks(dist, device, units, "sum") / over_ranks(dist, device, seconds, "max")
+
+
 def long_pool(cache: Path, rank: int, name: str = "c2"):
     long = cache / f"long-{name}-r{rank}"
     return (np.fromfile(str(long) + ".bases", dtype=np.uint8),
@@ -486,11 +503,10 @@ def ours(args):
             ms = e0.elapsed_time(e1) / args.steps
     if world > 1:
         dist.barrier()
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * seeds / (ms / 1e3)
+    ddist = dist if world > 1 else None
+    value = job_rate(ddist, dev, seeds, ms / 1e3)
+    bases_rate = job_rate(ddist, dev, len(bases), ms / 1e3)
+    ms = over_ranks(ddist, dev, ms, "max")
     launches = 5 * args.steps  # pack, count_tiles, fill_tiles, fused query, reduce per step
 
     log("stage: kernel timing")
@@ -522,10 +538,7 @@ def ours(args):
         c_e2e, t_e2e = ix.query_records(hb, ho)
         times.append(time.perf_counter() - t0)
     e2e_s = statistics.median(times)
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_rate = job_rate(ddist, dev, seeds, e2e_s)
     assert t_e2e == seeds and np.array_equal(c_e2e, counts_dev), "e2e and device paths disagree"
 
     log("stage: planned form")
@@ -590,8 +603,8 @@ def ours(args):
                            l2=("L2 flushed (256 MiB write) before each timed step" if flush else
                                "no flush: index and reads exceed the 126 MB L2"),
                            launch=ix.launch()),
-            "bases_per_s": world * len(bases) / (ms / 1e3),
-            "e2e": {"value": world * seeds / e2e_s, "unit": "seeds/s",
+            "bases_per_s": bases_rate,
+            "e2e": {"value": e2e_rate, "unit": "seeds/s",
                     "h2d_bytes_per_step": int(len(bases) + 8 * (records + 1)),
                     "d2h_bytes_per_step": int(8 * ix.colors + 8)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

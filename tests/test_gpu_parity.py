@@ -212,6 +212,29 @@ def test_pipelined_host_chunks_equal_one_pass(gpu, oracle, tmp_path_factory, mod
             np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.parametrize("colors,H,b,groups", [
+    (1500, 4, 4, "0,1,2;7,9"),   # 47 chunks per row: two shared-plane words per lane
+    (2048, 3, 16, "5,6,7,8"),    # 256 chunks per row (4 KiB)
+])
+def test_wide_rows_shared_planes(gpu, oracle, tmp_path_factory, colors, H, b, groups):
+    """Rows wider than one register plane word per lane count in shared planes."""
+    ix, genomes = index_for(tmp_path_factory, colors=colors, length=3000, seed=61, mode="kmers",
+                            k=25, H=H, b=b, groups=groups)
+    reads = reads_for(genomes, n=600, length=150, n_runs=0.05)
+    gpu_vs_oracle(oracle, ix, reads, recover=True)
+    gpu_vs_oracle(oracle, ix, reads, recover=False)
+    import zindex_b200 as zx
+
+    bases, offsets = zx.pack_records(reads)
+    want, want_total = oracle.query_records(ix, bases, offsets)
+    with zx.Index(ix) as index:
+        for team, warps in ((32, 8), (16, 4), (8, 2)):
+            index.set_launch(team=team, warps=warps, planes=1, smem_counters=0)
+            got, total = index.query_records(bases, offsets)
+            assert total == want_total
+            np.testing.assert_array_equal(got, want)
+
+
 def test_multi_member_groups(gpu, oracle, tmp_path_factory):
     ix, genomes = index_for(tmp_path_factory, colors=8, mode="kmers", k=31, H=4, b=4,
                             groups="0,1,2;3,5;6,7")

@@ -626,13 +626,16 @@ QueryLaunch Engine::default_launch() const {
   for (uint32_t c = 0; c < host_ix_.classes; ++c) chunks = std::max(chunks, host_ix_.cls[c].fp_chunks);
   int team = 1;
   while (team < 32 && (uint32_t)team < chunks) team <<= 1;
-  // Row-index gather with bit-plane counters, teams of up to 16 lanes (one
-  // 16-byte chunk each) and 2 resident 8-warp blocks per SM measured fastest
-  // on B200 for 256-byte fingerprint rows (22.8 ms against 40.6 ms for the
-  // per-hit form with teams of 8 on 1.2e8 seeds). The per-hit form stays the
-  // fallback when the per-seed row indices do not fit shared memory.
+  // Row-index gather with bit-plane counters, 8 warps per block, 2 resident
+  // blocks per SM: teams of up to 16 lanes (one 16-byte chunk each) measured
+  // fastest on B200 for 256-byte fingerprint rows (22.8 ms against 40.6 ms
+  // for the per-hit form on 1.2e8 seeds); wider rows use whole-warp teams so
+  // that each lane's fields fit few shared-plane words. Shared memory above
+  // 110 KB per block moves the colour counters to global atomics (flushed
+  // planes make them rare), then halves the warps; the per-hit form is the
+  // last fallback.
   QueryLaunch l;
-  l.team = std::min(team, 16);
+  l.team = std::min(team, chunks > 16 ? 32 : 16);
   l.warps = 8;
   l.smem_counters = m_.colors.size() <= 16384 ? 1 : 0;
   l.blocks = 0;  // 0: fill the device (occupancy-derived)
@@ -642,7 +645,17 @@ QueryLaunch Engine::default_launch() const {
   l.min_blocks = 2;
   l.planes = 1;
   l.cut = 4;
-  if (fused_smem_bytes(l) > 110 * 1024) {
+  // Wide rows: fewer warps per block keep several blocks per SM (measured on
+  // 8 KiB rows of 16,384 colours: 2 warps x 3 blocks 64 ms, against 78 ms for
+  // the per-hit form); colour counters go to global atomics above 2,048
+  // colours, since flushed planes make them rare.
+  const size_t budget = 110 * 1024;
+  if (fused_smem_bytes(l) > budget && l.smem_counters && m_.colors.size() > 2048)
+    l.smem_counters = 0;
+  if (fused_smem_bytes(l) > budget) l.warps = 4;
+  if (fused_smem_bytes(l) > budget) l.warps = 2;
+  if (fused_smem_bytes(l) > budget) {
+    l.warps = 8;
     l.planes = 0;
     l.team = std::min(team, 8);
     l.min_blocks = 3;
@@ -652,7 +665,7 @@ QueryLaunch Engine::default_launch() const {
 
 size_t Engine::fused_smem_bytes(const QueryLaunch& l) const {
   return FusedSmem::total(sp_.mode, sp_.k, (uint32_t)m_.colors.size(), host_ix_.classes,
-                          m_.hashes, l);
+                          m_.hashes, l, FusedSmem::shared_words(sp_.mode, host_ix_, l));
 }
 
 int Engine::max_blocks(const QueryLaunch& l) const {

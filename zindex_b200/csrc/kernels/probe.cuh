@@ -378,15 +378,28 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
 // counted per field in vertical binary counters held in registers (bit p of
 // plane k is bit k of the count of field p) and added to the colour counters
 // only every few dozen seeds, instead of one shared-memory atomic per hit.
-// One class per lane is counted this way: the first whose fields of the lane
-// fit one 32-bit dense word (4 * chunks per lane <= b). Hits on multi-member
-// groups, every hit of a seed with recovered origins, and hits in the other
+// The first class whose fields of a lane fit one 32-bit dense word (4 x
+// chunks per lane <= b) keeps its planes in registers; the next classes, up
+// to kMaxSharedPlaneWords dense words per lane in all, keep theirs in the
+// warp's shared memory (each lane owns its words: no atomics, no bank
+// conflicts), which is what wide rows with many matching fields need (4 KiB
+// rows hit by hundreds of colours, or 8 KiB rows of 4-bit fingerprints with a
+// 1/16 chance of a false match per group). Hits on multi-member groups,
+// every hit of a seed with recovered origins, and hits in the remaining
 // classes take the per-hit path (membership decode, recovered-origin
 // exclusion).
-constexpr int kPlanes = 6;            // counts up to 63 per field
+constexpr int kPlanes = 6;            // register planes: counts up to 63 per field
 constexpr uint32_t kPlaneFlush = 31;  // team steps (two seeds each) between flushes
+constexpr int kSharedPlanes = 8;      // shared planes: counts up to 255 per field
+constexpr uint32_t kSharedFlush = 127;
+constexpr uint32_t kMaxSharedPlaneWords = 32;
+constexpr uint16_t kNoPlanes = 0xFFFF;
 
-__device__ __forceinline__ int log2_bits(int b) { return 31 - __clz(b); }
+__host__ __device__ __forceinline__ int log2_bits(int b) {
+  int l = 0;
+  while ((1 << (l + 1)) <= b) ++l;
+  return l;
+}
 
 // Dense layout of a lane's fields in a class: word q of the lane (its chunk
 // q / 4, 32-bit word q % 4 of that chunk) has its field-match flags at bits
@@ -417,9 +430,72 @@ __device__ __forceinline__ void plane_add(uint32_t (&c)[kPlanes], uint32_t m) {
 }
 
 // Dense words a lane needs for class C.
-__device__ __forceinline__ uint32_t plane_words(const DevClass& C, int b, int T) {
+__host__ __device__ __forceinline__ uint32_t plane_words(const DevClass& C, int b, int T) {
   const uint32_t jmax = (C.fp_chunks + (uint32_t)T - 1) / (uint32_t)T;
   return (4u * jmax + (uint32_t)b - 1) / (uint32_t)b;
+}
+
+// The register-plane class: the first class needing one dense word.
+__host__ __device__ __forceinline__ int register_plane_class(const DevIndex& ix, int T) {
+  for (uint32_t ci = 0; ci < ix.classes; ++ci)
+    if (plane_words(ix.cls[ci], ix.bits, T) == 1) return (int)ci;
+  return -1;
+}
+
+// Shared-plane layout: base[c] = first dense word of class c in the warp's
+// shared planes (kNoPlanes: not counted there); returns the words per lane.
+__host__ __device__ __forceinline__ uint32_t shared_plane_layout(const DevIndex& ix, int T,
+                                                                uint16_t* base) {
+  const int rc = register_plane_class(ix, T);
+  uint32_t used = 0;
+  for (uint32_t ci = 0; ci < ix.classes; ++ci) {
+    uint16_t b0 = kNoPlanes;
+    if ((int)ci != rc) {
+      const uint32_t w = plane_words(ix.cls[ci], ix.bits, T);
+      if (used + w <= kMaxSharedPlaneWords) {
+        b0 = (uint16_t)used;
+        used += w;
+      }
+    }
+    if (base) base[ci] = b0;
+  }
+  return used;
+}
+
+// Per-warp shared planes: for each of `words` dense words per lane,
+// kSharedPlanes count planes, then the valid and multi-member masks; element
+// (word, row) of lane l at ((word * (kSharedPlanes + 2) + row) * 32 + l).
+struct SharedPlanes {
+  uint32_t* base;
+  uint32_t words;
+  uint32_t steps;
+  __device__ __forceinline__ uint32_t* at(uint32_t word, int row, int lane) const {
+    return base + ((size_t)word * (kSharedPlanes + 2) + row) * 32 + lane;
+  }
+};
+
+__device__ __forceinline__ void shared_plane_add(uint32_t* p, uint32_t m) {
+  for (int k = 0; k < kSharedPlanes && m; ++k) {
+    const uint32_t c = p[k * 32];
+    p[k * 32] = c ^ m;
+    m &= c;
+  }
+}
+
+// Masks of dense word d of a lane in class C: positions that are fields of
+// the lane, and those whose group has several members.
+__device__ __forceinline__ void plane_masks(const DevClass& C, uint32_t d, int b, int tl, int T,
+                                            uint32_t& valid, uint32_t& multi) {
+  const int lb = log2_bits(b);
+  valid = multi = 0;
+  for (uint32_t bit = 0; bit < 32; ++bit) {
+    const uint32_t q = d * (uint32_t)b + (bit & (uint32_t)(b - 1));
+    if ((uint32_t)tl + (q >> 2) * (uint32_t)T >= C.fp_chunks) continue;
+    const uint32_t g = dense_group(bit, d, b, lb, tl, T);
+    if (g >= C.groups) continue;
+    valid |= 1u << bit;
+    if (__ldg(C.group_color + g) & kMultiGroup) multi |= 1u << bit;
+  }
 }
 
 __device__ __forceinline__ void planes_init(LanePlanes& P, const DevIndex& ix, int tl, int T) {
@@ -428,21 +504,8 @@ __device__ __forceinline__ void planes_init(LanePlanes& P, const DevIndex& ix, i
   P.cls = -1;
   P.valid = P.multi = 0;
   P.steps = 0;
-  const int b = ix.bits, lb = log2_bits(b);
-  for (uint32_t ci = 0; ci < ix.classes; ++ci) {
-    const DevClass& C = ix.cls[ci];
-    if ((uint32_t)tl >= C.fp_chunks || plane_words(C, b, T) != 1) continue;
-    P.cls = (int)ci;
-    for (uint32_t bit = 0; bit < 32; ++bit) {
-      const uint32_t q = bit & (uint32_t)(b - 1);
-      if ((uint32_t)tl + (q >> 2) * (uint32_t)T >= C.fp_chunks) continue;
-      const uint32_t g = dense_group(bit, 0, b, lb, tl, T);
-      if (g >= C.groups) continue;
-      P.valid |= 1u << bit;
-      if (__ldg(C.group_color + g) & kMultiGroup) P.multi |= 1u << bit;
-    }
-    return;
-  }
+  P.cls = register_plane_class(ix, T);
+  if (P.cls >= 0) plane_masks(ix.cls[P.cls], 0, ix.bits, tl, T, P.valid, P.multi);
 }
 
 template <class Sink>
@@ -465,6 +528,52 @@ __device__ __forceinline__ void planes_flush(LanePlanes& P, const DevIndex& ix, 
   }
 #pragma unroll
   for (int k = 0; k < kPlanes; ++k) P.c[k] = 0;
+}
+
+// Zeroes a lane's shared planes and fills its masks (class c owns words
+// base[c] .. base[c] + plane_words - 1).
+__device__ __forceinline__ void shared_planes_init(SharedPlanes& S, const DevIndex& ix,
+                                                   const uint16_t* base, int tl, int T, int lane) {
+  S.steps = 0;
+  for (uint32_t ci = 0; ci < ix.classes; ++ci) {
+    if (base[ci] == kNoPlanes) continue;
+    const uint32_t w = plane_words(ix.cls[ci], ix.bits, T);
+    for (uint32_t d = 0; d < w; ++d) {
+      const uint32_t word = base[ci] + d;
+      for (int k = 0; k < kSharedPlanes; ++k) *S.at(word, k, lane) = 0;
+      uint32_t valid, multi;
+      plane_masks(ix.cls[ci], d, ix.bits, tl, T, valid, multi);
+      *S.at(word, kSharedPlanes, lane) = valid;
+      *S.at(word, kSharedPlanes + 1, lane) = multi;
+    }
+  }
+}
+
+template <class Sink>
+__device__ __forceinline__ void shared_planes_flush(SharedPlanes& S, const DevIndex& ix,
+                                                    const uint16_t* base, int tl, int T, int lane,
+                                                    const Sink& cnt) {
+  S.steps = 0;
+  const int b = ix.bits, lb = log2_bits(b);
+  for (uint32_t ci = 0; ci < ix.classes; ++ci) {
+    if (base[ci] == kNoPlanes) continue;
+    const DevClass& C = ix.cls[ci];
+    const uint32_t w = plane_words(C, b, T);
+    for (uint32_t d = 0; d < w; ++d) {
+      uint32_t* p = S.at(base[ci] + d, 0, lane);
+      uint32_t any = 0;
+      for (int k = 0; k < kSharedPlanes; ++k) any |= p[k * 32];
+      if (!any) continue;
+      while (any) {
+        const uint32_t bit = __ffs(any) - 1;
+        any &= any - 1;
+        uint32_t v = 0;
+        for (int k = 0; k < kSharedPlanes; ++k) v |= ((p[k * 32] >> bit) & 1u) << k;
+        cnt.add(__ldg(C.group_color + dense_group(bit, d, b, lb, tl, T)), v);
+      }
+      for (int k = 0; k < kSharedPlanes; ++k) p[k * 32] = 0;
+    }
+  }
 }
 
 // Colours of a hit group given the seed's H row indices (singleton, or
@@ -527,7 +636,8 @@ __device__ __forceinline__ int padded_hashes(int H) { return (H + 3) & ~3; }
 template <class Sink, class OnRound>
 __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
                            const uint32_t* kvalid, SeedDesc* desc, uint32_t* rows, int T,
-                           LanePlanes& P, const Sink& sink, int lane, OnRound&& on_round) {
+                           LanePlanes& P, SharedPlanes& S, const uint16_t* pbase, const Sink& sink,
+                           int lane, OnRound&& on_round) {
   const int H = ix.hashes, Hp = padded_hashes(H), b = ix.bits, lb = log2_bits(b);
   const uint32_t ones = field_ones(b), hi = ones << (b - 1);
   const uint32_t classes = ix.classes;
@@ -616,6 +726,54 @@ __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
             });
           continue;
         }
+        if (S.words && pbase[ci] != kNoPlanes) {
+          // Shared planes: each dense word is committed once the lane's
+          // chunks have filled it.
+          const uint32_t wbase = pbase[ci];
+          uint32_t xa = 0, xb = 0, dcur = 0;
+          auto commit = [&](uint32_t d) {
+            const uint32_t word = wbase + d;
+            const uint32_t valid = *S.at(word, kSharedPlanes, lane);
+            const uint32_t multi = *S.at(word, kSharedPlanes + 1, lane);
+            const uint32_t ma = va ? (xa & valid) : 0u, mb = vb ? (xb & valid) : 0u;
+            const uint32_t slowa = slow_a ? ma : (ma & multi);
+            const uint32_t slowb = slow_b ? mb : (mb & multi);
+            uint32_t* p = S.at(word, 0, lane);
+            shared_plane_add(p, ma & ~slowa);
+            shared_plane_add(p, mb & ~slowb);
+            for (uint32_t x = slowa; x; x &= x - 1)
+              group_hit_rows(C, dense_group(__ffs(x) - 1, d, b, lb, tl, T), ra, H, [&](uint32_t c) {
+                if (da.rec_len && desc_rec_contains(da, c)) return;
+                sink.hit(c, s);
+              });
+            for (uint32_t x = slowb; x; x &= x - 1)
+              group_hit_rows(C, dense_group(__ffs(x) - 1, d, b, lb, tl, T), rb, H, [&](uint32_t c) {
+                if (db.rec_len && desc_rec_contains(db, c)) return;
+                sink.hit(c, s2);
+              });
+          };
+          uint32_t q0 = 0;
+          for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T, q0 += 4) {
+            uint4 aa, ab;
+            gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, va, vb, aa, ab);
+            const uint32_t wa[4] = {aa.x, aa.y, aa.z, aa.w}, wb[4] = {ab.x, ab.y, ab.z, ab.w};
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+              const uint32_t q = q0 + (uint32_t)w;
+              const uint32_t d = q >> lb;
+              if (d != dcur) {
+                commit(dcur);
+                xa = xb = 0;
+                dcur = d;
+              }
+              const uint32_t sh = (uint32_t)(b - 1) - (q & (uint32_t)(b - 1));
+              xa |= zero_fields_hi(wa[w] ^ pa, hi) >> sh;
+              xb |= zero_fields_hi(wb[w] ^ pb, hi) >> sh;
+            }
+          }
+          commit(dcur);
+          continue;
+        }
         for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T) {
           uint4 aa, ab;
           gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, va, vb, aa, ab);
@@ -636,6 +794,7 @@ __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
         }
       }
       if (P.cls >= 0 && ++P.steps == kPlaneFlush) planes_flush(P, ix, tl, T, sink);
+      if (S.words && ++S.steps == kSharedFlush) shared_planes_flush(S, ix, pbase, tl, T, lane, sink);
     }
     __syncwarp();
     on_round(r0, m);

@@ -78,6 +78,7 @@ struct BatchView {
 // pos).
 struct FusedSmem {
   static constexpr size_t ix_bytes = (sizeof(DevIndex) + 15) / 16 * 16;
+  static constexpr size_t map_bytes = (kMaxClasses * 2 + 15) / 16 * 16;  // shared-plane bases
   static __host__ __device__ size_t counter_bytes(uint32_t colors, int smem_counters) {
     return smem_counters ? ((size_t)colors * 4 + 15) / 16 * 16 : 0;
   }
@@ -94,21 +95,35 @@ struct FusedSmem {
   static __host__ __device__ size_t ring_bytes(int stage_bytes, int stages) {
     return stage_bytes > 0 ? (size_t)stage_bytes * stages + 8 * 8 : 0;
   }
+  static __host__ __device__ size_t shared_plane_bytes(uint32_t words) {
+    return (size_t)words * (kSharedPlanes + 2) * 32 * 4;
+  }
   static __host__ __device__ size_t warp_bytes(int mode, int k, uint32_t classes, int stage_bytes = 0,
-                                               int stages = 0, int hashes = 4, int planes = 0) {
+                                               int stages = 0, int hashes = 4, int planes = 0,
+                                               uint32_t shared_words = 0) {
     size_t b = 2 * kTileWindows * 8 + probe_bytes(classes, hashes, planes) +
-               ring_bytes(stage_bytes, stages);
+               ring_bytes(stage_bytes, stages) + shared_plane_bytes(shared_words);
     if (mode == 1) b += 2 * ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
     if (mode == 3) b += 64;  // findere: valid bits of up to 512 s-mer positions
     return (b + 15) / 16 * 16;
   }
   // Findere always runs the row-index probe without a staged ring.
+  // shared_words: shared-plane words per lane (shared_plane_layout).
   static __host__ __device__ size_t total(int mode, int k, uint32_t colors, uint32_t classes,
-                                          int hashes, const QueryLaunch& l) {
+                                          int hashes, const QueryLaunch& l,
+                                          uint32_t shared_words = 0) {
     const bool fin = mode == 3;
-    return ix_bytes + counter_bytes(colors, l.smem_counters) + (mode == 1 ? 256 * 8 : 0) +
+    return ix_bytes + map_bytes + counter_bytes(colors, l.smem_counters) +
+           (mode == 1 ? 256 * 8 : 0) +
            (size_t)l.warps * warp_bytes(mode, k, classes, fin ? 0 : l.stage_bytes, l.stages, hashes,
-                                        fin ? 1 : l.planes);
+                                        fin ? 1 : l.planes, shared_words);
+  }
+  // Shared-plane words per lane a launch uses (0 unless the row-index form
+  // counts in planes).
+  static __host__ __device__ uint32_t shared_words(int mode, const DevIndex& ix,
+                                                   const QueryLaunch& l) {
+    if (mode == 3 || !l.planes || l.stage_bytes > 0) return 0;
+    return shared_plane_layout(ix, l.team, nullptr);
   }
 };
 
@@ -158,7 +173,8 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
                                                           uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) uint8_t smem[];
   DevIndex* six = reinterpret_cast<DevIndex*>(smem);
-  uint8_t* p = smem + FusedSmem::ix_bytes;
+  uint16_t* pbase = reinterpret_cast<uint16_t*>(smem + FusedSmem::ix_bytes);
+  uint8_t* p = smem + FusedSmem::ix_bytes + FusedSmem::map_bytes;
   uint32_t* scount = nullptr;
   const uint32_t colors = gix->colors, classes = gix->classes;
   if (lc.smem_counters) {
@@ -175,13 +191,17 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   // Findere always runs the row-index probe (VARIANT 2) without a ring.
   constexpr bool ROWS = VARIANT == 2 || MODE == 3;
   const int stage_bytes = MODE == 3 ? 0 : lc.stage_bytes;
-  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, classes, stage_bytes,
-                                                            lc.stages, hashes, ROWS);
+  const uint32_t swords = VARIANT == 2 ? FusedSmem::shared_words(MODE, *gix, lc) : 0u;
+  const size_t wstride =
+      FusedSmem::warp_bytes(MODE, sp.k, classes, stage_bytes, lc.stages, hashes, ROWS, swords);
+  uint8_t* wbase = p + (size_t)warp * wstride;
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
   SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + 2 * kTileWindows * 8);
   uint64_t* row0s = reinterpret_cast<uint64_t*>(desc + 64);
   uint8_t* ring_base = wbase + 2 * kTileWindows * 8 + FusedSmem::probe_bytes(classes, hashes, ROWS);
   uint8_t* ocm = ring_base + FusedSmem::ring_bytes(stage_bytes, lc.stages);
+  SharedPlanes splanes{reinterpret_cast<uint32_t*>(wbase + wstride - FusedSmem::shared_plane_bytes(swords)),
+                       swords, 0u};
   StageRing ring{ring_base + 64, reinterpret_cast<uint64_t*>(ring_base), (uint32_t)lc.stage_bytes,
                  (uint32_t)lc.stages, 0u, 0u, lc.bulk != 0};
   constexpr bool STAGED = VARIANT == 1;
@@ -202,6 +222,12 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   LanePlanes planes;
   if (ROWS) planes_init(planes, ix, lane % lc.team, lc.team);
   if (MODE == 3) planes.cls = -1;  // findere: every hit goes to the position masks
+  if (swords) {
+    if (threadIdx.x == 0) shared_plane_layout(ix, lc.team, pbase);
+    __syncthreads();
+    shared_planes_init(splanes, ix, pbase, lane % lc.team, lc.team, lane);
+    __syncwarp();
+  }
   const uint32_t wpb = blockDim.x >> 5;
   const uint32_t gwarp = blockIdx.x * wpb + warp;
   // Tile range of this warp: the whole list, or its block's segment.
@@ -239,7 +265,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
       uint32_t* frun = fmask + colors;
       const FindereSink fs{fmask};
       probe_rows(ix, keys, npos, kvalid, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
-                 fs, lane, [&](uint32_t r0, uint32_t m) {
+                 splanes, pbase, fs, lane, [&](uint32_t r0, uint32_t m) {
                    findere_sweep(fmask, frun, colors, z, m, r0 + m >= npos, cnt, lane);
                    __syncwarp();
                  });
@@ -255,7 +281,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
       }
     } else if (VARIANT == 2) {
       probe_rows(ix, keys, n, nullptr, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
-                 CountSink{cnt}, lane, [](uint32_t, uint32_t) {});
+                 splanes, pbase, CountSink{cnt}, lane, [](uint32_t, uint32_t) {});
     } else {
       probe_batch(ix, keys, n, desc, row0s, lc.team, cnt, lane);
     }
@@ -263,6 +289,8 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   }
   if (ROWS && planes.cls >= 0)
     planes_flush(planes, ix, lane % lc.team, lc.team, CountSink{cnt});
+  if (swords)
+    shared_planes_flush(splanes, ix, pbase, lane % lc.team, lc.team, lane, CountSink{cnt});
   if (lane == 0 && seeds) atomicAdd(total + seg, seeds);
   __syncthreads();
   if (scount)
