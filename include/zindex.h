@@ -61,7 +61,8 @@ typedef struct zx_launch {
   int stage_bytes;    /* > 0: staged gather, bytes per ring stage (multiple of 16) */
   int stages;         /* stages per warp ring for the staged gather, 1..8 */
   int bulk;           /* staged gather: 1 = cp.async.bulk per row slice, 0 = 16-byte cp.async */
-  int min_blocks;     /* kernel variant register budget: 2 or 3 resident 256-thread blocks */
+  int min_blocks;     /* kernel variant register budget: 2 or 3 resident 256-thread blocks, or 1
+                         (255 registers; planes 1 only: pipelines the row loads of wide rows) */
   int planes;         /* register gather: 1 = per-seed row indices and per-lane bit-plane colour
                          counters, 0 = per-seed descriptors and one counter update per hit */
   int cut;            /* host-buffer queries: the batch is cut at record boundaries into this many

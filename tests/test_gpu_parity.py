@@ -213,6 +213,7 @@ def test_pipelined_host_chunks_equal_one_pass(gpu, oracle, tmp_path_factory, mod
 
 
 @pytest.mark.parametrize("colors,H,b,groups", [
+    (600, 2, 8, "1,2"),         # 38 chunks, H = 2: the chunk pipeline with two rows
     (1500, 4, 4, "0,1,2;7,9"),   # 47 chunks per row: two shared-plane words per lane
     (2048, 3, 16, "5,6,7,8"),    # 256 chunks per row (4 KiB)
 ])
@@ -228,8 +229,8 @@ def test_wide_rows_shared_planes(gpu, oracle, tmp_path_factory, colors, H, b, gr
     bases, offsets = zx.pack_records(reads)
     want, want_total = oracle.query_records(ix, bases, offsets)
     with zx.Index(ix) as index:
-        for team, warps in ((32, 8), (16, 4), (8, 2)):
-            index.set_launch(team=team, warps=warps, planes=1, smem_counters=0)
+        for team, warps, minb in ((32, 8, 2), (16, 4, 2), (8, 2, 2), (32, 4, 1), (8, 4, 1)):
+            index.set_launch(team=team, warps=warps, planes=1, smem_counters=0, min_blocks=minb)
             got, total = index.query_records(bases, offsets)
             assert total == want_total
             np.testing.assert_array_equal(got, want)
@@ -368,6 +369,7 @@ LAUNCHES = [
     dict(team=1, warps=4, planes=1), dict(team=2, warps=3, planes=1),
     dict(team=8, warps=8, planes=1, min_blocks=2), dict(team=32, warps=1, planes=1),
     dict(team=4, warps=8, planes=1, min_blocks=2), dict(team=16, warps=8, planes=1),
+    dict(team=1, warps=4, planes=1, min_blocks=1), dict(team=2, warps=8, planes=1, min_blocks=1),
     dict(warps=4, stage_bytes=8192, stages=2, bulk=1), dict(warps=8, stage_bytes=4096, stages=3, bulk=1),
     dict(warps=2, stage_bytes=64, stages=1, bulk=1), dict(warps=4, stage_bytes=128, stages=4, bulk=1),
     dict(warps=1, stage_bytes=16384, stages=8, bulk=1),

@@ -185,8 +185,11 @@ class Index:
                    min_blocks: Optional[int] = None, planes: Optional[int] = None,
                    cut: Optional[int] = None, **_ignored):
         """Change the launch configuration (never changes results); unset
-        fields keep their default values."""
+        fields keep their default values (a default 255-register budget,
+        min_blocks 1, becomes 2 when the per-hit or staged form is asked for)."""
         d = self.default_launch()
+        if min_blocks is None and d["min_blocks"] == 1 and (planes == 0 or (stage_bytes or 0) > 0):
+            d["min_blocks"] = 2
         l = ZxLaunch(int(d["team"] if team is None else team), int(d["warps"] if warps is None else warps),
                      int(blocks), int(d["smem_counters"] if smem_counters is None else smem_counters),
                      int(d["stage_bytes"] if stage_bytes is None else stage_bytes),

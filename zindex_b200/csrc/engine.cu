@@ -120,6 +120,8 @@ FusedFn fused_for(int mode, const QueryLaunch& l) {
   // Findere has one form: the row-index probe with per-colour position masks.
   if (mode == 3) return l.min_blocks == 3 ? fused_query_kernel<3, 3, 2> : fused_query_kernel<3, 2, 2>;
   const int v = l.stage_bytes > 0 ? 1 : (l.planes ? 2 : 0);
+  // One resident block per SM: the row-index form with the chunk pipeline.
+  if (l.min_blocks == 1 && v == 2) return fused_mode<1, 2>(mode);
   if (l.min_blocks == 3) {
     if (v == 1) return fused_mode<3, 1>(mode);
     return v == 2 ? fused_mode<3, 2>(mode) : fused_mode<3, 0>(mode);
@@ -174,6 +176,13 @@ __global__ void hp_offsets_kernel(const uint64_t* __restrict__ offsets, uint64_t
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r <= records;
        r += (uint64_t)gridDim.x * blockDim.x)
     out[r] = pos[offsets[r]];
+}
+
+// offsets[i] -= base (chunk-relative record offsets after a raw copy).
+__global__ void rebase_offsets_kernel(uint64_t* __restrict__ offsets, uint64_t n, uint64_t base) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    offsets[i] -= base;
 }
 
 uint64_t le64(const uint8_t* p) {
@@ -654,6 +663,11 @@ QueryLaunch Engine::default_launch() const {
     l.smem_counters = 0;
   if (fused_smem_bytes(l) > budget) l.warps = 4;
   if (fused_smem_bytes(l) > budget) l.warps = 2;
+  // Wide rows counted in shared planes with H <= 4: the 255-register variant
+  // keeps two stages of row chunks in flight per lane.
+  if (FusedSmem::shared_words(sp_.mode, host_ix_, l) > 0 && m_.hashes <= 4 &&
+      fused_smem_bytes(l) <= budget)
+    l.min_blocks = 1;
   if (fused_smem_bytes(l) > budget) {
     l.warps = 8;
     l.planes = 0;
@@ -715,7 +729,9 @@ void Engine::set_launch(const QueryLaunch& l) {
         kEInval, "staged gather needs 16-byte multiple stages of at least 16*H bytes, 1..8 stages");
   check(m_.index_mode != kFindere || l.stage_bytes == 0, kEInval,
         "findere indexes use the register gather only");
-  check(l.min_blocks >= 2 && l.min_blocks <= 3, kEInval, "min_blocks must be 2 or 3");
+  check(l.min_blocks >= 1 && l.min_blocks <= 3, kEInval, "min_blocks must be 1, 2 or 3");
+  check(l.min_blocks != 1 || (l.planes == 1 && l.stage_bytes == 0), kEInval,
+        "min_blocks 1 (255 registers) is compiled for the row-index form (planes 1) only");
   check(l.planes == 0 || l.planes == 1, kEInval, "planes must be 0 or 1");
   check(l.cut >= 1 && l.cut <= 64, kEInval, "cut must be in 1..64");
   check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
@@ -1134,12 +1150,18 @@ void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     return a.type == cudaMemoryTypeHost;
   };
   const bool direct = nbases && pinned(bases);
+  const bool direct_offsets = pinned(offsets);
   cuda_check(cudaMemsetAsync(ws.counts, 0, colors * 8, s), "memset");
   cuda_check(cudaMemsetAsync(ws.total, 0, 8, s), "memset");
   for (uint64_t c = 0; c < chunks; ++c) {
     const uint64_t r0 = bounds[c], r1 = bounds[c + 1], b0 = offsets[r0], nb = offsets[r1] - b0;
-    uint64_t* h_off = ws.h_offsets + r0 + c;  // chunk-relative offsets, records + 1 entries
-    for (uint64_t r = r0; r <= r1; ++r) h_off[r - r0] = offsets[r] - b0;
+    // The chunk's records + 1 absolute offsets, made chunk-relative on the
+    // device after the copy.
+    const uint64_t* h_off = offsets + r0;
+    if (!direct_offsets) {
+      memcpy(ws.h_offsets + r0 + c, offsets + r0, (r1 - r0 + 1) * 8);
+      h_off = ws.h_offsets + r0 + c;
+    }
     const uint8_t* src = bases + b0;
     if (!direct && nb) {
       memcpy(ws.h_bases + b0, bases + b0, nb);
@@ -1151,6 +1173,12 @@ void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     cuda_check(cudaMemcpyAsync(ws.offsets + r0 + c, h_off, (r1 - r0 + 1) * 8,
                                cudaMemcpyHostToDevice, ws.copy_stream),
                "H2D");
+    if (b0) {
+      const uint64_t n = r1 - r0 + 1;
+      rebase_offsets_kernel<<<(int)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms_ * 4), 256, 0,
+                              ws.copy_stream>>>(ws.offsets + r0 + c, n, b0);
+      cuda_check(cudaGetLastError(), "rebase_offsets_kernel");
+    }
     cuda_check(cudaEventRecord(ws.chunk_events[c], ws.copy_stream), "cudaEventRecord");
     cuda_check(cudaStreamWaitEvent(s, ws.chunk_events[c], 0), "cudaStreamWaitEvent");
     enqueue(ws, ws.bases + b0, nb, ws.offsets + r0 + c, r1 - r0, recover, ws.counts, ws.total, s);

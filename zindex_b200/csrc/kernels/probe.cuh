@@ -633,7 +633,9 @@ __device__ __forceinline__ int padded_hashes(int H) { return (H + 3) & ~3; }
 // sink.hit(colour, s), except singleton hits counted in the lane's bit planes
 // (flushed through sink.add(colour, count)); on_round(r0, m) runs after each
 // round with the warp converged.
-template <class Sink, class OnRound>
+// PIPE: compile the two-stage chunk pipeline of shared-plane classes (kernel
+// variants with the 255-register budget only; it needs about 40 registers).
+template <bool PIPE, class Sink, class OnRound>
 __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
                            const uint32_t* kvalid, SeedDesc* desc, uint32_t* rows, int T,
                            LanePlanes& P, SharedPlanes& S, const uint16_t* pbase, const Sink& sink,
@@ -752,10 +754,9 @@ __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
                 sink.hit(c, s2);
               });
           };
-          uint32_t q0 = 0;
-          for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T, q0 += 4) {
-            uint4 aa, ab;
-            gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, va, vb, aa, ab);
+          // Match flags of one chunk (XORed rows of both seeds) into the
+          // dense words, committing each word when the next one starts.
+          auto consume = [&](const uint4& aa, const uint4& ab, uint32_t q0) {
             const uint32_t wa[4] = {aa.x, aa.y, aa.z, aa.w}, wb[4] = {ab.x, ab.y, ab.z, ab.w};
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
@@ -769,6 +770,54 @@ __device__ void probe_rows(const DevIndex& ix, const uint64_t* keys, uint32_t n,
               const uint32_t sh = (uint32_t)(b - 1) - (q & (uint32_t)(b - 1));
               xa |= zero_fields_hi(wa[w] ^ pa, hi) >> sh;
               xb |= zero_fields_hi(wb[w] ^ pb, hi) >> sh;
+            }
+          };
+          if (PIPE && H <= 4) {
+            // Up to 4 rows: two stages of row chunks in registers, the next
+            // chunk's loads issued before the current chunk is compared.
+            const uint4 ia = *reinterpret_cast<const uint4*>(ra);
+            const uint4 ib = *reinterpret_cast<const uint4*>(rb);
+            const uint32_t xi[4] = {ia.x, ia.y, ia.z, ia.w}, yi[4] = {ib.x, ib.y, ib.z, ib.w};
+            uint4 a0[4], b0[4], a1[4], b1[4];
+            auto load = [&](uint4 (&la)[4], uint4 (&lb4)[4], uint32_t chunk) {
+              const uint8_t* col = C.data + chunk * 16u;
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                la[j] = lb4[j] = make_uint4(0, 0, 0, 0);
+                if (j < H) {
+                  if (va) la[j] = ld_row_chunk(col + (uint64_t)xi[j] * stride);
+                  if (vb) lb4[j] = ld_row_chunk(col + (uint64_t)yi[j] * stride);
+                }
+              }
+            };
+            auto fold = [&](const uint4 (&la)[4], const uint4 (&lb4)[4], uint32_t q0) {
+              uint4 aa = la[0], ab = lb4[0];
+#pragma unroll
+              for (int j = 1; j < 4; ++j) {
+                aa.x ^= la[j].x; aa.y ^= la[j].y; aa.z ^= la[j].z; aa.w ^= la[j].w;
+                ab.x ^= lb4[j].x; ab.y ^= lb4[j].y; ab.z ^= lb4[j].z; ab.w ^= lb4[j].w;
+              }
+              consume(aa, ab, q0);
+            };
+            uint32_t chunk = tl, q0 = 0;
+            if (chunk < C.fp_chunks) load(a0, b0, chunk);
+            while (chunk < C.fp_chunks) {
+              const uint32_t c1 = chunk + T;
+              if (c1 < C.fp_chunks) load(a1, b1, c1);
+              fold(a0, b0, q0);
+              if (c1 >= C.fp_chunks) break;
+              const uint32_t c2 = c1 + T;
+              if (c2 < C.fp_chunks) load(a0, b0, c2);
+              fold(a1, b1, q0 + 4);
+              chunk = c2;
+              q0 += 8;
+            }
+          } else {
+            uint32_t q0 = 0;
+            for (uint32_t chunk = tl; chunk < C.fp_chunks; chunk += T, q0 += 4) {
+              uint4 aa, ab;
+              gather_xor2(C.data + chunk * 16u, stride, ra, rb, H, va, vb, aa, ab);
+              consume(aa, ab, q0);
             }
           }
           commit(dcur);

@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
       uint32_t* fmask = bv.fstate + (uint64_t)gwarp * 2 * colors;
       uint32_t* frun = fmask + colors;
       const FindereSink fs{fmask};
-      probe_rows(ix, keys, npos, kvalid, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
+      probe_rows<MINB == 1>(ix, keys, npos, kvalid, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
                  splanes, pbase, fs, lane, [&](uint32_t r0, uint32_t m) {
                    findere_sweep(fmask, frun, colors, z, m, r0 + m >= npos, cnt, lane);
                    __syncwarp();
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
         break;
       }
     } else if (VARIANT == 2) {
-      probe_rows(ix, keys, n, nullptr, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
+      probe_rows<MINB == 1>(ix, keys, n, nullptr, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
                  splanes, pbase, CountSink{cnt}, lane, [](uint32_t, uint32_t) {});
     } else {
       probe_batch(ix, keys, n, desc, row0s, lc.team, cnt, lane);

@@ -33,7 +33,8 @@ struct QueryLaunch {
   int stage_bytes;    // > 0: staged gather with this stage size per warp
   int stages;         // stages in each warp's ring (staged gather)
   int bulk;           // staged gather: 1 = bulk copy per row slice, 0 = 16-byte cp.async
-  int min_blocks;     // kernel variant compiled for 2 or 3 resident 256-thread blocks/SM
+  int min_blocks;     // register budget: 1 (255 registers; row-index form with the chunk
+                      // pipeline), 2 or 3 resident 256-thread blocks per SM
   int planes;         // register gather: 1 = row indices + bit-plane colour counters, 0 = descriptors
   int cut;            // host batches: pipelined chunks (copy of chunk i+1 overlaps chunk i), 1..64
 };

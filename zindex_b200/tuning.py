@@ -28,7 +28,7 @@ TEAMS = (2, 4, 8, 16, 32)
 WARPS = (2, 4, 8)
 STAGE_BYTES = (4096, 8192, 16384)
 STAGES = (2, 3, 4)
-MIN_BLOCKS = (2, 3)
+MIN_BLOCKS = (1, 2, 3)
 PLANES = (0, 1)
 
 
@@ -53,6 +53,8 @@ class Autotuner:
         out = []
         if register_gather:
             for team, warps, minb, planes in itertools.product(TEAMS, WARPS, MIN_BLOCKS, PLANES):
+                if minb == 1 and not planes:
+                    continue
                 out.append({"team": team, "warps": warps, "blocks": 0, "smem_counters": smem,
                             "stage_bytes": 0, "stages": 1, "bulk": 0, "min_blocks": minb,
                             "planes": planes})
@@ -172,7 +174,8 @@ SETTINGS = [
     ("k63-H4-b8-c128-long", dict(mode="kmers", k=63, H=4, b=8), (128, 100_000, 800_000), ("long", 4000, 4000)),
 ]
 REGISTER_LAUNCHES = [dict(team=t, warps=w, min_blocks=mb, planes=pl)
-                     for t in (2, 4, 8, 16, 32) for w in (4, 8) for mb in (2, 3) for pl in (0, 1)]
+                     for t in (2, 4, 8, 16, 32) for w in (2, 4, 8) for pl in (0, 1)
+                     for mb in ((1, 2, 3) if pl else (2, 3))]
 CUTS = (1, 2, 4, 8, 16)
 
 
