@@ -73,9 +73,11 @@ def test_training_fits_and_prediction_matches_cpu(gpu):
 
 def test_planner_gain_over_default_and_regret(gpu):
     """Leave-one-setting-out on the committed autotuner measurements: for each
-    setting the planner is trained on the others' timings only, chooses among
-    that setting's measured launches (and cuts), and is scored against the
-    exhaustive best (regret) and the default launch (gain)."""
+    setting the planner is trained on the other settings' timings only, ranks
+    that setting's launches, and its shortlist (3 predictions and the default)
+    is scored with the measured times against the exhaustive best over all
+    candidates (regret) and the default launch (gain); the cut decision is
+    scored the same way on the end-to-end rows."""
     from zindex_b200 import planner as pl
 
     rows, defaults = pl.load_rows()
@@ -91,13 +93,16 @@ def test_planner_gain_over_default_and_regret(gpu):
     gm = lambda v: float(np.exp(np.mean(np.log(v))))
     gain = gm([r["gain_over_default"] for r in dev])
     regret = gm([1 + r["regret"] for r in dev]) - 1
+    top1 = gm([r["top1_gain_over_default"] for r in dev])
+    timed = float(np.mean([r["timed_per_setting"] for r in dev]))
+    cands = float(np.mean([r["candidates_per_setting"] for r in dev]))
     e2e_gain = gm([r["gain_over_default"] for r in e2e])
-    print(f"launch: gain over the default {gain:.3f}, regret {regret:.3f}; "
+    print(f"launch: gain over the default {gain:.3f}, regret {regret:.3f} with {timed:.1f} of "
+          f"{cands:.0f} candidates timed (network's top pick alone: {top1:.3f}); "
           f"cut: gain over the default {e2e_gain:.3f}")
-    # Measured timings are the ground truth: the planner's launches must beat
-    # the default launch on average and stay near the exhaustive best; its cut
-    # decision (little headroom: the default cut was within 2% of the best)
-    # must not lose more than a few percent.
-    assert gain >= 1.0
-    assert regret <= 0.15
+    # The default launch is itself fitted to these measurements, so the gain
+    # is over a strong baseline; the shortlist can only match or beat it.
+    assert gain >= 1.02
+    assert regret <= 0.08
+    assert timed <= 4.0 and cands >= 40
     assert e2e_gain >= 0.95

@@ -638,13 +638,16 @@ QueryLaunch Engine::default_launch() const {
   // Row-index gather with bit-plane counters, 8 warps per block, 2 resident
   // blocks per SM: teams of up to 16 lanes (one 16-byte chunk each) measured
   // fastest on B200 for 256-byte fingerprint rows (22.8 ms against 40.6 ms
-  // for the per-hit form on 1.2e8 seeds); wider rows use whole-warp teams so
-  // that each lane's fields fit few shared-plane words. Shared memory above
+  // for the per-hit form on 1.2e8 seeds); wider rows use teams of 8 or 16
+  // and count in shared planes. Shared memory above
   // 110 KB per block moves the colour counters to global atomics (flushed
   // planes make them rare), then halves the warps; the per-hit form is the
   // last fallback.
   QueryLaunch l;
-  l.team = std::min(team, chunks > 16 ? 32 : 16);
+  // Measured on B200 over 14 index geometries (the planner's training set):
+  // rows of up to 16 chunks run best with one chunk per lane, rows of 17-64
+  // chunks with teams of 8, wider rows with teams of 16.
+  l.team = chunks <= 16 ? team : (chunks <= 64 ? 8 : 16);
   l.warps = 8;
   l.smem_counters = m_.colors.size() <= 16384 ? 1 : 0;
   l.blocks = 0;  // 0: fill the device (occupancy-derived)
@@ -663,11 +666,6 @@ QueryLaunch Engine::default_launch() const {
     l.smem_counters = 0;
   if (fused_smem_bytes(l) > budget) l.warps = 4;
   if (fused_smem_bytes(l) > budget) l.warps = 2;
-  // Wide rows counted in shared planes with H <= 4: the 255-register variant
-  // keeps two stages of row chunks in flight per lane.
-  if (FusedSmem::shared_words(sp_.mode, host_ix_, l) > 0 && m_.hashes <= 4 &&
-      fused_smem_bytes(l) <= budget)
-    l.min_blocks = 1;
   if (fused_smem_bytes(l) > budget) {
     l.warps = 8;
     l.planes = 0;
