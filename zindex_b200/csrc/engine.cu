@@ -644,10 +644,11 @@ QueryLaunch Engine::default_launch() const {
   // planes make them rare), then halves the warps; the per-hit form is the
   // last fallback.
   QueryLaunch l;
-  // Measured on B200 over 14 index geometries (the planner's training set):
-  // rows of up to 16 chunks run best with one chunk per lane, rows of 17-64
-  // chunks with teams of 8, wider rows with teams of 16.
-  l.team = chunks <= 16 ? team : (chunks <= 64 ? 8 : 16);
+  // Measured on B200 over 14 index geometries (the planner's training set)
+  // and the wide-row workloads: rows of up to 16 chunks run best with one
+  // chunk per lane, rows of 17-64 chunks with teams of 8, wider rows with
+  // whole-warp teams (512-chunk rows: 64 ms against 142 ms with teams of 16).
+  l.team = chunks <= 16 ? team : (chunks <= 64 ? 8 : 32);
   l.warps = 8;
   l.smem_counters = m_.colors.size() <= 16384 ? 1 : 0;
   l.blocks = 0;  // 0: fill the device (occupancy-derived)
