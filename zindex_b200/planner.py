@@ -11,9 +11,9 @@ with the lowest prediction. Two decisions are made per incoming batch:
 
 The network (hidden 32, ReLU) is trained by the library's own CUDA forward,
 backward and Adam kernels (zx_mlp_* in include/zindex.h) on rows measured by
-the autotuner (zindex_b200.tuning). Launches are chosen by verification: the
-network ranks all candidates, the top few and the default launch are timed on
-the batch, and the fastest wins, so a plan is never slower than the default
+the autotuner (zindex_b200.tuning). Launches and cuts are chosen by
+verification: the network ranks all candidates, its top few and the default
+are timed on the batch, and the fastest wins, so a plan is never slower than the default
 (up to timing noise) and costs a handful of timings instead of an exhaustive
 search, which stays the fallback and the judge of its regret. The planner
 never changes results: every launch configuration and cut gives the same
@@ -213,10 +213,11 @@ class Planner:
         return dict(launches[k])
 
     def shortlist(self, features: Dict[str, float], launches: Sequence[Dict[str, int]],
-                  default: Dict[str, int], k: int = SHORTLIST) -> List[Dict[str, int]]:
+                  default: Dict[str, int], k: int = SHORTLIST,
+                  e2e: bool = False) -> List[Dict[str, int]]:
         """The k candidates with the lowest predicted time, then the default
         (without duplicates): the launches worth timing on the batch."""
-        order = np.argsort(self.predict_cost(features, launches))
+        order = np.argsort(self.predict_cost(features, launches, e2e))
         out, seen = [], set()
         for i in list(order[:k]):
             key = launch_key(launches[int(i)])
@@ -256,7 +257,7 @@ def evaluate(planner: Planner, rows: Sequence[Row], default: Dict[str, int],
     means over settings. Device rows: the shortlist is "timed" by reading its
     measured times (the fastest of the k predictions and the default wins),
     and the network's top prediction alone is scored too. End-to-end rows:
-    the cut decision with its margin."""
+    the network's best cut and the default cut, the faster kept."""
     by: Dict[str, List[Row]] = {}
     for r in rows:
         if r.e2e == e2e:
@@ -270,10 +271,10 @@ def evaluate(planner: Planner, rows: Sequence[Row], default: Dict[str, int],
         best = min(r.ms for r in rs)
         launches = [r.launch for r in rs]
         if e2e:
-            pick = planner.choose(rs[0].features, launches, True, default=default,
-                                  margin=CUT_MARGIN)
-            chosen = table[launch_key(pick)].ms
-            timed.append(1)
+            # The network's best cut and the default, timed end to end.
+            short = planner.shortlist(rs[0].features, launches, default, 1, e2e=True)
+            chosen = min(table[launch_key(l)].ms for l in short)
+            timed.append(len(short))
         else:
             short = planner.shortlist(rs[0].features, launches, default, k)
             chosen = min(table[launch_key(l)].ms for l in short)
