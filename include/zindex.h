@@ -156,9 +156,12 @@ int zx_get_launch(const zx_index* index, zx_launch* out);
 int zx_set_launch(zx_index* index, const zx_launch* launch);
 int zx_default_launch(const zx_index* index, zx_launch* out);
 
-/* Status of the last asynchronous zx_query_device calls of this index: ZX_OK,
- * or ZX_ETIMEOUT when a bounded device wait expired (counts incomplete). The
- * device error word is cleared. Synchronous calls report it directly. */
+/* Status of the last asynchronous zx_query_device / zx_query_device_noalloc
+ * calls of this index: ZX_OK; ZX_EINVAL when record offsets were invalid
+ * (decreasing, past the bases, or a record of 2^31 bases or more: those
+ * records were skipped, counts incomplete); ZX_ETIMEOUT when a bounded device
+ * wait expired. The device error words are cleared. Synchronous calls report
+ * these directly. */
 int zx_query_status(zx_index* index);
 
 /* Measurement hook: with timing on, zx_query_device calls made with

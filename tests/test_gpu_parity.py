@@ -236,6 +236,54 @@ def test_wide_rows_shared_planes(gpu, oracle, tmp_path_factory, colors, H, b, gr
             np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.parametrize("mode", ["kmers", "homopolymer"])
+def test_invalid_offsets_are_reported_and_skipped(gpu, oracle, tmp_path_factory, mode):
+    """Decreasing interior offsets (and offsets past the bases) are checked on
+    the device: the query fails with ZX_EINVAL, no memory outside the batch is
+    touched, and the index keeps answering correctly."""
+    import torch
+
+    import zindex_b200 as zx
+
+    opts = dict(mode="kmers", k=31, H=4, b=8, homopolymer=(mode == "homopolymer"))
+    ix, genomes = index_for(tmp_path_factory, colors=4, length=20000, seed=71, **opts)
+    reads = reads_for(genomes, n=2000, length=150)
+    bases, offsets = zx.pack_records(reads)
+    bad = offsets.copy()
+    bad[5] = bad[7] + 40          # record 5 ends before it starts; record 4 runs long
+    bad[9] = len(bases) + 10**9   # an interior offset past the bases
+    want, want_total = oracle.query_records(ix, bases, offsets)
+    with zx.Index(ix) as index:
+        with pytest.raises(zx.ZxError) as err:
+            index.query_records(bases, bad)
+        assert err.value.code == 1 and "offsets" in str(err.value)
+        got, total = index.query_records(bases, offsets)
+        assert total == want_total
+        np.testing.assert_array_equal(got, want)
+        dev = torch.device("cuda", 0)
+        d_b = torch.from_numpy(bases).to(dev)
+        d_bad = torch.from_numpy(bad.view(np.int64)).to(dev)
+        counts = torch.zeros(index.colors, dtype=torch.int64, device=dev)
+        total_d = torch.zeros(1, dtype=torch.int64, device=dev)
+        for fn in (lambda: index.query_device(d_b.data_ptr(), len(bases), d_bad.data_ptr(),
+                                              len(reads), counts.data_ptr(), total_d.data_ptr(),
+                                              use_graph=False),
+                   lambda: index.query_device_noalloc(d_b.data_ptr(), len(bases), d_bad.data_ptr(),
+                                                      len(reads), counts.data_ptr(),
+                                                      total_d.data_ptr())):
+            try:
+                fn()
+            except zx.ZxError:
+                continue  # refused before any launch
+            torch.cuda.synchronize(dev)
+            with pytest.raises(zx.ZxError) as err:
+                index.query_status()
+            assert err.value.code == 1
+        got, total = index.query_records(bases, offsets)
+        assert total == want_total
+        np.testing.assert_array_equal(got, want)
+
+
 def test_multi_member_groups(gpu, oracle, tmp_path_factory):
     ix, genomes = index_for(tmp_path_factory, colors=8, mode="kmers", k=31, H=4, b=4,
                             groups="0,1,2;3,5;6,7")

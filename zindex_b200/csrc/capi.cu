@@ -218,8 +218,11 @@ int zx_query_status(zx_index* index) {
     zx::check(index, zx::kEInval, "null argument");
     std::lock_guard<std::mutex> lock(index->mu);
     auto& e = *index->engine;
-    if (e.take_error(e.default_workspace()))
-      zx::raise(zx::kETimeout, "a bounded device wait expired during a query");
+    const uint32_t err = e.take_error(e.default_workspace()) | e.take_noalloc_error();
+    if (err & zx::kErrOffsets)
+      zx::raise(zx::kEInval, "record offsets of an asynchronous query were invalid (decreasing, "
+                             "past the bases or spanning 2^31 bases); those records were skipped");
+    if (err) zx::raise(zx::kETimeout, "a bounded device wait expired during a query");
   });
 }
 

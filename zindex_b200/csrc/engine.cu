@@ -141,12 +141,14 @@ ExtractFn extract_for(int mode) {
 // ---- homopolymer compression of a batch (lib.rs:211-222, applied per ACGT
 // run by scan_index_features, lib.rs:574-589): inside a run of A/C/G/T a base
 // equal to the one before it is dropped; other bytes are kept as separators.
+// Offsets are not trusted here (the tile planner reports bad ones): a start
+// past the bases is ignored and positions are read at min(offset, nbases).
 __global__ void hp_mark_starts_kernel(const uint64_t* __restrict__ offsets, uint64_t records,
-                                      uint32_t* __restrict__ starts) {
+                                      uint64_t nbases, uint32_t* __restrict__ starts) {
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < records;
        r += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t p = offsets[r];
-    atomicOr(starts + (p >> 5), 1u << (p & 31));
+    if (p < nbases) atomicOr(starts + (p >> 5), 1u << (p & 31));
   }
 }
 
@@ -172,10 +174,14 @@ __global__ void hp_compact_kernel(const uint8_t* __restrict__ bases, uint64_t nb
 }
 
 __global__ void hp_offsets_kernel(const uint64_t* __restrict__ offsets, uint64_t records,
-                                  const uint32_t* __restrict__ pos, uint64_t* __restrict__ out) {
+                                  uint64_t nbases, const uint32_t* __restrict__ pos,
+                                  uint64_t* __restrict__ out) {
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r <= records;
-       r += (uint64_t)gridDim.x * blockDim.x)
-    out[r] = pos[offsets[r]];
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t o = offsets[r];
+    // An offset past the bases stays invalid for the tile planner.
+    out[r] = o <= nbases ? pos[o] : ~0ull;
+  }
 }
 
 // offsets[i] -= base (chunk-relative record offsets after a raw copy).
@@ -307,6 +313,7 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
         "the allocation-free query does not run homopolymer compression (the compressed batch "
         "needs scratch of its own): use zx_query_device");
   uint8_t* base = static_cast<uint8_t*>(noalloc_scratch(device_));
+  noalloc_used_ = true;
   const uint64_t words = nbases / 32 + 2;
   const uint64_t tiles = nbases / kTileWindows + nbases / kFindereTask + records + 16;
   // Register gather, colour counts added straight into the caller's counters.
@@ -359,7 +366,8 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
   const int findere = m_.index_mode == kFindere;
   int rgrid = std::max(1, (int)std::min<uint64_t>((records + 255) / 256, (uint64_t)sms_ * 16));
   if (records) {
-    count_tiles_kernel<<<rgrid, 256, 0, s>>>(offsets, records, span(), findere, tile_counts);
+    count_tiles_kernel<<<rgrid, 256, 0, s>>>(offsets, records, nbases, span(), findere,
+                                             tile_counts, err);
     cuda_check(cudaGetLastError(), "count_tiles_kernel");
   }
   size_t tmp = scan_bytes;
@@ -367,7 +375,8 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
                                            (int)(records + 1), s),
              "tile scan");
   if (records) {
-    fill_tiles_kernel<<<rgrid, 256, 0, s>>>(offsets, records, span(), tile_first, tile_list);
+    fill_tiles_kernel<<<rgrid, 256, 0, s>>>(offsets, records, nbases, span(), tile_first,
+                                            tile_list);
     cuda_check(cudaGetLastError(), "fill_tiles_kernel");
   }
   BatchView bv{PackedView{packed, invalid}, offsets, tile_list, tile_first + records, fstate};
@@ -867,7 +876,7 @@ void Engine::compress_homopolymers(Workspace& ws, const uint8_t*& bases, uint64_
   const int bgrid = std::max(1, (int)std::min<uint64_t>((nbases + 256) / 256, (uint64_t)sms_ * 16));
   const int rgrid = std::max(1, (int)std::min<uint64_t>((records + 256) / 256, (uint64_t)sms_ * 16));
   cuda_check(cudaMemsetAsync(ws.hp_starts, 0, (nbases / 32 + 2) * 4, s), "memset");
-  if (records) hp_mark_starts_kernel<<<rgrid, 256, 0, s>>>(offsets, records, ws.hp_starts);
+  if (records) hp_mark_starts_kernel<<<rgrid, 256, 0, s>>>(offsets, records, nbases, ws.hp_starts);
   hp_keep_kernel<<<bgrid, 256, 0, s>>>(bases, nbases, ws.hp_starts, ws.hp_keep);
   cuda_check(cudaGetLastError(), "hp_keep_kernel");
   size_t tmp = ws.hp_scan_bytes;
@@ -875,20 +884,21 @@ void Engine::compress_homopolymers(Workspace& ws, const uint8_t*& bases, uint64_
                                            (int)(nbases + 1), s),
              "homopolymer scan");
   hp_compact_kernel<<<bgrid, 256, 0, s>>>(bases, nbases, ws.hp_pos, ws.hp_bases);
-  hp_offsets_kernel<<<rgrid, 256, 0, s>>>(offsets, records, ws.hp_pos, ws.hp_offsets);
+  hp_offsets_kernel<<<rgrid, 256, 0, s>>>(offsets, records, nbases, ws.hp_pos, ws.hp_offsets);
   cuda_check(cudaGetLastError(), "hp_offsets_kernel");
   bases = ws.hp_bases;
   offsets = ws.hp_offsets;
 }
 
 void Engine::plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records,
-                        cudaStream_t s) {
+                        uint64_t nbases, cudaStream_t s) {
   const int findere = m_.index_mode == kFindere;
   int grid = (int)std::min<uint64_t>((records + 255) / 256, (uint64_t)sms_ * 16);
   grid = std::max(grid, 1);
   cuda_check(cudaMemsetAsync(ws.tile_counts + records, 0, 4, s), "memset");
   if (records) {
-    count_tiles_kernel<<<grid, 256, 0, s>>>(offsets, records, span(), findere, ws.tile_counts);
+    count_tiles_kernel<<<grid, 256, 0, s>>>(offsets, records, nbases, span(), findere,
+                                            ws.tile_counts, ws.error);
     cuda_check(cudaGetLastError(), "count_tiles_kernel");
   }
   size_t tmp = ws.scan_tmp_bytes;
@@ -896,7 +906,8 @@ void Engine::plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records
                                            (int)(records + 1), s),
              "tile scan");
   if (records) {
-    fill_tiles_kernel<<<grid, 256, 0, s>>>(offsets, records, span(), ws.tile_first, ws.tiles);
+    fill_tiles_kernel<<<grid, 256, 0, s>>>(offsets, records, nbases, span(), ws.tile_first,
+                                           ws.tiles);
     cuda_check(cudaGetLastError(), "fill_tiles_kernel");
   }
 }
@@ -911,7 +922,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     pack_kernel<<<std::max(grid, 1), 256, 0, s>>>(bases, nbases, ws.packed, ws.invalid, words);
     cuda_check(cudaGetLastError(), "pack_kernel");
   }
-  plan_tiles(ws, offsets, records, s);
+  plan_tiles(ws, offsets, records, nbases, s);
   QueryLaunch l = launch_;
   const size_t smem = fused_smem_bytes(l);
   const int blocks_cap = max_blocks(l);
@@ -964,6 +975,8 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   check(segments > 0, kEInval, "a segmented query needs at least one segment");
   check(seg_records[0] == 0 && seg_records[segments] == records, kEInval,
         "segments must span the records");
+  for (uint32_t i = 0; i < segments; ++i)
+    check(seg_records[i] <= seg_records[i + 1], kEInval, "segment records must be non-decreasing");
   ensure_capacity(ws, nbases, records);
   QueryLaunch l = launch_;
   const int cap = max_blocks(l);
@@ -1026,7 +1039,7 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
     pack_kernel<<<std::max(grid, 1), 256, 0, s>>>(bases, nbases, ws.packed, ws.invalid, words);
     cuda_check(cudaGetLastError(), "pack_kernel");
   }
-  plan_tiles(ws, offsets, records, s);
+  plan_tiles(ws, offsets, records, nbases, s);
   segment_tiles_kernel<<<(segments + 256) / 256, 256, 0, s>>>(ws.tile_first, ws.seg_records,
                                                               segments, ws.seg_tiles);
   cuda_check(cudaGetLastError(), "segment_tiles_kernel");
@@ -1051,13 +1064,30 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   }
 }
 
+static void raise_error_word(uint32_t err) {
+  if (err & kErrOffsets)
+    raise(kEInval, "record offsets must be non-decreasing, end within the bases and span fewer "
+                   "than 2^31 bases (offending records were skipped; counts are incomplete)");
+  if (err) raise(kETimeout, "a bounded device wait expired during the query");
+}
+
 void Engine::check_error_word(Workspace& ws) {
   uint32_t err = 0;
   cuda_check(cudaMemcpy(&err, ws.error, 4, cudaMemcpyDeviceToHost), "error word");
   if (err) {
     cuda_check(cudaMemset(ws.error, 0, 4), "memset");
-    raise(kETimeout, "a bounded device wait expired during the query");
+    raise_error_word(err);
   }
+}
+
+uint32_t Engine::take_noalloc_error() {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  if (!noalloc_used_) return 0;
+  uint32_t* err = static_cast<uint32_t*>(noalloc_scratch(device_));
+  uint32_t v = 0;
+  cuda_check(cudaMemcpy(&v, err, 4, cudaMemcpyDeviceToHost), "error word");
+  if (v) cuda_check(cudaMemset(err, 0, 4), "memset");
+  return v;
 }
 
 uint32_t Engine::take_error(Workspace& ws) {
@@ -1108,9 +1138,9 @@ void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                         const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
                         uint64_t* total) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  // Offsets are checked per record by the tile planner on the device
+  // (kErrOffsets): a host pass over a million records cost about 1 ms.
   check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
-  for (uint64_t r = 0; r < records; ++r)
-    check(offsets[r] <= offsets[r + 1], kEInval, "offsets must be non-decreasing");
   // Chunks: record-aligned cuts near multiples of nbases / cut, at least
   // 1 MiB of bases each.
   const uint64_t min_chunk = 1ull << 20;
@@ -1124,6 +1154,10 @@ void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   }
   bounds.push_back(records);
   const uint64_t chunks = bounds.size() - 1;
+  // Chunk copies must stay inside the batch whatever the interior offsets.
+  for (uint64_t c = 0; c < chunks; ++c)
+    check(offsets[bounds[c]] <= offsets[bounds[c + 1]] && offsets[bounds[c + 1]] <= nbases, kEInval,
+          "offsets must be non-decreasing");
   ensure_capacity(ws, nbases, records + chunks);
   ensure_host_capacity(ws, nbases, records + chunks);
   const uint64_t colors = m_.colors.size();
@@ -1195,6 +1229,8 @@ void Engine::query_host_plain(Workspace& ws, const uint8_t* bases, uint64_t nbas
                               uint64_t* counts, uint64_t* total) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
+  for (uint64_t r = 0; r < records; ++r)  // records are sliced on the host here
+    check(offsets[r] <= offsets[r + 1], kEInval, "offsets must be non-decreasing");
   ensure_capacity(ws, nbases, records);
   ensure_host_capacity(ws, nbases, records);
   const uint64_t colors = m_.colors.size();
@@ -1243,7 +1279,7 @@ void Engine::extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   pack_kernel<<<std::max<int>(1, (int)std::min<uint64_t>((words + 255) / 256, sms_ * 16ull)), 256, 0, s>>>(
       d_bases, nbases, ws.packed, ws.invalid, words);
   cuda_check(cudaGetLastError(), "pack_kernel");
-  plan_tiles(ws, d_offsets, records, s);
+  plan_tiles(ws, d_offsets, records, nbases, s);
   uint32_t ntiles = 0;
   cuda_check(cudaMemcpyAsync(&ntiles, ws.tile_first + records, 4, cudaMemcpyDeviceToHost, s), "D2H");
   cuda_check(cudaStreamSynchronize(s), "tiles");
@@ -1274,6 +1310,7 @@ void Engine::extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   cuda_check(cudaMemcpyAsync(cnt.data(), ws.keys_count, ntiles * 4ull, cudaMemcpyDeviceToHost, s),
              "D2H");
   cuda_check(cudaStreamSynchronize(s), "extract");
+  check_error_word(ws);
   keys.clear();
   for (uint32_t t = 0; t < ntiles; ++t)
     keys.insert(keys.end(), all.begin() + (uint64_t)t * kTileWindows,

@@ -132,6 +132,9 @@ class Engine {
   // Device error word of a workspace (read and cleared); nonzero means a
   // bounded wait expired and the query's counts are incomplete.
   uint32_t take_error(Workspace& ws);
+  // Error word of the allocation-free query's scratch on this device (read
+  // and cleared; 0 if that entry point was never used by this engine).
+  uint32_t take_noalloc_error();
   // Asynchronous query of several requests coalesced into one launch: the
   // batch's records are the requests' records back to back, request s owning
   // records seg_records[s] .. seg_records[s+1]-1 (host array, segments + 1
@@ -159,7 +162,8 @@ class Engine {
   void enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
                uint64_t records, bool recover, uint64_t* counts, unsigned long long* total,
                cudaStream_t stream);
-  void plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records, cudaStream_t stream);
+  void plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records, uint64_t nbases,
+                  cudaStream_t stream);
   void check_error_word(Workspace& ws);
 
   Manifest m_;
@@ -177,6 +181,7 @@ class Engine {
   bool timing_ = false;
   cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
   int cached_blocks_ = 0;
+  bool noalloc_used_ = false;
   QueryLaunch cached_for_{};
 };
 

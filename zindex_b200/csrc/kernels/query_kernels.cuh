@@ -20,18 +20,28 @@ namespace zx {
 constexpr uint32_t kTileWindows = 256;
 constexpr uint32_t kFindereTask = 16384;  // src/findere.rs:13-16
 
-// Windows of record r: k-windows fully inside the record.
-__device__ __forceinline__ uint32_t record_windows(const uint64_t* offsets, uint64_t r, int span) {
-  uint64_t len = offsets[r + 1] - offsets[r];
+// Windows of record r: k-windows fully inside the record. A record whose
+// offsets decrease, pass the end of the bases or span 2^31 bases or more has
+// no windows and sets kErrOffsets (the query then fails with ZX_EINVAL), so
+// no tile ever points outside the batch.
+__device__ __forceinline__ uint32_t record_windows(const uint64_t* offsets, uint64_t r, int span,
+                                                   uint64_t nbases, uint32_t* err) {
+  const uint64_t a = offsets[r], b = offsets[r + 1];
+  if (a > b || b > nbases || b - a >= (1ull << 31)) {
+    if (err) atomicOr(err, kErrOffsets);
+    return 0u;
+  }
+  const uint64_t len = b - a;
   return len >= (uint64_t)span ? (uint32_t)(len - span + 1) : 0u;
 }
 
 // Tiles per record. Findere tiles never cross a 16,384-window task.
 __global__ void count_tiles_kernel(const uint64_t* __restrict__ offsets, uint64_t records,
-                                   int span, int findere, uint32_t* __restrict__ counts) {
+                                   uint64_t nbases, int span, int findere,
+                                   uint32_t* __restrict__ counts, uint32_t* __restrict__ err) {
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < records;
        r += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t w = record_windows(offsets, r, span);
+    uint32_t w = record_windows(offsets, r, span, nbases, err);
     uint32_t n;
     if (!findere) {
       n = (w + kTileWindows - 1) / kTileWindows;
@@ -43,11 +53,12 @@ __global__ void count_tiles_kernel(const uint64_t* __restrict__ offsets, uint64_
   }
 }
 
-__global__ void fill_tiles_kernel(const uint64_t* __restrict__ offsets, uint64_t records, int span,
-                                  const uint32_t* __restrict__ first, Tile* __restrict__ tiles) {
+__global__ void fill_tiles_kernel(const uint64_t* __restrict__ offsets, uint64_t records,
+                                  uint64_t nbases, int span, const uint32_t* __restrict__ first,
+                                  Tile* __restrict__ tiles) {
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < records;
        r += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t w = record_windows(offsets, r, span);
+    uint32_t w = record_windows(offsets, r, span, nbases, nullptr);
     uint32_t t = first[r];
     for (uint32_t w0 = 0; w0 < w;) {
       uint32_t task = (w0 / kFindereTask) * kFindereTask;

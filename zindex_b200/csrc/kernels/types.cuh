@@ -7,6 +7,10 @@
 
 namespace zx {
 
+// Bits of a query's device error word.
+constexpr uint32_t kErrWait = 1u;     // a bounded wait expired (staged gather)
+constexpr uint32_t kErrOffsets = 2u;  // a record's offsets decrease, leave the bases, or span 2^31
+
 struct SeedParams {
   int mode;        // 0 kmers, 1 minimizers, 2 modimizers, 3 findere
   int k;           // window span (k-mer length, minimizer window, findere k)
