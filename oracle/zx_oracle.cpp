@@ -1068,6 +1068,161 @@ void run_query(const Index& ix, const Work& w, int threads, std::vector<uint64_t
     for (size_t c = 0; c < C; ++c) counts[c] += p[c];
 }
 
+// ------------------------------------------------------- per-record query ---
+// query_records_command_with_memory (src/power_merge/storage.rs:3626-3720).
+
+struct NamedRecord {
+  std::string name;
+  std::vector<uint8_t> seq;
+};
+
+// read_batches (src/power_merge/records.rs:150-290): trailing whitespace of a
+// line is dropped and empty lines are skipped; the first line decides FASTQ
+// ('@') or FASTA; the identifier is the header up to the first whitespace;
+// sequence lines may not contain whitespace; FASTQ qualities are consumed by
+// length.
+std::vector<NamedRecord> parse_named_records(const std::vector<uint8_t>& d) {
+  std::vector<NamedRecord> out;
+  size_t i = 0;
+  auto next_line = [&](std::string& line) {
+    if (i >= d.size()) return false;
+    size_t e = i;
+    while (e < d.size() && d[e] != '\n') ++e;
+    line.assign((const char*)d.data() + i, e - i);
+    i = e < d.size() ? e + 1 : e;
+    return true;
+  };
+  auto is_ws = [](char c) {
+    return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\f' || c == '\v';
+  };
+  auto ident = [&](const std::string& line, const char* what) {
+    size_t e = 1;
+    while (e < line.size() && !is_ws(line[e])) ++e;
+    std::string id = line.substr(1, e - 1);
+    ensure(!id.empty(), (std::string("empty ") + what + " identifier").c_str());
+    return id;
+  };
+  int fastq = -1;
+  std::string line;
+  bool have = false;
+  while (next_line(line)) {
+    while (!line.empty() && is_ws(line.back())) line.pop_back();
+    if (line.empty()) continue;
+    if (fastq == 1 || (fastq == -1 && line[0] == '@')) {
+      fastq = 1;
+      ensure(line[0] == '@', "expected FASTQ identifier");
+      NamedRecord r;
+      r.name = ident(line, "FASTQ");
+      for (;;) {
+        ensure(next_line(line), "truncated FASTQ sequence");
+        while (!line.empty() && (line.back() == '\n' || line.back() == '\r')) line.pop_back();
+        if (!line.empty() && line[0] == '+') break;
+        for (char c : line) ensure(!is_ws(c), "whitespace inside FASTQ sequence");
+        r.seq.insert(r.seq.end(), line.begin(), line.end());
+      }
+      size_t q = 0;
+      while (q < r.seq.size()) {
+        ensure(next_line(line), "truncated FASTQ quality");
+        while (!line.empty() && (line.back() == '\n' || line.back() == '\r')) line.pop_back();
+        q += line.size();
+        ensure(q <= r.seq.size(), "FASTQ sequence and quality lengths differ");
+      }
+      out.push_back(std::move(r));
+      continue;
+    }
+    fastq = 0;
+    if (line[0] == '>') {
+      NamedRecord r;
+      r.name = ident(line, "FASTA");
+      out.push_back(std::move(r));
+      have = true;
+    } else {
+      ensure(have, "--records requires FASTA or FASTQ");
+      for (char c : line) ensure(!is_ws(c), "whitespace inside FASTA sequence");
+      out.back().seq.insert(out.back().seq.end(), line.begin(), line.end());
+    }
+  }
+  return out;
+}
+
+// write_field (src/power_merge/record_output.rs:64-80): CSV quoting of names
+// holding a tab, CR, LF or quote.
+void write_field(std::string& out, const std::string& v) {
+  if (v.find_first_of("\t\r\n\"") == std::string::npos) {
+    out += v;
+    return;
+  }
+  out += '"';
+  for (char c : v) {
+    out += c;
+    if (c == '"') out += '"';
+  }
+  out += '"';
+}
+
+const char* records_header(bool compact) {
+  return compact ? "query_id\tvalid_kmers\thits"
+                 : "query_id\tdataset_id\tdataset_name\tmatches\tqueried_seeds\tratio";
+}
+
+// RecordScores::write_record (storage.rs:3109-3146) and
+// RecordFormat::write_record (record_output.rs:21-62): with min_ratio 0 every
+// colour is reported, otherwise the touched colours in id order whose ratio
+// reaches min_ratio.
+void format_record(const Index& ix, const std::string& name, uint64_t total,
+                   const std::vector<uint64_t>& counts, double min_ratio, bool compact,
+                   std::string& out) {
+  std::vector<std::pair<size_t, uint64_t>> hits;
+  for (size_t c = 0; c < counts.size(); ++c) {
+    if (min_ratio > 0.0 && (total == 0 || counts[c] == 0)) continue;
+    double ratio = total == 0 ? 0.0 : (double)counts[c] / (double)total;
+    if (ratio >= min_ratio) hits.emplace_back(c, counts[c]);
+  }
+  char buf[96];
+  if (compact) {
+    out += name;
+    snprintf(buf, sizeof buf, "\t%llu\t", (unsigned long long)total);
+    out += buf;
+    for (size_t i = 0; i < hits.size(); ++i) {
+      snprintf(buf, sizeof buf, i ? ",%zu:%llu" : "%zu:%llu", hits[i].first,
+               (unsigned long long)hits[i].second);
+      out += buf;
+    }
+    out += '\n';
+    return;
+  }
+  for (auto& h : hits) {
+    write_field(out, name);
+    snprintf(buf, sizeof buf, "\t%zu\t", h.first);
+    out += buf;
+    write_field(out, ix.colors[h.first].name);
+    double ratio = total == 0 ? 0.0 : (double)h.second / (double)total;
+    snprintf(buf, sizeof buf, "\t%llu\t%llu\t%.8f\n", (unsigned long long)h.second,
+             (unsigned long long)total, ratio);
+    out += buf;
+  }
+  if (hits.empty()) {
+    write_field(out, name);
+    snprintf(buf, sizeof buf, "\t.\t.\t0\t%llu\t0.00000000\n", (unsigned long long)total);
+    out += buf;
+  }
+}
+
+// Per-record counts and totals of named records (each record queried alone).
+std::string query_records_output(const Index& ix, const std::vector<NamedRecord>& recs,
+                                 double min_ratio, bool compact) {
+  std::string out = records_header(compact);
+  out += '\n';
+  for (auto& r : recs) {
+    Work w;
+    prepare_record(ix.f, r.seq.data(), r.seq.size(), w);
+    std::vector<uint64_t> counts;
+    run_query(ix, w, 1, counts);
+    format_record(ix, r.name, w.total, counts, min_ratio, compact, out);
+  }
+  return out;
+}
+
 int guarded(const std::function<void()>& body) {
   try {
     body();
@@ -1235,6 +1390,20 @@ int oracle_query_timed(const char* index_dir, const uint8_t* bases, const uint64
   });
 }
 
+// Per-record report of a query file (TSV or compact), as
+// `zorindex query --records` prints it.
+int oracle_query_records_report(const char* index_dir, const char* query_path, int recover,
+                                double min_ratio, int compact, char* buf, size_t cap,
+                                size_t* written) {
+  return guarded([&] {
+    auto ix = load_index(index_dir, recover != 0);
+    std::string s = query_records_output(*ix, parse_named_records(read_decoded(query_path)),
+                                         min_ratio, compact != 0);
+    *written = s.size();
+    if (buf) memcpy(buf, s.data(), std::min(cap, s.size()));
+  });
+}
+
 struct oracle_index {
   std::unique_ptr<Index> ix;
 };
@@ -1273,18 +1442,37 @@ int oracle_query_handle(oracle_index* h, const uint8_t* bases, const uint64_t* o
 // zx_oracle query -i DIR -q FILE [-a RATIO] [-t THREADS]: the aggregate TSV of
 // `zorindex query` on stdout and its #query line on stderr.
 int main(int argc, char** argv) {
-  std::string dir, query;
+  std::string dir, query, format = "tsv";
   double ratio = 0;
+  bool records = false;
   int threads = (int)std::thread::hardware_concurrency();
-  for (int i = 2; i + 1 < argc; i += 2) {
+  for (int i = 2; i < argc; ++i) {
     std::string a = argv[i];
-    if (a == "-i") dir = argv[i + 1];
-    else if (a == "-q") query = argv[i + 1];
-    else if (a == "-a") ratio = atof(argv[i + 1]);
-    else if (a == "-t") threads = atoi(argv[i + 1]);
+    if (a == "-r") {
+      records = true;
+      continue;
+    }
+    if (i + 1 >= argc) break;
+    if (a == "-i") dir = argv[++i];
+    else if (a == "-q") query = argv[++i];
+    else if (a == "-a") ratio = atof(argv[++i]);
+    else if (a == "-t") threads = atoi(argv[++i]);
+    else if (a == "-F") format = argv[++i];
+  }
+  if (records && !dir.empty() && !query.empty()) {
+    try {
+      auto ix = load_index(dir, true);
+      std::string s = query_records_output(*ix, parse_named_records(read_decoded(query)), ratio,
+                                           format == "compact");
+      fwrite(s.data(), 1, s.size(), stdout);
+      return 0;
+    } catch (const std::exception& e) {
+      fprintf(stderr, "error: %s\n", e.what());
+      return 1;
+    }
   }
   if (argc < 2 || std::string(argv[1]) != "query" || dir.empty() || query.empty()) {
-    fprintf(stderr, "usage: zx_oracle query -i DIR -q FILE [-a RATIO] [-t THREADS]\n");
+    fprintf(stderr, "usage: zx_oracle query -i DIR -q FILE [-a RATIO] [-t THREADS] [-r [-F tsv|compact]]\n");
     return 2;
   }
   try {

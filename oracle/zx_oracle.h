@@ -57,6 +57,14 @@ int oracle_query_handle(oracle_index* index, const uint8_t* bases, const uint64_
                         size_t records, int threads, uint64_t* counts, size_t colors,
                         uint64_t* total, double* seconds);
 
+// Per-record report of a query file as `zorindex query --records` prints it
+// (query_records_command_with_memory, src/power_merge/storage.rs:3626-3720):
+// TSV (compact = 0) or compact rows; *written = its bytes (copied up to cap
+// when buf is not NULL).
+int oracle_query_records_report(const char* index_dir, const char* query_path, int recover,
+                                double min_ratio, int compact, char* buf, size_t cap,
+                                size_t* written);
+
 const char* oracle_last_error(void);
 
 #ifdef __cplusplus
