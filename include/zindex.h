@@ -113,6 +113,26 @@ int zx_query_host(zx_index* index, const uint8_t* bases, const uint64_t* offsets
 int zx_query_host_plain(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
                         uint64_t records, int recover, uint64_t* counts, uint64_t* total);
 
+/* Per-record query of records in host memory (the counting step of
+ * query_records_command_with_memory, storage.rs:3626-3720, and of the
+ * findere branch's Scorer per record): counts (records x colours, row-major)
+ * receives each record's match counts and totals (records) its feature count,
+ * each exactly as a query of that record alone would give. */
+int zx_query_per_record(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
+                        uint64_t records, int recover, uint64_t* counts, uint64_t* totals);
+
+/* Per-record report of a FASTA/FASTQ file: `zorindex query --records`
+ * (query_records_command_with_memory, storage.rs:3626-3720). Records are read
+ * by the rules of read_batches (src/power_merge/records.rs:150-290) and
+ * reported in input order; compact = 0 writes RecordFormat::Tsv, 1
+ * RecordFormat::Compact (src/power_merge/record_output.rs:13-62) with the
+ * colour selection of RecordScores::write_record (storage.rs:3109-3146).
+ * min_ratio must be in [0, 1] and batch_records (--record-batch-size) > 0;
+ * the batch size does not change the output. out_path NULL = stdout. */
+int zx_query_records_report(zx_index* index, const char* query_path, int recover,
+                            double min_ratio, int compact, uint64_t batch_records,
+                            const char* out_path);
+
 /* Asynchronous query of a batch already in device memory of the index's GPU.
  * d_bases / d_offsets / d_counts / d_total are device pointers; counts and
  * total are ACCUMULATED (the caller zeroes them). stream is a cudaStream_t

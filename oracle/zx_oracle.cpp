@@ -1076,11 +1076,32 @@ struct NamedRecord {
   std::vector<uint8_t> seq;
 };
 
+// std::str::from_utf8 acceptance: decodes each sequence and rejects
+// overlong forms, surrogates and code points above U+10FFFF.
+bool utf8_ok(const std::string& s) {
+  size_t i = 0;
+  while (i < s.size()) {
+    const unsigned char c = (unsigned char)s[i];
+    const int len = c < 0x80 ? 1 : (c >> 5) == 6 ? 2 : (c >> 4) == 14 ? 3 : (c >> 3) == 30 ? 4 : 0;
+    if (!len || i + len > s.size()) return false;
+    uint32_t cp = len == 1 ? c : c & (0x7f >> len);
+    for (int j = 1; j < len; ++j) {
+      const unsigned char d = (unsigned char)s[i + j];
+      if ((d >> 6) != 2) return false;
+      cp = cp << 6 | (d & 0x3f);
+    }
+    static const uint32_t least[5] = {0, 0, 0x80, 0x800, 0x10000};
+    if (cp < least[len] || cp > 0x10ffff || (cp >= 0xd800 && cp <= 0xdfff)) return false;
+    i += len;
+  }
+  return true;
+}
+
 // read_batches (src/power_merge/records.rs:150-290): trailing whitespace of a
 // line is dropped and empty lines are skipped; the first line decides FASTQ
 // ('@') or FASTA; the identifier is the header up to the first whitespace;
 // sequence lines may not contain whitespace; FASTQ qualities are consumed by
-// length.
+// length; identifiers must be UTF-8 and at least one record is required.
 std::vector<NamedRecord> parse_named_records(const std::vector<uint8_t>& d) {
   std::vector<NamedRecord> out;
   size_t i = 0;
@@ -1100,6 +1121,7 @@ std::vector<NamedRecord> parse_named_records(const std::vector<uint8_t>& d) {
     while (e < line.size() && !is_ws(line[e])) ++e;
     std::string id = line.substr(1, e - 1);
     ensure(!id.empty(), (std::string("empty ") + what + " identifier").c_str());
+    ensure(utf8_ok(id), (std::string("invalid ") + what + " identifier").c_str());
     return id;
   };
   int fastq = -1;
@@ -1142,6 +1164,7 @@ std::vector<NamedRecord> parse_named_records(const std::vector<uint8_t>& d) {
       out.back().seq.insert(out.back().seq.end(), line.begin(), line.end());
     }
   }
+  ensure(!out.empty(), "no FASTA/FASTQ records");
   return out;
 }
 

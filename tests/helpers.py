@@ -58,6 +58,9 @@ class Oracle:
         lib.oracle_format_aggregate.argtypes = [c_char_p, P64, c_uint64, c_double, c_char_p,
                                                 c_size_t, POINTER(c_size_t)]
         lib.oracle_last_error.restype = c_char_p
+        lib.oracle_query_records_report.restype = c_int
+        lib.oracle_query_records_report.argtypes = [c_char_p, c_char_p, c_int, c_double, c_int,
+                                                    c_char_p, c_size_t, POINTER(c_size_t)]
         lib.oracle_query_timed.restype = c_int
         lib.oracle_query_timed.argtypes = [c_char_p, c_void_p, P64, c_size_t, c_int, P64, c_size_t,
                                            P64, POINTER(c_double)]
@@ -118,6 +121,17 @@ class Oracle:
             offsets.ctypes.data_as(POINTER(c_uint64)), len(offsets) - 1, threads, int(recover),
             counts.ctypes.data_as(POINTER(c_uint64)), colors, byref(total), byref(probes)))
         return counts, int(total.value)
+
+    def records_report(self, index_dir, query, recover=True, min_ratio=0.0,
+                       fmt="tsv") -> bytes:
+        """Per-record report bytes (`zorindex query --records`) of a query file."""
+        n = c_size_t()
+        args = (str(index_dir).encode(), str(query).encode(), int(recover), float(min_ratio),
+                int(fmt == "compact"))
+        self._check(self.lib.oracle_query_records_report(*args, None, 0, byref(n)))
+        buf = ctypes.create_string_buffer(max(n.value, 1))
+        self._check(self.lib.oracle_query_records_report(*args, buf, n.value, byref(n)))
+        return buf.raw[: n.value]
 
     def format_aggregate(self, index_dir, counts, total, min_ratio=0.0) -> str:
         counts = np.ascontiguousarray(counts, dtype=np.uint64)

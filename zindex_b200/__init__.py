@@ -107,6 +107,30 @@ class Index:
                       int(recover), _p64(counts), byref(total)))
         return counts, int(total.value)
 
+    def query_per_record(self, bases: np.ndarray, offsets: np.ndarray, recover: bool = True):
+        """(counts uint64[records, colors], totals uint64[records]): each record
+        bases[offsets[r]:offsets[r+1]] counted as if queried alone."""
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        records = len(offsets) - 1
+        counts = np.zeros((records, self.colors), dtype=np.uint64)
+        totals = np.zeros(records, dtype=np.uint64)
+        _lib.check(_lib.load().zx_query_per_record(self._h, bases.ctypes.data_as(c_void_p),
+                                                  _p64(offsets), records, int(recover),
+                                                  _p64(counts), _p64(totals)))
+        return counts, totals
+
+    def query_records_report(self, path: Union[str, Path], out: Union[str, Path, None] = None,
+                             min_ratio: float = 0.0, fmt: str = "tsv", batch: int = 4096,
+                             recover: bool = True) -> None:
+        """Per-record report of a FASTA/FASTQ file (`zorindex query --records`)
+        written to `out` (None: stdout); fmt "tsv" or "compact"."""
+        if fmt not in ("tsv", "compact"):
+            raise ValueError("fmt must be 'tsv' or 'compact'")
+        _lib.check(_lib.load().zx_query_records_report(
+            self._h, str(path).encode(), int(recover), float(min_ratio), int(fmt == "compact"),
+            int(batch), None if out is None else str(out).encode()))
+
     def query_device(self, d_bases: int, nbases: int, d_offsets: int, records: int,
                      d_counts: int, d_total: int, stream: int = 0, recover: bool = True,
                      use_graph: bool = True) -> None:

@@ -31,7 +31,8 @@ EXPORTED = (
     "zx_query_status", "zx_query_device_noalloc", "zx_query_segments", "zx_server_start",
     "zx_server_submit", "zx_server_wait", "zx_server_stats", "zx_server_stop", "zx_mlp_create",
     "zx_mlp_destroy", "zx_mlp_param_count", "zx_mlp_get_params", "zx_mlp_set_params",
-    "zx_mlp_loss_grad", "zx_mlp_train", "zx_mlp_predict",
+    "zx_mlp_loss_grad", "zx_mlp_train", "zx_mlp_predict", "zx_query_per_record",
+    "zx_query_records_report",
 )
 
 
@@ -94,6 +95,9 @@ def load() -> ctypes.CDLL:
         "zx_query_file": (c_int, [c_void_p, c_char_p, c_int, P64, P64, P64]),
         "zx_query_host": (c_int, [c_void_p, c_void_p, P64, c_uint64, c_int, P64, P64]),
         "zx_query_host_plain": (c_int, [c_void_p, c_void_p, P64, c_uint64, c_int, P64, P64]),
+        "zx_query_per_record": (c_int, [c_void_p, c_void_p, P64, c_uint64, c_int, P64, P64]),
+        "zx_query_records_report": (c_int, [c_void_p, c_char_p, c_int, c_double, c_int,
+                                            c_uint64, c_char_p]),
         "zx_query_device": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_int,
                                     c_void_p, c_void_p, c_void_p, c_int]),
         "zx_query_device_noalloc": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64,

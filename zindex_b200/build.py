@@ -20,7 +20,8 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "_lib"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-HOST_SOURCES = ["host/json.cpp", "host/manifest.cpp", "host/zstd_io.cpp", "host/fastx.cpp"]
+HOST_SOURCES = ["host/json.cpp", "host/manifest.cpp", "host/zstd_io.cpp", "host/fastx.cpp",
+                "host/record_report.cpp"]
 CUDA_SOURCES = ["engine.cu", "server.cu", "planner.cu", "capi.cu"]
 LIBS = ["-lz", "-l:libzstd.so.1", "-lpthread"]
 

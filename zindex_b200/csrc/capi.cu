@@ -11,6 +11,8 @@
 #include "planner.h"
 #include "server.h"
 #include "host/fastx.h"
+#include "host/record_report.h"
+#include <thread>
 
 struct zx_index {
   std::unique_ptr<zx::Engine> engine;
@@ -148,6 +150,88 @@ int zx_query_file(zx_index* index, const char* query_path, int recover, uint64_t
     e.query_host(e.default_workspace(), batch.bases.data(), batch.bases.size(),
                  batch.offsets.data(), batch.records(), recover != 0, counts, total);
     if (probes) *probes = *total;
+  });
+}
+
+int zx_query_per_record(zx_index* index, const uint8_t* bases, const uint64_t* offsets,
+                        uint64_t records, int recover, uint64_t* counts, uint64_t* totals) {
+  return guarded([&] {
+    zx::check(index && offsets && (counts || !records) && (totals || !records) &&
+                  (bases || !offsets[records]),
+              zx::kEInval, "null argument");
+    std::lock_guard<std::mutex> lock(index->mu);
+    auto& e = *index->engine;
+    e.query_per_record(e.default_workspace(), bases, offsets[records], offsets, records,
+                       recover != 0, counts, totals);
+  });
+}
+
+int zx_query_records_report(zx_index* index, const char* query_path, int recover,
+                            double min_ratio, int compact, uint64_t batch_records,
+                            const char* out_path) {
+  return guarded([&] {
+    zx::check(index && query_path, zx::kEInval, "null argument");
+    zx::check(min_ratio >= 0.0 && min_ratio <= 1.0, zx::kEInval, "--min-ratio must be in [0, 1]");
+    zx::check(batch_records > 0, zx::kEInval, "record batch size must be positive");
+    zx::check(compact == 0 || compact == 1, zx::kEInval, "format must be 0 (tsv) or 1 (compact)");
+    const zx::RecordFormat format = compact ? zx::RecordFormat::kCompact : zx::RecordFormat::kTsv;
+    zx::RecordBatch rb = zx::read_named_records(query_path);
+    std::lock_guard<std::mutex> lock(index->mu);
+    auto& e = *index->engine;
+    const auto& colors = e.manifest().colors;
+    const uint64_t C = std::max<uint64_t>(colors.size(), 1);
+    const uint64_t records = rb.records();
+    // Host counters of one step stay within 256 MiB; the step does not
+    // change the output (records are reported in input order).
+    const uint64_t step = std::min<uint64_t>(batch_records, std::max<uint64_t>(1, (32ull << 20) / C));
+    FILE* f = out_path ? fopen(out_path, "wb") : stdout;
+    if (!f) zx::raise(zx::kEIo, std::string("cannot create ") + out_path);
+    struct Closer {
+      FILE* f;
+      bool own;
+      ~Closer() {
+        if (own) fclose(f);
+      }
+    } closer{f, out_path != nullptr};
+    std::string head = zx::record_header(format);
+    head += '\n';
+    bool write_ok = fwrite(head.data(), 1, head.size(), f) == head.size();
+    // Step i's report is formatted and written on a second thread while the
+    // GPU runs step i + 1.
+    std::vector<uint64_t> counts[2], totals[2];
+    std::vector<uint64_t> rel;
+    std::string text[2];
+    std::thread writer;
+    auto join = [&] {
+      if (writer.joinable()) writer.join();
+    };
+    try {
+      uint64_t i = 0;
+      for (uint64_t r0 = 0; r0 < records; r0 += step, ++i) {
+        const uint64_t n = std::min(step, records - r0), b = i & 1, b0 = rb.offsets[r0];
+        counts[b].resize(n * colors.size());
+        totals[b].resize(n);
+        rel.resize(n + 1);
+        for (uint64_t r = 0; r <= n; ++r) rel[r] = rb.offsets[r0 + r] - b0;
+        e.query_per_record(e.default_workspace(), rb.bases.data() + b0, rel[n], rel.data(), n,
+                           recover != 0, counts[b].data(), totals[b].data());
+        join();
+        writer = std::thread([&, b, r0, n] {
+          std::string& t = text[b];
+          t.clear();
+          for (uint64_t r = 0; r < n; ++r)
+            zx::append_record(t, format, rb.names[r0 + r], totals[b][r],
+                              counts[b].data() + r * colors.size(), colors, min_ratio);
+          if (fwrite(t.data(), 1, t.size(), f) != t.size()) write_ok = false;
+        });
+      }
+      join();
+    } catch (...) {
+      join();
+      throw;
+    }
+    if (fflush(f) != 0) write_ok = false;
+    zx::check(write_ok, zx::kEIo, "writing the per-record report failed");
   });
 }
 

@@ -2,11 +2,13 @@
 // (src/bin/zorindex.rs:161-196 QueryArgs, 426-450 query_command) running on
 // the GPU through include/zindex.h, plus `build` (the host-side builder).
 //
-//   zorindex [-t T] query -i DIR -q FILE [-a MIN_RATIO] [-M subindex|all] [--device N]
+//   zorindex [-t T] query -i DIR -q FILE [-a MIN_RATIO] [-r [-F tsv|compact] [-B N]]
+//                         [-M subindex|all] [--device N]
 //   zorindex [-t T] build -f FOF -o DIR [build options, see zx_build]
 //
-// stdout carries the aggregate TSV of print_aggregate (storage.rs:3817-3844);
-// stderr the "#query" statistics line and query_timings.
+// stdout carries the aggregate TSV of print_aggregate (storage.rs:3817-3844),
+// or with -r the per-record report (record_output.rs:13-62); stderr the
+// "#query" statistics line (aggregate only) and query_timings.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -22,8 +24,8 @@ namespace {
 
 int usage() {
   fprintf(stderr,
-          "usage: zorindex [-t THREADS] query -i DIR -q FILE [-a MIN_RATIO] [-M subindex|all]\n"
-          "                [--device N]\n"
+          "usage: zorindex [-t THREADS] query -i DIR -q FILE [-a MIN_RATIO]\n"
+          "                [-r [-F tsv|compact] [-B RECORDS]] [-M subindex|all] [--device N]\n"
           "       zorindex [-t THREADS] build -f FOF -o DIR [-k K] [-m M] [-H H] [-b BITS]\n"
           "                [-s SEED] [-i MODE] [-z Z] [-d D] [-S SCALE] [-L SEG] [-D MIN_DOCS]\n"
           "                [-N MAX] [-X SIZE] [-R] [--groups 0,1;2,3]\n");
@@ -34,6 +36,9 @@ int query(int argc, char** argv, int) {
   std::string dir, path;
   double min_ratio = 0.0;
   int device = 0;
+  bool records = false, format_given = false;
+  int compact = 0;
+  long long batch = 4096;
   for (int i = 0; i < argc; ++i) {
     std::string a = argv[i];
     auto val = [&]() -> const char* {
@@ -49,14 +54,26 @@ int query(int argc, char** argv, int) {
     else if (a == "-M" || a == "--query-memory") {
       std::string v = val();
       if (v != "subindex" && v != "all") return usage();
-    } else if (a == "-B" || a == "--record-batch-size") val();
-    else if (a == "--device") device = atoi(val());
-    else if (a == "-r" || a == "--records") {
-      fprintf(stderr, "Error: --records (per-record output) is not supported by this build yet\n");
-      return 1;
-    } else return usage();
+    } else if (a == "-B" || a == "--record-batch-size") {
+      char* end = nullptr;
+      const char* v = val();
+      batch = strtoll(v, &end, 10);
+      if (!*v || *end || batch < 0) return usage();
+    } else if (a == "-F" || a == "--output-format") {
+      std::string v = val();
+      if (v == "tsv") compact = 0;
+      else if (v == "compact") compact = 1;
+      else return usage();
+      format_given = true;
+    } else if (a == "--device") device = atoi(val());
+    else if (a == "-r" || a == "--records") records = true;
+    else return usage();
   }
   if (dir.empty() || path.empty()) return usage();
+  if (format_given && !records) {  // clap: output_format requires records
+    fprintf(stderr, "error: --output-format requires --records\n");
+    return 2;
+  }
   if (!(min_ratio >= 0.0 && min_ratio <= 1.0)) {
     fprintf(stderr, "Error: --min-ratio must be in [0, 1]\n");
     return 1;
@@ -68,6 +85,16 @@ int query(int argc, char** argv, int) {
     return 1;
   }
   double load_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (records) {
+    auto t1 = std::chrono::steady_clock::now();
+    int rc = zx_query_records_report(ix, path.c_str(), 1, min_ratio, compact, (uint64_t)batch,
+                                     nullptr);
+    double query_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+    if (rc != ZX_OK) fprintf(stderr, "Error: %s\n", zx_last_error());
+    else fprintf(stderr, "query_timings\tload_s=%.6f\tquery_s=%.6f\n", load_s, query_s);
+    zx_close(ix);
+    return rc == ZX_OK ? 0 : 1;
+  }
   zx_info info;
   zx_index_info(ix, &info);
   std::vector<uint64_t> counts(info.colors);

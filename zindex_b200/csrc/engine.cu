@@ -390,7 +390,8 @@ Workspace::~Workspace() {
   void* dev[] = {bases,      offsets,  packed,    invalid,  tile_counts, tile_first,
                  tiles,      scan_tmp, partial,   counts,   total,       keys_out,
                  keys_count, error,    fstate,    hp_starts, hp_keep,    hp_pos,
-                 hp_bases,   hp_offsets, hp_scan_tmp, seg_blocks, seg_tiles, seg_records};
+                 hp_bases,   hp_offsets, hp_scan_tmp, seg_blocks, seg_tiles, seg_records,
+                 rec_counts, rec_totals};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total, h_seg_blocks, h_seg_records};
@@ -970,15 +971,18 @@ uint64_t Engine::tiles_for_length(uint64_t len) const {
 void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                             const uint64_t* offsets, uint64_t records, const uint64_t* seg_records,
                             const uint64_t* est_tiles, uint32_t segments, bool recover,
-                            uint64_t* counts, unsigned long long* totals, cudaStream_t s) {
+                            uint64_t* counts, unsigned long long* totals, cudaStream_t s,
+                            int warps) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   check(segments > 0, kEInval, "a segmented query needs at least one segment");
+  check(warps >= 0 && warps <= 8, kEInval, "warps per block must be in 1..8");
   check(seg_records[0] == 0 && seg_records[segments] == records, kEInval,
         "segments must span the records");
   for (uint32_t i = 0; i < segments; ++i)
     check(seg_records[i] <= seg_records[i + 1], kEInval, "segment records must be non-decreasing");
   ensure_capacity(ws, nbases, records);
   QueryLaunch l = launch_;
+  if (warps > 0 && warps < l.warps) l.warps = warps;
   const int cap = max_blocks(l);
   const uint32_t wpb = (uint32_t)l.warps;
   // Grid shares: proportional to the estimated tiles, at least one block,
@@ -1013,7 +1017,7 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   ws.h_seg_blocks[segments] = blocks;
   ws.h_seg_records[segments] = seg_records[segments];
   const uint64_t colors = m_.colors.size();
-  if ((uint64_t)blocks * colors > ws.cap_partial) {
+  if (l.smem_counters && (uint64_t)blocks * colors > ws.cap_partial) {
     if (ws.partial) cudaFree(ws.partial);
     dev_alloc(&ws.partial, (uint64_t)blocks * colors, "block counters");
     ws.cap_partial = (uint64_t)blocks * colors;
@@ -1061,6 +1065,73 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
     reduce_segments_kernel<<<grid, 256, 0, s>>>(ws.partial, ws.seg_blocks, segments,
                                                 (uint32_t)colors, counts);
     cuda_check(cudaGetLastError(), "reduce_segments_kernel");
+  }
+}
+
+void Engine::query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                              const uint64_t* offsets, uint64_t records, bool recover,
+                              uint64_t* counts, uint64_t* totals) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
+  for (uint64_t r = 0; r < records; ++r)  // groups are cut and sized on the host
+    check(offsets[r] <= offsets[r + 1], kEInval, "offsets must be non-decreasing");
+  const uint64_t colors = std::max<uint64_t>(m_.colors.size(), 1);
+  // Group size: the group's counters (records x colours x 8 bytes), the extra
+  // block counters (one block per short record, colours x 4 bytes each) and,
+  // for findere, the extra per-warp colour state stay within 256 MiB each.
+  const uint64_t budget = 256ull << 20;
+  uint64_t gmax = budget / (colors * 8);
+  if (m_.index_mode == kFindere) gmax = std::min<uint64_t>(gmax, budget / (colors * 8 * launch_.warps));
+  gmax = std::max<uint64_t>(1, std::min<uint64_t>(gmax, 1ull << 20));
+  const uint64_t group_bases = 256ull << 20;
+  if (gmax > ws.cap_rec_totals || !ws.rec_counts) {
+    if (ws.rec_counts) cudaFree(ws.rec_counts);
+    if (ws.rec_totals) cudaFree(ws.rec_totals);
+    ws.rec_counts = nullptr;
+    ws.rec_totals = nullptr;
+    dev_alloc(&ws.rec_counts, gmax * colors, "record counters");
+    dev_alloc(&ws.rec_totals, gmax, "record totals");
+    ws.cap_rec_counts = gmax * colors;
+    ws.cap_rec_totals = gmax;
+  }
+  cudaStream_t s = ws.stream;
+  std::vector<uint64_t> seg, est;
+  for (uint64_t r0 = 0; r0 < records;) {
+    uint64_t r1 = r0 + 1, tiles = tiles_for_length(offsets[r0 + 1] - offsets[r0]);
+    while (r1 < records && r1 - r0 < gmax && offsets[r1 + 1] - offsets[r0] <= group_bases)
+      tiles += tiles_for_length(offsets[r1 + 1] - offsets[r1]), ++r1;
+    const uint64_t n = r1 - r0, b0 = offsets[r0], nb = offsets[r1] - b0;
+    ensure_capacity(ws, nb, n);
+    ensure_host_capacity(ws, nb, n);
+    seg.resize(n + 1);
+    est.resize(n);
+    for (uint64_t i = 0; i <= n; ++i) {
+      seg[i] = i;
+      ws.h_offsets[i] = offsets[r0 + i] - b0;
+    }
+    for (uint64_t i = 0; i < n; ++i)
+      est[i] = std::max<uint64_t>(1, tiles_for_length(offsets[r0 + i + 1] - offsets[r0 + i]));
+    if (nb) {
+      memcpy(ws.h_bases, bases + b0, nb);
+      cuda_check(cudaMemcpyAsync(ws.bases, ws.h_bases, nb, cudaMemcpyHostToDevice, s), "H2D");
+    }
+    cuda_check(cudaMemcpyAsync(ws.offsets, ws.h_offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s),
+               "H2D");
+    cuda_check(cudaMemsetAsync(ws.rec_counts, 0, n * colors * 8, s), "memset");
+    cuda_check(cudaMemsetAsync(ws.rec_totals, 0, n * 8, s), "memset");
+    // Short records: warps per block near the mean tiles per record.
+    int warps = 0;
+    const uint64_t mean = (tiles + n - 1) / n;
+    if (mean < (uint64_t)launch_.warps) warps = mean <= 2 ? 2 : (mean <= 4 ? 4 : 8);
+    query_segments(ws, ws.bases, nb, ws.offsets, n, seg.data(), est.data(), (uint32_t)n, recover,
+                   ws.rec_counts, ws.rec_totals, s, warps);
+    cuda_check(cudaMemcpyAsync(counts + r0 * m_.colors.size(), ws.rec_counts,
+                               n * m_.colors.size() * 8, cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaMemcpyAsync(totals + r0, ws.rec_totals, n * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "per-record query");
+    check_error_word(ws);
+    r0 = r1;
   }
 }
 

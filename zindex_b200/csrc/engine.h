@@ -60,6 +60,10 @@ struct Workspace {
   uint64_t* h_seg_records = nullptr;  // pinned staging
   uint64_t cap_segments = 0;
   cudaEvent_t seg_staged = nullptr;   // the last segmented call's staging copies are done
+  // Per-record queries: counters of one record group (records x colours).
+  uint64_t* rec_counts = nullptr;
+  unsigned long long* rec_totals = nullptr;
+  uint64_t cap_rec_counts = 0, cap_rec_totals = 0;
   // Pinned host staging.
   uint8_t* h_bases = nullptr;
   uint64_t* h_offsets = nullptr;
@@ -140,11 +144,20 @@ class Engine {
   // records seg_records[s] .. seg_records[s+1]-1 (host array, segments + 1
   // entries). counts (segments x colours) and totals (segments) are
   // accumulated, not cleared. est_tiles[s] (host) sizes each request's share
-  // of the grid; any positive estimate gives exact results.
+  // of the grid; any positive estimate gives exact results. warps > 0
+  // overrides the launch's warps per block (short requests leave most warps
+  // of a block idle).
   void query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
                       uint64_t records, const uint64_t* seg_records, const uint64_t* est_tiles,
                       uint32_t segments, bool recover, uint64_t* counts,
-                      unsigned long long* totals, cudaStream_t stream);
+                      unsigned long long* totals, cudaStream_t stream, int warps = 0);
+  // Per-record query of host records (--records): counts (records x colours,
+  // row-major) and totals (records) receive each record's own result, exactly
+  // as if the record were queried alone. Records run in groups whose device
+  // counters fit a fixed budget, one segment per record in a segmented launch.
+  void query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                        const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
+                        uint64_t* totals);
   // Upper bound of the tiles of one record of `len` bases.
   uint64_t tiles_for_length(uint64_t len) const;
   // Seeds of host records in record/window order (extraction only).

@@ -113,6 +113,126 @@ void parse_fastx(const uint8_t* data, size_t len, RecordBatch& out, bool keep_na
   }
 }
 
+namespace {
+
+inline bool ascii_ws(uint8_t c) {
+  return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\f' || c == '\v';
+}
+
+// Well-formed UTF-8 (no overlong forms, no surrogates, at most U+10FFFF).
+bool valid_utf8(const uint8_t* p, const uint8_t* e) {
+  while (p < e) {
+    const uint8_t c = *p;
+    int n;
+    uint32_t cp;
+    if (c < 0x80) {
+      ++p;
+      continue;
+    } else if (c >= 0xc2 && c <= 0xdf) {
+      n = 1, cp = c & 0x1f;
+    } else if (c >= 0xe0 && c <= 0xef) {
+      n = 2, cp = c & 0x0f;
+    } else if (c >= 0xf0 && c <= 0xf4) {
+      n = 3, cp = c & 0x07;
+    } else {
+      return false;
+    }
+    if (e - p <= n) return false;
+    for (int i = 1; i <= n; ++i) {
+      if ((p[i] & 0xc0) != 0x80) return false;
+      cp = (cp << 6) | (p[i] & 0x3f);
+    }
+    if ((n == 2 && (cp < 0x800 || (cp >= 0xd800 && cp <= 0xdfff))) ||
+        (n == 3 && (cp < 0x10000 || cp > 0x10ffff)))
+      return false;
+    p += n + 1;
+  }
+  return true;
+}
+
+// Line reader over a byte buffer: [a, b) is the line without its '\n'.
+struct Lines {
+  const uint8_t* p;
+  const uint8_t* e;
+  bool next(const uint8_t*& a, const uint8_t*& b) {
+    if (p >= e) return false;
+    a = p;
+    b = line_end(p, e);
+    p = b < e ? b + 1 : e;
+    return true;
+  }
+};
+
+}  // namespace
+
+void parse_named_records(const uint8_t* data, size_t len, RecordBatch& out) {
+  if (out.offsets.empty()) out.offsets.push_back(out.bases.size());
+  Lines lines{data, data + len};
+  const uint8_t *a, *b;
+  int fastq = -1;
+  bool open = false;  // a FASTA record is being read
+  auto identifier = [&](const char* kind) {
+    const uint8_t* q = a + 1;
+    while (q < b && !ascii_ws(*q)) ++q;
+    check_format(q > a + 1, (std::string("empty ") + kind + " identifier").c_str());
+    check_format(valid_utf8(a + 1, q), (std::string("invalid ") + kind + " identifier").c_str());
+    out.names.emplace_back(a + 1, q);
+  };
+  auto no_whitespace = [&](const char* msg) {
+    for (const uint8_t* q = a; q < b; ++q) check_format(!ascii_ws(*q), msg);
+  };
+  auto trim_line_end = [&] {
+    while (b > a && (b[-1] == '\n' || b[-1] == '\r')) --b;
+  };
+  while (lines.next(a, b)) {
+    while (b > a && ascii_ws(b[-1])) --b;
+    if (a == b) continue;
+    if (fastq == 1 || (fastq == -1 && *a == '@')) {
+      fastq = 1;
+      check_format(*a == '@', "expected FASTQ identifier");
+      identifier("FASTQ");
+      const size_t start = out.bases.size();
+      for (;;) {
+        check_format(lines.next(a, b), "truncated FASTQ sequence");
+        trim_line_end();
+        if (b > a && *a == '+') break;
+        no_whitespace("whitespace inside FASTQ sequence");
+        out.bases.insert(out.bases.end(), a, b);
+      }
+      const size_t seq = out.bases.size() - start;
+      size_t qualities = 0;
+      while (qualities < seq) {
+        check_format(lines.next(a, b), "truncated FASTQ quality");
+        trim_line_end();
+        qualities += (size_t)(b - a);
+        check_format(qualities <= seq, "FASTQ sequence and quality lengths differ");
+      }
+      out.offsets.push_back(out.bases.size());
+      continue;
+    }
+    fastq = 0;
+    if (*a == '>') {
+      if (open) out.offsets.push_back(out.bases.size());
+      identifier("FASTA");
+      open = true;
+    } else {
+      check_format(open, "--records requires FASTA or FASTQ");
+      no_whitespace("whitespace inside FASTA sequence");
+      out.bases.insert(out.bases.end(), a, b);
+    }
+  }
+  if (open) out.offsets.push_back(out.bases.size());
+  check_format(out.offsets.size() > 1, "no FASTA/FASTQ records");
+}
+
+RecordBatch read_named_records(const std::string& path) {
+  std::vector<uint8_t> data = decoded_input(path);
+  RecordBatch batch;
+  batch.bases.reserve(data.size());
+  parse_named_records(data.data(), data.size(), batch);
+  return batch;
+}
+
 RecordBatch read_fastx(const std::string& path, bool keep_names) {
   std::vector<uint8_t> data = decoded_input(path);
   RecordBatch batch;

@@ -23,4 +23,15 @@ RecordBatch read_fastx(const std::string& path, bool keep_names);
 // Parses FASTA/FASTQ bytes already in memory.
 void parse_fastx(const uint8_t* data, size_t len, RecordBatch& out, bool keep_names);
 
+// Named records for per-record reports, under the stricter rules of the
+// reference's record reader (src/power_merge/records.rs:150-290): trailing
+// ASCII whitespace of a line is dropped and empty lines are skipped; the
+// first line decides FASTQ ('@') or FASTA; the identifier is the header up to
+// the first whitespace and must be non-empty UTF-8; sequence lines may not
+// hold whitespace; FASTQ sequences run until the '+' line and qualities are
+// consumed by length; at least one record is required. Throws zx::Error
+// (kEFormat, kEIo) with the reference's messages.
+RecordBatch read_named_records(const std::string& path);
+void parse_named_records(const uint8_t* data, size_t len, RecordBatch& out);
+
 }  // namespace zx
