@@ -96,6 +96,10 @@ METRIC = "query seeds/s"
 # capture of a 1.2e7-seed slice (profiles/fused_query_kernel-c2-batched.md:
 # 12.034 GB read + 7.0 MB written); scaled by the seeds of a launch.
 TRAFFIC_BYTES_PER_SEED = 12.041e9 / 1.2e7
+# Per-record form: reads counted one by one, and the compact report threshold.
+PER_RECORD_READS = 200_000
+PER_RECORD_CPU_READS = 20_000
+PER_RECORD_MIN_RATIO = 0.5
 LIB = ROOT / "zindex_b200" / "_lib"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
@@ -174,6 +178,20 @@ def long_pool(cache: Path, rank: int, name: str = "c2"):
     long = cache / f"long-{name}-r{rank}"
     return (np.fromfile(str(long) + ".bases", dtype=np.uint8),
             np.fromfile(str(long) + ".offsets", dtype=np.uint64))
+
+
+def records_fasta(cache: Path, rank: int, name: str, bases, offsets, n: int) -> Path:
+    """The first n reads as a FASTA file with identifiers r0, r1, ... (the
+    per-record report's input), written once per cache dir."""
+    path = cache / f"records-{name}-r{rank}-{n}.fa"
+    if not path.exists():
+        tmp = Path(str(path) + f".tmp{os.getpid()}")
+        with open(tmp, "wb") as f:
+            for r in range(n):
+                f.write(b">r%d\n" % r)
+                f.write(bases[int(offsets[r]): int(offsets[r + 1])].tobytes() + b"\n")
+        os.replace(tmp, path)
+    return path
 
 
 def make_requests(bases, offsets, lbases, loffsets, n, seed):
@@ -398,6 +416,22 @@ class CpuOracle:
             secs = statistics.median(reps)
         return seeds, secs, counts, n
 
+    def records_report(self, path, min_ratio, compact):
+        """(report bytes, seconds) of the per-record report on all host cores."""
+        ct = self.ct
+        f = self.lib.oracle_records_report_handle
+        f.argtypes = [ct.c_void_p, ct.c_char_p, ct.c_double, ct.c_int, ct.c_int, ct.c_char_p,
+                      ct.c_size_t, ct.POINTER(ct.c_size_t), ct.POINTER(ct.c_double)]
+        f.restype = ct.c_int
+        n, secs = ct.c_size_t(), ct.c_double()
+        args = (self.h, str(path).encode(), float(min_ratio), int(compact), self.cores)
+        if f(*args, None, 0, ct.byref(n), ct.byref(secs)):
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        buf = ct.create_string_buffer(max(1, n.value))
+        if f(*args, buf, n.value, ct.byref(n), ct.byref(secs)):
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        return buf.raw[: n.value], secs.value
+
     def close(self):
         self.lib.oracle_close(self.h)
 
@@ -607,6 +641,40 @@ def ours(args):
     _, plain_seeds = ix.query_records(pb, po, plain=True)
     plain_rate = plain_seeds / (time.perf_counter() - t0)
 
+    log("stage: per-record form")
+    # Per-record form (`query --records`): each read counted alone. Counts of
+    # every read through zx_query_per_record (host buffers, copies inside the
+    # timed region), then the compact report of a FASTA file end to end
+    # (reading, counting, formatting, writing to /dev/null).
+    n_rec = min(PER_RECORD_READS, records)
+    rb, ro = bases[: int(offsets[n_rec])], offsets[: n_rec + 1]
+    pr_counts, pr_totals = ix.query_per_record(rb, ro)
+    agg_counts, agg_total = ix.query_records(rb, ro)
+    assert (int(pr_totals.sum()) == agg_total and
+            np.array_equal(pr_counts.sum(axis=0, dtype=np.uint64), agg_counts)), \
+        "per-record counts do not add up to the aggregate"
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ix.query_per_record(rb, ro)
+        times.append(time.perf_counter() - t0)
+    pr_s = statistics.median(times)
+    fasta = records_fasta(Path(args.cache), rank, args.config, bases, offsets, n_rec)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ix.query_records_report(fasta, os.devnull, min_ratio=PER_RECORD_MIN_RATIO, fmt="compact")
+        times.append(time.perf_counter() - t0)
+    rep_s = statistics.median(times)
+    per_record = {
+        "reads": n_rec, "seeds": agg_total,
+        "counts_reads_per_s": n_rec / pr_s, "counts_seeds_per_s": agg_total / pr_s,
+        "report_reads_per_s": n_rec / rep_s,
+        "report": f"compact, min_ratio {PER_RECORD_MIN_RATIO}, {fasta.stat().st_size} B FASTA "
+                  "read, counted and formatted per call",
+        "d2h_bytes_per_call": int(8 * n_rec * (ix.colors + 1)),
+    }
+
     if rank == 0:
         cb = None
         parity = None
@@ -615,6 +683,19 @@ def ours(args):
             cb, n_cpu, cpu_counts = cpu_baseline(index_dir, bases, offsets, ix.colors)
             c_part, _ = ix.query_records(bases[: int(offsets[n_cpu])], offsets[: n_cpu + 1])
             parity = bool(np.array_equal(c_part, cpu_counts))
+            # Per-record report on the host cores, on a bounded sample of reads.
+            n_s = min(n_rec, PER_RECORD_CPU_READS)
+            sample = records_fasta(Path(args.cache), rank, args.config, bases, offsets, n_s)
+            orc = CpuOracle(index_dir)
+            want, secs = orc.records_report(sample, PER_RECORD_MIN_RATIO, True)
+            orc.close()
+            got_path = Path(args.cache) / f"records-gpu-{os.getpid()}.txt"
+            ix.query_records_report(sample, got_path, min_ratio=PER_RECORD_MIN_RATIO, fmt="compact")
+            per_record["cpu_baseline"] = {
+                "value": n_s / secs, "unit": "reads/s", "cores": orc.cores, "kind": "port",
+                "sample": f"compact report of the first {n_s} reads, {secs:.2f}s"}
+            per_record["parity_vs_oracle_sample"] = got_path.read_bytes() == want
+            got_path.unlink()
         line = {
             "metric": METRIC, "value": value, "unit": "seeds/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -641,7 +722,7 @@ def ours(args):
             "forms": {"plain_seeds_per_s": plain_rate, "batched_seeds_per_s": value / world,
                       "served_seeds_per_s": served["closed_loop"]["seeds_per_s"],
                       "planned_seeds_per_s": world * planned["seeds_per_s"],
-                      "served": served, "planned": planned},
+                      "served": served, "planned": planned, "per_record": per_record},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cpu_baseline": cb,

@@ -1459,6 +1459,40 @@ int oracle_query_handle(oracle_index* h, const uint8_t* bases, const uint64_t* o
   });
 }
 
+// Per-record report of a query file over a resident index, records split
+// across `threads` workers in contiguous runs (the report keeps input order);
+// *seconds covers reading, querying and formatting (not the index load).
+int oracle_records_report_handle(oracle_index* h, const char* query_path, double min_ratio,
+                                 int compact, int threads, char* buf, size_t cap,
+                                 size_t* written, double* seconds) {
+  return guarded([&] {
+    const Index& ix = *h->ix;
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<NamedRecord> recs = parse_named_records(read_decoded(query_path));
+    const size_t T = (size_t)std::max(1, std::min<int>(threads, (int)recs.size()));
+    std::vector<std::string> parts(T);
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < T; ++t)
+      pool.emplace_back([&, t] {
+        const size_t a = recs.size() * t / T, b = recs.size() * (t + 1) / T;
+        for (size_t r = a; r < b; ++r) {
+          Work w;
+          prepare_record(ix.f, recs[r].seq.data(), recs[r].seq.size(), w);
+          std::vector<uint64_t> counts;
+          run_query(ix, w, 1, counts);
+          format_record(ix, recs[r].name, w.total, counts, min_ratio, compact != 0, parts[t]);
+        }
+      });
+    for (auto& th : pool) th.join();
+    std::string s = records_header(compact != 0);
+    s += '\n';
+    for (auto& p : parts) s += p;
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *written = s.size();
+    if (buf) memcpy(buf, s.data(), std::min(cap, s.size()));
+  });
+}
+
 }  // extern "C"
 
 #ifdef ZX_ORACLE_MAIN

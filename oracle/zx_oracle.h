@@ -65,6 +65,12 @@ int oracle_query_records_report(const char* index_dir, const char* query_path, i
                                 double min_ratio, int compact, char* buf, size_t cap,
                                 size_t* written);
 
+/* Per-record report over an open index: records split across `threads`
+ * workers; *seconds covers reading, querying and formatting. */
+int oracle_records_report_handle(oracle_index* index, const char* query_path, double min_ratio,
+                                 int compact, int threads, char* buf, size_t cap,
+                                 size_t* written, double* seconds);
+
 const char* oracle_last_error(void);
 
 #ifdef __cplusplus
