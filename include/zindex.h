@@ -127,8 +127,11 @@ int zx_query_per_record(zx_index* index, const uint8_t* bases, const uint64_t* o
  * reported in input order; compact = 0 writes RecordFormat::Tsv, 1
  * RecordFormat::Compact (src/power_merge/record_output.rs:13-62) with the
  * colour selection of RecordScores::write_record (storage.rs:3109-3146).
- * min_ratio must be in [0, 1] and batch_records (--record-batch-size) > 0;
- * the batch size does not change the output. out_path NULL = stdout. */
+ * min_ratio must be in [0, 1] and batch_records (--record-batch-size) > 0.
+ * As in the reference the batch size does not change the output; the GPU
+ * path sizes its own steps (with min_ratio > 0 the reported colours are
+ * selected on the device and only they are copied back). out_path NULL =
+ * stdout. */
 int zx_query_records_report(zx_index* index, const char* query_path, int recover,
                             double min_ratio, int compact, uint64_t batch_records,
                             const char* out_path);

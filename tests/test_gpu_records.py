@@ -64,7 +64,7 @@ def test_report_matches_oracle(gpu, oracle, tmp_path_factory, tmp_path, opts):
     q, _ = query_file(tmp_path / "q.fa", genomes)
     with zx.Index(ix) as index:
         for fmt in ("tsv", "compact"):
-            for min_ratio in (0.0, 0.4):
+            for min_ratio in (0.0, 1e-9, 0.4, 1.0):
                 out = tmp_path / f"out-{fmt}-{min_ratio}.tsv"
                 index.query_records_report(q, out, min_ratio=min_ratio, fmt=fmt)
                 want = oracle.records_report(ix, q, min_ratio=min_ratio, fmt=fmt)

@@ -181,9 +181,12 @@ int zx_query_records_report(zx_index* index, const char* query_path, int recover
     const auto& colors = e.manifest().colors;
     const uint64_t C = std::max<uint64_t>(colors.size(), 1);
     const uint64_t records = rb.records();
-    // Host counters of one step stay within 256 MiB; the step does not
-    // change the output (records are reported in input order).
-    const uint64_t step = std::min<uint64_t>(batch_records, std::max<uint64_t>(1, (32ull << 20) / C));
+    // With a threshold the reported colours are selected on the device and
+    // only they are copied back; with min_ratio 0 every colour is reported and
+    // the dense counts come back, at most 256 MiB of them per step. The step
+    // (like the reference's record batch size) does not change the output.
+    const bool sparse = min_ratio > 0.0;
+    const uint64_t step = sparse ? (1ull << 18) : std::max<uint64_t>(1, (32ull << 20) / C);
     FILE* f = out_path ? fopen(out_path, "wb") : stdout;
     if (!f) zx::raise(zx::kEIo, std::string("cannot create ") + out_path);
     struct Closer {
@@ -199,6 +202,7 @@ int zx_query_records_report(zx_index* index, const char* query_path, int recover
     // Step i's report is formatted and written on a second thread while the
     // GPU runs step i + 1.
     std::vector<uint64_t> counts[2], totals[2];
+    zx::Engine::RecordHits hits[2];
     std::vector<uint64_t> rel;
     std::string text[2];
     std::thread writer;
@@ -209,19 +213,32 @@ int zx_query_records_report(zx_index* index, const char* query_path, int recover
       uint64_t i = 0;
       for (uint64_t r0 = 0; r0 < records; r0 += step, ++i) {
         const uint64_t n = std::min(step, records - r0), b = i & 1, b0 = rb.offsets[r0];
-        counts[b].resize(n * colors.size());
-        totals[b].resize(n);
         rel.resize(n + 1);
         for (uint64_t r = 0; r <= n; ++r) rel[r] = rb.offsets[r0 + r] - b0;
-        e.query_per_record(e.default_workspace(), rb.bases.data() + b0, rel[n], rel.data(), n,
-                           recover != 0, counts[b].data(), totals[b].data());
+        if (sparse) {
+          e.query_record_hits(e.default_workspace(), rb.bases.data() + b0, rel[n], rel.data(), n,
+                              recover != 0, min_ratio, hits[b]);
+        } else {
+          counts[b].resize(n * colors.size());
+          totals[b].resize(n);
+          e.query_per_record(e.default_workspace(), rb.bases.data() + b0, rel[n], rel.data(), n,
+                             recover != 0, counts[b].data(), totals[b].data());
+        }
         join();
         writer = std::thread([&, b, r0, n] {
           std::string& t = text[b];
           t.clear();
-          for (uint64_t r = 0; r < n; ++r)
-            zx::append_record(t, format, rb.names[r0 + r], totals[b][r],
-                              counts[b].data() + r * colors.size(), colors, min_ratio);
+          for (uint64_t r = 0; r < n; ++r) {
+            if (sparse) {
+              const auto& h = hits[b];
+              zx::append_record_hits(t, format, rb.names[r0 + r], h.totals[r],
+                                     h.colors.data() + h.first[r], h.counts.data() + h.first[r],
+                                     h.first[r + 1] - h.first[r], colors);
+            } else {
+              zx::append_record(t, format, rb.names[r0 + r], totals[b][r],
+                                counts[b].data() + r * colors.size(), colors, 0.0);
+            }
+          }
           if (fwrite(t.data(), 1, t.size(), f) != t.size()) write_ok = false;
         });
       }

@@ -12,6 +12,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include "kernels/query_kernels.cuh"
+#include "kernels/record_hits.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -391,7 +392,8 @@ Workspace::~Workspace() {
                  tiles,      scan_tmp, partial,   counts,   total,       keys_out,
                  keys_count, error,    fstate,    hp_starts, hp_keep,    hp_pos,
                  hp_bases,   hp_offsets, hp_scan_tmp, seg_blocks, seg_tiles, seg_records,
-                 rec_counts, rec_totals};
+                 rec_counts, rec_totals, rec_hits, rec_first, rec_scan_tmp, hit_colors,
+                 hit_counts};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total, h_seg_blocks, h_seg_records};
@@ -1068,9 +1070,9 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   }
 }
 
-void Engine::query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbases,
-                              const uint64_t* offsets, uint64_t records, bool recover,
-                              uint64_t* counts, uint64_t* totals) {
+void Engine::record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                           const uint64_t* offsets, uint64_t records, bool recover,
+                           const std::function<void(uint64_t, uint64_t)>& on_group) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
   for (uint64_t r = 0; r < records; ++r)  // groups are cut and sized on the host
@@ -1085,12 +1087,21 @@ void Engine::query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbas
   gmax = std::max<uint64_t>(1, std::min<uint64_t>(gmax, 1ull << 20));
   const uint64_t group_bases = 256ull << 20;
   if (gmax > ws.cap_rec_totals || !ws.rec_counts) {
-    if (ws.rec_counts) cudaFree(ws.rec_counts);
-    if (ws.rec_totals) cudaFree(ws.rec_totals);
+    for (void* p : {(void*)ws.rec_counts, (void*)ws.rec_totals, (void*)ws.rec_hits,
+                    (void*)ws.rec_first, ws.rec_scan_tmp})
+      if (p) cudaFree(p);
     ws.rec_counts = nullptr;
     ws.rec_totals = nullptr;
+    ws.rec_hits = ws.rec_first = nullptr;
+    ws.rec_scan_tmp = nullptr;
     dev_alloc(&ws.rec_counts, gmax * colors, "record counters");
     dev_alloc(&ws.rec_totals, gmax, "record totals");
+    dev_alloc(&ws.rec_hits, gmax + 1, "record hit counts");
+    dev_alloc(&ws.rec_first, gmax + 1, "record hit offsets");
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, ws.rec_hits, ws.rec_first, (int)(gmax + 1));
+    dev_alloc((uint8_t**)&ws.rec_scan_tmp, tmp, "record hit scan scratch");
+    ws.rec_scan_bytes = tmp;
     ws.cap_rec_counts = gmax * colors;
     ws.cap_rec_totals = gmax;
   }
@@ -1125,14 +1136,84 @@ void Engine::query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbas
     if (mean < (uint64_t)launch_.warps) warps = mean <= 2 ? 2 : (mean <= 4 ? 4 : 8);
     query_segments(ws, ws.bases, nb, ws.offsets, n, seg.data(), est.data(), (uint32_t)n, recover,
                    ws.rec_counts, ws.rec_totals, s, warps);
-    cuda_check(cudaMemcpyAsync(counts + r0 * m_.colors.size(), ws.rec_counts,
-                               n * m_.colors.size() * 8, cudaMemcpyDeviceToHost, s),
-               "D2H");
-    cuda_check(cudaMemcpyAsync(totals + r0, ws.rec_totals, n * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    on_group(r0, n);
     cuda_check(cudaStreamSynchronize(s), "per-record query");
     check_error_word(ws);
     r0 = r1;
   }
+}
+
+void Engine::query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                              const uint64_t* offsets, uint64_t records, bool recover,
+                              uint64_t* counts, uint64_t* totals) {
+  const uint64_t colors = m_.colors.size();
+  cudaStream_t s = ws.stream;
+  record_groups(ws, bases, nbases, offsets, records, recover, [&](uint64_t r0, uint64_t n) {
+    cuda_check(cudaMemcpyAsync(counts + r0 * colors, ws.rec_counts, n * colors * 8,
+                               cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaMemcpyAsync(totals + r0, ws.rec_totals, n * 8, cudaMemcpyDeviceToHost, s), "D2H");
+  });
+}
+
+void Engine::query_record_hits(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                               const uint64_t* offsets, uint64_t records, bool recover,
+                               double min_ratio, RecordHits& out) {
+  check(min_ratio > 0.0 && min_ratio <= 1.0, kEInval, "hit selection needs min_ratio in (0, 1]");
+  const uint32_t colors = (uint32_t)m_.colors.size();
+  cudaStream_t s = ws.stream;
+  out.totals.assign(records, 0);
+  out.first.assign(records + 1, 0);
+  out.colors.clear();
+  out.counts.clear();
+  record_groups(ws, bases, nbases, offsets, records, recover, [&](uint64_t r0, uint64_t n) {
+    const int grid = (int)std::min<uint64_t>((n + 7) / 8, (uint64_t)sms_ * 16);
+    count_record_hits_kernel<<<grid, 256, 0, s>>>(ws.rec_counts, ws.rec_totals, n, colors,
+                                                  min_ratio, ws.rec_hits);
+    cuda_check(cudaGetLastError(), "count_record_hits_kernel");
+    size_t tmp = ws.rec_scan_bytes;
+    cuda_check(cub::DeviceScan::ExclusiveSum(ws.rec_scan_tmp, tmp, ws.rec_hits, ws.rec_first,
+                                             (int)(n + 1), s),
+               "scan");
+    uint64_t hits = 0;
+    cuda_check(cudaMemcpyAsync(&hits, ws.rec_first + n, 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "per-record hits");
+    if (hits > ws.cap_hits || !ws.hit_colors) {
+      if (ws.hit_colors) cudaFree(ws.hit_colors);
+      if (ws.hit_counts) cudaFree(ws.hit_counts);
+      ws.hit_colors = nullptr;
+      ws.hit_counts = nullptr;
+      const uint64_t cap = std::max<uint64_t>({hits, ws.cap_hits * 3 / 2, 4096});
+      dev_alloc(&ws.hit_colors, cap, "record hits");
+      dev_alloc(&ws.hit_counts, cap, "record hit counts");
+      ws.cap_hits = cap;
+    }
+    if (hits)
+      write_record_hits_kernel<<<grid, 256, 0, s>>>(ws.rec_counts, ws.rec_totals, n, colors,
+                                                    min_ratio, ws.rec_first, ws.hit_colors,
+                                                    ws.hit_counts);
+    cuda_check(cudaGetLastError(), "write_record_hits_kernel");
+    const uint64_t base = out.colors.size();
+    out.colors.resize(base + hits);
+    out.counts.resize(base + hits);
+    if (hits) {
+      cuda_check(cudaMemcpyAsync(out.colors.data() + base, ws.hit_colors, hits * 4,
+                                 cudaMemcpyDeviceToHost, s),
+                 "D2H");
+      cuda_check(cudaMemcpyAsync(out.counts.data() + base, ws.hit_counts, hits * 8,
+                                 cudaMemcpyDeviceToHost, s),
+                 "D2H");
+    }
+    cuda_check(cudaMemcpyAsync(out.first.data() + r0, ws.rec_first, (n + 1) * 8,
+                               cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaMemcpyAsync(out.totals.data() + r0, ws.rec_totals, n * 8,
+                               cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaStreamSynchronize(s), "per-record hits");
+    // Group-relative offsets to global ones (first[r0 + n] is the next group's base).
+    for (uint64_t i = 0; i <= n; ++i) out.first[r0 + i] += base;
+  });
 }
 
 static void raise_error_word(uint32_t err) {

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <map>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -64,6 +65,14 @@ struct Workspace {
   uint64_t* rec_counts = nullptr;
   unsigned long long* rec_totals = nullptr;
   uint64_t cap_rec_counts = 0, cap_rec_totals = 0;
+  // Thresholded reports: per-record hit counts, their scan and the hits.
+  uint64_t* rec_hits = nullptr;    // group records + 1
+  uint64_t* rec_first = nullptr;   // group records + 1
+  void* rec_scan_tmp = nullptr;
+  size_t rec_scan_bytes = 0;
+  uint32_t* hit_colors = nullptr;
+  uint64_t* hit_counts = nullptr;
+  uint64_t cap_hits = 0;
   // Pinned host staging.
   uint8_t* h_bases = nullptr;
   uint64_t* h_offsets = nullptr;
@@ -158,6 +167,18 @@ class Engine {
   void query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                         const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
                         uint64_t* totals);
+  // Per-record hits for a report with min_ratio in (0, 1]: totals (records)
+  // and, for record r, the colours hit_colors[first[r] .. first[r+1]) with
+  // their counts, in colour order: those with count > 0 and count / total >=
+  // min_ratio. Selected on the device; only the hits are copied back.
+  struct RecordHits {
+    std::vector<uint64_t> totals, first;
+    std::vector<uint32_t> colors;
+    std::vector<uint64_t> counts;
+  };
+  void query_record_hits(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                         const uint64_t* offsets, uint64_t records, bool recover, double min_ratio,
+                         RecordHits& out);
   // Upper bound of the tiles of one record of `len` bases.
   uint64_t tiles_for_length(uint64_t len) const;
   // Seeds of host records in record/window order (extraction only).
@@ -178,6 +199,12 @@ class Engine {
   void plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records, uint64_t nbases,
                   cudaStream_t stream);
   void check_error_word(Workspace& ws);
+  // Runs host records in device groups (one segment per record): after each
+  // group's launch, on_group(r0, n) enqueues its read-back on ws.stream; the
+  // stream is then synchronised and the error word checked.
+  void record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
+                     uint64_t records, bool recover,
+                     const std::function<void(uint64_t, uint64_t)>& on_group);
 
   Manifest m_;
   int device_ = 0;

@@ -27,4 +27,10 @@ const char* record_header(RecordFormat format);
 void append_record(std::string& out, RecordFormat format, const std::string& name, uint64_t total,
                    const uint64_t* counts, const std::vector<ColorMeta>& colors, double min_ratio);
 
+// Appends the lines of one record whose reported colours are already chosen:
+// hit_colors[i] (ascending) with count hit_counts[i], i < hits.
+void append_record_hits(std::string& out, RecordFormat format, const std::string& name,
+                        uint64_t total, const uint32_t* hit_colors, const uint64_t* hit_counts,
+                        size_t hits, const std::vector<ColorMeta>& colors);
+
 }  // namespace zx
