@@ -501,8 +501,12 @@ def ours(args):
     records = len(offsets) - 1
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    torch.zeros(1, device=dev)  # the CUDA context exists before the load is timed
+    t_load = time.perf_counter()
     ix = zx.Index(index_dir, device=local)
+    load_s = time.perf_counter() - t_load
     info = ix.info
+    file_bytes = sum(p.stat().st_size for p in Path(index_dir).iterdir() if p.is_file())
     # Device-resident batch.
     d_bases = torch.from_numpy(bases).to(dev)
     d_off = torch.from_numpy(offsets.view(np.int64)).to(dev)
@@ -723,6 +727,11 @@ def ours(args):
                       "served_seeds_per_s": served["closed_loop"]["seeds_per_s"],
                       "planned_seeds_per_s": world * planned["seeds_per_s"],
                       "served": served, "planned": planned, "per_record": per_record},
+            "index_load": {"seconds": load_s, "file_bytes": file_bytes,
+                           "resident_bytes": int(info.resident_bytes),
+                           "resident_gb_per_s": info.resident_bytes / load_s / 1e9,
+                           "note": "zx_open: manifest, bank files (page cache), zstd frames "
+                                   "decoded on the host cores, upload and repack into HBM"},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cpu_baseline": cb,
