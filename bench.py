@@ -727,11 +727,14 @@ def ours(args):
                       "served_seeds_per_s": served["closed_loop"]["seeds_per_s"],
                       "planned_seeds_per_s": world * planned["seeds_per_s"],
                       "served": served, "planned": planned, "per_record": per_record},
-            "index_load": {"seconds": load_s, "file_bytes": file_bytes,
+            "index_load": {"seconds": load_s, "banks_s": info.load_banks_s,
+                           "recovery_s": info.load_recovery_s, "file_bytes": file_bytes,
                            "resident_bytes": int(info.resident_bytes),
                            "resident_gb_per_s": info.resident_bytes / load_s / 1e9,
-                           "note": "zx_open: manifest, bank files (page cache), zstd frames "
-                                   "decoded on the host cores, upload and repack into HBM"},
+                           "note": "zx_open: manifest; bank frames read (page cache) and "
+                                   "zstd-decoded on the host cores into a pinned ring whose "
+                                   "pieces are copied to HBM while later frames decode; the "
+                                   "recovery map decoded concurrently"},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cpu_baseline": cb,

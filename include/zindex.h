@@ -51,6 +51,9 @@ typedef struct zx_info {
   uint64_t gather_bytes_per_seed; /* fingerprint-plane bytes read per seed, all classes */
   uint64_t abandoned_hashes;
   int recovery;               /* manifest abandoned_recovery */
+  double load_s;              /* zx_open wall time */
+  double load_banks_s;        /* bank files read, decoded and uploaded (overlapped) */
+  double load_recovery_s;     /* recovery map read and decoded (concurrent with the banks) */
 } zx_info;
 
 typedef struct zx_launch {

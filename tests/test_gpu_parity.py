@@ -192,6 +192,29 @@ def test_legacy_interleaved_banks(gpu, oracle, tmp_path_factory, opts):
     gpu_vs_oracle(oracle, ix, reads_for(genomes, n=300, length=200, n_runs=0.1))
 
 
+@pytest.mark.parametrize("colors,length,legacy", [
+    (16, 1100000, False),  # 32-byte rows (64 MiB): pieces go straight to the resident rows
+    (20, 900000, False),   # 40-byte rows (48-byte stride, 40 MiB): staged and repacked
+    (20, 900000, True),    # legacy rows: staged and permuted
+])
+def test_multi_frame_banks_stream_into_hbm(gpu, oracle, tmp_path_factory, colors, length, legacy):
+    """Banks of many 4 MiB zstd frames and several 32 MiB upload pieces (frames
+    straddle piece boundaries) load to the same filters the oracle reads."""
+    import json
+
+    import zindex_b200 as zx
+
+    ix, genomes = index_for(tmp_path_factory, colors=colors, length=length, seed=17, k=31, H=4,
+                            b=16, legacy=legacy)
+    manifest = json.loads((ix / "manifest.json").read_text())
+    raw = sum(b["slots"] * ((b["row_bits"] + 7) // 8) for b in manifest["banks"])
+    assert raw > (32 << 20), raw
+    with zx.Index(ix) as index:
+        info = index.info
+        assert info.load_s >= info.load_banks_s > 0
+    gpu_vs_oracle(oracle, ix, reads_for(genomes, n=400, length=150, n_runs=0.1))
+
+
 @pytest.mark.parametrize("mode", ["kmers", "findere"])
 def test_pipelined_host_chunks_equal_one_pass(gpu, oracle, tmp_path_factory, mode):
     """A host batch cut into record-aligned chunks (copies overlapping the

@@ -103,6 +103,9 @@ int zx_index_info(const zx_index* index, zx_info* out) {
     out->gather_bytes_per_seed = index->engine->gather_bytes_per_seed();
     out->abandoned_hashes = m.abandoned_hashes;
     out->recovery = m.abandoned_recovery ? 1 : 0;
+    out->load_s = index->engine->load_seconds();
+    out->load_banks_s = index->engine->banks_load_seconds();
+    out->load_recovery_s = index->engine->recovery_load_seconds();
   });
 }
 

@@ -15,6 +15,7 @@
 #include "kernels/record_hits.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <thread>
 
@@ -424,7 +425,72 @@ Engine::~Engine() {
 
 int Engine::span() const { return (int)m_.k; }
 
+namespace {
+
+// Bank pieces from the host ring to the device: straight into the resident
+// rows when the padded stride equals the row (fingerprint-first banks of
+// 16-byte multiple rows), else through a device stage and the repack kernel.
+// One stream: a piece's copy and repack run in order; events tell the
+// decoder when a ring slot may be rewritten.
+struct UploadSink : PieceSink {
+  static constexpr int kSlots = 6;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done[kSlots] = {};
+  bool pending[kSlots] = {};
+  uint8_t* ring[kSlots] = {};
+  uint8_t* stage[kSlots] = {};
+  uint64_t piece_cap = 0;
+  int sms = 1;
+  // Current bank.
+  uint8_t* dst = nullptr;
+  uint64_t row_bytes = 0;
+  uint32_t stride = 0;
+  bool legacy = false;
+  const uint2* fields = nullptr;
+  uint32_t groups = 0;
+  int bits = 0;
+
+  void consume(int slot, uint64_t offset, uint64_t len) override {
+    const uint64_t rows = len / row_bytes, r0 = offset / row_bytes;
+    check(len % row_bytes == 0 && offset % row_bytes == 0, kEFormat, "bank piece splits a row");
+    if (!legacy && stride == row_bytes) {
+      cuda_check(cudaMemcpyAsync(dst + offset, ring[slot], len, cudaMemcpyHostToDevice, stream),
+                 "bank upload");
+    } else {
+      cuda_check(cudaMemcpyAsync(stage[slot], ring[slot], len, cudaMemcpyHostToDevice, stream),
+                 "bank upload");
+      if (!legacy)
+        repack_rows_kernel<<<sms * 8, 256, 0, stream>>>(stage[slot], rows, (uint32_t)row_bytes,
+                                                        stride, dst + r0 * stride);
+      else
+        repack_legacy_kernel<<<sms * 8, 256, 0, stream>>>(stage[slot], rows, (uint32_t)row_bytes,
+                                                          stride, fields, groups, bits,
+                                                          dst + r0 * stride);
+      cuda_check(cudaGetLastError(), "repack kernel");
+    }
+    cuda_check(cudaEventRecord(done[slot], stream), "cudaEventRecord");
+    pending[slot] = true;
+  }
+  void drain(int slot) override {
+    if (!pending[slot]) return;
+    pending[slot] = false;
+    cuda_check(cudaEventSynchronize(done[slot]), "bank upload");
+  }
+  ~UploadSink() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (int i = 0; i < kSlots; ++i) {
+      if (done[i]) cudaEventDestroy(done[i]);
+      if (ring[i]) cudaFreeHost(ring[i]);
+      if (stage[i]) cudaFree(stage[i]);
+    }
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+}  // namespace
+
 void Engine::load(const std::string& dir, const OpenOptions& options) {
+  const auto t_start = std::chrono::steady_clock::now();
   m_ = load_manifest(dir);
   device_ = options.device;
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
@@ -471,11 +537,48 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
   host_ix_.hashes = m_.hashes;
   host_ix_.bits = b;
 
-  // Staging for bank uploads.
-  const uint64_t stage_bytes = 256ull << 20;
-  uint8_t* d_stage = nullptr;
-  dev_alloc(&d_stage, stage_bytes, "bank staging");
-  std::vector<uint8_t> payload;
+  // The recovery map is read and decoded on its own thread while the banks
+  // stream in.
+  RecoveryRecords rr;
+  std::string rr_error;
+  int rr_code = kOk;
+  double recovery_s = 0;
+  std::thread recovery_thread;
+  if (m_.abandoned_recovery && m_.abandoned_hashes)
+    recovery_thread = std::thread([&] {
+      const auto t0 = std::chrono::steady_clock::now();
+      try {
+        rr = read_recovery(dir, m_);
+      } catch (const Error& e) {
+        rr_code = e.code;
+        rr_error = e.what();
+      } catch (const std::exception& e) {
+        rr_code = kEFormat;
+        rr_error = e.what();
+      }
+      recovery_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    });
+  struct Joiner {
+    std::thread& t;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+    }
+  } joiner{recovery_thread};
+
+  // Bank streaming: a pinned ring of 32 MiB pieces (row-aligned) filled by
+  // the frame decoders and drained by asynchronous copies.
+  const auto t_banks = std::chrono::steady_clock::now();
+  UploadSink up;
+  up.sms = sms_;
+  uint64_t max_row = 16;
+  for (auto& bm : m_.banks) max_row = std::max<uint64_t>(max_row, bm.row_bytes());
+  up.piece_cap = std::max<uint64_t>(32ull << 20, max_row);
+  cuda_check(cudaStreamCreateWithFlags(&up.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (int i = 0; i < UploadSink::kSlots; ++i) {
+    cuda_check(cudaEventCreateWithFlags(&up.done[i], cudaEventDisableTiming), "cudaEventCreate");
+    cuda_check(cudaHostAlloc((void**)&up.ring[i], up.piece_cap, cudaHostAllocDefault),
+               "pinned bank ring");
+  }
   for (size_t ci = 0; ci < m_.classes.size(); ++ci) {
     const auto& banks = m_.classes[ci];
     const BankMeta& first = m_.banks[banks[0]];
@@ -506,6 +609,7 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
         fields[g] = make_uint2((uint32_t)gm.offset, (uint32_t)gm.width);
       }
       dev_alloc(&d_fields, G, "legacy field table");
+      allocations_.push_back(d_fields);
       cuda_check(cudaMemcpy(d_fields, fields.data(), G * sizeof(uint2), cudaMemcpyHostToDevice),
                  "upload");
     }
@@ -516,33 +620,25 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
     for (size_t pi = 0; pi < banks.size(); ++pi) {
       const BankMeta& bm = m_.banks[banks[pi]];
       const uint64_t bytes = bm.slots * row_bytes;
-      payload.resize(bytes);
+      up.dst = data + pi * bm.slots * stride;
+      up.row_bytes = row_bytes;
+      up.stride = stride;
+      up.legacy = !bm.fingerprint_first;
+      up.fields = d_fields;
+      up.groups = (uint32_t)G;
+      up.bits = b;
+      if (up.legacy || stride != row_bytes)
+        for (int i = 0; i < UploadSink::kSlots; ++i)
+          if (!up.stage[i]) dev_alloc(&up.stage[i], up.piece_cap, "bank staging");
       uint8_t header[40];
-      read_bank_stream(dir + "/" + bm.file, header, payload.data(), bytes, threads);
+      const uint64_t piece = up.piece_cap / row_bytes * row_bytes;
+      stream_bank(dir + "/" + bm.file, header, bytes, piece, up.ring, UploadSink::kSlots, threads,
+                  up);
       check_format(!memcmp(header, bm.fingerprint_first ? "ZORPOW3\0" : "ZORPOW1\0", 8),
                    "invalid bank magic");
       check_format(le64(header + 8) == bm.slots && le64(header + 16) == bm.row_bits &&
                        le64(header + 24) == bm.groups.size() && le64(header + 32) == bytes,
                    "bank header differs from manifest");
-      uint8_t* dst = data + pi * bm.slots * stride;
-      const uint64_t rows_per_chunk = std::max<uint64_t>(1, stage_bytes / row_bytes);
-      for (uint64_t r0 = 0; r0 < bm.slots; r0 += rows_per_chunk) {
-        uint64_t rows = std::min(rows_per_chunk, bm.slots - r0);
-        cuda_check(cudaMemcpy(d_stage, payload.data() + r0 * row_bytes, rows * row_bytes,
-                              cudaMemcpyHostToDevice),
-                   "bank upload");
-        if (bm.fingerprint_first)
-          repack_rows_kernel<<<sms_ * 8, 256>>>(d_stage, rows, (uint32_t)row_bytes, stride,
-                                                dst + r0 * stride);
-        else
-          repack_legacy_kernel<<<sms_ * 8, 256>>>(d_stage, rows, (uint32_t)row_bytes, stride,
-                                                  d_fields, (uint32_t)G, b, dst + r0 * stride);
-        cuda_check(cudaGetLastError(), "repack kernel");
-      }
-    }
-    if (d_fields) {
-      cuda_check(cudaDeviceSynchronize(), "legacy repack");
-      cudaFree(d_fields);
     }
     // Group -> colour table, multi-member decode table.
     std::vector<uint32_t> gc(G), multi, members;
@@ -578,12 +674,15 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
     C.multi = d_multi;
     C.members = d_members;
   }
+  cuda_check(cudaStreamSynchronize(up.stream), "bank upload");
   cuda_check(cudaDeviceSynchronize(), "bank upload");
-  cudaFree(d_stage);
+  banks_load_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_banks).count();
 
   // Recovery directory.
+  if (recovery_thread.joinable()) recovery_thread.join();
+  recovery_load_s_ = recovery_s;
+  if (rr_code != kOk) raise(rr_code, rr_error);
   if (m_.abandoned_recovery && m_.abandoned_hashes) {
-    RecoveryRecords rr = read_recovery(dir, m_);
     const uint64_t n = rr.hashes.size();
     check(n < (1ull << 31), kEUnsupported, "too many abandoned hashes for the device directory");
     check(rr.origins.size() < (1ull << 32), kEUnsupported, "too many abandoned origins");
@@ -634,6 +733,7 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
   cuda_check(cudaMemcpy(d_ix_norec_, &norec, sizeof(DevIndex), cudaMemcpyHostToDevice), "upload");
   launch_ = default_launch();
   ws_ = make_workspace();
+  load_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
 }
 
 uint64_t Engine::gather_bytes_per_seed() const {

@@ -99,6 +99,11 @@ class Engine {
   Engine& operator=(const Engine&) = delete;
 
   const Manifest& manifest() const { return m_; }
+  // Seconds of the load: total, the bank streaming (read, decode, upload) and
+  // the recovery map (read and decoded concurrently with the banks).
+  double load_seconds() const { return load_s_; }
+  double banks_load_seconds() const { return banks_load_s_; }
+  double recovery_load_seconds() const { return recovery_load_s_; }
   int device() const { return device_; }
   uint64_t resident_bytes() const { return resident_bytes_; }
   int span() const;  // k-window span of the index mode
@@ -222,6 +227,7 @@ class Engine {
   cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
   int cached_blocks_ = 0;
   bool noalloc_used_ = false;
+  double load_s_ = 0, banks_load_s_ = 0, recovery_load_s_ = 0;
   QueryLaunch cached_for_{};
 };
 

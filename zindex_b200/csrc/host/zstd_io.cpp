@@ -1,9 +1,15 @@
 #include "zstd_io.h"
 
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <atomic>
 #include <cerrno>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <thread>
 
 #include "error.h"
@@ -101,17 +107,15 @@ struct FrameInfo {
 };
 
 // Seek table of a framed bank (bank_io.rs:114-197). Empty when absent.
-std::vector<FrameInfo> seek_table(const std::vector<uint8_t>& f, size_t raw_total) {
+// tail: the file's last len + 8 bytes (the skippable frame holding the
+// table), which start at file offset `start`.
+std::vector<FrameInfo> seek_table(const std::vector<uint8_t>& tail, uint64_t start,
+                                  size_t raw_total) {
   std::vector<FrameInfo> frames;
-  size_t length = f.size();
-  if (length < 16 || memcmp(&f[length - 16], "ZORSEEK1", 8) != 0) return frames;
-  uint64_t len = le64(&f[length - 8]);
-  check_format(len >= 40 && len <= (64u << 20) && (len - 40) % 32 == 0 && len + 8 <= length,
-               "invalid bank seek table length");
-  size_t start = length - len - 8;
-  check_format(le32(&f[start]) == kSkip && le32(&f[start + 4]) == len,
-               "invalid skippable bank index");
-  const uint8_t* t = &f[start + 8];
+  const uint64_t len = tail.size() - 8;
+  check_format(len >= 40 && (len - 40) % 32 == 0, "invalid bank seek table length");
+  check_format(le32(&tail[0]) == kSkip && le32(&tail[4]) == len, "invalid skippable bank index");
+  const uint8_t* t = &tail[8];
   check_format(memcmp(t, "ZORFRM1\0", 8) == 0 && memcmp(t + len - 16, "ZORSEEK1", 8) == 0 &&
                    le64(t + len - 8) == len,
                "invalid bank seek table tag");
@@ -167,27 +171,79 @@ std::vector<uint8_t> zstd_decode_all(const uint8_t* data, size_t len) {
   return out;
 }
 
-void read_bank_stream(const std::string& path, uint8_t header[40], uint8_t* payload,
-                      size_t payload_len, int threads) {
-  std::vector<uint8_t> file = read_file_bytes(path);
-  const size_t raw_total = payload_len + kHeader;
-  std::vector<FrameInfo> frames = seek_table(file, raw_total);
+namespace {
+
+struct Fd {
+  int fd = -1;
+  ~Fd() {
+    if (fd >= 0) close(fd);
+  }
+};
+
+void pread_full(int fd, uint8_t* dst, size_t n, uint64_t off, const std::string& path) {
+  while (n) {
+    ssize_t r = pread(fd, dst, n, (off_t)off);
+    if (r < 0 && errno == EINTR) continue;
+    if (r <= 0) raise(kEIo, "short read of " + path);
+    dst += r;
+    n -= (size_t)r;
+    off += (uint64_t)r;
+  }
+}
+
+}  // namespace
+
+void stream_bank(const std::string& path, uint8_t header[40], uint64_t payload_len,
+                 uint64_t piece_bytes, uint8_t* const* ring, int slots, int threads,
+                 PieceSink& sink) {
+  check(slots >= 3 && piece_bytes > 0, kEInval, "bank streaming needs three ring slots");
+  const uint64_t raw_total = payload_len + kHeader;
+  const uint64_t pieces = (payload_len + piece_bytes - 1) / piece_bytes;
+  auto piece_len = [&](uint64_t c) { return std::min(piece_bytes, payload_len - c * piece_bytes); };
+  Fd f;
+  f.fd = open(path.c_str(), O_RDONLY);
+  if (f.fd < 0) raise(kEIo, "cannot open " + path + ": " + strerror(errno));
+  struct stat st;
+  if (fstat(f.fd, &st) != 0) raise(kEIo, "cannot stat " + path);
+  const uint64_t file_len = (uint64_t)st.st_size;
+  // The seek table is the file's tail: read only that, then frames on demand.
+  std::vector<FrameInfo> frames;
+  if (file_len >= 16) {
+    uint8_t tail16[16];
+    pread_full(f.fd, tail16, 16, file_len - 16, path);
+    if (!memcmp(tail16, "ZORSEEK1", 8)) {
+      const uint64_t len = le64(tail16 + 8);
+      check_format(len >= 40 && len <= (64u << 20) && len + 8 <= file_len,
+                   "invalid bank seek table length");
+      std::vector<uint8_t> tail(len + 8);
+      pread_full(f.fd, tail.data(), tail.size(), file_len - len - 8, path);
+      frames = seek_table(tail, file_len - len - 8, raw_total);
+    }
+  }
   if (frames.size() <= 1) {
-    // Stream decode (legacy single stream or one frame).
-    size_t at = 0;
+    // Legacy single stream (or one frame): decoded in order on this thread.
+    std::vector<uint8_t> file = read_file_bytes(path);
+    uint64_t at = 0, c = 0, fill = 0;
     bool extra = false;
-    auto sink = [&](const uint8_t* p, size_t n) {
+    auto emit = [&](const uint8_t* p, size_t n) {
       for (size_t i = 0; i < n;) {
         if (at < kHeader) {
-          size_t take = std::min(n - i, kHeader - at);
+          size_t take = std::min<uint64_t>(n - i, kHeader - at);
           memcpy(header + at, p + i, take);
           at += take;
           i += take;
         } else if (at - kHeader < payload_len) {
-          size_t take = std::min(n - i, payload_len - (at - kHeader));
-          memcpy(payload + (at - kHeader), p + i, take);
+          if (fill == 0 && c >= (uint64_t)slots) sink.drain((int)(c % slots));
+          size_t take = std::min<uint64_t>(n - i, piece_len(c) - fill);
+          memcpy(ring[c % slots] + fill, p + i, take);
+          fill += take;
           at += take;
           i += take;
+          if (fill == piece_len(c)) {
+            sink.consume((int)(c % slots), c * piece_bytes, fill);
+            ++c;
+            fill = 0;
+          }
         } else {
           extra = true;
           return;
@@ -195,42 +251,122 @@ void read_bank_stream(const std::string& path, uint8_t header[40], uint8_t* payl
       }
     };
     if (is_zstd(file.data(), file.size()))
-      stream_decode(file.data(), file.size(), sink);
+      stream_decode(file.data(), file.size(), emit);
     else
-      sink(file.data(), file.size());
+      emit(file.data(), file.size());
     check_format(at == raw_total, "short bank data");
     check_format(!extra, "unexpected bank data");
+    for (int sl = 0; sl < slots; ++sl) sink.drain(sl);
     return;
   }
-  // Parallel frames straight into the destination (bank_io.rs:235-292).
-  std::atomic<size_t> next{0};
-  std::atomic<bool> failed{false};
+  // Frames (bank_io.rs:235-292) are decoded by the workers in frame order
+  // into the ring; piece c lives in slot c % slots and may be written once
+  // the consumer has released piece c - slots. The calling thread hands
+  // every complete piece to the sink in order.
+  std::mutex mu;
+  std::condition_variable cv_filled, cv_free;
+  std::vector<uint64_t> filled(pieces, 0);
+  uint64_t released = 0;  // pieces [0, released) no longer occupy their slots
+  bool failed = false;
   std::string error;
-  std::vector<uint8_t> first(frames[0].raw_len);
+  std::atomic<size_t> next{0};
+  auto fail = [&](const std::string& msg) {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!failed) error = msg;
+    failed = true;
+    cv_filled.notify_all();
+    cv_free.notify_all();
+  };
   auto worker = [&]() {
     ZSTD_DCtx* d = ZSTD_createDCtx();
-    for (size_t i; !failed && (i = next.fetch_add(1)) < frames.size();) {
-      const FrameInfo& fr = frames[i];
-      const uint8_t* src = file.data() + fr.compressed;
-      bool ok = ZSTD_findFrameCompressedSize(src, fr.compressed_len) == fr.compressed_len &&
-                ZSTD_getFrameContentSize(src, fr.compressed_len) == fr.raw_len;
-      uint8_t* dst = i == 0 ? first.data() : payload + (fr.raw - kHeader);
-      if (ok) {
-        size_t r = ZSTD_decompressDCtx(d, dst, fr.raw_len, src, fr.compressed_len);
-        ok = !ZSTD_isError(r) && r == fr.raw_len;
+    std::vector<uint8_t> src, tmp;
+    try {
+      for (size_t i; (i = next.fetch_add(1)) < frames.size();) {
+        {
+          std::lock_guard<std::mutex> lock(mu);
+          if (failed) break;
+        }
+        const FrameInfo& fr = frames[i];
+        // Payload bytes of this frame (frame 0 also carries the header).
+        const uint64_t p0 = fr.raw < kHeader ? 0 : fr.raw - kHeader;
+        const uint64_t p1 = fr.raw + fr.raw_len - kHeader;
+        const uint64_t c0 = p0 / piece_bytes, c1 = p1 > p0 ? (p1 - 1) / piece_bytes : c0;
+        src.resize(fr.compressed_len);
+        pread_full(f.fd, src.data(), src.size(), fr.compressed, path);
+        bool ok = ZSTD_findFrameCompressedSize(src.data(), src.size()) == fr.compressed_len &&
+                  ZSTD_getFrameContentSize(src.data(), src.size()) == fr.raw_len;
+        if (!ok) {
+          fail("corrupt bank frame in " + path);
+          break;
+        }
+        {
+          std::unique_lock<std::mutex> lock(mu);
+          cv_free.wait(lock, [&] { return failed || (p1 <= p0) || c1 < released + slots; });
+          if (failed) break;
+        }
+        const bool direct = i != 0 && c0 == c1;
+        uint8_t* dst;
+        if (direct) {
+          dst = ring[c0 % slots] + (p0 - c0 * piece_bytes);
+        } else {
+          tmp.resize(fr.raw_len);
+          dst = tmp.data();
+        }
+        size_t r = ZSTD_decompressDCtx(d, dst, fr.raw_len, src.data(), src.size());
+        if (ZSTD_isError(r) || r != fr.raw_len) {
+          fail("corrupt bank frame in " + path);
+          break;
+        }
+        const uint8_t* body = dst;
+        if (i == 0) {
+          memcpy(header, dst, kHeader);
+          body = dst + kHeader;
+        }
+        if (!direct)
+          for (uint64_t c = c0; p1 > p0 && c <= c1; ++c) {
+            const uint64_t a = std::max(p0, c * piece_bytes);
+            const uint64_t b = std::min(p1, c * piece_bytes + piece_len(c));
+            memcpy(ring[c % slots] + (a - c * piece_bytes), body + (a - p0), b - a);
+          }
+        std::lock_guard<std::mutex> lock(mu);
+        for (uint64_t c = c0; p1 > p0 && c <= c1; ++c) {
+          const uint64_t a = std::max(p0, c * piece_bytes);
+          const uint64_t b = std::min(p1, c * piece_bytes + piece_len(c));
+          filled[c] += b - a;
+        }
+        cv_filled.notify_all();
       }
-      if (!ok && !failed.exchange(true)) error = "corrupt bank frame in " + path;
+    } catch (const std::exception& e) {
+      fail(e.what());
     }
     ZSTD_freeDCtx(d);
   };
-  int n = std::max(1, std::min<int>(threads, (int)frames.size()));
+  const int n = std::max(1, std::min<int>(threads, (int)frames.size()));
   std::vector<std::thread> pool;
-  for (int t = 1; t < n; ++t) pool.emplace_back(worker);
-  worker();
+  for (int t = 0; t < n; ++t) pool.emplace_back(worker);
+  try {
+    for (uint64_t c = 0; c < pieces; ++c) {
+      {
+        std::unique_lock<std::mutex> lock(mu);
+        cv_filled.wait(lock, [&] { return failed || filled[c] == piece_len(c); });
+        if (failed) break;
+      }
+      sink.consume((int)(c % slots), c * piece_bytes, piece_len(c));
+      // One piece in flight: once the previous piece is consumed its slot
+      // is free for piece c - 1 + slots.
+      if (c >= 1) {
+        sink.drain((int)((c - 1) % slots));
+        std::lock_guard<std::mutex> lock(mu);
+        released = c;
+        cv_free.notify_all();
+      }
+    }
+  } catch (const std::exception& e) {
+    fail(e.what());
+  }
   for (auto& th : pool) th.join();
+  for (int sl = 0; sl < slots; ++sl) sink.drain(sl);
   if (failed) raise(kEFormat, error);
-  memcpy(header, first.data(), kHeader);
-  memcpy(payload, first.data() + kHeader, frames[0].raw_len - kHeader);
 }
 
 FramedWriter::FramedWriter(const std::string& path, int level) : path_(path), level_(level) {

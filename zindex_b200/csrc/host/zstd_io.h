@@ -17,12 +17,31 @@ void write_file_bytes(const std::string& path, const void* data, size_t len);
 // raw input without the zstd magic is returned unchanged.
 std::vector<uint8_t> zstd_decode_all(const uint8_t* data, size_t len);
 
-// Decoded bank stream = 40-byte header + payload. Frames are decoded in
-// parallel (threads) straight into `payload` (payload_len bytes). When the
-// file has no seek table it is stream-decoded. Throws zx::Error on any
-// mismatch, corruption or trailing data.
-void read_bank_stream(const std::string& path, uint8_t header[40], uint8_t* payload,
-                      size_t payload_len, int threads);
+// Consumer of a streamed bank payload (see stream_bank).
+class PieceSink {
+ public:
+  virtual ~PieceSink() = default;
+  // Payload bytes [offset, offset + len) are complete in ring slot `slot`:
+  // start consuming them (for example an asynchronous copy to the device).
+  virtual void consume(int slot, uint64_t offset, uint64_t len) = 0;
+  // Returns once the slot's last consumed piece is no longer read (its
+  // buffer may be rewritten); a no-op for a slot with nothing in flight.
+  virtual void drain(int slot) = 0;
+};
+
+// Decoded bank stream = 40-byte header + payload (payload_len bytes). The
+// header goes to `header`; the payload is handed to `sink` in order, in
+// pieces of piece_bytes (the last may be shorter) through a ring of `slots`
+// (>= 3) caller-owned buffers of piece_bytes each (piece c in slot
+// c % slots). Frames are read with pread and decoded by `threads` workers in
+// frame order straight into the ring, so reading, decoding and the sink's
+// consumption overlap; the file is never held whole in memory. When the file
+// has no seek table it is stream-decoded on the calling thread. Throws
+// zx::Error on any mismatch, corruption or trailing data; every slot is
+// drained before it returns or throws.
+void stream_bank(const std::string& path, uint8_t header[40], uint64_t payload_len,
+                 uint64_t piece_bytes, uint8_t* const* ring, int slots, int threads,
+                 PieceSink& sink);
 
 // Writer of the framed format with its seek table.
 class FramedWriter {
