@@ -575,6 +575,10 @@ def ours(args):
     alg_bytes = seeds * (gather + rec_bytes) + len(bases) * 3 // 8
     peak, peak_kind = hbm_peak()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    # The same gather in whole 32-byte DRAM sectors (each row touch costs its sectors).
+    sector = info.gather_sector_bytes_per_seed
+    sector_bytes = seeds * (sector + (32 if rec_bytes else 0)) + len(bases) * 3 // 8
+    sector_achieved = sector_bytes / (kernel_ms / 1e3) / 1e9
 
     log("stage: end to end")
     # End to end through the C ABI with pinned host buffers.
@@ -722,7 +726,10 @@ def ours(args):
                          "peak_kind": peak_kind,
                          "kernel": "fused_query_kernel", "kernel_ms": kernel_ms,
                          "algorithmic_bytes_per_launch": int(alg_bytes),
-                         "gather_bytes_per_seed": int(gather)},
+                         "gather_bytes_per_seed": int(gather),
+                         "sector_bytes_per_seed": int(sector),
+                         "sector_achieved": sector_achieved, "sector_frac": sector_achieved / peak,
+                         "l2_resident": bool(info.resident_bytes < (126 << 20))},
             "forms": {"plain_seeds_per_s": plain_rate, "batched_seeds_per_s": value / world,
                       "served_seeds_per_s": served["closed_loop"]["seeds_per_s"],
                       "planned_seeds_per_s": world * planned["seeds_per_s"],

@@ -49,6 +49,7 @@ typedef struct zx_info {
   uint64_t classes;           /* source size classes */
   uint64_t resident_bytes;    /* HBM held by the index */
   uint64_t gather_bytes_per_seed; /* fingerprint-plane bytes read per seed, all classes */
+  uint64_t gather_sector_bytes_per_seed; /* the same reads in whole 32-byte DRAM sectors */
   uint64_t abandoned_hashes;
   int recovery;               /* manifest abandoned_recovery */
   double load_s;              /* zx_open wall time */

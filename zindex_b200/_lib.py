@@ -42,6 +42,7 @@ class ZxInfo(ctypes.Structure):
         ("fingerprint_bits", c_uint32), ("index_mode", c_uint32), ("minimizer_size", c_uint32),
         ("seed", c_uint64), ("colors", c_uint64), ("banks", c_uint64), ("classes", c_uint64),
         ("resident_bytes", c_uint64), ("gather_bytes_per_seed", c_uint64),
+        ("gather_sector_bytes_per_seed", c_uint64),
         ("abandoned_hashes", c_uint64), ("recovery", c_int),
         ("load_s", c_double), ("load_banks_s", c_double), ("load_recovery_s", c_double),
     ]

@@ -101,6 +101,7 @@ int zx_index_info(const zx_index* index, zx_info* out) {
     out->classes = m.classes.size();
     out->resident_bytes = index->engine->resident_bytes();
     out->gather_bytes_per_seed = index->engine->gather_bytes_per_seed();
+    out->gather_sector_bytes_per_seed = index->engine->gather_sector_bytes_per_seed();
     out->abandoned_hashes = m.abandoned_hashes;
     out->recovery = m.abandoned_recovery ? 1 : 0;
     out->load_s = index->engine->load_seconds();

@@ -736,6 +736,19 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
   load_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
 }
 
+uint64_t Engine::gather_sector_bytes_per_seed() const {
+  uint64_t s = 0;
+  for (uint32_t c = 0; c < host_ix_.classes; ++c) {
+    const DevClass& C = host_ix_.cls[c];
+    const uint64_t len = (uint64_t)C.fp_chunks * 16;
+    const uint64_t at0 = (len + 31) / 32, at16 = (16 + len + 31) / 32;
+    // Sectors per row, times 2 so the average over both row phases stays exact.
+    const uint64_t twice = C.row_stride % 32 == 0 ? 2 * at0 : at0 + at16;
+    s += (uint64_t)m_.hashes * twice * 16;
+  }
+  return s;
+}
+
 uint64_t Engine::gather_bytes_per_seed() const {
   uint64_t s = 0;
   for (auto& cls : m_.classes) s += (uint64_t)m_.hashes * m_.banks[cls[0]].lookup_bytes(m_.fingerprint_bits);

@@ -116,6 +116,10 @@ class Engine {
   int max_blocks(const QueryLaunch& l) const;
   // Bytes of fingerprint planes gathered per seed, summed over classes.
   uint64_t gather_bytes_per_seed() const;
+  // The same gather counted in 32-byte DRAM sectors: per class H rows of
+  // fp_chunks 16-byte chunks, each row starting at row * stride (rows of a
+  // 16-byte-odd stride alternate between sector offsets 0 and 16).
+  uint64_t gather_sector_bytes_per_seed() const;
 
   std::unique_ptr<Workspace> make_workspace();
   // Sizes a workspace's device buffers for batches up to these sizes.
