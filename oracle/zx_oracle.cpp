@@ -285,10 +285,45 @@ struct Features {
   size_t z = 10;
   bool homopolymer = false;
   int scheme = 1;  // 1 open-closed-mod (0 = simd: not restated, third-party)
+  // Spaced seed (src/anchors.rs:10-90): 2 bits per pattern base, '#' = 3;
+  // width 0 = none.
+  uint64_t pattern_mask = 0;
+  size_t pattern_width = 0;
 };
 
-// scan_plain_features_uncompressed (src/lib.rs:608-642) on one ACGT run.
+// SpacedSeed::from_str (src/anchors.rs:15-42).
+bool parse_pattern(const std::string& p, uint64_t* mask, size_t* width) {
+  if (p.empty() || p.size() > 31) return false;
+  bool any = false;
+  uint64_t m = 0;
+  for (size_t i = 0; i < p.size(); ++i) {
+    if (p[i] != '#' && p[i] != '_') return false;
+    if (p[i] != p[p.size() - 1 - i]) return false;
+    any |= p[i] == '#';
+    m = (m << 2) | (p[i] == '#' ? 3 : 0);
+  }
+  if (!any) return false;
+  *mask = m;
+  *width = p.size();
+  return true;
+}
+
+// SpacedSeed::project_portable and ::canonical (src/anchors.rs:72-90).
+uint64_t pattern_project(uint64_t mask, size_t width, uint64_t key) {
+  uint64_t r = 0;
+  for (size_t i = width; i-- > 0;)
+    if (mask & (3ull << (2 * i))) r = (r << 2) | ((key >> (2 * i)) & 3);
+  return r;
+}
+uint64_t pattern_canonical(uint64_t mask, size_t width, uint64_t key) {
+  return canonical_encoded(pattern_project(mask, width, key),
+                           (size_t)__builtin_popcountll(mask) / 2);
+}
+
+// scan_plain_features_uncompressed (src/lib.rs:608-642) on one ACGT run,
+// then the spaced-seed mapping of anchors::scan (src/anchors.rs:265-281).
 void scan_run_features(const uint8_t* seq, size_t n, const Features& f, Emit& keys) {
+  const size_t first = keys.size();
   switch (f.mode) {
     case 0:
       scan_canonical_kmers(seq, n, f.k, keys);
@@ -307,6 +342,9 @@ void scan_run_features(const uint8_t* seq, size_t n, const Features& f, Emit& ke
       if (n >= f.k) scan_canonical_kmers(seq, n, f.k - f.z, keys);
       break;
   }
+  if (f.pattern_width && f.mode <= 1)
+    for (size_t i = first; i < keys.size(); ++i)
+      keys[i] = pattern_canonical(f.pattern_mask, f.pattern_width, keys[i]);
 }
 
 // Calls visit(run, len) for every maximal ACGT run of a sequence, after the
@@ -827,7 +865,15 @@ std::unique_ptr<Index> load_index(const std::string& dir, bool recover, bool pay
   ix->f.scheme = (sch && sch->kind == Json::Str && sch->s == "open-closed-mod") ? 1 : 0;
   ensure(!(ix->f.mode == 1 && ix->f.scheme == 0), "simd minimizer scheme is not restated");
   const Json* sp = m.get("seed_pattern");
-  ensure(!sp || sp->kind == Json::Null, "spaced seeds are not restated");
+  if (sp && sp->kind != Json::Null) {
+    // FeatureConfig::validate_anchors (src/lib.rs:177-206).
+    ensure(sp->kind == Json::Str && parse_pattern(sp->s, &ix->f.pattern_mask, &ix->f.pattern_width),
+           "invalid seed pattern");
+    ensure(ix->f.mode == 0 || ix->f.mode == 1,
+           "spaced seeds and randstrobemers require --index-mode kmers or minimizers");
+    ensure(ix->f.pattern_width == (ix->f.mode == 1 ? ix->f.m : ix->f.k),
+           "seed pattern width must match k (or m in minimizer mode)");
+  }
   const Json* rs = m.get("randstrobemers");
   ensure(!rs || rs->kind == Json::Null, "randstrobemers are not restated");
   const Json* ar = m.get("abandoned_recovery");
@@ -1301,6 +1347,19 @@ int oracle_features(const uint8_t* seq, size_t len, int mode, int k, int m, uint
                  [&](const uint8_t* run, size_t n) { scan_run_features(run, n, f, keys); });
     *count = keys.size();
     memcpy(out, keys.data(), std::min(cap, keys.size()) * 8);
+  });
+}
+
+// Spaced-seed key of a 2-bit key under a pattern (anchors.rs:86-90); returns
+// ZX error when the pattern is invalid.
+int oracle_pattern_canonical(const char* pattern, uint64_t key, uint64_t* projected,
+                             uint64_t* canonical) {
+  return guarded([&] {
+    uint64_t mask = 0;
+    size_t width = 0;
+    ensure(parse_pattern(pattern, &mask, &width), "invalid seed pattern");
+    *projected = pattern_project(mask, width, key);
+    *canonical = pattern_canonical(mask, width, key);
   });
 }
 

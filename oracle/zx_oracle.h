@@ -71,6 +71,11 @@ int oracle_records_report_handle(oracle_index* index, const char* query_path, do
                                  int compact, int threads, char* buf, size_t cap,
                                  size_t* written, double* seconds);
 
+/* Spaced seed (anchors.rs:15-90): the projection and canonical key of a
+ * 2-bit key under a '#'/'_' pattern. */
+int oracle_pattern_canonical(const char* pattern, uint64_t key, uint64_t* projected,
+                             uint64_t* canonical);
+
 const char* oracle_last_error(void);
 
 #ifdef __cplusplus

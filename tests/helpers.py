@@ -203,7 +203,7 @@ def build_index(fof: Path, out: Path, **opts) -> Path:
     args = [str(ZX_BUILD), "-f", str(fof), "-o", str(out), "-q"]
     flag = {"k": "-k", "m": "-m", "H": "-H", "b": "-b", "seed": "-s", "mode": "-i", "z": "-z",
             "d": "-d", "scale": "-S", "seg": "-L", "min_docs": "-D", "max_sub": "-N",
-            "max_size": "-X", "threads": "-t", "groups": "--groups"}
+            "max_size": "-X", "threads": "-t", "groups": "--groups", "pattern": "-p"}
     for key, val in opts.items():
         if key == "drop_abandoned":
             if val:

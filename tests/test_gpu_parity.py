@@ -192,6 +192,25 @@ def test_legacy_interleaved_banks(gpu, oracle, tmp_path_factory, opts):
     gpu_vs_oracle(oracle, ix, reads_for(genomes, n=300, length=200, n_runs=0.1))
 
 
+SPACED_CASES = [
+    dict(mode="kmers", k=21, H=4, b=8, pattern="###_#_##_" + "###" + "_##_#_###"),
+    dict(mode="kmers", k=31, H=3, b=16, pattern="#_" * 15 + "#", homopolymer=True),
+    dict(mode="kmers", k=15, H=4, b=4, pattern="#" * 15),
+    dict(mode="minimizers", k=31, m=15, H=4, b=8, pattern="##_##_###_##_##"),
+    dict(mode="minimizers", k=21, m=21, H=2, b=8, pattern="##__" + "#" * 13 + "__##"),
+]
+
+
+@pytest.mark.parametrize("case", SPACED_CASES, ids=lambda c: f"{c['mode']}-k{c['k']}-{c['pattern']}")
+def test_spaced_seeds_match_oracle(gpu, oracle, tmp_path_factory, case):
+    """Spaced seeds (anchors.rs:265-281): the selected canonical k-mers or
+    minimizers mapped through the pattern, counted as the oracle counts them."""
+    ix, genomes = index_for(tmp_path_factory, colors=5, length=20000, seed=23, **case)
+    reads = reads_for(genomes, n=400, length=180, n_runs=0.1, lower=0.01)
+    gpu_vs_oracle(oracle, ix, reads)
+    gpu_vs_oracle(oracle, ix, reads, recover=False)
+
+
 @pytest.mark.parametrize("colors,length,legacy", [
     (16, 1100000, False),  # 32-byte rows (64 MiB): pieces go straight to the resident rows
     (20, 900000, False),   # 40-byte rows (48-byte stride, 40 MiB): staged and repacked

@@ -53,6 +53,7 @@ MODES = [
     dict(mode="modimizers", k=31, d=8, H=2, b=16),
     dict(mode="findere", k=31, z=10, H=4, b=8),
     dict(mode="kmers", k=31, H=4, b=8, homopolymer=True),
+    dict(mode="minimizers", k=31, m=15, H=4, b=8, pattern="##_##_###_##_##"),
 ]
 
 

@@ -138,3 +138,81 @@ def test_planner_measurements_and_features():
     assert rows and set(defaults) == {r.setting for r in rows}
     x = pl.encode(rows[0].features, rows[0].launch, rows[0].e2e)
     assert x.shape == (len(pl.FEATURES),) and np.isfinite(x).all()
+
+
+# ---- spaced seeds (src/anchors.rs:751-773 pattern_validation_and_projection) ----
+def _encode(seq: str) -> int:
+    v = 0
+    for ch in seq:
+        v = (v << 2) | "ACGT".index(ch)
+    return v
+
+
+def _rc(seq: str) -> str:
+    return seq[::-1].translate(str.maketrans("ACGT", "TGCA"))
+
+
+def _pattern(oracle, pattern, key):
+    import ctypes
+    from ctypes import POINTER, c_char_p, c_int, c_uint64
+
+    f = oracle.lib.oracle_pattern_canonical
+    f.argtypes = [c_char_p, c_uint64, POINTER(c_uint64), POINTER(c_uint64)]
+    f.restype = c_int
+    proj, canon = c_uint64(), c_uint64()
+    rc = f(pattern.encode(), key, ctypes.byref(proj), ctypes.byref(canon))
+    return rc, proj.value, canon.value
+
+
+@pytest.mark.parametrize("invalid", ["", "___", "#x#", "##_", "#" * 31 + "_"])
+def test_spaced_seed_pattern_validation(oracle, invalid):
+    assert _pattern(oracle, invalid, 0)[0] != 0
+
+
+def test_spaced_seed_projection_and_canonical(oracle):
+    p = "##_##_##"
+    rc, proj, _ = _pattern(oracle, p, _encode("ACGTAACG"))
+    assert rc == 0 and proj == _encode("ACTACG")
+    a, b = "ACATACCG", "ACGTAGCG"
+    ca = _pattern(oracle, p, _encode(a))[2]
+    assert ca == _pattern(oracle, p, _encode(b))[2]
+    assert ca == _pattern(oracle, p, _encode(_rc(a)))[2]
+
+
+def test_all_retained_pattern_leaves_keys_unchanged(oracle):
+    # anchors.rs:841-855: a pattern of only '#' maps every canonical key to itself.
+    seq = dna(2000, 77)
+    for key in oracle.features(seq, k=9)[:500]:
+        assert _pattern(oracle, "#########", int(key))[2] == int(key)
+
+
+def test_builder_spaced_seed_keys_match_oracle(oracle, tmp_path):
+    """The builder's distinct spaced-seed keys per colour (manifest unique_kmers)
+    equal the oracle's plain canonical keys mapped through the pattern."""
+    import json
+
+    import helpers
+
+    pattern = "##_#_##_#_##"  # width 12 = k, weight 8
+    for mode, extra in (("kmers", dict(k=12)), ("minimizers", dict(k=21, m=12))):
+        d = tmp_path / mode
+        fof = helpers.make_genomes(d / "g", 3, 6000, 91)
+        ix = helpers.build_index(fof, d / "ix", mode=mode, H=3, b=8, pattern=pattern, **extra)
+        manifest = json.loads((ix / "manifest.json").read_text())
+        assert manifest["seed_pattern"] == pattern
+        for c, col in enumerate(manifest["colors"]):
+            plain = oracle.features(dna(6000, 91 + c), mode=mode, **extra)
+            mapped = {_pattern(oracle, pattern, int(k))[2] for k in plain}
+            assert col["unique_kmers"] == len(mapped), (mode, c)
+
+
+def test_builder_rejects_invalid_patterns(native, tmp_path):
+    import subprocess
+
+    import helpers
+
+    fof = helpers.make_genomes(tmp_path / "g", 2, 3000, 5)
+    for i, (pattern, opts) in enumerate([("##_", dict(k=3)), ("#_#", dict(k=5)),
+                                         ("###", dict(mode="findere", k=13, z=10))]):
+        with pytest.raises(subprocess.CalledProcessError):
+            helpers.build_index(fof, tmp_path / f"ix{i}", pattern=pattern, **opts)

@@ -365,7 +365,7 @@ void build_index(const BuildOptions& opt) {
   const auto t0 = std::chrono::steady_clock::now();
   const int threads = opt.threads > 0 ? opt.threads : (int)std::thread::hardware_concurrency();
   const int H = opt.hashes, b = opt.fingerprint_bits;
-  const FeatureParams& fp = opt.features;
+  FeatureParams fp = opt.features;
   check(H >= 2 && H <= kMaxHashes, kEInval, "invalid hash count");
   check(b == 1 || b == 2 || b == 4 || b == 8 || b == 16 || b == 32, kEInval,
         "fingerprint bits must be 1, 2, 4, 8, 16 or 32");
@@ -382,6 +382,17 @@ void build_index(const BuildOptions& opt) {
       break;
     case 3: check(fp.z < fp.k, kEInval, "--findere-z must be smaller than query k"); break;
     default: raise(kEInval, "invalid index mode");
+  }
+  if (!fp.seed_pattern.empty()) {
+    // SpacedSeed::from_str (src/anchors.rs:15-42), FeatureConfig::validate_anchors
+    // (src/lib.rs:177-206).
+    check(parse_spaced_seed(fp.seed_pattern.c_str(), &fp.pattern), kEInval,
+          "seed pattern must be 1..=31 symmetric '#'/'_' characters with at least one '#'");
+    check(fp.mode == 0 || fp.mode == 1, kEInval,
+          "spaced seeds and randstrobemers require --index-mode kmers or minimizers");
+    check(fp.pattern.width == (fp.mode == 1 ? fp.m : fp.k), kEInval,
+          "seed pattern width must match k (or m in minimizer mode)");
+    fp.spaced = true;
   }
   struct stat st;
   check(stat(opt.output.c_str(), &st) != 0, kEInval,
@@ -695,7 +706,7 @@ void build_index(const BuildOptions& opt) {
   m.set("minimizer_size", JsonValue::uint((uint64_t)fp.m));
   m.set("minimizer_scheme", JsonValue::str("open-closed-mod"));
   m.set("homopolymer_compression", JsonValue::boolean(fp.homopolymer));
-  m.set("seed_pattern", JsonValue::null());
+  m.set("seed_pattern", fp.spaced ? JsonValue::str(fp.seed_pattern) : JsonValue::null());
   m.set("randstrobemers", JsonValue::null());
   m.set("randstrobe_scheme", JsonValue::null());
   m.set("modimizer_sampling", JsonValue::uint(fp.sampling));

@@ -9,6 +9,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "../zx_hash.h"
@@ -21,6 +22,11 @@ struct FeatureParams {
   uint64_t seed = 69, sampling = 16;
   int z = 10;
   bool homopolymer = false;
+  // Spaced seed (k-mer and minimizer modes): the selected canonical keys are
+  // mapped through the pattern (src/anchors.rs:265-281).
+  std::string seed_pattern;
+  bool spaced = false;
+  SpacedSeed pattern;
 };
 
 namespace cpu {
@@ -177,6 +183,7 @@ inline std::vector<uint8_t> homopolymer(const uint8_t* s, size_t n) {
 // Features of one ACGT run (already homopolymer-compressed when requested).
 inline void run_features(const uint8_t* s, size_t n, const FeatureParams& f,
                          std::vector<uint64_t>& out) {
+  const size_t first = out.size();
   switch (f.mode) {
     case 0: kmers(s, n, f.k, out); break;
     case 1: ocm(s, n, f.k, f.m, f.seed, out); break;
@@ -193,6 +200,8 @@ inline void run_features(const uint8_t* s, size_t n, const FeatureParams& f,
       if (n >= (size_t)f.k) kmers(s, n, f.k - f.z, out);
       break;
   }
+  if (f.spaced && f.mode <= 1)
+    for (size_t i = first; i < out.size(); ++i) out[i] = spaced_canonical(f.pattern, out[i]);
 }
 
 // Features of a sequence that may contain non-ACGT bytes.

@@ -47,6 +47,7 @@ int main(int argc, char** argv) {
     else if (a == "-z" || a == "--findere-z") o.features.z = std::stoi(val());
     else if (a == "-d" || a == "--modimizer-sampling") o.features.sampling = std::stoull(val());
     else if (a == "-c" || a == "--homopolymer-compression") o.features.homopolymer = true;
+    else if (a == "-p" || a == "--seed-pattern") o.features.seed_pattern = val();
     else if (a == "--legacy-layout") o.legacy_layout = true;
     else if (a == "-S" || a == "--slot-scale") o.slot_scale = std::stod(val());
     else if (a == "-L" || a == "--segment-length") o.segment_length = std::stoull(val());
@@ -61,7 +62,7 @@ int main(int argc, char** argv) {
     else {
       fprintf(stderr,
               "usage: zx_build -f FOF -o DIR [-k K] [-m M] [-H H] [-b BITS] [-s SEED]\n"
-              "  [-i kmers|minimizers|modimizers|findere] [-z Z] [-d D] [-c] [-S SCALE]\n"
+              "  [-i kmers|minimizers|modimizers|findere] [-z Z] [-d D] [-c] [-p PATTERN] [-S SCALE]\n"
               "  [-L SEG] [-D MIN_DOCS] [-N MAX_SUBINDEXES] [-X MAX_SIZE] [-R] [-t THREADS]\n"
               "  [--groups 0,1;2,3]\n");
       return 2;

@@ -27,7 +27,8 @@ int usage() {
           "usage: zorindex [-t THREADS] query -i DIR -q FILE [-a MIN_RATIO]\n"
           "                [-r [-F tsv|compact] [-B RECORDS]] [-M subindex|all] [--device N]\n"
           "       zorindex [-t THREADS] build -f FOF -o DIR [-k K] [-m M] [-H H] [-b BITS]\n"
-          "                [-s SEED] [-i MODE] [-z Z] [-d D] [-S SCALE] [-L SEG] [-D MIN_DOCS]\n"
+          "                [-s SEED] [-i MODE] [-z Z] [-d D] [-c] [-p PATTERN] [-S SCALE] [-L SEG]\n"
+          "                [-D MIN_DOCS]\n"
           "                [-N MAX] [-X SIZE] [-R] [--groups 0,1;2,3]\n");
   return 2;
 }
@@ -151,6 +152,7 @@ int build(int argc, char** argv, int threads) {
     else if (a == "-z" || a == "--findere-z") o.features.z = std::stoi(val());
     else if (a == "-d" || a == "--modimizer-sampling") o.features.sampling = std::stoull(val());
     else if (a == "-c" || a == "--homopolymer-compression") o.features.homopolymer = true;
+    else if (a == "-p" || a == "--seed-pattern") o.features.seed_pattern = val();
     else if (a == "-S" || a == "--slot-scale") o.slot_scale = std::stod(val());
     else if (a == "-L" || a == "--segment-length") o.segment_length = std::stoull(val());
     else if (a == "-D" || a == "--min-subindex-documents") o.min_subindex_documents = std::stoull(val());

@@ -513,6 +513,11 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
   else
     sp_.ocm = OcmParams{1, (int)m_.minimizer_size, 1};
   if (sp_.klen > 32) sp_.lk = long_kmer_consts(sp_.klen);
+  sp_.spaced = 0;
+  if (m_.has_seed_pattern) {
+    check_format(parse_spaced_seed(m_.seed_pattern.c_str(), &sp_.pattern), "invalid seed pattern");
+    sp_.spaced = 1;
+  }
 
   // Memory admission: banks (padded rows) + recovery directory.
   uint64_t need = 0;

@@ -95,8 +95,20 @@ void validate_manifest(Manifest& m) {
                "inconsistent abandoned recovery metadata");
   check_format(m.abandoned_recovery || (m.abandoned_hashes == 0 && m.abandoned_origins == 0),
                "disabled recovery has abandoned records");
-  check(!m.has_seed_pattern && !m.has_randstrobemers, kEUnsupported,
-        "spaced seeds and randstrobemers are not supported by the GPU query path");
+  check(!m.has_randstrobemers, kEUnsupported,
+        "randstrobemers are not supported by the GPU query path");
+  if (m.has_seed_pattern) {
+    // FeatureConfig::validate_anchors (src/lib.rs:177-206) and SpacedSeed::from_str
+    // (src/anchors.rs:15-42).
+    SpacedSeed sp;
+    check_format(parse_spaced_seed(m.seed_pattern.c_str(), &sp),
+                 "seed pattern must be 1..=31 symmetric '#'/'_' characters with at least one '#'");
+    check_format(m.index_mode == kKmers || m.index_mode == kMinimizers,
+                 "spaced seeds and randstrobemers require --index-mode kmers or minimizers");
+    const uint64_t length = m.index_mode == kMinimizers ? m.minimizer_size : m.k;
+    check_format((uint64_t)sp.width == length,
+                 "seed pattern width must match k (or m in minimizer mode)");
+  }
   switch (m.index_mode) {
     case kFindere:
       check_format(m.k > 0 && m.findere_z < m.k, "--findere-z must be smaller than query k");
@@ -240,6 +252,10 @@ Manifest load_manifest(const std::string& dir) {
   m.homopolymer_compression = bool_or(j, "homopolymer_compression", false);
   const JsonValue* sp = j.find("seed_pattern");
   m.has_seed_pattern = sp && !sp->is_null();
+  if (m.has_seed_pattern) {
+    check_format(sp->kind == JsonValue::Str, "manifest: seed_pattern");
+    m.seed_pattern = sp->s;
+  }
   const JsonValue* rs = j.find("randstrobemers");
   m.has_randstrobemers = rs && !rs->is_null();
   m.modimizer_sampling = u64_field(j, "modimizer_sampling");

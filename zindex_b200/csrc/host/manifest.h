@@ -57,6 +57,7 @@ struct Manifest {
   int minimizer_scheme = 0;  // 0 simd, 1 open-closed-mod
   bool homopolymer_compression = false;
   bool has_seed_pattern = false, has_randstrobemers = false;
+  std::string seed_pattern;  // '#'/'_' spaced-seed pattern when has_seed_pattern
   uint64_t modimizer_sampling = 16;
   uint64_t findere_z = 10;
   std::vector<ColorMeta> colors;

@@ -144,18 +144,31 @@ __device__ __forceinline__ uint32_t extract_tile(const BatchView& bv, const Seed
                                                  const Tile& t, uint64_t* keys, uint8_t* ocm,
                                                  const uint64_t* inner, int lane) {
   const uint64_t rb = bv.offsets[t.record];
+  uint32_t n;
   if (MODE == 1) {
-    if (sp.k == sp.m) return tile_ocm_full(bv.pv, rb, t.w0, t.nw, sp.m, keys, lane);
-    Rank16* pre = reinterpret_cast<Rank16*>(ocm);
-    Rank16* suf = pre + FusedSmem::ocm_entries(sp.k);
-    uint32_t* pos = reinterpret_cast<uint32_t*>(suf + FusedSmem::ocm_entries(sp.k));
-    return tile_ocm(bv.pv, rb, t.w0, t.nw, sp, inner, pre, suf, pos, keys, lane);
+    if (sp.k == sp.m) {
+      n = tile_ocm_full(bv.pv, rb, t.w0, t.nw, sp.m, keys, lane);
+    } else {
+      Rank16* pre = reinterpret_cast<Rank16*>(ocm);
+      Rank16* suf = pre + FusedSmem::ocm_entries(sp.k);
+      uint32_t* pos = reinterpret_cast<uint32_t*>(suf + FusedSmem::ocm_entries(sp.k));
+      n = tile_ocm(bv.pv, rb, t.w0, t.nw, sp, inner, pre, suf, pos, keys, lane);
+    }
+  } else if (sp.klen <= 32) {
+    n = tile_kmers_short(bv.pv, rb, t.w0, t.nw, sp.klen, MODE == 2, sp.seed, sp.sampling, keys,
+                         lane);
+  } else {
+    n = tile_kmers_long(bv.pv, rb, t.w0, t.nw, sp.klen, sp.lk, MODE == 2, sp.seed, sp.sampling,
+                        keys, keys + kTileWindows, lane);
   }
-  const bool modi = MODE == 2;
-  if (sp.klen <= 32)
-    return tile_kmers_short(bv.pv, rb, t.w0, t.nw, sp.klen, modi, sp.seed, sp.sampling, keys, lane);
-  return tile_kmers_long(bv.pv, rb, t.w0, t.nw, sp.klen, sp.lk, modi, sp.seed, sp.sampling, keys,
-                         keys + kTileWindows, lane);
+  // Spaced seeds (anchors.rs:265-281; k-mer and minimizer indexes, patterns of
+  // width k or m <= 31): the plain canonical keys, selected first, are mapped
+  // through the pattern.
+  if (MODE <= 1 && sp.spaced) {
+    __syncwarp();
+    for (uint32_t i = lane; i < n; i += 32) keys[i] = spaced_canonical(sp.pattern, keys[i]);
+  }
+  return n;
 }
 
 __device__ __forceinline__ void load_index_smem(const DevIndex* __restrict__ gix, DevIndex* six) {

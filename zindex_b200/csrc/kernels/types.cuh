@@ -20,6 +20,8 @@ struct SeedParams {
   uint64_t sampling;
   OcmParams ocm;
   LongKmerConsts lk;
+  int spaced;       // 1: keys are mapped through `pattern` (k-mers and minimizers)
+  SpacedSeed pattern;
 };
 
 struct Tile {

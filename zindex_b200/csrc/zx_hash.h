@@ -59,6 +59,81 @@ ZX_HD uint64_t canonical_encoded(uint64_t encoded, int k) {
   return encoded < rc ? encoded : rc;
 }
 
+// Spaced seed (src/anchors.rs:10-90): a symmetric '#'/'_' pattern of width
+// w <= 31 laid over a canonical k-mer (or minimizer m-mer) key, its first
+// base in the key's top 2-bit field. The projection keeps the '#' bases in
+// order (the reference's pext of the key with the 2-bit pattern mask); the
+// seed's key is canonical_encoded(projection, weight). The '#' runs are
+// precomputed so the projection is one shift-and-mask per run.
+struct SpacedSeed {
+  int width = 0, weight = 0, runs = 0;
+  uint8_t shift[16] = {};  // per run, most significant first: source bit offset of its last base
+  uint8_t len[16] = {};    // per run: bases
+};
+
+// Parses a pattern; returns false when it is invalid (the reference's rules:
+// width 1..31, only '#' and '_', at least one '#', symmetric under reversal).
+static inline bool parse_spaced_seed(const char* pattern, SpacedSeed* out) {
+  int w = 0;
+  while (pattern[w]) ++w;
+  if (w < 1 || w > 31) return false;
+  bool any = false;
+  for (int i = 0; i < w; ++i) {
+    if (pattern[i] != '#' && pattern[i] != '_') return false;
+    if (pattern[i] != pattern[w - 1 - i]) return false;
+    any |= pattern[i] == '#';
+  }
+  if (!any) return false;
+  SpacedSeed p;
+  p.width = w;
+  for (int i = 0; i < w;) {
+    if (pattern[i] != '#') {
+      ++i;
+      continue;
+    }
+    int j = i;
+    while (j < w && pattern[j] == '#') ++j;
+    // Bases i..j-1 sit at 2-bit fields w-1-i .. w-j (from the bottom).
+    p.shift[p.runs] = (uint8_t)(2 * (w - j));
+    p.len[p.runs] = (uint8_t)(j - i);
+    ++p.runs;
+    p.weight += j - i;
+    i = j;
+  }
+  *out = p;
+  return true;
+}
+
+ZX_HD uint64_t spaced_project(const SpacedSeed& p, uint64_t key) {
+  uint64_t r = 0;
+  for (int i = 0; i < p.runs; ++i) {
+    const int bits = 2 * p.len[i];
+    r = (r << bits) | ((key >> p.shift[i]) & ((1ull << bits) - 1));
+  }
+  return r;
+}
+
+// Reverse complement of a k-base 2-bit value (k <= 32).
+ZX_HD uint64_t revcomp_encoded(uint64_t v, int k) {
+#if defined(__CUDA_ARCH__)
+  uint64_t y = __brevll(~v);
+  y = ((y >> 1) & 0x5555555555555555ull) | ((y & 0x5555555555555555ull) << 1);
+  return k == 32 ? y : y >> (64 - 2 * k);
+#else
+  uint64_t rc = 0;
+  for (int i = 0; i < k; ++i) {
+    rc = (rc << 2) | ((v & 3) ^ 3);
+    v >>= 2;
+  }
+  return rc;
+#endif
+}
+
+ZX_HD uint64_t spaced_canonical(const SpacedSeed& p, uint64_t key) {
+  const uint64_t f = spaced_project(p, key), r = revcomp_encoded(f, p.weight);
+  return f < r ? f : r;
+}
+
 ZX_HD uint64_t fingerprint(uint64_t key, uint64_t seed, int bits) {
   uint64_t mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1);
   return splitmix64(key ^ seed ^ kFingerprintSeed) & mask;
