@@ -72,6 +72,10 @@ typedef struct zx_launch {
   int cut;            /* host-buffer queries: the batch is cut at record boundaries into this many
                          chunks (1..64) whose host-to-device copies overlap the previous chunk's
                          kernels; chunks below 1 MiB of bases are merged */
+  int split;          /* minimizer indexes: 1 = seeds are extracted by a kernel of their own into
+                         per-tile slots and probed by a kernel without the extraction scratch
+                         (more resident warps); applies to the row-index form (planes 1, no
+                         staged gather) and is ignored elsewhere */
 } zx_launch;
 
 /* Thread-local message of the last failed call on this thread. */

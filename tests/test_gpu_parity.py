@@ -192,6 +192,76 @@ def test_legacy_interleaved_banks(gpu, oracle, tmp_path_factory, opts):
     gpu_vs_oracle(oracle, ix, reads_for(genomes, n=300, length=200, n_runs=0.1))
 
 
+SPLIT_CASES = [
+    dict(mode="minimizers", k=31, m=21, H=4, b=8),
+    dict(mode="minimizers", k=21, m=21, H=3, b=16),
+    dict(mode="minimizers", k=49, m=31, H=3, b=16, homopolymer=True),
+    dict(mode="minimizers", k=31, m=15, H=4, b=8, pattern="##_##_###_##_##"),
+]
+
+
+@pytest.mark.parametrize("case", SPLIT_CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+def test_split_minimizer_extraction_matches_oracle(gpu, oracle, tmp_path_factory, case):
+    """Split minimizer queries (seeds extracted into per-tile slots by their own
+    kernel, then probed) count exactly what the fused kernel and the oracle count."""
+    import zindex_b200 as zx
+
+    ix, genomes = index_for(tmp_path_factory, colors=6, length=30000, seed=29, **case)
+    reads = reads_for(genomes, n=300, length=2500, n_runs=0.1, lower=0.01)
+    bases, offsets = zx.pack_records(reads)
+    want, want_total = oracle.query_records(ix, bases, offsets)
+    with zx.Index(ix) as index:
+        for minb in (2, 1, 3):
+            index.set_launch(split=1, planes=1, min_blocks=minb)
+            assert index.launch()["split"] == 1
+            got, total = index.query_records(bases, offsets)
+            assert total == want_total, minb
+            np.testing.assert_array_equal(got, want)
+
+
+def test_split_rounds_equal_fused(gpu, tmp_path_factory):
+    """A batch of more tiles than one split round (262,144) gives the fused
+    kernel's counts, through host buffers and device graphs."""
+    import torch
+
+    import zindex_b200 as zx
+
+    ix, genomes = index_for(tmp_path_factory, colors=6, length=30000, seed=29, mode="minimizers",
+                            k=31, m=21, H=4, b=8)
+    rng = np.random.default_rng(5)
+    n, length = 300_000, 120
+    codes = rng.integers(0, 4, size=n * length, dtype=np.uint8)
+    bases = np.frombuffer(b"ACGT", dtype=np.uint8)[codes]
+    src = np.frombuffer(b"".join(genomes), dtype=np.uint8)
+    for i in range(0, n, 3):  # a third of the reads copied from the genomes
+        at = int(rng.integers(0, len(src) - length))
+        bases[i * length:(i + 1) * length] = src[at:at + length]
+    offsets = np.arange(n + 1, dtype=np.uint64) * length
+    with zx.Index(ix) as index:
+        index.set_launch(split=0)
+        want, want_total = index.query_records(bases, offsets)
+    with zx.Index(ix) as index:
+        # A fresh index: the first split query is a graph capture.
+        index.set_launch(split=1)
+        dev = torch.device("cuda", 0)
+        d_bases = torch.from_numpy(bases).to(dev)
+        d_off = torch.from_numpy(offsets.view(np.int64)).to(dev)
+        d_counts = torch.zeros(index.colors, dtype=torch.int64, device=dev)
+        d_total = torch.zeros(1, dtype=torch.int64, device=dev)
+        stream = torch.cuda.current_stream(dev)
+        for _ in range(2):  # the second call replays the captured graph
+            d_counts.zero_()
+            d_total.zero_()
+            index.query_device(d_bases.data_ptr(), len(bases), d_off.data_ptr(), n,
+                               d_counts.data_ptr(), d_total.data_ptr(), stream=stream.cuda_stream)
+            torch.cuda.synchronize(dev)
+            assert int(d_total.item()) == want_total
+            np.testing.assert_array_equal(d_counts.cpu().numpy().astype(np.uint64), want)
+        got, total = index.query_records(bases, offsets)
+        assert total == want_total and total > 0
+        np.testing.assert_array_equal(got, want)
+
+
 SPACED_CASES = [
     dict(mode="kmers", k=21, H=4, b=8, pattern="###_#_##_" + "###" + "_##_#_###"),
     dict(mode="kmers", k=31, H=3, b=16, pattern="#_" * 15 + "#", homopolymer=True),

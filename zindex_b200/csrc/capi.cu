@@ -61,6 +61,7 @@ void fill_launch(const zx::QueryLaunch& l, zx_launch* out) {
   out->min_blocks = l.min_blocks;
   out->planes = l.planes;
   out->cut = l.cut;
+  out->split = l.split;
 }
 
 }  // namespace
@@ -314,7 +315,7 @@ int zx_set_launch(zx_index* index, const zx_launch* l) {
     std::lock_guard<std::mutex> lock(index->mu);
     index->engine->set_launch(
         zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters, l->stage_bytes, l->stages,
-                        l->bulk, l->min_blocks, l->planes, l->cut});
+                        l->bulk, l->min_blocks, l->planes, l->cut, l->split});
   });
 }
 

@@ -121,6 +121,11 @@ FusedFn fused_mode(int mode) {
 FusedFn fused_for(int mode, const QueryLaunch& l) {
   // Findere has one form: the row-index probe with per-colour position masks.
   if (mode == 3) return l.min_blocks == 3 ? fused_query_kernel<3, 3, 2> : fused_query_kernel<3, 2, 2>;
+  // Probe of seeds extracted beforehand (split minimizer queries): row-index form only.
+  if (mode == 4)
+    return l.min_blocks == 1   ? fused_query_kernel<4, 1, 2>
+           : l.min_blocks == 3 ? fused_query_kernel<4, 3, 2>
+                               : fused_query_kernel<4, 2, 2>;
   const int v = l.stage_bytes > 0 ? 1 : (l.planes ? 2 : 0);
   // One resident block per SM: the row-index form with the chunk pipeline.
   if (l.min_blocks == 1 && v == 2) return fused_mode<1, 2>(mode);
@@ -323,6 +328,7 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
   l.smem_counters = 0;
   l.stage_bytes = 0;
   l.blocks = 0;
+  l.split = 0;
   const size_t smem = fused_smem_bytes(l);
   FusedFn fn = fused_for(sp_.mode, l);
   cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -394,7 +400,7 @@ Workspace::~Workspace() {
                  keys_count, error,    fstate,    hp_starts, hp_keep,    hp_pos,
                  hp_bases,   hp_offsets, hp_scan_tmp, seg_blocks, seg_tiles, seg_records,
                  rec_counts, rec_totals, rec_hits, rec_first, rec_scan_tmp, hit_colors,
-                 hit_counts};
+                 hit_counts, split_keys, split_counts};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total, h_seg_blocks, h_seg_records};
@@ -788,6 +794,10 @@ QueryLaunch Engine::default_launch() const {
   l.min_blocks = 2;
   l.planes = 1;
   l.cut = 4;
+  // Minimizer seeds are extracted by a kernel of their own: the probe kernel
+  // then needs no extraction scratch and keeps twice the warps resident
+  // (C3 slice on B200: 22.3 ms against 36.7 ms for the fused kernel).
+  l.split = m_.index_mode == kMinimizers ? 1 : 0;
   // Wide rows: fewer warps per block keep several blocks per SM (measured on
   // 8 KiB rows of 16,384 colours: 2 warps x 3 blocks 64 ms, against 78 ms for
   // the per-hit form); colour counters go to global atomics above 2,048
@@ -806,9 +816,14 @@ QueryLaunch Engine::default_launch() const {
   return l;
 }
 
+int Engine::kernel_mode(const QueryLaunch& l) const {
+  return l.split && sp_.mode == kMinimizers && l.planes == 1 && l.stage_bytes == 0 ? 4 : sp_.mode;
+}
+
 size_t Engine::fused_smem_bytes(const QueryLaunch& l) const {
-  return FusedSmem::total(sp_.mode, sp_.k, (uint32_t)m_.colors.size(), host_ix_.classes,
-                          m_.hashes, l, FusedSmem::shared_words(sp_.mode, host_ix_, l));
+  const int mode = kernel_mode(l);
+  return FusedSmem::total(mode, sp_.k, (uint32_t)m_.colors.size(), host_ix_.classes, m_.hashes, l,
+                          FusedSmem::shared_words(mode, host_ix_, l));
 }
 
 int Engine::max_blocks(const QueryLaunch& l) const {
@@ -816,11 +831,11 @@ int Engine::max_blocks(const QueryLaunch& l) const {
       cached_for_.smem_counters == l.smem_counters && cached_for_.stage_bytes == l.stage_bytes &&
       cached_for_.stages == l.stages && cached_for_.bulk == l.bulk &&
       cached_for_.min_blocks == l.min_blocks && cached_for_.planes == l.planes &&
-      cached_for_.cut == l.cut)
+      cached_for_.cut == l.cut && cached_for_.split == l.split)
     return cached_blocks_;
   int per_sm = 0;
   size_t smem = fused_smem_bytes(l);
-  FusedFn fn = fused_for(sp_.mode, l);
+  FusedFn fn = fused_for(kernel_mode(l), l);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
                                                            l.warps * 32, smem),
@@ -863,6 +878,7 @@ void Engine::set_launch(const QueryLaunch& l) {
         "min_blocks 1 (255 registers) is compiled for the row-index form (planes 1) only");
   check(l.planes == 0 || l.planes == 1, kEInval, "planes must be 0 or 1");
   check(l.cut >= 1 && l.cut <= 64, kEInval, "cut must be in 1..64");
+  check(l.split == 0 || l.split == 1, kEInval, "split must be 0 or 1");
   check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
   check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
   std::lock_guard<std::mutex> lock(mu_);
@@ -880,6 +896,8 @@ std::unique_ptr<Workspace> Engine::make_workspace() {
 
 void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
   const uint64_t colors = m_.colors.size();
+  // Split minimizer queries: key slots allocated before any graph capture.
+  if (kernel_mode(launch_) == 4) ensure_split_capacity(ws);
   if (nbases > ws.cap_bases || !ws.bases) {
     uint64_t cap = std::max<uint64_t>({nbases, ws.cap_bases * 3 / 2, 4096});
     cap = round_up(cap, 4096);
@@ -1045,6 +1063,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   }
   plan_tiles(ws, offsets, records, nbases, s);
   QueryLaunch l = launch_;
+  const int kmode = kernel_mode(l);
   const size_t smem = fused_smem_bytes(l);
   const int blocks_cap = max_blocks(l);
   uint64_t tiles_bound = nbases / kTileWindows + records + nbases / kFindereTask + 1;
@@ -1062,21 +1081,60 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   cuda_check(cudaStreamIsCapturing(s, &capturing), "cudaStreamIsCapturing");
   const bool timed = timing_ && capturing == cudaStreamCaptureStatusNone;
   if (timed) cuda_check(cudaEventRecord(ev_begin_, s), "cudaEventRecord");
-  FusedFn fn = fused_for(sp_.mode, l);
+  FusedFn fn = fused_for(kmode, l);
   // The dynamic shared-memory limit is a property of the kernel function, shared by
   // every engine in the process: set it for this launch's size every time.
   cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "cudaFuncSetAttribute");
-  fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, ws.partial,
-                                        counts, total, ws.error);
-  cuda_check(cudaGetLastError(), "fused_query_kernel");
-  if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
-  if (l.smem_counters) {
-    const uint32_t colors = (uint32_t)m_.colors.size();
+  const uint32_t colors = (uint32_t)m_.colors.size();
+  auto reduce = [&] {
+    if (!l.smem_counters) return;
     reduce_counters_kernel<<<std::max(1u, (colors + 255) / 256), 256, 0, s>>>(ws.partial, blocks,
                                                                                colors, counts);
     cuda_check(cudaGetLastError(), "reduce_counters_kernel");
+  };
+  if (kmode != 4) {
+    fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, ws.partial,
+                                          counts, total, ws.error);
+    cuda_check(cudaGetLastError(), "fused_query_kernel");
+    if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
+    reduce();
+    return;
   }
+  // Split minimizer query: rounds of up to kSplitTiles tiles; per round the
+  // extraction kernel fills each tile's key slot, the probe kernel (no
+  // extraction scratch, so more warps per SM) counts them, and the block
+  // counters are added up. The rounds cover the host's tile bound; tiles past
+  // the planned count are skipped on the device.
+  ensure_split_capacity(ws);
+  const int ewarps = 4;
+  const size_t esmem = 256 * 8 + ewarps * FusedSmem::warp_bytes(kMinimizers, sp_.k, 0);
+  ExtractFn efn = extract_for(kMinimizers);
+  cuda_check(cudaFuncSetAttribute(efn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem),
+             "cudaFuncSetAttribute");
+  const int egrid = (int)std::min<uint64_t>((kSplitTiles + ewarps - 1) / ewarps,
+                                            (uint64_t)sms_ * 8);
+  for (uint64_t lo = 0; lo < tiles_bound; lo += kSplitTiles) {
+    BatchView rb = bv;
+    rb.tile_lo = (uint32_t)lo;
+    rb.tile_hi = (uint32_t)std::min<uint64_t>(lo + kSplitTiles, tiles_bound);
+    rb.prekeys = ws.split_keys;
+    rb.prekey_count = ws.split_counts;
+    efn<<<egrid, ewarps * 32, esmem, s>>>(rb, sp_, ws.split_keys, ws.split_counts, ewarps);
+    cuda_check(cudaGetLastError(), "extract_kernel");
+    fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, rb, sp_, l,
+                                          ws.partial, counts, total, ws.error);
+    cuda_check(cudaGetLastError(), "fused_query_kernel");
+    reduce();
+  }
+  if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
+}
+
+void Engine::ensure_split_capacity(Workspace& ws) {
+  if (ws.split_keys) return;
+  dev_alloc(&ws.split_keys, kSplitTiles * kTileWindows, "split key slots");
+  dev_alloc(&ws.split_counts, kSplitTiles, "split key counts");
+  ws.release_graphs();
 }
 
 uint64_t Engine::tiles_for_length(uint64_t len) const {
@@ -1102,6 +1160,7 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
     check(seg_records[i] <= seg_records[i + 1], kEInval, "segment records must be non-decreasing");
   ensure_capacity(ws, nbases, records);
   QueryLaunch l = launch_;
+  l.split = 0;  // every segment extracts its own tiles in the fused kernel
   if (warps > 0 && warps < l.warps) l.warps = warps;
   const int cap = max_blocks(l);
   const uint32_t wpb = (uint32_t)l.warps;

@@ -61,6 +61,9 @@ struct Workspace {
   uint64_t* h_seg_records = nullptr;  // pinned staging
   uint64_t cap_segments = 0;
   cudaEvent_t seg_staged = nullptr;   // the last segmented call's staging copies are done
+  // Split minimizer queries: key slots of one round of tiles.
+  uint64_t* split_keys = nullptr;
+  uint32_t* split_counts = nullptr;
   // Per-record queries: counters of one record group (records x colours).
   uint64_t* rec_counts = nullptr;
   unsigned long long* rec_totals = nullptr;
@@ -208,6 +211,10 @@ class Engine {
   void plan_tiles(Workspace& ws, const uint64_t* offsets, uint64_t records, uint64_t nbases,
                   cudaStream_t stream);
   void check_error_word(Workspace& ws);
+  // Kernel form of a launch: the seed mode, or 4 (probe of pre-extracted
+  // seeds) for split minimizer queries.
+  int kernel_mode(const QueryLaunch& l) const;
+  void ensure_split_capacity(Workspace& ws);
   // Runs host records in device groups (one segment per record): after each
   // group's launch, on_group(r0, n) enqueues its read-back on ws.stream; the
   // stream is then synchronised and the error word checked.

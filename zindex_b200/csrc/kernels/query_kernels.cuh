@@ -19,6 +19,7 @@ namespace zx {
 
 constexpr uint32_t kTileWindows = 256;
 constexpr uint32_t kFindereTask = 16384;  // src/findere.rs:13-16
+constexpr uint32_t kSplitTiles = 1u << 18;  // tiles per round of a split minimizer query
 
 // Windows of record r: k-windows fully inside the record. A record whose
 // offsets decrease, pass the end of the bases or span 2^31 bases or more has
@@ -81,6 +82,12 @@ struct BatchView {
   uint32_t segments;
   const uint32_t* seg_blocks;
   const uint32_t* seg_tiles;
+  // Tile range of a launch over part of the list: tiles tile_lo .. tile_hi-1
+  // (tile_hi 0 = to the end). Seeds extracted beforehand (MODE 4): tile t's
+  // keys are prekeys[(t - tile_lo) * kTileWindows ...], prekey_count[t - tile_lo] of them.
+  uint32_t tile_lo, tile_hi;
+  const uint64_t* prekeys;
+  const uint32_t* prekey_count;
 };
 
 // Shared memory of the fused kernel, in order: DevIndex copy, counters,
@@ -109,10 +116,15 @@ struct FusedSmem {
   static __host__ __device__ size_t shared_plane_bytes(uint32_t words) {
     return (size_t)words * (kSharedPlanes + 2) * 32 * 4;
   }
+  // Key buffer of a warp: one tile's keys, plus the lane-run staging of the
+  // polynomial k-mer hashes (k > 32) and findere s-mers in modes 0, 2 and 3.
+  static __host__ __device__ size_t key_bytes(int mode) {
+    return (mode == 1 || mode == 4 ? 1 : 2) * (size_t)kTileWindows * 8;
+  }
   static __host__ __device__ size_t warp_bytes(int mode, int k, uint32_t classes, int stage_bytes = 0,
                                                int stages = 0, int hashes = 4, int planes = 0,
                                                uint32_t shared_words = 0) {
-    size_t b = 2 * kTileWindows * 8 + probe_bytes(classes, hashes, planes) +
+    size_t b = key_bytes(mode) + probe_bytes(classes, hashes, planes) +
                ring_bytes(stage_bytes, stages) + shared_plane_bytes(shared_words);
     if (mode == 1) b += 2 * ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
     if (mode == 3) b += 64;  // findere: valid bits of up to 512 s-mer positions
@@ -220,9 +232,9 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
       FusedSmem::warp_bytes(MODE, sp.k, classes, stage_bytes, lc.stages, hashes, ROWS, swords);
   uint8_t* wbase = p + (size_t)warp * wstride;
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
-  SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + 2 * kTileWindows * 8);
+  SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + FusedSmem::key_bytes(MODE));
   uint64_t* row0s = reinterpret_cast<uint64_t*>(desc + 64);
-  uint8_t* ring_base = wbase + 2 * kTileWindows * 8 + FusedSmem::probe_bytes(classes, hashes, ROWS);
+  uint8_t* ring_base = wbase + FusedSmem::key_bytes(MODE) + FusedSmem::probe_bytes(classes, hashes, ROWS);
   uint8_t* ocm = ring_base + FusedSmem::ring_bytes(stage_bytes, lc.stages);
   SharedPlanes splanes{reinterpret_cast<uint32_t*>(wbase + wstride - FusedSmem::shared_plane_bytes(swords)),
                        swords, 0u};
@@ -238,7 +250,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   }
 
   load_index_smem(gix, six);
-  build_inner_table(sp, inner);
+  if (MODE == 1) build_inner_table(sp, inner);
   if (scount)
     for (uint32_t c = threadIdx.x; c < colors; c += blockDim.x) scount[c] = 0;
   __syncthreads();
@@ -255,7 +267,8 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   const uint32_t wpb = blockDim.x >> 5;
   const uint32_t gwarp = blockIdx.x * wpb + warp;
   // Tile range of this warp: the whole list, or its block's segment.
-  uint32_t t_first = gwarp, t_end = *bv.ntiles, t_stride = gridDim.x * wpb, seg = 0;
+  uint32_t t_first = bv.tile_lo + gwarp, t_end = *bv.ntiles, t_stride = gridDim.x * wpb, seg = 0;
+  if (bv.tile_hi && bv.tile_hi < t_end) t_end = bv.tile_hi;
   if (bv.segments) {
     uint32_t lo = 0, hi = bv.segments;
     while (hi - lo > 1) {
@@ -295,7 +308,15 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
                  });
       continue;
     } else {
-    uint32_t n = extract_tile<MODE>(bv, sp, tile, keys, ocm, inner, lane);
+    uint32_t n;
+    if constexpr (MODE == 4) {
+      // Seeds extracted beforehand into this tile's slot.
+      const uint64_t slot = (uint64_t)(t - bv.tile_lo) * kTileWindows;
+      n = bv.prekey_count[t - bv.tile_lo];
+      for (uint32_t i = lane; i < n; i += 32) keys[i] = bv.prekeys[slot + i];
+    } else {
+      n = extract_tile<MODE>(bv, sp, tile, keys, ocm, inner, lane);
+    }
     __syncwarp();
     seeds += n;
     if (STAGED) {
@@ -368,16 +389,20 @@ __global__ void extract_kernel(BatchView bv, SeedParams sp, uint64_t* __restrict
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, 0);
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
-  uint8_t* ocm = wbase + 2 * kTileWindows * 8 + FusedSmem::probe_bytes(0);
+  uint8_t* ocm = wbase + FusedSmem::key_bytes(MODE) + FusedSmem::probe_bytes(0);
   build_inner_table(sp, inner);
   __syncthreads();
-  const uint32_t ntiles = *bv.ntiles;
+  // Tiles tile_lo .. tile_hi-1 (tile_hi 0 = to the end); tile t's slot is t - tile_lo.
+  uint32_t ntiles = *bv.ntiles;
+  if (bv.tile_hi && bv.tile_hi < ntiles) ntiles = bv.tile_hi;
   const uint32_t warps_total = gridDim.x * warps_per_block;
-  for (uint32_t t = blockIdx.x * warps_per_block + warp; t < ntiles; t += warps_total) {
+  for (uint32_t t = bv.tile_lo + blockIdx.x * warps_per_block + warp; t < ntiles;
+       t += warps_total) {
     uint32_t n = extract_tile<MODE>(bv, sp, bv.tiles[t], keys, ocm, inner, lane);
     __syncwarp();
-    for (uint32_t i = lane; i < n; i += 32) out[(uint64_t)t * kTileWindows + i] = keys[i];
-    if (lane == 0) out_count[t] = n;
+    const uint64_t slot = (uint64_t)(t - bv.tile_lo) * kTileWindows;
+    for (uint32_t i = lane; i < n; i += 32) out[slot + i] = keys[i];
+    if (lane == 0) out_count[t - bv.tile_lo] = n;
     __syncwarp();
   }
 }

@@ -43,6 +43,8 @@ struct QueryLaunch {
                       // pipeline), 2 or 3 resident 256-thread blocks per SM
   int planes;         // register gather: 1 = row indices + bit-plane colour counters, 0 = descriptors
   int cut;            // host batches: pipelined chunks (copy of chunk i+1 overlaps chunk i), 1..64
+  int split;          // minimizers: 1 = seeds extracted by their own kernel into per-tile slots,
+                      // then probed by a kernel without the extraction scratch (more warps per SM)
 };
 
 }  // namespace zx
