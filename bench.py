@@ -766,16 +766,42 @@ def main():
                     help="workload: c2 (default line) or another configuration")
     ap.add_argument("--reads", type=int, default=None,
                     help="query only the first N reads (smaller case for profiler captures)")
+    ap.add_argument("--slice", type=int, default=None,
+                    help="profiler case: three plain launches over the first N reads, no timing")
     args = ap.parse_args()
     global CONFIG, WORKLOAD
     CONFIG = CONFIGS[args.config]
     WORKLOAD = dict(CONFIG["workload"])
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.slice:
+        profile_slice(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         ours(args)
+
+
+def profile_slice(args):
+    """A small case of the workload for an ncu capture: the first N reads of
+    the batch, queried three times without graphs (the third launch of each
+    kernel is the one to capture), then the seed count."""
+    import torch
+
+    build_native()
+    import zindex_b200 as zx
+    from zindex_b200.tuning import DeviceBatch
+
+    index_dir, bases, offsets = prepare(Path(args.cache), 0, args.config)
+    offsets = offsets[: args.slice + 1].copy()
+    bases = bases[: int(offsets[-1])].copy()
+    with zx.Index(index_dir) as ix:
+        batch = DeviceBatch(bases, offsets, ix.colors)
+        for _ in range(3):
+            batch.run(ix, torch.cuda.current_stream(), use_graph=False)
+        torch.cuda.synchronize()
+        print(json.dumps({"slice_reads": args.slice, "bases": int(len(bases)),
+                          "seeds": int(batch.d_total.item()), "launch": ix.launch()}))
 
 
 if __name__ == "__main__":
