@@ -146,3 +146,19 @@ def test_per_record_small_cases(gpu, oracle, tmp_path_factory):
         bases, offsets = zx.pack_records([b"", b""])   # a group without bases
         counts, totals = index.query_per_record(bases, offsets)
         assert list(totals) == [0, 0] and counts.sum() == 0
+        # Page-locked inputs and caller-owned page-locked outputs.
+        import torch
+
+        reads = [genomes[r % 5][r * 37: r * 37 + 150] for r in range(200)]
+        bases, offsets = zx.pack_records(reads)
+        want_c, want_t = index.query_per_record(bases, offsets)
+        pb = torch.from_numpy(bases).pin_memory().numpy()
+        po = torch.from_numpy(offsets.view(np.int64)).pin_memory().numpy().view(np.uint64)
+        pc = torch.zeros((200, index.colors), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+        pt = torch.zeros(200, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+        got_c, got_t = index.query_per_record(pb, po, counts=pc, totals=pt)
+        assert got_c is pc and got_t is pt
+        np.testing.assert_array_equal(pc, want_c)
+        np.testing.assert_array_equal(pt, want_t)
+        with pytest.raises(ValueError):
+            index.query_per_record(bases, offsets, counts=np.zeros((3, 3), np.uint64))

@@ -107,14 +107,24 @@ class Index:
                       int(recover), _p64(counts), byref(total)))
         return counts, int(total.value)
 
-    def query_per_record(self, bases: np.ndarray, offsets: np.ndarray, recover: bool = True):
+    def query_per_record(self, bases: np.ndarray, offsets: np.ndarray, recover: bool = True,
+                         counts: Optional[np.ndarray] = None, totals: Optional[np.ndarray] = None):
         """(counts uint64[records, colors], totals uint64[records]): each record
-        bases[offsets[r]:offsets[r+1]] counted as if queried alone."""
+        bases[offsets[r]:offsets[r+1]] counted as if queried alone. `counts` and
+        `totals` may be given (C-contiguous uint64 of those shapes, e.g. views of
+        page-locked buffers, which the device writes at full PCIe rate)."""
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
         records = len(offsets) - 1
-        counts = np.zeros((records, self.colors), dtype=np.uint64)
-        totals = np.zeros(records, dtype=np.uint64)
+        if counts is None:
+            counts = np.zeros((records, self.colors), dtype=np.uint64)
+        if totals is None:
+            totals = np.zeros(records, dtype=np.uint64)
+        if (counts.dtype != np.uint64 or counts.shape != (records, self.colors)
+                or not counts.flags.c_contiguous or totals.dtype != np.uint64
+                or totals.shape != (records,) or not totals.flags.c_contiguous):
+            raise ValueError("counts must be uint64[records, colors] and totals uint64[records], "
+                             "C-contiguous")
         _lib.check(_lib.load().zx_query_per_record(self._h, bases.ctypes.data_as(c_void_p),
                                                   _p64(offsets), records, int(recover),
                                                   _p64(counts), _p64(totals)))

@@ -1283,6 +1283,14 @@ void Engine::record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     ws.cap_rec_totals = gmax;
   }
   cudaStream_t s = ws.stream;
+  // Page-locked caller bases are copied directly, pageable ones through the
+  // workspace's pinned staging.
+  cudaPointerAttributes attr;
+  bool direct = false;
+  if (nbases && cudaPointerGetAttributes(&attr, bases) == cudaSuccess)
+    direct = attr.type == cudaMemoryTypeHost;
+  else
+    cudaGetLastError();
   std::vector<uint64_t> seg, est;
   for (uint64_t r0 = 0; r0 < records;) {
     uint64_t r1 = r0 + 1, tiles = tiles_for_length(offsets[r0 + 1] - offsets[r0]);
@@ -1300,8 +1308,12 @@ void Engine::record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     for (uint64_t i = 0; i < n; ++i)
       est[i] = std::max<uint64_t>(1, tiles_for_length(offsets[r0 + i + 1] - offsets[r0 + i]));
     if (nb) {
-      memcpy(ws.h_bases, bases + b0, nb);
-      cuda_check(cudaMemcpyAsync(ws.bases, ws.h_bases, nb, cudaMemcpyHostToDevice, s), "H2D");
+      const uint8_t* src = bases + b0;
+      if (!direct) {
+        memcpy(ws.h_bases, src, nb);
+        src = ws.h_bases;
+      }
+      cuda_check(cudaMemcpyAsync(ws.bases, src, nb, cudaMemcpyHostToDevice, s), "H2D");
     }
     cuda_check(cudaMemcpyAsync(ws.offsets, ws.h_offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s),
                "H2D");
