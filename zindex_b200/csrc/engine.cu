@@ -125,7 +125,6 @@ FusedFn fused_for(int mode, const QueryLaunch& l) {
   if (mode == 4)
     return l.min_blocks == 1   ? fused_query_kernel<4, 1, 2>
            : l.min_blocks == 3 ? fused_query_kernel<4, 3, 2>
-           : l.min_blocks == 5 ? fused_query_kernel<4, 5, 2>
                                : fused_query_kernel<4, 2, 2>;
   const int v = l.stage_bytes > 0 ? 1 : (l.planes ? 2 : 0);
   // One resident block per SM: the row-index form with the chunk pipeline.
@@ -874,10 +873,7 @@ void Engine::set_launch(const QueryLaunch& l) {
         kEInval, "staged gather needs 16-byte multiple stages of at least 16*H bytes, 1..8 stages");
   check(m_.index_mode != kFindere || l.stage_bytes == 0, kEInval,
         "findere indexes use the register gather only");
-  check((l.min_blocks >= 1 && l.min_blocks <= 3) ||
-            (l.min_blocks == 5 && kernel_mode(l) == 4 && l.warps <= 4),
-        kEInval,
-        "min_blocks must be 1, 2 or 3 (5: split minimizer probes of at most 4 warps per block)");
+  check(l.min_blocks >= 1 && l.min_blocks <= 3, kEInval, "min_blocks must be 1, 2 or 3");
   check(l.min_blocks != 1 || (l.planes == 1 && l.stage_bytes == 0), kEInval,
         "min_blocks 1 (255 registers) is compiled for the row-index form (planes 1) only");
   check(l.planes == 0 || l.planes == 1, kEInval, "planes must be 0 or 1");

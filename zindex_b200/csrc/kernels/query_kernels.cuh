@@ -199,11 +199,8 @@ __device__ __forceinline__ void build_inner_table(const SeedParams& sp, uint64_t
 // Fused extraction + probe over the tile list (one instantiation per seed
 // mode). partial: gridDim.x x colors block counters (smem_counters); counts:
 // global counters (used directly when smem_counters == 0). total: seeds.
-// MINB: resident blocks the register budget is compiled for, 256-thread
-// blocks for 1, 2 and 3 (255, 128 and 85 registers); 5 means five 128-thread
-// blocks (102 registers; split minimizer probes of at most 4 warps per block).
 template <int MODE, int MINB, int VARIANT>
-__global__ void __launch_bounds__(MINB == 5 ? 128 : 256, MINB) fused_query_kernel(const DevIndex* __restrict__ gix,
+__global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* __restrict__ gix,
                                                           BatchView bv, SeedParams sp,
                                                           QueryLaunch lc,
                                                           uint32_t* __restrict__ partial,
