@@ -417,16 +417,31 @@ void Workspace::release_graphs() {
   graphs.clear();
 }
 
-Engine::Engine(const std::string& dir, const OpenOptions& options) { load(dir, options); }
+Engine::Engine(const std::string& dir, const OpenOptions& options) {
+  // A failed load (corrupt bank, short file, no memory) returns every device
+  // allocation made so far: the destructor does not run for a constructor
+  // that throws.
+  try {
+    load(dir, options);
+  } catch (...) {
+    release();
+    throw;
+  }
+}
 
-Engine::~Engine() {
+Engine::~Engine() { release(); }
+
+void Engine::release() {
   ws_.reset();
   cudaSetDevice(device_);
   if (ev_begin_) cudaEventDestroy(ev_begin_);
   if (ev_end_) cudaEventDestroy(ev_end_);
+  ev_begin_ = ev_end_ = nullptr;
   for (void* p : allocations_) cudaFree(p);
+  allocations_.clear();
   if (d_ix_rec_) cudaFree(d_ix_rec_);
   if (d_ix_norec_) cudaFree(d_ix_norec_);
+  d_ix_rec_ = d_ix_norec_ = nullptr;
 }
 
 int Engine::span() const { return (int)m_.k; }

@@ -199,6 +199,7 @@ class Engine {
 
  private:
   void load(const std::string& dir, const OpenOptions& options);
+  void release();  // frees every device allocation and event of the engine
   void ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records);
   // Homopolymer compression on the device (lib.rs:211-222 per ACGT run):
   // replaces (bases, offsets) by the compressed batch in the workspace.
