@@ -390,8 +390,8 @@ __device__ void probe_batch(const DevIndex& ix, const uint64_t* keys, uint32_t n
 // exclusion).
 constexpr int kPlanes = 6;            // register planes: counts up to 63 per field
 constexpr uint32_t kPlaneFlush = 31;  // team steps (two seeds each) between flushes
-constexpr int kSharedPlanes = 8;      // shared planes: counts up to 255 per field
-constexpr uint32_t kSharedFlush = 127;
+constexpr int kSharedPlanes = 5;      // shared planes: counts up to 31 per field
+constexpr uint32_t kSharedFlush = 15; // team steps (two seeds each) between flushes
 constexpr uint32_t kMaxSharedPlaneWords = 32;
 constexpr uint16_t kNoPlanes = 0xFFFF;
 

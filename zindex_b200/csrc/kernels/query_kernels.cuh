@@ -117,14 +117,15 @@ struct FusedSmem {
     return (size_t)words * (kSharedPlanes + 2) * 32 * 4;
   }
   // Key buffer of a warp: one tile's keys, plus the lane-run staging of the
-  // polynomial k-mer hashes (k > 32) and findere s-mers in modes 0, 2 and 3.
-  static __host__ __device__ size_t key_bytes(int mode) {
-    return (mode == 1 || mode == 4 ? 1 : 2) * (size_t)kTileWindows * 8;
+  // polynomial k-mer hashes (modes 0 and 2 with k > 32) and of findere s-mers.
+  static __host__ __device__ size_t key_bytes(int mode, int k) {
+    const bool staged = mode == 3 || ((mode == 0 || mode == 2) && k > 32);
+    return (staged ? 2 : 1) * (size_t)kTileWindows * 8;
   }
   static __host__ __device__ size_t warp_bytes(int mode, int k, uint32_t classes, int stage_bytes = 0,
                                                int stages = 0, int hashes = 4, int planes = 0,
                                                uint32_t shared_words = 0) {
-    size_t b = key_bytes(mode) + probe_bytes(classes, hashes, planes) +
+    size_t b = key_bytes(mode, k) + probe_bytes(classes, hashes, planes) +
                ring_bytes(stage_bytes, stages) + shared_plane_bytes(shared_words);
     if (mode == 1) b += 2 * ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
     if (mode == 3) b += 64;  // findere: valid bits of up to 512 s-mer positions
@@ -232,9 +233,9 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
       FusedSmem::warp_bytes(MODE, sp.k, classes, stage_bytes, lc.stages, hashes, ROWS, swords);
   uint8_t* wbase = p + (size_t)warp * wstride;
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
-  SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + FusedSmem::key_bytes(MODE));
+  SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + FusedSmem::key_bytes(MODE, sp.k));
   uint64_t* row0s = reinterpret_cast<uint64_t*>(desc + 64);
-  uint8_t* ring_base = wbase + FusedSmem::key_bytes(MODE) + FusedSmem::probe_bytes(classes, hashes, ROWS);
+  uint8_t* ring_base = wbase + FusedSmem::key_bytes(MODE, sp.k) + FusedSmem::probe_bytes(classes, hashes, ROWS);
   uint8_t* ocm = ring_base + FusedSmem::ring_bytes(stage_bytes, lc.stages);
   SharedPlanes splanes{reinterpret_cast<uint32_t*>(wbase + wstride - FusedSmem::shared_plane_bytes(swords)),
                        swords, 0u};
@@ -389,7 +390,7 @@ __global__ void extract_kernel(BatchView bv, SeedParams sp, uint64_t* __restrict
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, 0);
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
-  uint8_t* ocm = wbase + FusedSmem::key_bytes(MODE) + FusedSmem::probe_bytes(0);
+  uint8_t* ocm = wbase + FusedSmem::key_bytes(MODE, sp.k) + FusedSmem::probe_bytes(0);
   build_inner_table(sp, inner);
   __syncthreads();
   // Tiles tile_lo .. tile_hi-1 (tile_hi 0 = to the end); tile t's slot is t - tile_lo.
