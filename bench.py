@@ -696,10 +696,21 @@ def ours(args):
         ix.query_records_report(fasta, os.devnull, min_ratio=PER_RECORD_MIN_RATIO, fmt="compact")
         times.append(time.perf_counter() - t0)
     rep_s = statistics.median(times)
+    # The reference's default report: TSV rows for every colour of every read.
+    n_tsv = min(n_rec, PER_RECORD_CPU_READS)
+    tsv_fasta = records_fasta(Path(args.cache), rank, args.config, bases, offsets, n_tsv)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ix.query_records_report(tsv_fasta, os.devnull, min_ratio=0.0, fmt="tsv")
+        times.append(time.perf_counter() - t0)
+    tsv_s = statistics.median(times)
     per_record = {
         "reads": n_rec, "seeds": agg_total,
         "counts_reads_per_s": n_rec / pr_s, "counts_seeds_per_s": agg_total / pr_s,
         "report_reads_per_s": n_rec / rep_s,
+        "report_tsv_all_colours_reads_per_s": n_tsv / tsv_s,
+        "report_tsv_sample_reads": n_tsv,
         "report": f"compact, min_ratio {PER_RECORD_MIN_RATIO}, {fasta.stat().st_size} B FASTA "
                   "read, counted and formatted per call",
         "d2h_bytes_per_call": int(8 * n_rec * (ix.colors + 1)),
@@ -725,6 +736,14 @@ def ours(args):
                 "value": n_s / secs, "unit": "reads/s", "cores": orc.cores, "kind": "port",
                 "sample": f"compact report of the first {n_s} reads, {secs:.2f}s"}
             per_record["parity_vs_oracle_sample"] = got_path.read_bytes() == want
+            orc = CpuOracle(index_dir)
+            want_tsv, secs_tsv = orc.records_report(sample, 0.0, False)
+            orc.close()
+            ix.query_records_report(sample, got_path, min_ratio=0.0, fmt="tsv")
+            per_record["cpu_baseline_tsv_all_colours"] = {
+                "value": n_s / secs_tsv, "unit": "reads/s", "cores": orc.cores, "kind": "port",
+                "sample": f"TSV report, every colour, of the first {n_s} reads, {secs_tsv:.2f}s"}
+            per_record["parity_vs_oracle_sample_tsv"] = got_path.read_bytes() == want_tsv
             got_path.unlink()
         line = {
             "metric": METRIC, "value": value, "unit": "seeds/s", "n_gpus": world,

@@ -209,7 +209,8 @@ int zx_query_records_report(zx_index* index, const char* query_path, int recover
     std::vector<uint64_t> counts[2], totals[2];
     zx::Engine::RecordHits hits[2];
     std::vector<uint64_t> rel;
-    std::string text[2];
+    std::vector<std::string> text[2];
+    const uint64_t formatters = std::max(1u, std::thread::hardware_concurrency() / 2);
     std::thread writer;
     auto join = [&] {
       if (writer.joinable()) writer.join();
@@ -231,20 +232,36 @@ int zx_query_records_report(zx_index* index, const char* query_path, int recover
         }
         join();
         writer = std::thread([&, b, r0, n] {
-          std::string& t = text[b];
-          t.clear();
-          for (uint64_t r = 0; r < n; ++r) {
-            if (sparse) {
-              const auto& h = hits[b];
-              zx::append_record_hits(t, format, rb.names[r0 + r], h.totals[r],
-                                     h.colors.data() + h.first[r], h.counts.data() + h.first[r],
-                                     h.first[r + 1] - h.first[r], colors);
-            } else {
-              zx::append_record(t, format, rb.names[r0 + r], totals[b][r],
-                                counts[b].data() + r * colors.size(), colors, 0.0);
+          // Records are formatted by up to `formatters` threads in contiguous
+          // runs (a dense report writes every colour of every record) and
+          // written in input order.
+          auto format_range = [&](uint64_t lo, uint64_t hi, std::string& t) {
+            t.clear();
+            for (uint64_t r = lo; r < hi; ++r) {
+              if (sparse) {
+                const auto& h = hits[b];
+                zx::append_record_hits(t, format, rb.names[r0 + r], h.totals[r],
+                                       h.colors.data() + h.first[r], h.counts.data() + h.first[r],
+                                       h.first[r + 1] - h.first[r], colors);
+              } else {
+                zx::append_record(t, format, rb.names[r0 + r], totals[b][r],
+                                  counts[b].data() + r * colors.size(), colors, 0.0);
+              }
             }
-          }
-          if (fwrite(t.data(), 1, t.size(), f) != t.size()) write_ok = false;
+          };
+          const uint64_t cells = n * (sparse ? 1 : colors.size());
+          const uint64_t parts =
+              std::max<uint64_t>(1, std::min<uint64_t>({formatters, n, cells / 65536 + 1}));
+          std::vector<std::string>& pieces = text[b];
+          pieces.resize(parts);
+          std::vector<std::thread> pool;
+          for (uint64_t i = 1; i < parts; ++i)
+            pool.emplace_back(format_range, n * i / parts, n * (i + 1) / parts,
+                              std::ref(pieces[i]));
+          format_range(0, n / parts, pieces[0]);
+          for (auto& th : pool) th.join();
+          for (const std::string& t : pieces)
+            if (fwrite(t.data(), 1, t.size(), f) != t.size()) write_ok = false;
         });
       }
       join();
