@@ -210,7 +210,7 @@ int zx_query_records_report(zx_index* index, const char* query_path, int recover
     zx::Engine::RecordHits hits[2];
     std::vector<uint64_t> rel;
     std::vector<std::string> text[2];
-    const uint64_t formatters = std::max(1u, std::thread::hardware_concurrency() / 2);
+    const uint64_t formatters = std::max(1u, std::thread::hardware_concurrency());
     std::thread writer;
     auto join = [&] {
       if (writer.joinable()) writer.join();
