@@ -289,6 +289,9 @@ struct Features {
   // width 0 = none.
   uint64_t pattern_mask = 0;
   size_t pattern_width = 0;
+  // Randstrobemers (src/anchors.rs:92-110): strobe-start distance range.
+  bool strobes = false;
+  size_t strobe_min = 0, strobe_max = 0;
 };
 
 // SpacedSeed::from_str (src/anchors.rs:15-42).
@@ -320,9 +323,61 @@ uint64_t pattern_canonical(uint64_t mask, size_t width, uint64_t key) {
                            (size_t)__builtin_popcountll(mask) / 2);
 }
 
+// strobe_hash (src/anchors.rs:136-151): XXH64 of one little-endian u64 with
+// seed 0 (the published short-input rounds and avalanche).
+uint64_t strobe_hash(uint64_t v) {
+  auto rotl = [](uint64_t x, int r) { return (x << r) | (x >> (64 - r)); };
+  const uint64_t p1 = 0x9E3779B185EBCA87ull, p2 = 0xC2B2AE3D27D4EB4Full,
+                 p3 = 0x165667B19E3779F9ull, p4 = 0x85EBCA77C2B2AE63ull,
+                 p5 = 0x27D4EB2F165667C5ull;
+  uint64_t h = (p5 + 8) ^ (rotl(v * p2, 31) * p1);
+  h = rotl(h, 27) * p1 + p4;
+  h ^= h >> 33;
+  h *= p2;
+  h ^= h >> 29;
+  h *= p3;
+  return h ^ (h >> 32);
+}
+
+// Linker (src/anchors.rs:182-256) restated as a direct loop: candidates of
+// one run in position order; each anchor emits (anchor.hash / 2) +
+// (partner.hash / 2) for the first later candidate at distance in
+// [dmin, dmax] with the fewest differing low 8 hash bits (the anchor itself
+// when there is none).
+void link_strobes(const std::vector<std::pair<size_t, uint64_t>>& cand, size_t dmin, size_t dmax,
+                  Emit& keys) {
+  for (size_t i = 0; i < cand.size(); ++i) {
+    const uint64_t a = cand[i].second;
+    uint64_t partner = a;
+    int best = 99;
+    for (size_t j = i + 1; j < cand.size(); ++j) {
+      const size_t d = cand[j].first - cand[i].first;
+      if (d > dmax) break;
+      if (d < dmin) continue;
+      const int rank = __builtin_popcountll((a ^ cand[j].second) & 255);
+      if (rank < best) {
+        best = rank;
+        partner = cand[j].second;
+        if (rank == 0) break;
+      }
+    }
+    keys.push_back(a / 2 + partner / 2);
+  }
+}
+
+// anchors::scan with randstrobemers (src/anchors.rs:265-347) on one ACGT run:
+// the candidates are the run's canonical k-mers (position = window start) or
+// its selected minimizer positions (sorted, one per position), hashed by
+// strobe_hash of the plain key, or of its spaced-seed key under a pattern.
+void scan_run_strobes(const uint8_t* seq, size_t n, const Features& f, Emit& keys);
+
 // scan_plain_features_uncompressed (src/lib.rs:608-642) on one ACGT run,
 // then the spaced-seed mapping of anchors::scan (src/anchors.rs:265-281).
 void scan_run_features(const uint8_t* seq, size_t n, const Features& f, Emit& keys) {
+  if (f.strobes && f.mode <= 1) {
+    scan_run_strobes(seq, n, f, keys);
+    return;
+  }
   const size_t first = keys.size();
   switch (f.mode) {
     case 0:
@@ -345,6 +400,28 @@ void scan_run_features(const uint8_t* seq, size_t n, const Features& f, Emit& ke
   if (f.pattern_width && f.mode <= 1)
     for (size_t i = first; i < keys.size(); ++i)
       keys[i] = pattern_canonical(f.pattern_mask, f.pattern_width, keys[i]);
+}
+
+void scan_run_strobes(const uint8_t* seq, size_t n, const Features& f, Emit& keys) {
+  std::vector<std::pair<size_t, uint64_t>> cand;
+  if (f.mode == 1) {
+    if (n >= f.k && (f.k & 1) && f.m >= 1 && f.m <= 31 && f.m <= f.k)
+      ocm_scan_run(seq, n, f.k, f.m, f.seed, cand);
+    std::sort(cand.begin(), cand.end(),
+              [](const auto& a, const auto& b) { return a.first < b.first; });
+    cand.erase(std::unique(cand.begin(), cand.end(),
+                           [](const auto& a, const auto& b) { return a.first == b.first; }),
+               cand.end());
+  } else {
+    Emit plain;
+    scan_canonical_kmers(seq, n, f.k, plain);
+    for (size_t i = 0; i < plain.size(); ++i) cand.emplace_back(i, plain[i]);
+  }
+  for (auto& c : cand) {
+    if (f.pattern_width) c.second = pattern_canonical(f.pattern_mask, f.pattern_width, c.second);
+    c.second = strobe_hash(c.second);
+  }
+  link_strobes(cand, f.strobe_min, f.strobe_max, keys);
 }
 
 // Calls visit(run, len) for every maximal ACGT run of a sequence, after the
@@ -875,7 +952,26 @@ std::unique_ptr<Index> load_index(const std::string& dir, bool recover, bool pay
            "seed pattern width must match k (or m in minimizer mode)");
   }
   const Json* rs = m.get("randstrobemers");
-  ensure(!rs || rs->kind == Json::Null, "randstrobemers are not restated");
+  if (rs && rs->kind != Json::Null) {
+    // Manifest::features (storage.rs:240-256), RandstrobeConfig::validate
+    // (anchors.rs:98-110), FeatureConfig::validate_anchors (lib.rs:177-206).
+    const Json* scheme = m.get("randstrobe_scheme");
+    ensure(ix->version >= 6 && scheme && scheme->kind == Json::Str &&
+               scheme->s == "strobealign-popcount8-symmetric64-downstream-v1",
+           "unsupported legacy/custom randstrobemer extraction; rebuild this index with the "
+           "current downstream scheme");
+    ensure(ix->f.mode == 0 || ix->f.mode == 1,
+           "spaced seeds and randstrobemers require --index-mode kmers or minimizers");
+    const Json* lo = rs->get("min_distance");
+    const Json* hi = rs->get("max_distance");
+    ensure(lo && hi, "manifest: randstrobemers");
+    ix->f.strobes = true;
+    ix->f.strobe_min = lo->as_u64();
+    ix->f.strobe_max = hi->as_u64();
+    ensure(ix->f.strobe_min > 0, "randstrobemer minimum distance must be greater than zero");
+    ensure(ix->f.strobe_min <= ix->f.strobe_max,
+           "randstrobemer minimum distance must not exceed maximum distance");
+  }
   const Json* ar = m.get("abandoned_recovery");
   bool recovery = !ar || (ar->kind == Json::Bool && ar->b);
   ix->recovery = recover && recovery;
@@ -1277,17 +1373,99 @@ void format_record(const Index& ix, const std::string& name, uint64_t total,
   }
 }
 
+// reverse_complement (src/anchors.rs:257-263): reversed, ACGT complemented
+// (upper case), every other byte kept as a separator.
+std::vector<uint8_t> reverse_complement(const uint8_t* seq, size_t n) {
+  std::vector<uint8_t> r(n);
+  for (size_t i = 0; i < n; ++i) {
+    const uint8_t b = seq[n - 1 - i];
+    const int c = encode_base(b);
+    r[i] = c < 0 ? b : (uint8_t)"TGCA"[c];
+  }
+  return r;
+}
+
+// Counts of one record queried alone. Randstrobemer indexes extract both
+// strands (PreparedRead::new, query_stream.rs:516-534) and keep per colour
+// the larger strand count (Scores::score, query_stream.rs:690-701); total =
+// forward anchors, probes = anchors of both strands.
+void record_counts(const Index& ix, const uint8_t* seq, size_t n, std::vector<uint64_t>& counts,
+                   uint64_t& total, uint64_t& probes) {
+  Work w;
+  prepare_record(ix.f, seq, n, w);
+  run_query(ix, w, 1, counts);
+  total = w.total;
+  probes = w.probes;
+  if (!ix.f.strobes) return;
+  std::vector<uint8_t> rc = reverse_complement(seq, n);
+  Work wr;
+  prepare_record(ix.f, rc.data(), rc.size(), wr);
+  ensure(wr.keys.size() == w.keys.size(), "canonical anchor counts must agree across strands");
+  std::vector<uint64_t> reverse;
+  run_query(ix, wr, 1, reverse);
+  for (size_t c = 0; c < counts.size(); ++c) counts[c] = std::max(counts[c], reverse[c]);
+  probes += wr.probes;
+}
+
+// Aggregate counts of records seq(r), r < records: one pass over all seeds,
+// or for randstrobemer indexes the per-record strand maxima summed (records
+// spread over `threads` workers).
+void query_many(const Index& ix, size_t records,
+                const std::function<std::pair<const uint8_t*, size_t>(size_t)>& seq, int threads,
+                std::vector<uint64_t>& counts, uint64_t& total, uint64_t& probes) {
+  if (!ix.f.strobes) {
+    Work w;
+    for (size_t r = 0; r < records; ++r) {
+      auto sq = seq(r);
+      prepare_record(ix.f, sq.first, sq.second, w);
+    }
+    run_query(ix, w, threads, counts);
+    total = w.total;
+    probes = w.probes;
+    return;
+  }
+  const size_t C = ix.colors.size(), T = (size_t)std::max(1, threads);
+  std::vector<std::vector<uint64_t>> part(T, std::vector<uint64_t>(C, 0));
+  std::vector<uint64_t> tot(T, 0), prb(T, 0);
+  std::vector<std::string> err(T);
+  std::vector<std::thread> pool;
+  for (size_t t = 0; t < T; ++t)
+    pool.emplace_back([&, t] {
+      try {
+        std::vector<uint64_t> c;
+        for (size_t r = records * t / T; r < records * (t + 1) / T; ++r) {
+          auto sq = seq(r);
+          uint64_t a = 0, b = 0;
+          record_counts(ix, sq.first, sq.second, c, a, b);
+          for (size_t i = 0; i < C; ++i) part[t][i] += c[i];
+          tot[t] += a;
+          prb[t] += b;
+        }
+      } catch (const std::exception& e) {
+        err[t] = e.what();
+      }
+    });
+  for (auto& th : pool) th.join();
+  for (auto& e : err) ensure(e.empty(), e.c_str());
+  counts.assign(C, 0);
+  total = probes = 0;
+  for (size_t t = 0; t < T; ++t) {
+    for (size_t i = 0; i < C; ++i) counts[i] += part[t][i];
+    total += tot[t];
+    probes += prb[t];
+  }
+}
+
 // Per-record counts and totals of named records (each record queried alone).
 std::string query_records_output(const Index& ix, const std::vector<NamedRecord>& recs,
                                  double min_ratio, bool compact) {
   std::string out = records_header(compact);
   out += '\n';
   for (auto& r : recs) {
-    Work w;
-    prepare_record(ix.f, r.seq.data(), r.seq.size(), w);
     std::vector<uint64_t> counts;
-    run_query(ix, w, 1, counts);
-    format_record(ix, r.name, w.total, counts, min_ratio, compact, out);
+    uint64_t total = 0, probes = 0;
+    record_counts(ix, r.seq.data(), r.seq.size(), counts, total, probes);
+    format_record(ix, r.name, total, counts, min_ratio, compact, out);
   }
   return out;
 }
@@ -1342,6 +1520,45 @@ int oracle_features(const uint8_t* seq, size_t len, int mode, int k, int m, uint
     f.sampling = sampling;
     f.z = (size_t)findere_z;
     f.homopolymer = homopolymer != 0;
+    Emit keys;
+    for_each_run(seq, len, f.homopolymer,
+                 [&](const uint8_t* run, size_t n) { scan_run_features(run, n, f, keys); });
+    *count = keys.size();
+    memcpy(out, keys.data(), std::min(cap, keys.size()) * 8);
+  });
+}
+
+uint64_t oracle_strobe_hash(uint64_t v) { return strobe_hash(v); }
+
+// Links candidates (ascending positions, their strobe hashes) into keys.
+void oracle_link_strobes(const uint64_t* positions, const uint64_t* hashes, size_t n,
+                         uint64_t dmin, uint64_t dmax, uint64_t* out) {
+  std::vector<std::pair<size_t, uint64_t>> cand(n);
+  for (size_t i = 0; i < n; ++i) cand[i] = {(size_t)positions[i], hashes[i]};
+  Emit keys;
+  link_strobes(cand, dmin, dmax, keys);
+  memcpy(out, keys.data(), keys.size() * 8);
+}
+
+// Seeds of a sequence with a spaced-seed pattern ("" = none) and, when
+// strobe_max > 0, randstrobemers linked over [strobe_min, strobe_max].
+int oracle_features_anchored(const uint8_t* seq, size_t len, int mode, int k, int m, uint64_t seed,
+                             int homopolymer, const char* pattern, uint64_t strobe_min,
+                             uint64_t strobe_max, uint64_t* out, size_t cap, size_t* count) {
+  return guarded([&] {
+    Features f;
+    f.mode = mode;
+    f.k = (size_t)k;
+    f.m = (size_t)m;
+    f.seed = seed;
+    f.homopolymer = homopolymer != 0;
+    if (pattern && *pattern)
+      ensure(parse_pattern(pattern, &f.pattern_mask, &f.pattern_width), "invalid seed pattern");
+    if (strobe_max) {
+      f.strobes = true;
+      f.strobe_min = strobe_min;
+      f.strobe_max = strobe_max;
+    }
     Emit keys;
     for_each_run(seq, len, f.homopolymer,
                  [&](const uint8_t* run, size_t n) { scan_run_features(run, n, f, keys); });
@@ -1414,13 +1631,12 @@ int oracle_query_file(const char* index_dir, const char* query_path, int threads
     ensure(colors == ix->colors.size(), "colour count differs from the index");
     std::vector<std::vector<uint8_t>> records;
     parse_fastx(read_decoded(query_path), records);
-    Work w;
-    for (auto& r : records) prepare_record(ix->f, r.data(), r.size(), w);
     std::vector<uint64_t> out;
-    run_query(*ix, w, threads, out);
+    query_many(
+        *ix, records.size(),
+        [&](size_t r) { return std::make_pair((const uint8_t*)records[r].data(), records[r].size()); },
+        threads, out, *total, *probes);
     memcpy(counts, out.data(), colors * 8);
-    *total = w.total;
-    *probes = w.probes;
   });
 }
 
@@ -1430,14 +1646,12 @@ int oracle_query_records(const char* index_dir, const uint8_t* bases, const uint
   return guarded([&] {
     auto ix = load_index(index_dir, recover != 0);
     ensure(colors == ix->colors.size(), "colour count differs from the index");
-    Work w;
-    for (size_t r = 0; r < records; ++r)
-      prepare_record(ix->f, bases + offsets[r], offsets[r + 1] - offsets[r], w);
     std::vector<uint64_t> out;
-    run_query(*ix, w, threads, out);
+    query_many(
+        *ix, records,
+        [&](size_t r) { return std::make_pair(bases + offsets[r], (size_t)(offsets[r + 1] - offsets[r])); },
+        threads, out, *total, *probes);
     memcpy(counts, out.data(), colors * 8);
-    *total = w.total;
-    *probes = w.probes;
   });
 }
 
@@ -1461,14 +1675,14 @@ int oracle_query_timed(const char* index_dir, const uint8_t* bases, const uint64
     auto ix = load_index(index_dir, true);
     ensure(colors == ix->colors.size(), "colour count differs from the index");
     auto t0 = std::chrono::steady_clock::now();
-    Work w;
-    for (size_t r = 0; r < records; ++r)
-      prepare_record(ix->f, bases + offsets[r], offsets[r + 1] - offsets[r], w);
     std::vector<uint64_t> out;
-    run_query(*ix, w, threads, out);
+    uint64_t probes = 0;
+    query_many(
+        *ix, records,
+        [&](size_t r) { return std::make_pair(bases + offsets[r], (size_t)(offsets[r + 1] - offsets[r])); },
+        threads, out, *total, probes);
     *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     memcpy(counts, out.data(), colors * 8);
-    *total = w.total;
   });
 }
 
@@ -1507,14 +1721,14 @@ int oracle_query_handle(oracle_index* h, const uint8_t* bases, const uint64_t* o
     const Index& ix = *h->ix;
     ensure(colors == ix.colors.size(), "colour count differs from the index");
     auto t0 = std::chrono::steady_clock::now();
-    Work w;
-    for (size_t r = 0; r < records; ++r)
-      prepare_record(ix.f, bases + offsets[r], offsets[r + 1] - offsets[r], w);
     std::vector<uint64_t> out;
-    run_query(ix, w, threads, out);
+    uint64_t probes = 0;
+    query_many(
+        ix, records,
+        [&](size_t r) { return std::make_pair(bases + offsets[r], (size_t)(offsets[r + 1] - offsets[r])); },
+        threads, out, *total, probes);
     *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     memcpy(counts, out.data(), colors * 8);
-    *total = w.total;
   });
 }
 
@@ -1535,11 +1749,10 @@ int oracle_records_report_handle(oracle_index* h, const char* query_path, double
       pool.emplace_back([&, t] {
         const size_t a = recs.size() * t / T, b = recs.size() * (t + 1) / T;
         for (size_t r = a; r < b; ++r) {
-          Work w;
-          prepare_record(ix.f, recs[r].seq.data(), recs[r].seq.size(), w);
           std::vector<uint64_t> counts;
-          run_query(ix, w, 1, counts);
-          format_record(ix, recs[r].name, w.total, counts, min_ratio, compact != 0, parts[t]);
+          uint64_t total = 0, probes = 0;
+          record_counts(ix, recs[r].seq.data(), recs[r].seq.size(), counts, total, probes);
+          format_record(ix, recs[r].name, total, counts, min_ratio, compact != 0, parts[t]);
         }
       });
     for (auto& th : pool) th.join();
@@ -1596,18 +1809,19 @@ int main(int argc, char** argv) {
     auto t0 = std::chrono::steady_clock::now();
     std::vector<std::vector<uint8_t>> records;
     parse_fastx(read_decoded(query), records);
-    Work w;
-    for (auto& r : records) prepare_record(ix->f, r.data(), r.size(), w);
     std::vector<uint64_t> counts;
-    run_query(*ix, w, threads, counts);
+    uint64_t total = 0, probes = 0;
+    query_many(
+        *ix, records.size(),
+        [&](size_t r) { return std::make_pair((const uint8_t*)records[r].data(), records[r].size()); },
+        threads, counts, total, probes);
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     fprintf(stderr,
             "#query\t%s\tk=%zu\tindex_mode=%s\ttotal_features=%llu\tstack_probes=%llu\t"
             "bank_probes=%llu\telapsed_s=%.6f\n",
-            query.c_str(), ix->k, mode_label(ix->f.mode), (unsigned long long)w.total,
-            (unsigned long long)w.probes,
-            (unsigned long long)(w.probes * ix->classes.size()), secs);
-    fputs(format_aggregate(*ix, counts.data(), w.total, ratio).c_str(), stdout);
+            query.c_str(), ix->k, mode_label(ix->f.mode), (unsigned long long)total,
+            (unsigned long long)probes, (unsigned long long)(probes * ix->classes.size()), secs);
+    fputs(format_aggregate(*ix, counts.data(), total, ratio).c_str(), stdout);
     return 0;
   } catch (const std::exception& e) {
     fprintf(stderr, "Error: %s\n", e.what());

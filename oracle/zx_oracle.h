@@ -76,6 +76,15 @@ int oracle_records_report_handle(oracle_index* index, const char* query_path, do
 int oracle_pattern_canonical(const char* pattern, uint64_t key, uint64_t* projected,
                              uint64_t* canonical);
 
+/* Randstrobemers (anchors.rs:129-347): the XXH64 strobe hash of one u64, and
+ * the seeds of a sequence with an optional pattern and strobe linking. */
+uint64_t oracle_strobe_hash(uint64_t v);
+void oracle_link_strobes(const uint64_t* positions, const uint64_t* hashes, size_t n,
+                         uint64_t dmin, uint64_t dmax, uint64_t* out);
+int oracle_features_anchored(const uint8_t* seq, size_t len, int mode, int k, int m, uint64_t seed,
+                             int homopolymer, const char* pattern, uint64_t strobe_min,
+                             uint64_t strobe_max, uint64_t* out, size_t cap, size_t* count);
+
 const char* oracle_last_error(void);
 
 #ifdef __cplusplus

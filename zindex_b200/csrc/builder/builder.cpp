@@ -394,6 +394,18 @@ void build_index(const BuildOptions& opt) {
           "seed pattern width must match k (or m in minimizer mode)");
     fp.spaced = true;
   }
+  if (fp.strobes) {
+    // RandstrobeConfig defaults and checks (src/bin/zorindex.rs:471-484,
+    // src/anchors.rs:98-110): distances default to the strobe length (k, or
+    // m in minimizer mode) and three times it.
+    check(fp.mode == 0 || fp.mode == 1, kEInval,
+          "spaced seeds and randstrobemers require --index-mode kmers or minimizers");
+    const uint64_t length = (uint64_t)(fp.mode == 1 ? fp.m : fp.k);
+    if (!fp.strobe_min) fp.strobe_min = length;
+    if (!fp.strobe_max) fp.strobe_max = 3 * length;
+    check(fp.strobe_min <= fp.strobe_max, kEInval,
+          "randstrobemer minimum distance must not exceed maximum distance");
+  }
   struct stat st;
   check(stat(opt.output.c_str(), &st) != 0, kEInval,
         ("output " + opt.output + " already exists; choose a new directory").c_str());
@@ -707,8 +719,16 @@ void build_index(const BuildOptions& opt) {
   m.set("minimizer_scheme", JsonValue::str("open-closed-mod"));
   m.set("homopolymer_compression", JsonValue::boolean(fp.homopolymer));
   m.set("seed_pattern", fp.spaced ? JsonValue::str(fp.seed_pattern) : JsonValue::null());
-  m.set("randstrobemers", JsonValue::null());
-  m.set("randstrobe_scheme", JsonValue::null());
+  if (fp.strobes) {
+    JsonValue rs = JsonValue::object();
+    rs.set("min_distance", JsonValue::uint(fp.strobe_min));
+    rs.set("max_distance", JsonValue::uint(fp.strobe_max));
+    m.set("randstrobemers", rs);
+    m.set("randstrobe_scheme", JsonValue::str("strobealign-popcount8-symmetric64-downstream-v1"));
+  } else {
+    m.set("randstrobemers", JsonValue::null());
+    m.set("randstrobe_scheme", JsonValue::null());
+  }
   m.set("modimizer_sampling", JsonValue::uint(fp.sampling));
   m.set("findere_z", JsonValue::uint((uint64_t)fp.z));
   m.set("sketch_size", JsonValue::uint(128));

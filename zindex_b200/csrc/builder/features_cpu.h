@@ -7,6 +7,7 @@
 // (utils/ocm-minimizers/src/implementation.rs:108-236), modimizers (796-806),
 // findere s-mers (632-640) and homopolymer compression (211-222).
 #pragma once
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -27,6 +28,10 @@ struct FeatureParams {
   std::string seed_pattern;
   bool spaced = false;
   SpacedSeed pattern;
+  // Randstrobemers (src/anchors.rs:92-110, 182-347): each candidate seed is
+  // linked to a partner starting strobe_min..strobe_max bases downstream.
+  bool strobes = false;
+  uint64_t strobe_min = 0, strobe_max = 0;
 };
 
 namespace cpu {
@@ -104,15 +109,19 @@ inline AnchorRank rank_combine(const AnchorRank& a, const AnchorRank& b) {
 }
 
 // Open-closed mod-minimizers of one all-ACGT run (n >= k).
+// positions (optional) receives the run offset of each emitted minimizer.
 inline void ocm_run(const uint8_t* s, size_t n, int k, int m, uint64_t seed,
-                    std::vector<uint64_t>& out) {
+                    std::vector<uint64_t>& out, std::vector<uint64_t>* positions = nullptr) {
   auto canon = [&](size_t p, int len) {
     uint64_t v = 0;
     for (int q = 0; q < len; ++q) v = (v << 2) | encode_base(s[p + q]);
     return canonical_encoded(v, len);
   };
   if (k == m) {
-    for (size_t p = 0; p + m <= n; ++p) out.push_back(canon(p, m));
+    for (size_t p = 0; p + m <= n; ++p) {
+      out.push_back(canon(p, m));
+      if (positions) positions->push_back(p);
+    }
     return;
   }
   const OcmParams g = ocm_params(k, m);
@@ -150,9 +159,44 @@ inline void ocm_run(const uint8_t* s, size_t n, int k, int m, uint64_t seed,
     size_t pos = st + (anchor - st) % (size_t)g.w;
     if (!have || pos != prev) {
       out.push_back(canon(pos, m));
+      if (positions) positions->push_back(pos);
       prev = pos;
       have = true;
     }
+  }
+}
+
+// The strobe hash of a seed key (src/anchors.rs:136-151): XXH64 of the key's
+// eight little-endian bytes with seed 0.
+inline uint64_t strobe_hash(uint64_t key) {
+  constexpr uint64_t P1 = 0x9E3779B185EBCA87ull, P2 = 0xC2B2AE3D27D4EB4Full,
+                     P3 = 0x165667B19E3779F9ull, P4 = 0x85EBCA77C2B2AE63ull,
+                     P5 = 0x27D4EB2F165667C5ull;
+  uint64_t lane = key * P2;
+  lane = ((lane << 31) | (lane >> 33)) * P1;
+  uint64_t h = (P5 + 8) ^ lane;
+  h = ((h << 27) | (h >> 37)) * P1 + P4;
+  h = (h ^ (h >> 33)) * P2;
+  h = (h ^ (h >> 29)) * P3;
+  return h ^ (h >> 32);
+}
+
+// Links the candidates of one run (offsets ascending, one per offset) into
+// randstrobemer keys, one per candidate in order: the partner is the first
+// candidate strobe_min..strobe_max bases downstream with the fewest differing
+// low 8 hash bits, or the candidate itself (Linker, src/anchors.rs:182-256).
+inline void link_run(const std::vector<uint64_t>& offsets, const std::vector<uint64_t>& hashes,
+                     uint64_t dmin, uint64_t dmax, std::vector<uint64_t>& out) {
+  const size_t n = hashes.size();
+  for (size_t i = 0; i < n; ++i) {
+    size_t pick = i;
+    int fewest = 9;
+    for (size_t j = i + 1; j < n && offsets[j] - offsets[i] <= dmax && fewest; ++j) {
+      if (offsets[j] - offsets[i] < dmin) continue;
+      const int d = __builtin_popcountll((hashes[i] ^ hashes[j]) & 0xFF);
+      if (d < fewest) fewest = d, pick = j;
+    }
+    out.push_back((hashes[i] >> 1) + (hashes[pick] >> 1));
   }
 }
 
@@ -183,6 +227,29 @@ inline std::vector<uint8_t> homopolymer(const uint8_t* s, size_t n) {
 // Features of one ACGT run (already homopolymer-compressed when requested).
 inline void run_features(const uint8_t* s, size_t n, const FeatureParams& f,
                          std::vector<uint64_t>& out) {
+  if (f.strobes && f.mode <= 1) {
+    // Candidates: every canonical k-mer (offset = window start) or the
+    // run's selected minimizers, sorted by offset, one per offset.
+    std::vector<uint64_t> keys, offsets;
+    if (f.mode == 0) {
+      kmers(s, n, f.k, keys);
+      for (size_t i = 0; i < keys.size(); ++i) offsets.push_back(i);
+    } else if (n >= (size_t)f.k && (f.k & 1) && f.m >= 1 && f.m <= 31 && f.m <= f.k) {
+      std::vector<uint64_t> raw, at;
+      ocm_run(s, n, f.k, f.m, f.seed, raw, &at);
+      std::vector<size_t> order(raw.size());
+      for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+      std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return at[a] < at[b]; });
+      for (size_t i : order)
+        if (offsets.empty() || at[i] != offsets.back()) {
+          offsets.push_back(at[i]);
+          keys.push_back(raw[i]);
+        }
+    }
+    for (uint64_t& k : keys) k = strobe_hash(f.spaced ? spaced_canonical(f.pattern, k) : k);
+    link_run(offsets, keys, f.strobe_min, f.strobe_max, out);
+    return;
+  }
   const size_t first = out.size();
   switch (f.mode) {
     case 0: kmers(s, n, f.k, out); break;

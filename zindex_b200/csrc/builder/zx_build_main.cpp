@@ -48,6 +48,9 @@ int main(int argc, char** argv) {
     else if (a == "-d" || a == "--modimizer-sampling") o.features.sampling = std::stoull(val());
     else if (a == "-c" || a == "--homopolymer-compression") o.features.homopolymer = true;
     else if (a == "-p" || a == "--seed-pattern") o.features.seed_pattern = val();
+    else if (a == "-r" || a == "--randstrobemers") o.features.strobes = true;
+    else if (a == "-l" || a == "--strobe-min") o.features.strobe_min = std::stoull(val());
+    else if (a == "-u" || a == "--strobe-max") o.features.strobe_max = std::stoull(val());
     else if (a == "--legacy-layout") o.legacy_layout = true;
     else if (a == "-S" || a == "--slot-scale") o.slot_scale = std::stod(val());
     else if (a == "-L" || a == "--segment-length") o.segment_length = std::stoull(val());
