@@ -166,21 +166,6 @@ inline void ocm_run(const uint8_t* s, size_t n, int k, int m, uint64_t seed,
   }
 }
 
-// The strobe hash of a seed key (src/anchors.rs:136-151): XXH64 of the key's
-// eight little-endian bytes with seed 0.
-inline uint64_t strobe_hash(uint64_t key) {
-  constexpr uint64_t P1 = 0x9E3779B185EBCA87ull, P2 = 0xC2B2AE3D27D4EB4Full,
-                     P3 = 0x165667B19E3779F9ull, P4 = 0x85EBCA77C2B2AE63ull,
-                     P5 = 0x27D4EB2F165667C5ull;
-  uint64_t lane = key * P2;
-  lane = ((lane << 31) | (lane >> 33)) * P1;
-  uint64_t h = (P5 + 8) ^ lane;
-  h = ((h << 27) | (h >> 37)) * P1 + P4;
-  h = (h ^ (h >> 33)) * P2;
-  h = (h ^ (h >> 29)) * P3;
-  return h ^ (h >> 32);
-}
-
 // Links the candidates of one run (offsets ascending, one per offset) into
 // randstrobemer keys, one per candidate in order: the partner is the first
 // candidate strobe_min..strobe_max bases downstream with the fewest differing

@@ -190,7 +190,7 @@ int zx_query_records_report(zx_index* index, const char* query_path, int recover
     // only they are copied back; with min_ratio 0 every colour is reported and
     // the dense counts come back, at most 256 MiB of them per step. The step
     // (like the reference's record batch size) does not change the output.
-    const bool sparse = min_ratio > 0.0;
+    const bool sparse = min_ratio > 0.0 && !e.strobes();
     const uint64_t step = sparse ? (1ull << 18) : std::max<uint64_t>(1, (32ull << 20) / C);
     FILE* f = out_path ? fopen(out_path, "wb") : stdout;
     if (!f) zx::raise(zx::kEIo, std::string("cannot create ") + out_path);
@@ -245,7 +245,7 @@ int zx_query_records_report(zx_index* index, const char* query_path, int recover
                                        h.first[r + 1] - h.first[r], colors);
               } else {
                 zx::append_record(t, format, rb.names[r0 + r], totals[b][r],
-                                  counts[b].data() + r * colors.size(), colors, 0.0);
+                                  counts[b].data() + r * colors.size(), colors, min_ratio);
               }
             }
           };
@@ -374,6 +374,7 @@ int zx_query_segments(zx_index* index, const uint8_t* bases, uint64_t nbases,
               zx::kEInval, "null argument");
     std::lock_guard<std::mutex> lock(index->mu);
     auto& e = *index->engine;
+    e.check_not_strobes();
     if (!index->seg_ws) index->seg_ws = e.make_workspace();
     // Grid shares from the record counts (the lengths stay on the device).
     std::vector<uint64_t> est(segments);

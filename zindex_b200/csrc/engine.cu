@@ -315,6 +315,7 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
                                   uint64_t records, bool recover, uint64_t* counts,
                                   unsigned long long* total, cudaStream_t s) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  check_not_strobes();
   check(records < (1ull << 31), kEInval, "too many records for one query");
   check(!m_.homopolymer_compression, kEUnsupported,
         "the allocation-free query does not run homopolymer compression (the compressed batch "
@@ -538,6 +539,15 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
   if (m_.has_seed_pattern) {
     check_format(parse_spaced_seed(m_.seed_pattern.c_str(), &sp_.pattern), "invalid seed pattern");
     sp_.spaced = 1;
+  }
+  sp_.strobe_min = sp_.strobe_max = 0;
+  if (m_.has_randstrobemers) {
+    check(m_.index_mode == kKmers && m_.k <= 32, kEUnsupported,
+          "the GPU query path links randstrobemers over k-mers with k <= 32 only");
+    check(m_.strobe_max <= kMaxStrobeSpan, kEUnsupported,
+          "randstrobemer distances above 256 are not supported by the GPU query path");
+    sp_.strobe_min = (uint32_t)m_.strobe_min;
+    sp_.strobe_max = (uint32_t)m_.strobe_max;
   }
 
   // Memory admission: banks (padded rows) + recovery directory.
@@ -831,6 +841,12 @@ QueryLaunch Engine::default_launch() const {
   return l;
 }
 
+void Engine::check_not_strobes() const {
+  check(!sp_.strobe_max, kEUnsupported,
+        "randstrobemer indexes score each record's two strands: query them through host-buffer "
+        "calls (zx_query_host, zx_query_file, zx_query_per_record, per-record reports)");
+}
+
 int Engine::kernel_mode(const QueryLaunch& l) const {
   return l.split && sp_.mode == kMinimizers && l.planes == 1 && l.stage_bytes == 0 ? 4 : sp_.mode;
 }
@@ -838,7 +854,7 @@ int Engine::kernel_mode(const QueryLaunch& l) const {
 size_t Engine::fused_smem_bytes(const QueryLaunch& l) const {
   const int mode = kernel_mode(l);
   return FusedSmem::total(mode, sp_.k, (uint32_t)m_.colors.size(), host_ix_.classes, m_.hashes, l,
-                          FusedSmem::shared_words(mode, host_ix_, l));
+                          FusedSmem::shared_words(mode, host_ix_, l), sp_.strobe_max != 0);
 }
 
 int Engine::max_blocks(const QueryLaunch& l) const {
@@ -1352,12 +1368,70 @@ void Engine::query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbas
                               uint64_t* counts, uint64_t* totals) {
   const uint64_t colors = m_.colors.size();
   cudaStream_t s = ws.stream;
-  record_groups(ws, bases, nbases, offsets, records, recover, [&](uint64_t r0, uint64_t n) {
-    cuda_check(cudaMemcpyAsync(counts + r0 * colors, ws.rec_counts, n * colors * 8,
-                               cudaMemcpyDeviceToHost, s),
-               "D2H");
-    cuda_check(cudaMemcpyAsync(totals + r0, ws.rec_totals, n * 8, cudaMemcpyDeviceToHost, s), "D2H");
-  });
+  auto run = [&](const uint8_t* b, uint64_t* c, uint64_t* t) {
+    record_groups(ws, b, nbases, offsets, records, recover, [&](uint64_t r0, uint64_t n) {
+      cuda_check(cudaMemcpyAsync(c + r0 * colors, ws.rec_counts, n * colors * 8,
+                                 cudaMemcpyDeviceToHost, s),
+                 "D2H");
+      cuda_check(cudaMemcpyAsync(t + r0, ws.rec_totals, n * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    });
+  };
+  run(bases, counts, totals);
+  if (!sp_.strobe_max) return;
+  // Randstrobemers: the reverse-complement strand too, and per record and
+  // colour the larger count (PreparedRead::new, query_stream.rs:516-534;
+  // Scores::score, query_stream.rs:690-701).
+  std::vector<uint8_t> rc(nbases);
+  reverse_complement_records(bases, offsets, records, rc.data());
+  std::vector<uint64_t> rcounts(records * colors), rtotals(records);
+  run(rc.data(), rcounts.data(), rtotals.data());
+  for (uint64_t r = 0; r < records; ++r)
+    check(rtotals[r] == totals[r], kEFormat, "canonical anchor counts must agree across strands");
+  for (uint64_t i = 0; i < records * colors; ++i) counts[i] = std::max(counts[i], rcounts[i]);
+}
+
+void reverse_complement_records(const uint8_t* bases, const uint64_t* offsets, uint64_t records,
+                                uint8_t* out) {
+  // reverse_complement (src/anchors.rs:257-263): ACGT of either case become
+  // the upper-case complement, every other byte stays a separator.
+  static const struct Table {
+    uint8_t t[256];
+    Table() {
+      for (int i = 0; i < 256; ++i) t[i] = (uint8_t)i;
+      t['A'] = t['a'] = 'T';
+      t['C'] = t['c'] = 'G';
+      t['G'] = t['g'] = 'C';
+      t['T'] = t['t'] = 'A';
+    }
+  } table;
+  for (uint64_t r = 0; r < records; ++r) {
+    const uint64_t a = offsets[r], b = offsets[r + 1];
+    for (uint64_t i = a; i < b; ++i) out[a + (b - 1 - i)] = table.t[bases[i]];
+  }
+}
+
+void Engine::query_strobes_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                                const uint64_t* offsets, uint64_t records, bool recover,
+                                uint64_t* counts, uint64_t* total) {
+  check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
+  const uint64_t colors = std::max<uint64_t>(m_.colors.size(), 1);
+  const uint64_t step = std::max<uint64_t>(1, (32ull << 20) / colors);
+  std::vector<uint64_t> c, t, rel;
+  std::fill(counts, counts + m_.colors.size(), 0);
+  *total = 0;
+  for (uint64_t r0 = 0; r0 < records; r0 += step) {
+    const uint64_t n = std::min(step, records - r0), b0 = offsets[r0];
+    rel.resize(n + 1);
+    for (uint64_t r = 0; r <= n; ++r) rel[r] = offsets[r0 + r] - b0;
+    check(rel[n] <= nbases - b0, kEInval, "offsets must be non-decreasing");
+    c.resize(n * m_.colors.size());
+    t.resize(n);
+    query_per_record(ws, bases + b0, rel[n], rel.data(), n, recover, c.data(), t.data());
+    for (uint64_t r = 0; r < n; ++r) {
+      *total += t[r];
+      for (uint64_t i = 0; i < m_.colors.size(); ++i) counts[i] += c[r * m_.colors.size() + i];
+    }
+  }
 }
 
 void Engine::query_record_hits(Workspace& ws, const uint8_t* bases, uint64_t nbases,
@@ -1460,6 +1534,7 @@ void Engine::query_device(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                           uint64_t* counts, unsigned long long* total, cudaStream_t s,
                           bool use_graph) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  check_not_strobes();
   ensure_capacity(ws, nbases, records);
   if (!use_graph) {
     enqueue(ws, bases, nbases, offsets, records, recover, counts, total, s);
@@ -1494,6 +1569,10 @@ void Engine::query_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                         const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
                         uint64_t* total) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  if (sp_.strobe_max) {
+    query_strobes_host(ws, bases, nbases, offsets, records, recover, counts, total);
+    return;
+  }
   // Offsets are checked per record by the tile planner on the device
   // (kErrOffsets): a host pass over a million records cost about 1 ms.
   check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
@@ -1584,6 +1663,10 @@ void Engine::query_host_plain(Workspace& ws, const uint8_t* bases, uint64_t nbas
                               const uint64_t* offsets, uint64_t records, bool recover,
                               uint64_t* counts, uint64_t* total) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  if (sp_.strobe_max) {
+    query_strobes_host(ws, bases, nbases, offsets, records, recover, counts, total);
+    return;
+  }
   check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
   for (uint64_t r = 0; r < records; ++r)  // records are sliced on the host here
     check(offsets[r] <= offsets[r + 1], kEInval, "offsets must be non-decreasing");
@@ -1652,7 +1735,8 @@ void Engine::extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     ws.cap_keys = need;
   }
   const int warps = 4;
-  size_t smem = 256 * 8 + warps * FusedSmem::warp_bytes(sp_.mode, sp_.k, 0);
+  size_t smem = 256 * 8 + warps * FusedSmem::warp_bytes(sp_.mode, sp_.k, 0, 0, 0, 4, 0, 0,
+                                                        sp_.strobe_max != 0);
   ExtractFn efn = extract_for(sp_.mode);
   cudaFuncSetAttribute(efn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   BatchView bv{PackedView{ws.packed, ws.invalid}, d_offsets, ws.tiles, ws.tile_first + records,

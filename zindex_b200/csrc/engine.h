@@ -94,6 +94,10 @@ struct Workspace {
   void release_graphs();
 };
 
+// Reverse complement of every record of a host batch, records in place.
+void reverse_complement_records(const uint8_t* bases, const uint64_t* offsets, uint64_t records,
+                                uint8_t* out);
+
 class Engine {
  public:
   Engine(const std::string& dir, const OpenOptions& options);
@@ -179,6 +183,16 @@ class Engine {
   void query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                         const uint64_t* offsets, uint64_t records, bool recover, uint64_t* counts,
                         uint64_t* totals);
+  // Randstrobemer indexes (k-mer strobes on the GPU): aggregate of host
+  // records = the sum over records of the per-colour maximum of the two
+  // strands' counts; *total = forward anchors.
+  void query_strobes_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
+                          const uint64_t* offsets, uint64_t records, bool recover,
+                          uint64_t* counts, uint64_t* total);
+  bool strobes() const { return sp_.strobe_max != 0; }
+  // Raises ZX_EUNSUPPORTED for randstrobemer indexes (entry points that
+  // count one strand of device batches).
+  void check_not_strobes() const;
   // Per-record hits for a report with min_ratio in (0, 1]: totals (records)
   // and, for record r, the colours hit_colors[first[r] .. first[r+1]) with
   // their counts, in colour order: those with count > 0 and count / total >=

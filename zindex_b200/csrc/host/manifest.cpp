@@ -95,8 +95,19 @@ void validate_manifest(Manifest& m) {
                "inconsistent abandoned recovery metadata");
   check_format(m.abandoned_recovery || (m.abandoned_hashes == 0 && m.abandoned_origins == 0),
                "disabled recovery has abandoned records");
-  check(!m.has_randstrobemers, kEUnsupported,
-        "randstrobemers are not supported by the GPU query path");
+  if (m.has_randstrobemers) {
+    // Manifest::features (storage.rs:240-256), RandstrobeConfig::validate
+    // (anchors.rs:98-110), FeatureConfig::validate_anchors (lib.rs:177-206).
+    check_format(m.version >= 6 &&
+                     m.randstrobe_scheme == "strobealign-popcount8-symmetric64-downstream-v1",
+                 "unsupported legacy/custom randstrobemer extraction; rebuild this index with the "
+                 "current downstream scheme");
+    check_format(m.index_mode == kKmers || m.index_mode == kMinimizers,
+                 "spaced seeds and randstrobemers require --index-mode kmers or minimizers");
+    check_format(m.strobe_min > 0, "randstrobemer minimum distance must be greater than zero");
+    check_format(m.strobe_min <= m.strobe_max,
+                 "randstrobemer minimum distance must not exceed maximum distance");
+  }
   if (m.has_seed_pattern) {
     // FeatureConfig::validate_anchors (src/lib.rs:177-206) and SpacedSeed::from_str
     // (src/anchors.rs:15-42).
@@ -258,6 +269,12 @@ Manifest load_manifest(const std::string& dir) {
   }
   const JsonValue* rs = j.find("randstrobemers");
   m.has_randstrobemers = rs && !rs->is_null();
+  if (m.has_randstrobemers) {
+    m.strobe_min = u64_field(*rs, "min_distance");
+    m.strobe_max = u64_field(*rs, "max_distance");
+    const JsonValue* sch = j.find("randstrobe_scheme");
+    if (sch && sch->kind == JsonValue::Str) m.randstrobe_scheme = sch->s;
+  }
   m.modimizer_sampling = u64_field(j, "modimizer_sampling");
   m.findere_z = u64_field(j, "findere_z");
   for (auto& c : need(j, "colors").arr) {

@@ -58,6 +58,8 @@ struct Manifest {
   bool homopolymer_compression = false;
   bool has_seed_pattern = false, has_randstrobemers = false;
   std::string seed_pattern;  // '#'/'_' spaced-seed pattern when has_seed_pattern
+  uint64_t strobe_min = 0, strobe_max = 0;  // randstrobemer distances when has_randstrobemers
+  std::string randstrobe_scheme;
   uint64_t modimizer_sampling = 16;
   uint64_t findere_z = 10;
   std::vector<ColorMeta> colors;

@@ -20,6 +20,7 @@ namespace zx {
 constexpr uint32_t kTileWindows = 256;
 constexpr uint32_t kFindereTask = 16384;  // src/findere.rs:13-16
 constexpr uint32_t kSplitTiles = 1u << 18;  // tiles per round of a split minimizer query
+constexpr uint32_t kMaxStrobeSpan = 256;    // largest randstrobemer partner distance on the GPU
 
 // Windows of record r: k-windows fully inside the record. A record whose
 // offsets decrease, pass the end of the bases or span 2^31 bases or more has
@@ -118,14 +119,19 @@ struct FusedSmem {
   }
   // Key buffer of a warp: one tile's keys, plus the lane-run staging of the
   // polynomial k-mer hashes (modes 0 and 2 with k > 32) and of findere s-mers.
-  static __host__ __device__ size_t key_bytes(int mode, int k) {
+  // Randstrobemers (mode 0) add the strobe hashes of a tile's windows and of
+  // up to kMaxStrobeSpan windows past it, with their validity bits.
+  static __host__ __device__ size_t key_bytes(int mode, int k, bool strobes = false) {
+    if (strobes && mode == 0)
+      return (size_t)kTileWindows * 8 + (kTileWindows + kMaxStrobeSpan) * 8 +
+             (kTileWindows + kMaxStrobeSpan) / 8;
     const bool staged = mode == 3 || ((mode == 0 || mode == 2) && k > 32);
     return (staged ? 2 : 1) * (size_t)kTileWindows * 8;
   }
   static __host__ __device__ size_t warp_bytes(int mode, int k, uint32_t classes, int stage_bytes = 0,
                                                int stages = 0, int hashes = 4, int planes = 0,
-                                               uint32_t shared_words = 0) {
-    size_t b = key_bytes(mode, k) + probe_bytes(classes, hashes, planes) +
+                                               uint32_t shared_words = 0, bool strobes = false) {
+    size_t b = key_bytes(mode, k, strobes) + probe_bytes(classes, hashes, planes) +
                ring_bytes(stage_bytes, stages) + shared_plane_bytes(shared_words);
     if (mode == 1) b += 2 * ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
     if (mode == 3) b += 64;  // findere: valid bits of up to 512 s-mer positions
@@ -135,12 +141,12 @@ struct FusedSmem {
   // shared_words: shared-plane words per lane (shared_plane_layout).
   static __host__ __device__ size_t total(int mode, int k, uint32_t colors, uint32_t classes,
                                           int hashes, const QueryLaunch& l,
-                                          uint32_t shared_words = 0) {
+                                          uint32_t shared_words = 0, bool strobes = false) {
     const bool fin = mode == 3;
     return ix_bytes + map_bytes + counter_bytes(colors, l.smem_counters) +
            (mode == 1 ? 256 * 8 : 0) +
            (size_t)l.warps * warp_bytes(mode, k, classes, fin ? 0 : l.stage_bytes, l.stages, hashes,
-                                        fin ? 1 : l.planes, shared_words);
+                                        fin ? 1 : l.planes, shared_words, strobes);
   }
   // Shared-plane words per lane a launch uses (0 unless the row-index form
   // counts in planes).
@@ -167,6 +173,12 @@ __device__ __forceinline__ uint32_t extract_tile(const BatchView& bv, const Seed
       uint32_t* pos = reinterpret_cast<uint32_t*>(suf + FusedSmem::ocm_entries(sp.k));
       n = tile_ocm(bv.pv, rb, t.w0, t.nw, sp, inner, pre, suf, pos, keys, lane);
     }
+  } else if (MODE == 0 && sp.strobe_max) {
+    const uint64_t len = bv.offsets[t.record + 1] - rb;
+    const uint32_t windows = (uint32_t)(len - (uint64_t)sp.klen + 1);  // tiles exist: len >= k
+    return tile_strobes(bv.pv, rb, t.w0, t.nw, windows - t.w0, sp, keys, keys + kTileWindows,
+                        reinterpret_cast<uint32_t*>(keys + 2 * kTileWindows + kMaxStrobeSpan),
+                        lane);
   } else if (sp.klen <= 32) {
     n = tile_kmers_short(bv.pv, rb, t.w0, t.nw, sp.klen, MODE == 2, sp.seed, sp.sampling, keys,
                          lane);
@@ -229,13 +241,13 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   constexpr bool ROWS = VARIANT == 2 || MODE == 3;
   const int stage_bytes = MODE == 3 ? 0 : lc.stage_bytes;
   const uint32_t swords = VARIANT == 2 ? FusedSmem::shared_words(MODE, *gix, lc) : 0u;
-  const size_t wstride =
-      FusedSmem::warp_bytes(MODE, sp.k, classes, stage_bytes, lc.stages, hashes, ROWS, swords);
+  const size_t wstride = FusedSmem::warp_bytes(MODE, sp.k, classes, stage_bytes, lc.stages, hashes,
+                                               ROWS, swords, sp.strobe_max != 0);
   uint8_t* wbase = p + (size_t)warp * wstride;
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
-  SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + FusedSmem::key_bytes(MODE, sp.k));
+  SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + FusedSmem::key_bytes(MODE, sp.k, sp.strobe_max != 0));
   uint64_t* row0s = reinterpret_cast<uint64_t*>(desc + 64);
-  uint8_t* ring_base = wbase + FusedSmem::key_bytes(MODE, sp.k) + FusedSmem::probe_bytes(classes, hashes, ROWS);
+  uint8_t* ring_base = wbase + FusedSmem::key_bytes(MODE, sp.k, sp.strobe_max != 0) + FusedSmem::probe_bytes(classes, hashes, ROWS);
   uint8_t* ocm = ring_base + FusedSmem::ring_bytes(stage_bytes, lc.stages);
   SharedPlanes splanes{reinterpret_cast<uint32_t*>(wbase + wstride - FusedSmem::shared_plane_bytes(swords)),
                        swords, 0u};
@@ -388,9 +400,10 @@ __global__ void extract_kernel(BatchView bv, SeedParams sp, uint64_t* __restrict
   uint64_t* inner = reinterpret_cast<uint64_t*>(smem);
   uint8_t* p = smem + 256 * 8;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, 0);
+  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, 0, 0, 0, 4, 0, 0,
+                                                            sp.strobe_max != 0);
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
-  uint8_t* ocm = wbase + FusedSmem::key_bytes(MODE, sp.k) + FusedSmem::probe_bytes(0);
+  uint8_t* ocm = wbase + FusedSmem::key_bytes(MODE, sp.k, sp.strobe_max != 0) + FusedSmem::probe_bytes(0);
   build_inner_table(sp, inner);
   __syncthreads();
   // Tiles tile_lo .. tile_hi-1 (tile_hi 0 = to the end); tile t's slot is t - tile_lo.

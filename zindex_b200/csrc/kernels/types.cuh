@@ -22,6 +22,9 @@ struct SeedParams {
   LongKmerConsts lk;
   int spaced;       // 1: keys are mapped through `pattern` (k-mers and minimizers)
   SpacedSeed pattern;
+  // Randstrobemers over k-mers (strobe_max 0 = off): each window is linked to
+  // a partner window strobe_min..strobe_max downstream in the same run.
+  uint32_t strobe_min, strobe_max;
 };
 
 struct Tile {

@@ -34,6 +34,7 @@ T* pinned_array(uint64_t count) {
 
 Server::Server(Engine& engine, std::mutex& index_mu, const ServerOptions& options)
     : engine_(engine), index_mu_(index_mu), opt_(options) {
+  engine_.check_not_strobes();
   check(opt_.slots >= 1 && opt_.slots <= 16, kEInval, "server slots must be in 1..16");
   check(opt_.slot_bases >= 1024 && opt_.slot_records >= 1 && opt_.slot_requests >= 1, kEInval,
         "server slot capacities must be positive (at least 1024 bases)");
