@@ -5,8 +5,8 @@ Known answers and properties from the reference's own tests
 iterator witnesses (951-986), inclusive distances and self fallback
 (1040-1062), breaks and homopolymer compression (1016-1038), directional
 extraction (988-1014), plus the builder's distinct keys against the oracle's.
-The GPU query path does not run randstrobemer indexes yet (they are refused
-with ZX_EUNSUPPORTED); these tests pin the checker and the index builder.
+These tests pin the checker and the index builder; tests/test_gpu_strobes.py
+compares the GPU path with the checker.
 """
 import ctypes
 import json
