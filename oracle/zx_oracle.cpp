@@ -16,7 +16,13 @@
 // window formula (821-868), the slow open-closed minimizer reference against
 // the rolling scan for all odd k <= 65, m <= 31 (open_closed_minimizers.rs:
 // 87-130), packed-screen semantics (packed_fingerprints.rs:128-242) and the
-// README's distinct k-mer counts of the bundled bacteria (README.md:60-62).
+// README's distinct k-mer counts of the bundled bacteria (README.md:60-62);
+// spaced-seed validation and projection (anchors.rs:751-773, 841-855) and the
+// randstrobemer strobe hash and upstream strobealign iterator witnesses
+// (anchors.rs:824-825, 951-986) in tests/test_oracle_golden.py and
+// tests/test_strobes_oracle.py; per-record reports by the reference's identity
+// (power_merge_cli.rs:1170-1230) and quoting test (record_output.rs:90-112) in
+// tests/test_records_oracle.py.
 #include "zx_oracle.h"
 
 #include <zlib.h>

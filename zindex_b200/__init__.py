@@ -18,6 +18,7 @@ moves buffers across the C ABI (include/zindex.h).
 from __future__ import annotations
 
 import ctypes
+import sys
 import time
 from ctypes import POINTER, byref, c_uint64, c_void_p
 from pathlib import Path
@@ -28,7 +29,8 @@ import numpy as np
 from . import _lib
 from ._lib import ZxError, ZxInfo, ZxLaunch
 
-__all__ = ["Index", "Server", "ZxError", "query_command", "pack_records", "LIB_DIR"]
+__all__ = ["Index", "Server", "ZxError", "query_command", "query_records_command", "pack_records",
+           "LIB_DIR"]
 
 LIB_DIR = _lib.LIB_DIR
 INDEX_MODES = ("kmers", "minimizers", "modimizers", "findere")
@@ -312,6 +314,17 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def query_records_command(index_dir, query, min_ratio: float = 0.0, recover: bool = True,
+                          batch_size: int = 4096, fmt: str = "tsv", device: int = 0) -> None:
+    """Print the per-record report, as `zorindex query -i DIR -q FILE -r [-F FMT] [-a R]
+    [-B N]` (query_records_command_with_memory, storage.rs:3626-3720)."""
+    with Index(index_dir, device=device) as ix:
+        t0 = time.perf_counter()
+        ix.query_records_report(query, None, min_ratio=min_ratio, fmt=fmt, batch=batch_size,
+                                recover=recover)
+        print(f"query_timings\tquery_s={time.perf_counter() - t0:.6f}", file=sys.stderr)
 
 
 def query_command(index_dir, query, min_ratio: float = 0.0, recover: bool = True,
