@@ -213,3 +213,18 @@ def test_oracle_query_keeps_the_larger_strand(oracle, tmp_path):
     c12, t12 = q(r1, r2)
     np.testing.assert_array_equal(c12, c1 + c2)
     assert t12 == t1 + t2
+
+
+def test_cli_build_writes_anchor_settings(native, tmp_path):
+    """`zorindex build` takes the reference's anchor flags (-c, -p, -r, -l, -u)."""
+    import subprocess
+
+    fof = helpers.make_genomes(tmp_path / "g", 2, 3000, 8)
+    out = tmp_path / "ix"
+    subprocess.run([str(helpers.ZORINDEX), "build", "-f", str(fof), "-o", str(out), "-k", "15",
+                    "-c", "-p", "##_#_#_#_#_#_##", "-r", "-l", "4", "-u", "40"], check=True,
+                   capture_output=True)
+    m = json.loads((out / "manifest.json").read_text())
+    assert m["homopolymer_compression"] is True
+    assert m["seed_pattern"] == "##_#_#_#_#_#_##"
+    assert m["randstrobemers"] == {"min_distance": 4, "max_distance": 40}
