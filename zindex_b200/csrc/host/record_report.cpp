@@ -25,9 +25,50 @@ void append_field(std::string& out, const std::string& v) {
 }
 
 inline void append_u64(std::string& out, uint64_t v) {
-  char buf[24];
-  int n = snprintf(buf, sizeof buf, "%" PRIu64, v);
-  out.append(buf, (size_t)n);
+  char buf[20];
+  int n = 0;
+  do {
+    buf[n++] = (char)('0' + v % 10);
+    v /= 10;
+  } while (v);
+  while (n) out += buf[--n];
+}
+
+// `{:.8}` of a non-negative double (Rust's fixed-point formatting, like a
+// correctly rounding printf's "%.8f"): the exact binary value times 10^8,
+// rounded to the nearest integer with ties to even, in fixed point. A
+// normal double is m * 2^(E - 1075) with a 53-bit m; m * 10^8 fits in 81 bits.
+void append_fixed8(std::string& out, double r) {
+  uint64_t bits;
+  memcpy(&bits, &r, 8);
+  const int biased = (int)((bits >> 52) & 0x7FF);
+  if (r == 0.0 || biased == 0) {  // zero (ratios are never subnormal)
+    out += "0.00000000";
+    return;
+  }
+  const int sh = 1075 - biased;  // r = m / 2^sh
+  if (sh <= 0 || biased == 0x7FF) {  // huge or not finite: never a ratio
+    char buf[400];
+    int n = snprintf(buf, sizeof buf, "%.8f", r);
+    out.append(buf, (size_t)n);
+    return;
+  }
+  const uint64_t m = (bits & ((1ull << 52) - 1)) | (1ull << 52);
+  const unsigned __int128 num = (unsigned __int128)m * 100000000u;
+  uint64_t q = 0;
+  if (sh < 128) {
+    const unsigned __int128 whole = num >> sh;
+    const unsigned __int128 rem = num - (whole << sh);
+    const unsigned __int128 half = (unsigned __int128)1 << (sh - 1);
+    q = (uint64_t)whole;
+    if (rem > half || (rem == half && (q & 1))) ++q;
+  }
+  append_u64(out, q / 100000000u);
+  out += '.';
+  char frac[8];
+  uint64_t f = q % 100000000u;
+  for (int i = 7; i >= 0; --i, f /= 10) frac[i] = (char)('0' + f % 10);
+  out.append(frac, 8);
 }
 
 }  // namespace
@@ -41,16 +82,16 @@ const char* record_header(RecordFormat format) {
 void append_record_hits(std::string& out, RecordFormat format, const std::string& name,
                         uint64_t total, const uint32_t* hit_colors, const uint64_t* hit_counts,
                         size_t hits, const std::vector<ColorMeta>& colors) {
-  char buf[96];
   if (format == RecordFormat::kCompact) {
     out += name;
     out += '\t';
     append_u64(out, total);
     out += '\t';
     for (size_t i = 0; i < hits; ++i) {
-      int len = snprintf(buf, sizeof buf, i ? ",%u:%" PRIu64 : "%u:%" PRIu64, hit_colors[i],
-                         hit_counts[i]);
-      out.append(buf, (size_t)len);
+      if (i) out += ',';
+      append_u64(out, hit_colors[i]);
+      out += ':';
+      append_u64(out, hit_counts[i]);
     }
     out += '\n';
     return;
@@ -63,9 +104,13 @@ void append_record_hits(std::string& out, RecordFormat format, const std::string
     out += '\t';
     append_field(out, colors[c].name);
     const double ratio = total == 0 ? 0.0 : (double)hit_counts[i] / (double)total;
-    int len = snprintf(buf, sizeof buf, "\t%" PRIu64 "\t%" PRIu64 "\t%.8f\n", hit_counts[i], total,
-                       ratio);
-    out.append(buf, (size_t)len);
+    out += '\t';
+    append_u64(out, hit_counts[i]);
+    out += '\t';
+    append_u64(out, total);
+    out += '\t';
+    append_fixed8(out, ratio);
+    out += '\n';
   }
   if (!hits) {
     append_field(out, name);
