@@ -1038,16 +1038,39 @@ std::unique_ptr<Index> load_index(const std::string& dir, bool recover, bool pay
   return ix;
 }
 
+// PositionHash::positions (storage.rs:3452-3481): the H cells of a key in a
+// bank of `cells` slots; segment 0 = the legacy length, the power-of-two
+// floor of clamp(cells / H, 1, 4096).
+void positions(uint64_t key, uint64_t seed, uint64_t cells, size_t hashes, uint64_t segment,
+               uint64_t* out) {
+  uint64_t len = segment;
+  if (!len) {
+    uint64_t n = std::min<uint64_t>(std::max<uint64_t>(cells / hashes, 1), 4096);
+    len = 1;
+    while (len * 2 <= n) len *= 2;
+  }
+  const uint64_t first = mixsplit(key, seed), step = splitmix64(first);
+  const uint64_t count = cells / len - hashes + 1;
+  const uint64_t base = (uint64_t)(((unsigned __int128)first * count) >> 64) * len;
+  uint64_t h = first;
+  for (size_t i = 0; i < hashes; ++i) {
+    out[i] = base + i * len + ((h ^ (h >> 33)) & (len - 1));
+    h += step;
+  }
+}
+
+// abandoned::hash (abandoned.rs:5-10).
+uint32_t abandoned_hash(uint64_t key, uint64_t seed) {
+  return (uint32_t)(splitmix64(key ^ seed ^ 0xD6E8FEB86659FD93ull) >> 32);
+}
+
 // lookup_selected (storage.rs:2761-2925) for one key: every colour hit by a
 // filter or by the recovery map, each at most once, appended to `hits`.
 void lookup(const Index& ix, uint64_t key, std::vector<uint32_t>& hits) {
   hits.clear();
   size_t rlen = 0;
-  const uint32_t* rec = ix.recovery ? ix.recover.get(
-                                          (uint32_t)(splitmix64(key ^ ix.seed ^ 0xD6E8FEB86659FD93ull) >> 32), &rlen)
-                                    : nullptr;
+  const uint32_t* rec = ix.recovery ? ix.recover.get(abandoned_hash(key, ix.seed), &rlen) : nullptr;
   const uint64_t fp = splitmix64(key ^ ix.seed ^ 0x8E2D4F6A9B13C5D7ull) & ((1ull << ix.bits) - 1);
-  const uint64_t first = mixsplit(key, ix.seed), step = splitmix64(first);
   uint64_t slots[32];
   std::vector<uint8_t> row;
   for (auto& cls : ix.classes) {
@@ -1055,22 +1078,7 @@ void lookup(const Index& ix, uint64_t key, std::vector<uint32_t>& hits) {
     if (cls.size() > 1)
       bp = &ix.banks[cls[splitmix64(key ^ ix.seed ^ 0x34B61D8F29A7C053ull) & (cls.size() - 1)]];
     const Bank& b = *bp;
-    // PositionHash::positions (storage.rs:3452-3481).
-    uint64_t len;
-    if (ix.has_segment) {
-      len = ix.segment;
-    } else {
-      uint64_t n = std::min<uint64_t>(std::max<uint64_t>(b.slots / ix.hashes, 1), 4096);
-      len = 1;
-      while (len * 2 <= n) len *= 2;
-    }
-    uint64_t count = b.slots / len - ix.hashes + 1;
-    uint64_t base = (uint64_t)(((unsigned __int128)first * count) >> 64) * len;
-    uint64_t h = first;
-    for (size_t i = 0; i < ix.hashes; ++i) {
-      slots[i] = base + i * len + ((h ^ (h >> 33)) & (len - 1));
-      h += step;
-    }
+    positions(key, ix.seed, b.slots, ix.hashes, ix.has_segment ? ix.segment : 0, slots);
     const size_t rb = b.row_bytes(), G = b.groups.size(), bits = ix.bits;
     auto hit = [&](uint32_t c) { hits.push_back(c); };
     if (b.fp_first) {
@@ -1535,6 +1543,13 @@ int oracle_features(const uint8_t* seq, size_t len, int mode, int k, int m, uint
 }
 
 uint64_t oracle_strobe_hash(uint64_t v) { return strobe_hash(v); }
+
+void oracle_positions(uint64_t key, uint64_t seed, uint64_t cells, int hashes, uint64_t segment,
+                      uint64_t* out) {
+  positions(key, seed, cells, (size_t)hashes, segment, out);
+}
+
+uint32_t oracle_abandoned_hash(uint64_t key, uint64_t seed) { return abandoned_hash(key, seed); }
 
 // Links candidates (ascending positions, their strobe hashes) into keys.
 void oracle_link_strobes(const uint64_t* positions, const uint64_t* hashes, size_t n,

@@ -79,6 +79,11 @@ int oracle_pattern_canonical(const char* pattern, uint64_t key, uint64_t* projec
 /* Randstrobemers (anchors.rs:129-347): the XXH64 strobe hash of one u64, and
  * the seeds of a sequence with an optional pattern and strobe linking. */
 uint64_t oracle_strobe_hash(uint64_t v);
+/* PositionHash::positions (storage.rs:3452-3481; segment 0 = legacy length)
+ * and abandoned::hash (abandoned.rs:5-10). */
+void oracle_positions(uint64_t key, uint64_t seed, uint64_t cells, int hashes, uint64_t segment,
+                      uint64_t* out);
+uint32_t oracle_abandoned_hash(uint64_t key, uint64_t seed);
 void oracle_link_strobes(const uint64_t* positions, const uint64_t* hashes, size_t n,
                          uint64_t dmin, uint64_t dmax, uint64_t* out);
 int oracle_features_anchored(const uint8_t* seq, size_t len, int mode, int k, int m, uint64_t seed,

@@ -216,3 +216,52 @@ def test_builder_rejects_invalid_patterns(native, tmp_path):
                                          ("###", dict(mode="findere", k=13, z=10))]):
         with pytest.raises(subprocess.CalledProcessError):
             helpers.build_index(fof, tmp_path / f"ix{i}", pattern=pattern, **opts)
+
+
+# ---- position hash and recovery hash ----------------------------------------
+def _mix(x):
+    x = (x + 0x9E3779B97F4A7C15) & M64
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & M64
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & M64
+    return x ^ (x >> 31)
+
+
+def test_position_hash_matches_segment_mapping(oracle):
+    # storage.rs:4799-4825 (shared_position_hash_matches_original_segment_mapping):
+    # the legacy segment length and the cell formula, for H in {2,3,4,8,32}.
+    import ctypes
+    from ctypes import POINTER, c_int, c_uint64
+
+    f = oracle.lib.oracle_positions
+    f.argtypes = [c_uint64, c_uint64, c_uint64, c_int, c_uint64, POINTER(c_uint64)]
+    f.restype = None
+    for hashes in (2, 3, 4, 8, 32):
+        for exponent in range(5, 25):
+            cells = 1 << exponent
+            for key in (0, 1, 123, M64):
+                seed = 69
+                length = 1 << (min(max(cells // hashes, 1), 4096).bit_length() - 1)
+                count = cells // length - hashes + 1
+                h1 = _mix((key + seed) & M64)
+                h2 = _mix(h1)
+                base = ((h1 * count) >> 64) * length
+                h, want = h1, []
+                for i in range(hashes):
+                    want.append(base + i * length + ((h ^ (h >> 33)) & (length - 1)))
+                    h = (h + h2) & M64
+                out = (c_uint64 * hashes)()
+                f(key, seed, cells, hashes, 0, out)
+                assert list(out) == want, (hashes, exponent, key)
+
+
+def test_recovery_hash_collision(oracle):
+    # query_stream.rs:1114-1160: keys 83,843 and 95,900 share the stored
+    # 32-bit recovery hash under seed 69; 123 does not.
+    from ctypes import c_uint32, c_uint64
+
+    f = oracle.lib.oracle_abandoned_hash
+    f.argtypes = [c_uint64, c_uint64]
+    f.restype = c_uint32
+    assert f(83843, 69) == f(95900, 69)
+    assert f(123, 69) != f(83843, 69)
+    assert f(83843, 69) == _mix(83843 ^ 69 ^ 0xD6E8FEB86659FD93) >> 32
