@@ -196,7 +196,10 @@ void pread_full(int fd, uint8_t* dst, size_t n, uint64_t off, const std::string&
 void stream_bank(const std::string& path, uint8_t header[40], uint64_t payload_len,
                  uint64_t piece_bytes, uint8_t* const* ring, int slots, int threads,
                  PieceSink& sink) {
-  check(slots >= 3 && piece_bytes > 0, kEInval, "bank streaming needs three ring slots");
+  // A frame then touches at most two pieces, and a frame that straddles
+  // pieces c and c+1 can always be written while piece c is being filled.
+  check(slots >= 3 && piece_bytes >= kChunk, kEInval,
+        "bank streaming needs three ring slots of at least one 4 MiB frame");
   const uint64_t raw_total = payload_len + kHeader;
   const uint64_t pieces = (payload_len + piece_bytes - 1) / piece_bytes;
   auto piece_len = [&](uint64_t c) { return std::min(piece_bytes, payload_len - c * piece_bytes); };

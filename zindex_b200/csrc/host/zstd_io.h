@@ -31,9 +31,9 @@ class PieceSink {
 
 // Decoded bank stream = 40-byte header + payload (payload_len bytes). The
 // header goes to `header`; the payload is handed to `sink` in order, in
-// pieces of piece_bytes (the last may be shorter) through a ring of `slots`
-// (>= 3) caller-owned buffers of piece_bytes each (piece c in slot
-// c % slots). Frames are read with pread and decoded by `threads` workers in
+// pieces of piece_bytes (at least 4 MiB, one frame; the last piece may be
+// shorter) through a ring of `slots` (>= 3) caller-owned buffers of
+// piece_bytes each (piece c in slot c % slots). Frames are read with pread and decoded by `threads` workers in
 // frame order straight into the ring, so reading, decoding and the sink's
 // consumption overlap; the file is never held whole in memory. When the file
 // has no seek table it is stream-decoded on the calling thread. Throws
