@@ -233,7 +233,7 @@ def planned_form(ix, bases, offsets, seeds, step_ms, e2e_ms):
     ranks every candidate launch for this batch; its top predictions and the
     default are timed on the batch and the fastest is kept, and it picks the
     cut. Exhaustive autotuning over the same candidates is timed alongside as
-    the judge of the regret; the default launch gives the gain.
+    the measure of the regret; the default launch gives the gain.
     step_ms(launch) times device steps under a launch."""
     from zindex_b200 import planner as pl
     from zindex_b200 import tuning as tn
@@ -265,7 +265,7 @@ def planned_form(ix, bases, offsets, seeds, step_ms, e2e_ms):
                              dict(pick, cut=default["cut"]), 1, e2e=True)
     pick = min(cuts, key=e2e_ms)
     plan_s = time.perf_counter() - t0
-    for launch in cands:  # the judge: every candidate
+    for launch in cands:  # exhaustive: every candidate
         timed_ms(launch)
     best_key = min(timed, key=timed.get)
     t_pick = timed_ms(pick)

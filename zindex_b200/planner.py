@@ -15,7 +15,7 @@ the autotuner (zindex_b200.tuning). Launches and cuts are chosen by
 verification: the network ranks all candidates, its top few and the default
 are timed on the batch, and the fastest wins, so a plan is never slower than the default
 (up to timing noise) and costs a handful of timings instead of an exhaustive
-search, which stays the fallback and the judge of its regret. The planner
+search, which stays the fallback and the measure of its regret. The planner
 never changes results: every launch configuration and cut gives the same
 counts.
 """
