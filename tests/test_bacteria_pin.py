@@ -4,10 +4,11 @@ The reference README (lines 60-62) lists, for its bundled genomes, the
 distinct indexed 31-mers per dataset (`unique_kmers`) and states that the
 source genome of tests/data/bacteria/query.fa matches all 970 query 31-mers
 (guaranteed by recovery, README.md:65-66). The expected numbers are committed
-in tests/golden/bacteria_readme.json; the genomes are read from the reference
-tree, so the test runs only where that tree is mounted (CPU, not on GPU
-boxes). The false-positive count of the third row depends on the exact filter
-cells of the reference builder and is not pinned.
+in tests/golden/bacteria_readme.json and the genomes are the reference's
+bundled files, copied byte for byte into tests/golden/bacteria by
+tests/golden/make_bacteria_fixture.py. The false-positive count of the third
+row depends on the exact filter cells of the reference builder and is not
+pinned.
 """
 import gzip
 import json
@@ -18,10 +19,8 @@ import pytest
 
 import helpers
 
-REF = Path("/root/reference/tests/data/bacteria")
+REF = Path(__file__).parent / "golden" / "bacteria"
 GOLDEN = json.loads((Path(__file__).parent / "golden" / "bacteria_readme.json").read_text())
-
-pytestmark = pytest.mark.skipif(not REF.exists(), reason="reference tree not mounted")
 
 
 def fasta_records(path):
@@ -58,3 +57,17 @@ def test_source_genome_matches_every_query_kmer(oracle, tmp_path):
     manifest = json.loads((index / "manifest.json").read_text())
     for c in manifest["colors"]:
         assert c["unique_kmers"] == GOLDEN["unique_kmers"][c["name"]]
+
+
+@pytest.mark.parametrize("mode", ["kmers", "minimizers"])
+def test_oracle_report_meets_the_bacteria_source_truth(oracle, tmp_path, mode):
+    """The reference's end-to-end check (utils/scripts/demo.sh:36-43 and
+    prepare_bacteria_example.py:144-177) on the oracle's `--records
+    --min-ratio 0.8` report: every positive record's source dataset matches
+    all of its queried seeds, and the random negative reports nothing."""
+    from test_gpu_bacteria import MODES, _check_results, _fof
+
+    fof, names = _fof(tmp_path)
+    index = helpers.build_index(fof, tmp_path / "index", **MODES[mode])
+    report = oracle.records_report(index, REF / "queries.fa", min_ratio=0.8, fmt="tsv")
+    assert _check_results(report.decode(), names) == 20
