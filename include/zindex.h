@@ -170,7 +170,12 @@ int zx_query_device(zx_index* index, const uint8_t* d_bases, uint64_t nbases,
  * d_counts / d_total (caller-zeroed) with global atomics. Every call shares
  * the one array, so calls that overlap on the GPU (different streams, or
  * different indexes on the same GPU) race: serialise them. Asynchronous on
- * `stream` (a cudaStream_t; NULL = legacy default stream). */
+ * `stream` (a cudaStream_t; NULL = legacy default stream). Errors found on
+ * the device (invalid record offsets) are kept in an error word of this
+ * index inside the array (up to 1024 open indexes per GPU use the call; the
+ * first call of an index takes its word and clears it, synchronously): later
+ * calls do not clear it, and zx_query_status of this index reports and clears
+ * it. */
 int zx_query_device_noalloc(zx_index* index, const uint8_t* d_bases, uint64_t nbases,
                             const uint64_t* d_offsets, uint64_t records, int recover,
                             uint64_t* d_counts, uint64_t* d_total, void* stream);
@@ -187,8 +192,9 @@ int zx_get_launch(const zx_index* index, zx_launch* out);
 int zx_set_launch(zx_index* index, const zx_launch* launch);
 int zx_default_launch(const zx_index* index, zx_launch* out);
 
-/* Status of the last asynchronous zx_query_device / zx_query_device_noalloc
- * calls of this index: ZX_OK; ZX_EINVAL when record offsets were invalid
+/* Status of the asynchronous zx_query_device / zx_query_device_noalloc calls
+ * of this index since the last status call: ZX_OK; ZX_EINVAL when record
+ * offsets of any of them were invalid
  * (decreasing, past the bases, or a record of 2^31 bases or more: those
  * records were skipped, counts incomplete); ZX_ETIMEOUT when a bounded device
  * wait expired. The device error words are cleared. Synchronous calls report

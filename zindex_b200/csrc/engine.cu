@@ -289,13 +289,20 @@ RecoveryRecords read_recovery(const std::string& dir, const Manifest& m) {
 // ---- allocation-free query: scratch in a static device array ---------------
 // For callers that cannot allocate device memory (see zx_query_device_noalloc
 // in include/zindex.h). One 64 MiB array per GPU that loads the library, held
-// until process exit; its device address is resolved once per device.
+// until process exit; its device address is resolved once per device. The
+// first kNoAllocErrorSlots words are error words: every engine that uses the
+// entry point owns one of them (taken on its first call, returned when the
+// engine is released), so one index's status never reports or clears
+// another's. The batch scratch starts after them.
 constexpr uint64_t kNoAllocScratchBytes = 64ull << 20;
+constexpr uint32_t kNoAllocErrorSlots = 1024;
+constexpr uint64_t kNoAllocErrorBytes = kNoAllocErrorSlots * 4;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 namespace {
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[256] = {};
+std::vector<bool> g_noalloc_slot_used[256];
 
 // Device address of the static scratch on the current device (set-up on first
 // use per device; this device must be current).
@@ -309,6 +316,29 @@ void* noalloc_scratch(int device) {
   }
   return g_noalloc_ptr[device];
 }
+
+// Takes a free error slot of this device and clears its word (synchronously:
+// this runs once per engine, on its first allocation-free call).
+int noalloc_take_slot(int device) {
+  uint32_t* words = static_cast<uint32_t*>(noalloc_scratch(device));
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  auto& used = g_noalloc_slot_used[device];
+  if (used.empty()) used.assign(kNoAllocErrorSlots, false);
+  for (uint32_t i = 0; i < kNoAllocErrorSlots; ++i)
+    if (!used[i]) {
+      cuda_check(cudaMemset(words + i, 0, 4), "memset");
+      used[i] = true;
+      return (int)i;
+    }
+  raise(kENoMem, "more than " + std::to_string(kNoAllocErrorSlots) +
+                     " open indexes use the allocation-free query on this device");
+}
+
+void noalloc_return_slot(int device, int slot) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (device >= 0 && device < 256 && slot >= 0 && (size_t)slot < g_noalloc_slot_used[device].size())
+    g_noalloc_slot_used[device][slot] = false;
+}
 }  // namespace
 
 void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
@@ -321,7 +351,11 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
         "the allocation-free query does not run homopolymer compression (the compressed batch "
         "needs scratch of its own): use zx_query_device");
   uint8_t* base = static_cast<uint8_t*>(noalloc_scratch(device_));
-  noalloc_used_ = true;
+  if (noalloc_slot_ < 0) noalloc_slot_ = noalloc_take_slot(device_);
+  // This engine's error word. It is never cleared per call: a bit set by an
+  // earlier asynchronous call stays until zx_query_status reads it.
+  uint32_t* err = reinterpret_cast<uint32_t*>(base) + noalloc_slot_;
+  base += kNoAllocErrorBytes;
   const uint64_t words = nbases / 32 + 2;
   const uint64_t tiles = nbases / kTileWindows + nbases / kFindereTask + records + 16;
   // Register gather, colour counts added straight into the caller's counters.
@@ -353,7 +387,6 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
     at = round_up(at + bytes, 256);
     return base + off;
   };
-  uint32_t* err = reinterpret_cast<uint32_t*>(carve(4));
   uint64_t* packed = reinterpret_cast<uint64_t*>(carve(words * 8));
   uint32_t* invalid = reinterpret_cast<uint32_t*>(carve(words * 4));
   uint32_t* tile_counts = reinterpret_cast<uint32_t*>(carve((records + 1) * 4));
@@ -361,12 +394,11 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
   Tile* tile_list = reinterpret_cast<Tile*>(carve(tiles * sizeof(Tile)));
   void* scan_tmp = carve(scan_bytes);
   uint32_t* fstate = fstate_bytes ? reinterpret_cast<uint32_t*>(carve(fstate_bytes)) : nullptr;
-  if (at > kNoAllocScratchBytes)
+  if (at > kNoAllocScratchBytes - kNoAllocErrorBytes)
     raise(kEInval, "batch needs " + std::to_string(at) + " bytes of scratch; the allocation-free "
-                   "query holds at most " + std::to_string(kNoAllocScratchBytes) +
+                   "query holds at most " + std::to_string(kNoAllocScratchBytes - kNoAllocErrorBytes) +
                    " bytes (about 0.4 byte per base + 28 bytes per record): split the batch");
   // The array keeps the previous call's contents: reset what must start at zero.
-  cuda_check(cudaMemsetAsync(err, 0, 4, s), "memset");
   if (fstate) cuda_check(cudaMemsetAsync(fstate, 0, fstate_bytes, s), "memset");
   cuda_check(cudaMemsetAsync(tile_counts + records, 0, 4, s), "memset");
   int grid = (int)std::min<uint64_t>((words + 255) / 256, (uint64_t)sms_ * 16);
@@ -435,6 +467,12 @@ Engine::~Engine() { release(); }
 void Engine::release() {
   ws_.reset();
   cudaSetDevice(device_);
+  if (noalloc_slot_ >= 0) {
+    // The engine's calls are done with the slot once the device is idle.
+    cudaDeviceSynchronize();
+    noalloc_return_slot(device_, noalloc_slot_);
+    noalloc_slot_ = -1;
+  }
   if (ev_begin_) cudaEventDestroy(ev_begin_);
   if (ev_end_) cudaEventDestroy(ev_end_);
   ev_begin_ = ev_end_ = nullptr;
@@ -1512,8 +1550,8 @@ void Engine::check_error_word(Workspace& ws) {
 
 uint32_t Engine::take_noalloc_error() {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
-  if (!noalloc_used_) return 0;
-  uint32_t* err = static_cast<uint32_t*>(noalloc_scratch(device_));
+  if (noalloc_slot_ < 0) return 0;
+  uint32_t* err = static_cast<uint32_t*>(noalloc_scratch(device_)) + noalloc_slot_;
   uint32_t v = 0;
   cuda_check(cudaMemcpy(&v, err, 4, cudaMemcpyDeviceToHost), "error word");
   if (v) cuda_check(cudaMemset(err, 0, 4), "memset");

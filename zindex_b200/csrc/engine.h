@@ -161,7 +161,7 @@ class Engine {
   // Device error word of a workspace (read and cleared); nonzero means a
   // bounded wait expired and the query's counts are incomplete.
   uint32_t take_error(Workspace& ws);
-  // Error word of the allocation-free query's scratch on this device (read
+  // This engine's error word in the allocation-free query's scratch (read
   // and cleared; 0 if that entry point was never used by this engine).
   uint32_t take_noalloc_error();
   // Asynchronous query of several requests coalesced into one launch: the
@@ -252,7 +252,7 @@ class Engine {
   bool timing_ = false;
   cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
   int cached_blocks_ = 0;
-  bool noalloc_used_ = false;
+  int noalloc_slot_ = -1;  // error word of the allocation-free query, once used
   double load_s_ = 0, banks_load_s_ = 0, recovery_load_s_ = 0;
   QueryLaunch cached_for_{};
 };
