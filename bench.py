@@ -19,7 +19,8 @@ collective on the data path).
 
 --impl reference times the CPU restatement of the reference query (the
 reference is Rust and cannot be built here) on all host cores, on a bounded
-sample of the same workload.
+sample of the same workload, with the reference's own lookup speed measures
+(blocks of 32 keys, rows prefetched 4 keys ahead, AVX2 fingerprint screens).
 """
 from __future__ import annotations
 
@@ -92,10 +93,12 @@ CONFIGS = {
 CONFIG = CONFIGS["c2"]
 WORKLOAD = CONFIG["workload"]
 METRIC = "query seeds/s"
-# DRAM bytes (read + write) per seed of the fused kernel on this workload, from one ncu
-# capture of a 1.2e7-seed slice (profiles/fused_query_kernel-c2-batched.md:
-# 12.034 GB read + 7.0 MB written); scaled by the seeds of a launch.
-TRAFFIC_BYTES_PER_SEED = 12.041e9 / 1.2e7
+# DRAM bytes (read + write) per seed of the dominant kernel(s) of each workload, from
+# one ncu capture of a slice of the same batch (dram__bytes_read.sum +
+# dram__bytes_write.sum over the seeds of the slice); the line scales them by the
+# seeds of a launch (for a fixed index the traffic grows with the seeds).
+# c2: 12.034 GB read + 7.0 MB written over a 1.2e7-seed slice.
+TRAFFIC_BYTES_PER_SEED = {"c2": 12.041e9 / 1.2e7}
 # Per-record form: reads counted one by one, and the compact report threshold.
 PER_RECORD_READS = 200_000
 PER_RECORD_CPU_READS = 20_000
@@ -383,7 +386,10 @@ def hbm_peak():
 
 class CpuOracle:
     """The oracle (CPU restatement of the reference query) with its index
-    resident in host memory, timed on all host cores."""
+    resident in host memory, timed on all host cores. The timed queries take
+    its fast lookup (the reference's lookup_batch blocks, 4-ahead row
+    prefetch and AVX2 fingerprint screens; the same counts as the scalar
+    checker) where the index allows it: kind "port-simd", else "port"."""
 
     def __init__(self, index):
         import ctypes
@@ -398,12 +404,18 @@ class CpuOracle:
                                             POINTER(c_uint64), c_size_t, POINTER(c_uint64),
                                             POINTER(c_double)]
         lib.oracle_query_handle.restype = c_int
+        lib.oracle_query_handle_fast.argtypes = lib.oracle_query_handle.argtypes
+        lib.oracle_query_handle_fast.restype = c_int
+        lib.oracle_fast_serves.argtypes = [c_void_p]
+        lib.oracle_fast_serves.restype = c_int
         lib.oracle_last_error.restype = c_char_p
         self.lib = lib
         self.h = c_void_p()
         if lib.oracle_open(str(index).encode(), 1, ctypes.byref(self.h)):
             raise RuntimeError(lib.oracle_last_error().decode())
         self.cores = os.cpu_count() or 1
+        self.fast = bool(lib.oracle_fast_serves(self.h))
+        self.kind = "port-simd" if self.fast else "port"
 
     def run(self, bases, offsets, n, colors):
         if not 0 < n <= len(offsets) - 1:
@@ -412,7 +424,8 @@ class CpuOracle:
         off = np.ascontiguousarray(offsets[: n + 1])
         counts = np.zeros(colors, dtype=np.uint64)
         total, secs = ct.c_uint64(), ct.c_double()
-        rc = self.lib.oracle_query_handle(self.h, bases.ctypes.data_as(ct.c_void_p),
+        fn = self.lib.oracle_query_handle_fast if self.fast else self.lib.oracle_query_handle
+        rc = fn(self.h, bases.ctypes.data_as(ct.c_void_p),
                                           off.ctypes.data_as(ct.POINTER(ct.c_uint64)), n, self.cores,
                                           counts.ctypes.data_as(ct.POINTER(ct.c_uint64)), colors,
                                           ct.byref(total), ct.byref(secs))
@@ -457,7 +470,7 @@ def cpu_baseline(index, bases, offsets, colors, target_s=15.0):
     orc = CpuOracle(index)
     seeds, secs, counts, n = orc.sized(bases, offsets, colors, target_s)
     orc.close()
-    return {"value": seeds / secs, "unit": "seeds/s", "cores": orc.cores, "kind": "port",
+    return {"value": seeds / secs, "unit": "seeds/s", "cores": orc.cores, "kind": orc.kind,
             "sample": f"first {n} of the {len(offsets) - 1:,} query records ({seeds} seeds), query only "
                       f"(index load excluded), {secs:.2f}s"}, n, counts
 
@@ -481,9 +494,9 @@ def reference_arm(args):
         if i >= args.warmup:
             vals.append(seeds / secs)
     orc.close()
-    base = {"unit": "seeds/s", "cores": orc.cores, "kind": "port",
-            "sample": f"first {n} of the {len(offsets) - 1:,} query records per step, query only "
-                      f"(index load excluded)"}
+    base = {"unit": "seeds/s", "cores": orc.cores, "kind": orc.kind,
+            "sample": f"first {n} of the {len(offsets) - 1:,} query records per step (the rate "
+                      f"on that prefix), query only (index load excluded)"}
     value = statistics.median(vals)
     base = dict(base, value=value)
     line = {"metric": METRIC, "value": value, "unit": "seeds/s", "n_gpus": world, "steps": args.steps,
@@ -750,20 +763,21 @@ def ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic",
-            "config": dict(WORKLOAD, seeds_per_step=seeds, bases_per_step=int(len(bases)),
-                           parallelism=f"replicas{world}",
-                           config=args.config,
-                           l2=("L2 flushed (256 MiB write) before each timed step" if flush else
-                               "no flush: index and reads exceed the 126 MB L2"),
-                           launch=ix.launch()),
+            "config": dict(WORKLOAD, config=args.config),
+            "run": {"seeds_per_step": seeds, "bases_per_step": int(len(bases)),
+                    "parallelism": f"replicas{world}",
+                    "l2": ("L2 flushed (256 MiB write) before each timed step" if flush else
+                           "no flush: index and reads exceed the 126 MB L2"),
+                    "launch": ix.launch()},
             "bases_per_s": bases_rate,
             "e2e": {"value": e2e_rate, "unit": "seeds/s",
                     "h2d_bytes_per_step": int(len(bases) + 8 * (records + 1)),
                     "d2h_bytes_per_step": int(8 * ix.colors + 8)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": (TRAFFIC_BYTES_PER_SEED * seeds / 1e9
-                                     if args.config == "c2" else None), "traffic_unit": "GB",
+                         "traffic": (TRAFFIC_BYTES_PER_SEED[args.config] * seeds / 1e9
+                                     if args.config in TRAFFIC_BYTES_PER_SEED else None),
+                         "traffic_unit": "GB",
                          "peak_kind": peak_kind,
                          "kernel": "fused_query_kernel", "kernel_ms": kernel_ms,
                          "algorithmic_bytes_per_launch": int(alg_bytes),

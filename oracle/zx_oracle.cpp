@@ -25,6 +25,7 @@
 // tests/test_records_oracle.py.
 #include "zx_oracle.h"
 
+#include <immintrin.h>
 #include <zlib.h>
 
 #include <algorithm>
@@ -1164,6 +1165,248 @@ void prepare_record(const Features& f, const uint8_t* seq, size_t n, Work& w) {
   });
 }
 
+// ------------------------------------------------- fast CPU baseline path ---
+// The reference's own speed measures for the aggregate lookup, restated for
+// the timed CPU baseline (the scalar lookup above stays the checker):
+// lookup_batch (storage.rs:2929-2978) takes blocks of 32 weighted keys,
+// computes every selected bank's H positions for the whole block, and
+// prefetches the rows of key i + 4 (prefetch_lookup, 3014-3054: every 64
+// bytes of the fingerprint plane, and the recovery bucket) while key i is
+// looked up; fingerprint_matches_rows (3241-3350) screens 8/16/32-bit fields
+// with AVX2 XOR + compare + movemask, packed_fingerprints::matches_rows
+// (7-126) screens 2/4-bit fields by XOR, fold and and-not over 256 bits, and
+// 1-bit fields are read 64 at a time. Counts follow WeightedScores
+// (3083-3101): a hit adds the key's weight; recovered origins' counters are
+// read before the filter hits and raised afterwards only if unchanged
+// (lookup_selected, 2778-2787, 2916-2924).
+namespace fastpath {
+
+template <class Hit>
+void screen_bytes_scalar(const uint8_t* const* rows, size_t H, size_t bits, uint64_t fp,
+                         size_t byte0, size_t len, Hit& hit) {
+  const size_t width = bits / 8;
+  for (size_t byte = byte0; byte + width <= len; byte += width) {
+    uint64_t v = 0;
+    for (size_t i = 0; i < H; ++i) {
+      uint64_t x = 0;
+      memcpy(&x, rows[i] + byte, width);
+      v ^= x;
+    }
+    if (v == fp) hit(byte / width);
+  }
+}
+
+template <size_t B, class Hit>
+void screen_packed_scalar(const uint8_t* const* rows, size_t H, uint64_t fp, size_t count,
+                          size_t base, Hit& hit) {
+  const uint64_t ones = ~0ull / ((1ull << B) - 1), target = ones * fp;
+  auto fold = [&](uint64_t diff) {
+    uint64_t f = diff | (diff >> 1);
+    if (B == 4) f |= f >> 2;
+    return ~f & ones;
+  };
+  auto emit = [&](uint64_t m, size_t at) {
+    for (; m; m &= m - 1) hit(at + (size_t)__builtin_ctzll(m) / B);
+  };
+  while (count - base >= 64 / B) {
+    uint64_t v = 0;
+    for (size_t i = 0; i < H; ++i) {
+      uint64_t x;
+      memcpy(&x, rows[i] + base * B / 8, 8);
+      v ^= x;
+    }
+    emit(fold(v ^ target), base);
+    base += 64 / B;
+  }
+  if (base != count) {
+    const size_t bytes = ((count - base) * B + 7) / 8;
+    uint64_t v = 0;
+    for (size_t i = 0; i < H; ++i) {
+      uint64_t x = 0;
+      memcpy(&x, rows[i] + base * B / 8, bytes);
+      v ^= x;
+    }
+    emit(fold(v ^ target) & (~0ull >> (64 - (count - base) * B)), base);
+  }
+}
+
+template <class Hit>
+__attribute__((target("avx2"))) void screen_bytes_avx2(const uint8_t* const* rows, size_t H,
+                                                       size_t bits, uint64_t fp, size_t len,
+                                                       Hit& hit) {
+  const __m256i target = bits == 8    ? _mm256_set1_epi8((char)fp)
+                         : bits == 16 ? _mm256_set1_epi16((short)fp)
+                                      : _mm256_set1_epi32((int)fp);
+  const uint32_t keep = bits == 8 ? 0xFFFFFFFFu : (bits == 16 ? 0x55555555u : 0x11111111u);
+  const size_t end = len / 32 * 32;
+  for (size_t byte = 0; byte < end; byte += 32) {
+    __m256i v = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(rows[0] + byte));
+    for (size_t i = 1; i < H; ++i)
+      v = _mm256_xor_si256(v, _mm256_loadu_si256(reinterpret_cast<const __m256i*>(rows[i] + byte)));
+    const __m256i eq = bits == 8    ? _mm256_cmpeq_epi8(v, target)
+                       : bits == 16 ? _mm256_cmpeq_epi16(v, target)
+                                    : _mm256_cmpeq_epi32(v, target);
+    for (uint32_t m = (uint32_t)_mm256_movemask_epi8(eq) & keep; m; m &= m - 1)
+      hit((byte + (size_t)__builtin_ctz(m)) / (bits / 8));
+  }
+  screen_bytes_scalar(rows, H, bits, fp, end, len, hit);
+}
+
+template <size_t B, class Hit>
+__attribute__((target("avx2"))) void screen_packed_avx2(const uint8_t* const* rows, size_t H,
+                                                        uint64_t fp, size_t count, Hit& hit) {
+  const uint64_t ones = ~0ull / ((1ull << B) - 1);
+  const __m256i target = _mm256_set1_epi64x((long long)(ones * fp));
+  const __m256i low = _mm256_set1_epi64x((long long)ones);
+  size_t base = 0;
+  while (count - base >= 256 / B) {
+    const size_t byte = base * B / 8;
+    __m256i v = _mm256_setzero_si256();
+    for (size_t i = 0; i < H; ++i)
+      v = _mm256_xor_si256(v, _mm256_loadu_si256(reinterpret_cast<const __m256i*>(rows[i] + byte)));
+    const __m256i diff = _mm256_xor_si256(v, target);
+    __m256i f = _mm256_or_si256(diff, _mm256_srli_epi64(diff, 1));
+    if (B == 4) f = _mm256_or_si256(f, _mm256_srli_epi64(f, 2));
+    const __m256i m = _mm256_andnot_si256(f, low);
+    if (!_mm256_testz_si256(m, m)) {
+      alignas(32) uint64_t w[4];
+      _mm256_store_si256(reinterpret_cast<__m256i*>(w), m);
+      for (int q = 0; q < 4; ++q)
+        for (uint64_t x = w[q]; x; x &= x - 1)
+          hit(base + (size_t)q * (64 / B) + (size_t)__builtin_ctzll(x) / B);
+    }
+    base += 256 / B;
+  }
+  screen_packed_scalar<B>(rows, H, fp, count, base, hit);
+}
+
+template <class Hit>
+void screen(const uint8_t* const* rows, size_t H, size_t bits, uint64_t fp, size_t G, bool avx2,
+            Hit& hit) {
+  if (bits == 2 || bits == 4) {
+    if (avx2) bits == 2 ? screen_packed_avx2<2>(rows, H, fp, G, hit)
+                        : screen_packed_avx2<4>(rows, H, fp, G, hit);
+    else bits == 2 ? screen_packed_scalar<2>(rows, H, fp, G, 0, hit)
+                   : screen_packed_scalar<4>(rows, H, fp, G, 0, hit);
+    return;
+  }
+  if (bits == 1) {
+    for (size_t base = 0; base < G; base += 64) {
+      const size_t len = (std::min<size_t>(G - base, 64) + 7) / 8;
+      uint64_t v = 0;
+      for (size_t i = 0; i < H; ++i) {
+        uint64_t x = 0;
+        memcpy(&x, rows[i] + base / 8, len);
+        v ^= x;
+      }
+      const size_t rem = std::min<size_t>(G - base, 64);
+      uint64_t m = (fp == 1 ? v : ~v) & (~0ull >> (64 - rem));
+      for (; m; m &= m - 1) hit(base + (size_t)__builtin_ctzll(m));
+    }
+    return;
+  }
+  const size_t len = G * bits / 8;
+  if (avx2) screen_bytes_avx2(rows, H, bits, fp, len, hit);
+  else screen_bytes_scalar(rows, H, bits, fp, 0, len, hit);
+}
+
+struct Scratch {
+  std::vector<uint64_t> pos;            // block x classes x H cells
+  std::vector<const Bank*> bank;        // block x classes selected banks
+  std::vector<const uint8_t*> rows;     // H row starts of one key and class
+  std::vector<uint64_t> snap;           // recovered origins' counters
+};
+
+inline void prefetch_key(const Index& ix, uint64_t key, const Bank* const* banks,
+                         const uint64_t* pos) {
+  if (ix.recovery && !ix.recover.dir.empty())
+    __builtin_prefetch(&ix.recover.dir[ix.recover.first_slot(abandoned_hash(key, ix.seed))]);
+  for (size_t ci = 0; ci < ix.classes.size(); ++ci) {
+    const Bank& b = *banks[ci];
+    const size_t rb = b.row_bytes(), bytes = (b.groups.size() * ix.bits + 7) / 8;
+    for (size_t i = 0; i < ix.hashes; ++i)
+      for (size_t byte = 0; byte < bytes; byte += 64)
+        __builtin_prefetch(b.data.data() + pos[ci * ix.hashes + i] * rb + byte);
+  }
+}
+
+void lookup_weighted(const Index& ix, uint64_t key, uint64_t weight, const Bank* const* banks,
+                     const uint64_t* pos, bool avx2, Scratch& s, uint64_t* counts) {
+  size_t rlen = 0;
+  const uint32_t* rec = ix.recovery ? ix.recover.get(abandoned_hash(key, ix.seed), &rlen) : nullptr;
+  s.snap.resize(rlen);
+  for (size_t i = 0; i < rlen; ++i) s.snap[i] = counts[rec[i]];
+  const uint64_t fp = splitmix64(key ^ ix.seed ^ 0x8E2D4F6A9B13C5D7ull) & ((1ull << ix.bits) - 1);
+  s.rows.resize(ix.hashes);
+  for (size_t ci = 0; ci < ix.classes.size(); ++ci) {
+    const Bank& b = *banks[ci];
+    const size_t rb = b.row_bytes(), G = b.groups.size(), bits = ix.bits;
+    for (size_t i = 0; i < ix.hashes; ++i) s.rows[i] = b.data.data() + pos[ci * ix.hashes + i] * rb;
+    auto hit = [&](size_t g) {
+      const Group& gr = b.groups[g];
+      if (gr.members.size() == 1) {
+        counts[gr.members[0]] += weight;
+        return;
+      }
+      const size_t off = G * bits + gr.offset - g * bits;
+      uint64_t mask = 0;
+      for (size_t i = 0; i < ix.hashes; ++i) mask ^= get_bits(s.rows[i], off, gr.width - bits);
+      for (; mask; mask &= mask - 1) counts[gr.members[__builtin_ctzll(mask)]] += weight;
+    };
+    screen(s.rows.data(), ix.hashes, bits, fp, G, avx2, hit);
+  }
+  for (size_t i = 0; i < rlen; ++i)
+    if (counts[rec[i]] == s.snap[i]) counts[rec[i]] += weight;
+}
+
+// Weighted keys (sorted, distinct) of one block into counts.
+void lookup_block_batch(const Index& ix, const std::vector<std::pair<uint64_t, uint64_t>>& kw,
+                        bool avx2, Scratch& s, uint64_t* counts) {
+  constexpr size_t kBlock = 32, kAhead = 4;
+  const size_t C = ix.classes.size(), H = ix.hashes;
+  for (size_t b0 = 0; b0 < kw.size(); b0 += kBlock) {
+    const size_t n = std::min(kBlock, kw.size() - b0);
+    s.pos.resize(n * C * H);
+    s.bank.resize(n * C);
+    for (size_t j = 0; j < n; ++j) {
+      const uint64_t key = kw[b0 + j].first;
+      for (size_t ci = 0; ci < C; ++ci) {
+        const auto& cls = ix.classes[ci];
+        const Bank* bp = &ix.banks[cls[0]];
+        if (cls.size() > 1)
+          bp = &ix.banks[cls[splitmix64(key ^ ix.seed ^ 0x34B61D8F29A7C053ull) & (cls.size() - 1)]];
+        s.bank[j * C + ci] = bp;
+        positions(key, ix.seed, bp->slots, H, ix.has_segment ? ix.segment : 0,
+                  &s.pos[(j * C + ci) * H]);
+      }
+    }
+    for (size_t j = 0; j < std::min(n, kAhead); ++j)
+      prefetch_key(ix, kw[b0 + j].first, &s.bank[j * C], &s.pos[j * C * H]);
+    for (size_t j = 0; j < n; ++j) {
+      if (j + kAhead < n)
+        prefetch_key(ix, kw[b0 + j + kAhead].first, &s.bank[(j + kAhead) * C],
+                     &s.pos[(j + kAhead) * C * H]);
+      lookup_weighted(ix, kw[b0 + j].first, kw[b0 + j].second, &s.bank[j * C], &s.pos[j * C * H],
+                      avx2, s, counts);
+    }
+  }
+}
+
+// Indexes the fast path serves: ordinary (non-findere) modes over
+// fingerprint-first banks.
+bool serves(const Index& ix) {
+  if (ix.f.mode == 3 || ix.hashes > 32) return false;
+  for (auto& b : ix.banks)
+    if (!b.fp_first) return false;
+  return true;
+}
+
+}  // namespace fastpath
+
+// Set for the duration of one oracle_query_handle_fast call (the baseline's
+// calls do not overlap).
+bool g_fast_lookup = false;
+
 void run_query(const Index& ix, const Work& w, int threads, std::vector<uint64_t>& counts) {
   const size_t C = ix.colors.size();
   counts.assign(C, 0);
@@ -1180,6 +1423,25 @@ void run_query(const Index& ix, const Work& w, int threads, std::vector<uint64_t
       pool.emplace_back([&, t] {
         std::vector<uint32_t> hits;
         std::vector<uint64_t> keys;
+        if (g_fast_lookup && fastpath::serves(ix)) {
+          const bool avx2 = __builtin_cpu_supports("avx2");
+          fastpath::Scratch s;
+          std::vector<std::pair<uint64_t, uint64_t>> kw;
+          for (size_t bi; (bi = next.fetch_add(1)) < blocks;) {
+            size_t a = bi * block, e = std::min(w.keys.size(), a + block);
+            keys.assign(w.keys.begin() + a, w.keys.begin() + e);
+            std::sort(keys.begin(), keys.end());
+            kw.clear();
+            for (size_t i = 0; i < keys.size();) {
+              size_t j = i + 1;
+              while (j < keys.size() && keys[j] == keys[i]) ++j;
+              kw.emplace_back(keys[i], j - i);
+              i = j;
+            }
+            fastpath::lookup_block_batch(ix, kw, avx2, s, part[t].data());
+          }
+          return;
+        }
         for (size_t bi; (bi = next.fetch_add(1)) < blocks;) {
           size_t a = bi * block, e = std::min(w.keys.size(), a + block);
           keys.assign(w.keys.begin() + a, w.keys.begin() + e);
@@ -1734,6 +1996,18 @@ int oracle_open(const char* index_dir, int recover, oracle_index** out) {
 }
 
 void oracle_close(oracle_index* index) { delete index; }
+
+int oracle_query_handle_fast(oracle_index* h, const uint8_t* bases, const uint64_t* offsets,
+                             size_t records, int threads, uint64_t* counts, size_t colors,
+                             uint64_t* total, double* seconds) {
+  g_fast_lookup = true;
+  const int rc = oracle_query_handle(h, bases, offsets, records, threads, counts, colors, total,
+                                     seconds);
+  g_fast_lookup = false;
+  return rc;
+}
+
+int oracle_fast_serves(oracle_index* h) { return fastpath::serves(*h->ix) ? 1 : 0; }
 
 int oracle_query_handle(oracle_index* h, const uint8_t* bases, const uint64_t* offsets,
                         size_t records, int threads, uint64_t* counts, size_t colors,

@@ -56,6 +56,14 @@ void oracle_close(oracle_index* index);
 int oracle_query_handle(oracle_index* index, const uint8_t* bases, const uint64_t* offsets,
                         size_t records, int threads, uint64_t* counts, size_t colors,
                         uint64_t* total, double* seconds);
+// The same query with the reference's lookup_batch blocks, 4-ahead row
+// prefetch and AVX2 fingerprint screens (the timed CPU baseline; same
+// counts). oracle_fast_serves: 1 when the index takes that path (ordinary
+// modes over fingerprint-first banks), else the scalar lookup runs.
+int oracle_query_handle_fast(oracle_index* index, const uint8_t* bases, const uint64_t* offsets,
+                             size_t records, int threads, uint64_t* counts, size_t colors,
+                             uint64_t* total, double* seconds);
+int oracle_fast_serves(oracle_index* index);
 
 // Per-record report of a query file as `zorindex query --records` prints it
 // (query_records_command_with_memory, src/power_merge/storage.rs:3626-3720):

@@ -2,9 +2,14 @@
 fastx.cpp), compiled into a small harness: the aggregate reader (split at
 records, headers and qualities ignored, LF/CRLF, gzip) and the strict named
 record reader of per-record reports (records.rs:150-290), including its error
-messages, which must be the reference's.
+messages, which must be the reference's. Compressed inputs: gzip, zstd, xz and
+bzip2, single and concatenated streams, as the reference's reader decodes them
+(src/lib.rs:283-321; its test of identical features from every format,
+src/lib.rs:1214-1283).
 """
+import bz2
 import gzip
+import lzma
 import subprocess
 from pathlib import Path
 
@@ -40,7 +45,7 @@ def harness(tmp_path_factory):
     exe = d / "h"
     subprocess.run(["g++", "-O1", "-std=c++17", f"-I{HOST}", "-o", str(exe), str(d / "h.cpp"),
                     str(HOST / "fastx.cpp"), str(HOST / "zstd_io.cpp"), "-lz", "-l:libzstd.so.1",
-                    "-lpthread"], check=True)
+                    "-l:liblzma.so.5", "-l:libbz2.so.1.0", "-lpthread"], check=True)
     return exe
 
 
@@ -81,3 +86,25 @@ def test_named_reader_errors(harness, tmp_path, text, message):
     lines = run(harness, tmp_path, "named", text)
     assert len(lines) == 1 and lines[0].startswith("ERROR\t2\t"), lines
     assert lines[0].split("\t", 2)[2] == message
+
+
+def _zstd(data: bytes) -> bytes:
+    import pyarrow as pa
+
+    return pa.compress(data, codec="zstd", asbytes=True)
+
+
+@pytest.mark.parametrize("codec", ["gz", "zst", "xz", "bz2"])
+def test_compressed_inputs_read_like_plain(harness, tmp_path, codec):
+    data = b">r1 d\nACGTNN\nacgt\n>r2\n" + b"ACGT" * 20000 + b"\n>r3\nTTTT\n"
+    pack = {"gz": gzip.compress, "xz": lzma.compress, "bz2": bz2.compress, "zst": _zstd}[codec]
+    want = run(harness, tmp_path, "plain", data)
+    half = data.index(b">r2")
+    for blob in (pack(data), pack(data[:half]) + pack(data[half:])):  # one and two streams
+        p = tmp_path / f"q.fa.{codec}"
+        p.write_bytes(blob)
+        out = subprocess.run([str(harness), "plain", str(p)], capture_output=True, check=True)
+        assert out.stdout.decode().splitlines() == want
+    p.write_bytes(pack(data)[:-7])  # truncated
+    out = subprocess.run([str(harness), "plain", str(p)], capture_output=True, check=True)
+    assert out.stdout.decode().startswith("ERROR\t2\t"), out.stdout

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_SOURCES = ["host/json.cpp", "host/manifest.cpp", "host/zstd_io.cpp", "host/fastx.cpp",
                 "host/record_report.cpp"]
 CUDA_SOURCES = ["engine.cu", "server.cu", "planner.cu", "capi.cu"]
-LIBS = ["-lz", "-l:libzstd.so.1", "-lpthread"]
+LIBS = ["-lz", "-l:libzstd.so.1", "-l:liblzma.so.5", "-l:libbz2.so.1.0", "-lpthread"]
 
 
 def _nvcc() -> str:

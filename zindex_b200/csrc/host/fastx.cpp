@@ -2,14 +2,114 @@
 
 #include <zlib.h>
 
+#include <algorithm>
+#include <cstdint>
 #include <cstring>
 
 #include "error.h"
 #include "zstd_io.h"
 
+// The few entry points of liblzma (xz-utils 5.x) and libbzip2 (1.0.x) that
+// query decoding uses, declared here from their stable public C APIs (the
+// image ships the shared libraries without headers).
+extern "C" {
+struct zx_lzma_stream {
+  const uint8_t* next_in;
+  size_t avail_in;
+  uint64_t total_in;
+  uint8_t* next_out;
+  size_t avail_out;
+  uint64_t total_out;
+  const void* allocator;
+  void* internal;
+  void* reserved_ptr[4];
+  uint64_t reserved_int1, reserved_int2;
+  size_t reserved_int3, reserved_int4;
+  int reserved_enum1, reserved_enum2;
+};
+int lzma_stream_decoder(zx_lzma_stream* strm, uint64_t memlimit, uint32_t flags);
+int lzma_code(zx_lzma_stream* strm, int action);
+void lzma_end(zx_lzma_stream* strm);
+struct zx_bz_stream {
+  char* next_in;
+  unsigned int avail_in;
+  unsigned int total_in_lo32, total_in_hi32;
+  char* next_out;
+  unsigned int avail_out;
+  unsigned int total_out_lo32, total_out_hi32;
+  void* state;
+  void* (*bzalloc)(void*, int, int);
+  void (*bzfree)(void*, void*);
+  void* opaque;
+};
+int BZ2_bzDecompressInit(zx_bz_stream* strm, int verbosity, int small);
+int BZ2_bzDecompress(zx_bz_stream* strm);
+int BZ2_bzDecompressEnd(zx_bz_stream* strm);
+}
+
 namespace zx {
 
 namespace {
+
+constexpr int kLzmaOk = 0, kLzmaStreamEnd = 1, kLzmaFinish = 3;
+constexpr uint32_t kLzmaConcatenated = 0x08;
+constexpr int kBzOk = 0, kBzStreamEnd = 4;
+
+// .xz input (every stream of a concatenated file), as deko's xz decoder reads
+// it for the reference parser (src/lib.rs:283-321).
+std::vector<uint8_t> xz_decode_all(const std::vector<uint8_t>& raw, const std::string& path) {
+  zx_lzma_stream zs;
+  memset(&zs, 0, sizeof zs);
+  check(lzma_stream_decoder(&zs, UINT64_MAX, kLzmaConcatenated) == kLzmaOk, kEFormat,
+        "xz: cannot initialise decoder");
+  std::vector<uint8_t> out, buf(1 << 20);
+  zs.next_in = raw.data();
+  zs.avail_in = raw.size();
+  int rc = kLzmaOk;
+  for (;;) {
+    zs.next_out = buf.data();
+    zs.avail_out = buf.size();
+    rc = lzma_code(&zs, kLzmaFinish);
+    out.insert(out.end(), buf.data(), buf.data() + (buf.size() - zs.avail_out));
+    if (rc != kLzmaOk) break;
+  }
+  lzma_end(&zs);
+  check(rc == kLzmaStreamEnd, kEFormat, ("corrupt or truncated xz input " + path).c_str());
+  return out;
+}
+
+// .bz2 input, concatenated streams included.
+std::vector<uint8_t> bz2_decode_all(const std::vector<uint8_t>& raw, const std::string& path) {
+  std::vector<uint8_t> out, buf(1 << 20);
+  size_t at = 0;
+  while (at < raw.size()) {
+    zx_bz_stream bs;
+    memset(&bs, 0, sizeof bs);
+    check(BZ2_bzDecompressInit(&bs, 0, 0) == kBzOk, kEFormat, "bzip2: cannot initialise decoder");
+    bs.next_in = (char*)raw.data() + at;
+    const size_t avail = std::min<size_t>(raw.size() - at, 0xFFFFFFFFu);
+    bs.avail_in = (unsigned int)avail;
+    int rc = kBzOk;
+    for (;;) {
+      bs.next_out = (char*)buf.data();
+      bs.avail_out = (unsigned int)buf.size();
+      rc = BZ2_bzDecompress(&bs);
+      out.insert(out.end(), buf.data(), buf.data() + (buf.size() - bs.avail_out));
+      if (rc != kBzOk) break;
+      if (bs.avail_in == 0 && bs.avail_out != 0) break;  // input ended inside the stream
+    }
+    const size_t used = avail - bs.avail_in;
+    BZ2_bzDecompressEnd(&bs);
+    check(rc == kBzStreamEnd, kEFormat, ("corrupt or truncated bzip2 input " + path).c_str());
+    at += used;
+    // Trailing bytes that do not start another stream end the input.
+    if (at + 3 > raw.size() || memcmp(raw.data() + at, "BZh", 3)) {
+      check(at == raw.size(), kEFormat, ("unexpected data after bzip2 input " + path).c_str());
+      break;
+    }
+  }
+  return out;
+}
 
 std::vector<uint8_t> decoded_input(const std::string& path) {
   std::vector<uint8_t> raw = read_file_bytes(path);
@@ -40,9 +140,8 @@ std::vector<uint8_t> decoded_input(const std::string& path) {
     check(rc == Z_STREAM_END, kEFormat, ("corrupt or truncated gzip input " + path).c_str());
     return out;
   }
-  if ((raw.size() >= 6 && !memcmp(raw.data(), "\xfd" "7zXZ\0", 6)) ||
-      (raw.size() >= 3 && !memcmp(raw.data(), "BZh", 3)))
-    raise(kEUnsupported, "xz and bzip2 query inputs are not supported: " + path);
+  if (raw.size() >= 6 && !memcmp(raw.data(), "\xfd" "7zXZ\0", 6)) return xz_decode_all(raw, path);
+  if (raw.size() >= 3 && !memcmp(raw.data(), "BZh", 3)) return bz2_decode_all(raw, path);
   return raw;
 }
 
