@@ -203,7 +203,7 @@ class Index:
         return {"team": l.team, "warps": l.warps, "blocks": l.blocks,
                 "smem_counters": l.smem_counters, "stage_bytes": l.stage_bytes,
                 "stages": l.stages, "bulk": l.bulk, "min_blocks": l.min_blocks,
-                "planes": l.planes, "cut": l.cut, "split": l.split}
+                "planes": l.planes, "cut": l.cut, "split": l.split, "wide": l.wide}
 
     def launch(self) -> dict:
         l = ZxLaunch()
@@ -219,11 +219,17 @@ class Index:
                    smem_counters: Optional[int] = None, stage_bytes: Optional[int] = None,
                    stages: Optional[int] = None, bulk: Optional[int] = None,
                    min_blocks: Optional[int] = None, planes: Optional[int] = None,
-                   cut: Optional[int] = None, split: Optional[int] = None, **_ignored):
+                   cut: Optional[int] = None, split: Optional[int] = None,
+                   wide: Optional[int] = None, **_ignored):
         """Change the launch configuration (never changes results); unset
         fields keep their default values (a default 255-register budget,
-        min_blocks 1, becomes 2 when the per-hit or staged form is asked for)."""
+        min_blocks 1, becomes 2 when the per-hit or staged form is asked for;
+        naming a field of the fused kernel's forms - team, planes, stage_bytes,
+        split or min_blocks - without `wide` selects the fused kernel)."""
         d = self.default_launch()
+        if wide is None:
+            fused = any(v is not None for v in (team, planes, stage_bytes, split, min_blocks))
+            wide = 0 if fused else d["wide"]
         if min_blocks is None and d["min_blocks"] == 1 and (planes == 0 or (stage_bytes or 0) > 0):
             d["min_blocks"] = 2
         l = ZxLaunch(int(d["team"] if team is None else team), int(d["warps"] if warps is None else warps),
@@ -234,7 +240,7 @@ class Index:
                      int(d["min_blocks"] if min_blocks is None else min_blocks),
                      int(d["planes"] if planes is None else planes),
                      int(d["cut"] if cut is None else cut),
-                     int(d["split"] if split is None else split))
+                     int(d["split"] if split is None else split), int(wide))
         _lib.check(_lib.load().zx_set_launch(self._h, byref(l)))
 
     def query_status(self) -> None:

@@ -51,7 +51,7 @@ class ZxInfo(ctypes.Structure):
 class ZxLaunch(ctypes.Structure):
     _fields_ = [("team", c_int), ("warps", c_int), ("blocks", c_int), ("smem_counters", c_int),
                 ("stage_bytes", c_int), ("stages", c_int), ("bulk", c_int), ("min_blocks", c_int),
-                ("planes", c_int), ("cut", c_int), ("split", c_int)]
+                ("planes", c_int), ("cut", c_int), ("split", c_int), ("wide", c_int)]
 
 
 class ZxServerOptions(ctypes.Structure):

@@ -62,6 +62,7 @@ void fill_launch(const zx::QueryLaunch& l, zx_launch* out) {
   out->planes = l.planes;
   out->cut = l.cut;
   out->split = l.split;
+  out->wide = l.wide;
 }
 
 }  // namespace
@@ -332,7 +333,7 @@ int zx_set_launch(zx_index* index, const zx_launch* l) {
     std::lock_guard<std::mutex> lock(index->mu);
     index->engine->set_launch(
         zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters, l->stage_bytes, l->stages,
-                        l->bulk, l->min_blocks, l->planes, l->cut, l->split});
+                        l->bulk, l->min_blocks, l->planes, l->cut, l->split, l->wide});
   });
 }
 

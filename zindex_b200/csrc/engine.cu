@@ -13,6 +13,7 @@
 
 #include "kernels/query_kernels.cuh"
 #include "kernels/record_hits.cuh"
+#include "kernels/wide_probe.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -135,6 +136,25 @@ FusedFn fused_for(int mode, const QueryLaunch& l) {
   }
   if (v == 1) return fused_mode<2, 1>(mode);
   return v == 2 ? fused_mode<2, 2>(mode) : fused_mode<2, 0>(mode);
+}
+
+using WideFn = void (*)(const DevIndex*, const ColorLoc*, const uint64_t*,
+                       const unsigned long long*, int, uint32_t*, uint64_t*, unsigned long long*);
+using DenseExtractFn = void (*)(BatchView, SeedParams, uint64_t*, unsigned long long*, int);
+
+// Wide-row probe variant: J chunks per thread, S seeds per step, HQ rows
+// loaded per seed and chunk (16 loads in flight per thread).
+WideFn wide_fn(int J, int HQ) {
+  if (J == 1) return HQ == 8 ? wide_probe_kernel<1, 2, 8, 2> : wide_probe_kernel<1, 4, 4, 2>;
+  return HQ == 8 ? wide_probe_kernel<2, 1, 8, 2> : wide_probe_kernel<2, 2, 4, 2>;
+}
+
+DenseExtractFn dense_extract_for(int mode) {
+  switch (mode) {
+    case 1: return extract_dense_kernel<1>;
+    case 2: return extract_dense_kernel<2>;
+    default: return extract_dense_kernel<0>;
+  }
 }
 
 ExtractFn extract_for(int mode) {
@@ -359,7 +379,7 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
   const uint64_t words = nbases / 32 + 2;
   const uint64_t tiles = nbases / kTileWindows + nbases / kFindereTask + records + 16;
   // Register gather, colour counts added straight into the caller's counters.
-  QueryLaunch l = launch_;
+  QueryLaunch l = fused_launch(launch_);
   l.smem_counters = 0;
   l.stage_bytes = 0;
   l.blocks = 0;
@@ -433,7 +453,7 @@ Workspace::~Workspace() {
                  keys_count, error,    fstate,    hp_starts, hp_keep,    hp_pos,
                  hp_bases,   hp_offsets, hp_scan_tmp, seg_blocks, seg_tiles, seg_records,
                  rec_counts, rec_totals, rec_hits, rec_first, rec_scan_tmp, hit_colors,
-                 hit_counts, split_keys, split_counts};
+                 hit_counts, split_keys, split_counts, wide_cursor};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total, h_seg_blocks, h_seg_records};
@@ -481,6 +501,8 @@ void Engine::release() {
   if (d_ix_rec_) cudaFree(d_ix_rec_);
   if (d_ix_norec_) cudaFree(d_ix_norec_);
   d_ix_rec_ = d_ix_norec_ = nullptr;
+  if (d_color_loc_) cudaFree(d_color_loc_);
+  d_color_loc_ = nullptr;
 }
 
 int Engine::span() const { return (int)m_.k; }
@@ -748,6 +770,24 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
     C.multi = d_multi;
     C.members = d_members;
   }
+  {
+    // Colour -> (class, member index, group) for the wide probe's
+    // recovered-origin point probes; a colour in no bank stays ~0.
+    std::vector<ColorLoc> loc(std::max<size_t>(m_.colors.size(), 1), ColorLoc{0xFFFFFFFFu, 0u});
+    for (size_t ci = 0; ci < m_.classes.size(); ++ci) {
+      const BankMeta& first = m_.banks[m_.classes[ci][0]];
+      for (uint64_t g = 0; g < first.groups.size(); ++g) {
+        const auto& mem = first.groups[g].members;
+        for (size_t mi = 0; mi < mem.size(); ++mi)
+          if (mem[mi] < m_.colors.size())
+            loc[mem[mi]] = ColorLoc{(uint32_t)ci | ((uint32_t)mi << 8), (uint32_t)g};
+      }
+    }
+    dev_alloc(&d_color_loc_, loc.size(), "colour locations");
+    cuda_check(cudaMemcpy(d_color_loc_, loc.data(), loc.size() * sizeof(ColorLoc),
+                          cudaMemcpyHostToDevice),
+               "upload");
+  }
   cuda_check(cudaStreamSynchronize(up.stream), "bank upload");
   cuda_check(cudaDeviceSynchronize(), "bank upload");
   banks_load_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_banks).count();
@@ -830,6 +870,28 @@ uint64_t Engine::gather_bytes_per_seed() const {
 }
 
 QueryLaunch Engine::default_launch() const {
+  QueryLaunch l = default_fused_launch();
+  // Wide rows (2 KiB and more of fingerprint planes per cell over all
+  // classes): the block-team probe, one 16-byte chunk per thread for rows of
+  // up to 256 chunks (4 warps up to 128), two beyond; colour counters in
+  // shared memory while they leave room for two blocks per SM.
+  if (wide_eligible(8) && wide_chunks() >= 128) {
+    l.wide = 1;
+    l.warps = wide_chunks() <= 128 ? 4 : 8;
+    l.smem_counters = 1;
+    if (m_.colors.size() > 16384 || fused_smem_bytes(l) > 110 * 1024) l.smem_counters = 0;
+  }
+  return l;
+}
+
+QueryLaunch Engine::fused_launch(const QueryLaunch& l) const {
+  if (!l.wide) return l;
+  QueryLaunch f = default_fused_launch();
+  f.cut = l.cut;
+  return f;
+}
+
+QueryLaunch Engine::default_fused_launch() const {
   uint32_t chunks = 1;
   for (uint32_t c = 0; c < host_ix_.classes; ++c) chunks = std::max(chunks, host_ix_.cls[c].fp_chunks);
   int team = 1;
@@ -857,6 +919,7 @@ QueryLaunch Engine::default_launch() const {
   l.min_blocks = 2;
   l.planes = 1;
   l.cut = 4;
+  l.wide = 0;
   // Minimizer seeds are extracted by a kernel of their own: the probe kernel
   // then needs no extraction scratch and keeps twice the warps resident
   // (C3 slice on B200: 22.3 ms against 36.7 ms for the fused kernel).
@@ -879,6 +942,27 @@ QueryLaunch Engine::default_launch() const {
   return l;
 }
 
+uint32_t Engine::wide_chunks() const {
+  uint32_t n = 0;
+  for (uint32_t c = 0; c < host_ix_.classes; ++c) n += host_ix_.cls[c].fp_chunks;
+  return n;
+}
+
+bool Engine::wide_eligible(int warps) const {
+  return m_.fingerprint_bits >= 4 && sp_.mode >= 0 && sp_.mode <= 2 && !sp_.strobe_max &&
+         (warps == 4 || warps == 8) && wide_chunks() <= 2u * (uint32_t)warps * 32u &&
+         WideSmem::total((uint32_t)m_.colors.size(), host_ix_.classes, m_.hashes, 0) <= 200 * 1024;
+}
+
+bool Engine::wide_form(const QueryLaunch& l) const { return l.wide && wide_eligible(l.warps); }
+
+void Engine::wide_shape(const QueryLaunch& l, int& J, int& HQ) const {
+  const uint32_t T = (uint32_t)l.warps * 32u;
+  J = (int)((wide_chunks() + T - 1) / T);
+  const int Hp = (m_.hashes + 3) & ~3;
+  HQ = Hp % 8 == 0 ? 8 : 4;
+}
+
 void Engine::check_not_strobes() const {
   check(!sp_.strobe_max, kEUnsupported,
         "randstrobemer indexes score each record's two strands: query them through host-buffer "
@@ -890,6 +974,9 @@ int Engine::kernel_mode(const QueryLaunch& l) const {
 }
 
 size_t Engine::fused_smem_bytes(const QueryLaunch& l) const {
+  if (wide_form(l))
+    return WideSmem::total((uint32_t)m_.colors.size(), host_ix_.classes, m_.hashes,
+                           l.smem_counters);
   const int mode = kernel_mode(l);
   return FusedSmem::total(mode, sp_.k, (uint32_t)m_.colors.size(), host_ix_.classes, m_.hashes, l,
                           FusedSmem::shared_words(mode, host_ix_, l), sp_.strobe_max != 0);
@@ -900,15 +987,24 @@ int Engine::max_blocks(const QueryLaunch& l) const {
       cached_for_.smem_counters == l.smem_counters && cached_for_.stage_bytes == l.stage_bytes &&
       cached_for_.stages == l.stages && cached_for_.bulk == l.bulk &&
       cached_for_.min_blocks == l.min_blocks && cached_for_.planes == l.planes &&
-      cached_for_.cut == l.cut && cached_for_.split == l.split)
+      cached_for_.cut == l.cut && cached_for_.split == l.split && cached_for_.wide == l.wide)
     return cached_blocks_;
   int per_sm = 0;
   size_t smem = fused_smem_bytes(l);
-  FusedFn fn = fused_for(kernel_mode(l), l);
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
-                                                           l.warps * 32, smem),
-             "occupancy");
+  if (wide_form(l)) {
+    int J, HQ;
+    wide_shape(l, J, HQ);
+    WideFn fn = wide_fn(J, HQ);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, l.warps * 32, smem),
+               "occupancy");
+  } else {
+    FusedFn fn = fused_for(kernel_mode(l), l);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
+                                                             l.warps * 32, smem),
+               "occupancy");
+  }
   const_cast<Engine*>(this)->cached_blocks_ = std::max(1, per_sm) * sms_;
   const_cast<Engine*>(this)->cached_for_ = l;
   return cached_blocks_;
@@ -948,6 +1044,11 @@ void Engine::set_launch(const QueryLaunch& l) {
   check(l.planes == 0 || l.planes == 1, kEInval, "planes must be 0 or 1");
   check(l.cut >= 1 && l.cut <= 64, kEInval, "cut must be in 1..64");
   check(l.split == 0 || l.split == 1, kEInval, "split must be 0 or 1");
+  check(l.wide == 0 || l.wide == 1, kEInval, "wide must be 0 or 1");
+  check(!l.wide || wide_eligible(l.warps), kEInval,
+        "the wide-row form needs fingerprints of at least 4 bits, a k-mer, minimizer or "
+        "modimizer index without strobes, 4 or 8 warps per block and rows of at most "
+        "2 x 32 x warps chunks");
   check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
   check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
   std::lock_guard<std::mutex> lock(mu_);
@@ -965,8 +1066,8 @@ std::unique_ptr<Workspace> Engine::make_workspace() {
 
 void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
   const uint64_t colors = m_.colors.size();
-  // Split minimizer queries: key slots allocated before any graph capture.
-  if (kernel_mode(launch_) == 4) ensure_split_capacity(ws);
+  // Split minimizer and wide-row queries: key slots allocated before any graph capture.
+  if (kernel_mode(launch_) == 4 || wide_form(launch_)) ensure_split_capacity(ws);
   if (nbases > ws.cap_bases || !ws.bases) {
     uint64_t cap = std::max<uint64_t>({nbases, ws.cap_bases * 3 / 2, 4096});
     cap = round_up(cap, 4096);
@@ -1162,6 +1263,44 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                                                                                colors, counts);
     cuda_check(cudaGetLastError(), "reduce_counters_kernel");
   };
+  if (wide_form(l)) {
+    // Wide-row query: rounds of up to kSplitTiles tiles; per round the
+    // extraction kernel appends the tiles' seeds to one dense list, the wide
+    // probe counts them, and the block counters are added up.
+    ensure_split_capacity(ws);
+    int J, HQ;
+    wide_shape(l, J, HQ);
+    WideFn wfn = wide_fn(J, HQ);
+    cuda_check(cudaFuncSetAttribute(wfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+               "cudaFuncSetAttribute");
+    const int ewarps = 4;
+    const size_t esmem = 256 * 8 + ewarps * FusedSmem::warp_bytes(sp_.mode, sp_.k, 0);
+    DenseExtractFn efn = dense_extract_for(sp_.mode);
+    cuda_check(cudaFuncSetAttribute(efn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem),
+               "cudaFuncSetAttribute");
+    const int egrid = (int)std::min<uint64_t>((kSplitTiles + ewarps - 1) / ewarps,
+                                              (uint64_t)sms_ * 8);
+    const int wblocks = l.blocks > 0 ? std::min(l.blocks, blocks_cap) : blocks_cap;
+    for (uint64_t lo = 0; lo < tiles_bound; lo += kSplitTiles) {
+      BatchView rb = bv;
+      rb.tile_lo = (uint32_t)lo;
+      rb.tile_hi = (uint32_t)std::min<uint64_t>(lo + kSplitTiles, tiles_bound);
+      cuda_check(cudaMemsetAsync(ws.wide_cursor, 0, 8, s), "memset");
+      efn<<<egrid, ewarps * 32, esmem, s>>>(rb, sp_, ws.split_keys, ws.wide_cursor, ewarps);
+      cuda_check(cudaGetLastError(), "extract_dense_kernel");
+      wfn<<<wblocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, d_color_loc_,
+                                              ws.split_keys, ws.wide_cursor, l.smem_counters,
+                                              ws.partial, counts, total);
+      cuda_check(cudaGetLastError(), "wide_probe_kernel");
+      if (l.smem_counters) {
+        reduce_counters_kernel<<<std::max(1u, (colors + 255) / 256), 256, 0, s>>>(
+            ws.partial, wblocks, colors, counts);
+        cuda_check(cudaGetLastError(), "reduce_counters_kernel");
+      }
+    }
+    if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
+    return;
+  }
   if (kmode != 4) {
     fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, ws.partial,
                                           counts, total, ws.error);
@@ -1203,6 +1342,7 @@ void Engine::ensure_split_capacity(Workspace& ws) {
   if (ws.split_keys) return;
   dev_alloc(&ws.split_keys, kSplitTiles * kTileWindows, "split key slots");
   dev_alloc(&ws.split_counts, kSplitTiles, "split key counts");
+  dev_alloc(&ws.wide_cursor, 1, "dense key cursor");
   ws.release_graphs();
 }
 
@@ -1228,7 +1368,7 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   for (uint32_t i = 0; i < segments; ++i)
     check(seg_records[i] <= seg_records[i + 1], kEInval, "segment records must be non-decreasing");
   ensure_capacity(ws, nbases, records);
-  QueryLaunch l = launch_;
+  QueryLaunch l = fused_launch(launch_);
   l.split = 0;  // every segment extracts its own tiles in the fused kernel
   if (warps > 0 && warps < l.warps) l.warps = warps;
   const int cap = max_blocks(l);

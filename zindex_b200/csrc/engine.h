@@ -17,6 +17,10 @@
 #include "kernels/types.cuh"
 
 namespace zx {
+struct ColorLoc;
+}
+
+namespace zx {
 
 struct OpenOptions {
   int device = 0;
@@ -64,6 +68,7 @@ struct Workspace {
   // Split minimizer queries: key slots of one round of tiles.
   uint64_t* split_keys = nullptr;
   uint32_t* split_counts = nullptr;
+  unsigned long long* wide_cursor = nullptr;  // wide-row queries: keys in the dense list
   // Per-record queries: counters of one record group (records x colours).
   uint64_t* rec_counts = nullptr;
   unsigned long long* rec_totals = nullptr;
@@ -119,6 +124,16 @@ class Engine {
   QueryLaunch launch() const { return launch_; }
   void set_launch(const QueryLaunch& l);
   QueryLaunch default_launch() const;
+  // The fused kernel's default launch (segmented and allocation-free queries
+  // run the fused kernel; a wide-row launch maps to it, keeping its cut).
+  QueryLaunch default_fused_launch() const;
+  QueryLaunch fused_launch(const QueryLaunch& l) const;
+  // Wide-row form (kernels/wide_probe.cuh): fingerprint chunks over all
+  // classes, whether an index and block size admit it, and the kernel shape.
+  uint32_t wide_chunks() const;
+  bool wide_eligible(int warps) const;
+  bool wide_form(const QueryLaunch& l) const;
+  void wide_shape(const QueryLaunch& l, int& J, int& HQ) const;
   size_t fused_smem_bytes(const QueryLaunch& l) const;
   int max_blocks(const QueryLaunch& l) const;
   // Bytes of fingerprint planes gathered per seed, summed over classes.
@@ -245,6 +260,7 @@ class Engine {
   DevIndex host_ix_{};
   DevIndex* d_ix_rec_ = nullptr;    // with recovery
   DevIndex* d_ix_norec_ = nullptr;  // recovery disabled
+  ColorLoc* d_color_loc_ = nullptr;  // colour -> class, member, group (wide probe)
   std::vector<void*> allocations_;
   uint64_t resident_bytes_ = 0;
   std::unique_ptr<Workspace> ws_;

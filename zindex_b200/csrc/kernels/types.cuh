@@ -48,6 +48,8 @@ struct QueryLaunch {
   int cut;            // host batches: pipelined chunks (copy of chunk i+1 overlaps chunk i), 1..64
   int split;          // minimizers: 1 = seeds extracted by their own kernel into per-tile slots,
                       // then probed by a kernel without the extraction scratch (more warps per SM)
+  int wide;           // 1 = wide-row form: seeds extracted into a dense list, probed by blocks
+                      // whose threads own fixed 16-byte chunks of every row (wide_probe.cuh)
 };
 
 }  // namespace zx

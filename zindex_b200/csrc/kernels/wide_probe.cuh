@@ -1,0 +1,335 @@
+// Wide-row probe: the whole block is one team (K5 for rows of thousands of
+// colours).
+//
+// Same arithmetic as probe_rows (Index::lookup_selected, src/power_merge/
+// storage.rs:2761-2925: per class the partition bank, the H cells of
+// PositionHash, the XOR of the H fingerprint-plane rows, a compare of every
+// b-bit field with fingerprint(key), membership decode of multi-member groups;
+// recovered origins counted once per seed, 2769-2787 and 2916-2924), laid out
+// for indexes whose rows span many 16-byte chunks (2,048 colours at b = 16:
+// 4 KiB per cell; 16,384 colours at b = 4: 8 KiB):
+//
+// * Seeds come from a dense key list (extract_dense_kernel appends every
+//   tile's seeds; aggregate counts do not depend on their order).
+// * A block takes 256 seeds at a time. Thread i computes seed i's fingerprint
+//   pattern and the row index of each of its H cells per class into shared
+//   memory, then the block walks the seeds: thread t owns the 16-byte
+//   chunks t, t + T, ... of the concatenated fingerprint planes of all
+//   classes, so a warp reads 512 contiguous bytes of every row and each
+//   thread's field-match flags always land in the same few dense words. The
+//   flags are counted in bit planes held in registers (vertical binary
+//   counters, 63 per field) and added to the colour counters every 63 seeds.
+// * A recovered origin c is counted when the filter did not hit it: the
+//   seed's owner thread re-reads c's own field in the seed's H cells (and its
+//   membership bit for a multi-member group). Filter hits plus recovered
+//   origins the filter missed is the union lookup_selected counts, and no
+//   filter hit has to be checked against the recovery list.
+// * Hits on multi-member groups take the per-hit membership decode.
+//
+// Needs b >= 4 (one dense word per chunk) and at most J chunks per thread.
+#pragma once
+#include <stdint.h>
+
+#include "query_kernels.cuh"
+
+namespace zx {
+
+constexpr int kWideSeeds = 256;      // seeds per descriptor round of a block
+constexpr int kWidePlanes = 6;       // register planes: counts up to 63 per field
+constexpr uint32_t kWideFlush = 63;  // seeds between plane flushes
+
+// Colour location for recovered-origin point probes: cls_member = class |
+// member index << 8 (member index within a multi-member group, 0 for
+// singletons; ~0 for a colour in no bank), group = the colour's group.
+struct ColorLoc {
+  uint32_t cls_member;
+  uint32_t group;
+};
+
+// Appends the seeds of tiles [tile_lo, tile_hi) (tile_hi 0 = to the end) to
+// out[], one atomic cursor bump per warp and tile. out holds at least
+// (tile_hi - tile_lo) * kTileWindows keys.
+template <int MODE>
+__global__ void extract_dense_kernel(BatchView bv, SeedParams sp, uint64_t* __restrict__ out,
+                                     unsigned long long* __restrict__ cursor, int warps_per_block) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint64_t* inner = reinterpret_cast<uint64_t*>(smem);
+  uint8_t* p = smem + 256 * 8;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, 0, 0, 0, 4, 0, 0, false);
+  uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
+  uint8_t* ocm = wbase + FusedSmem::key_bytes(MODE, sp.k, false) + FusedSmem::probe_bytes(0);
+  build_inner_table(sp, inner);
+  __syncthreads();
+  uint32_t ntiles = *bv.ntiles;
+  if (bv.tile_hi && bv.tile_hi < ntiles) ntiles = bv.tile_hi;
+  const uint32_t warps_total = gridDim.x * warps_per_block;
+  for (uint32_t t = bv.tile_lo + blockIdx.x * warps_per_block + warp; t < ntiles;
+       t += warps_total) {
+    const uint32_t n = extract_tile<MODE>(bv, sp, bv.tiles[t], keys, ocm, inner, lane);
+    __syncwarp();
+    unsigned long long at = 0;
+    if (lane == 0 && n) at = atomicAdd(cursor, (unsigned long long)n);
+    at = __shfl_sync(0xFFFFFFFFu, at, 0);
+    for (uint32_t i = lane; i < n; i += 32) out[at + i] = keys[i];
+    __syncwarp();
+  }
+}
+
+// Shared memory of the wide probe: DevIndex copy, colour counters (optional),
+// then per seed of a round its fingerprint pattern and row indices (classes x
+// H rounded up to 4).
+struct WideSmem {
+  static __host__ __device__ size_t rows_per_seed(uint32_t classes, int hashes) {
+    return (size_t)classes * (size_t)((hashes + 3) & ~3);
+  }
+  static __host__ __device__ size_t total(uint32_t colors, uint32_t classes, int hashes,
+                                          int smem_counters) {
+    return FusedSmem::ix_bytes + FusedSmem::counter_bytes(colors, smem_counters) +
+           (size_t)kWideSeeds * 4 + (size_t)kWideSeeds * rows_per_seed(classes, hashes) * 4;
+  }
+};
+
+struct WideCounters {
+  uint32_t* smem;
+  uint64_t* gmem;
+  __device__ __forceinline__ void add(uint32_t c, uint32_t n) const {
+    if (smem) atomicAdd(smem + c, n);
+    else atomicAdd(reinterpret_cast<unsigned long long*>(gmem + c), (unsigned long long)n);
+  }
+};
+
+// Group of dense bit p of a chunk (chunk-local group 0 = first field): word
+// p % b of the chunk, field p / b of that word.
+__device__ __forceinline__ uint32_t wide_group(uint32_t g0, uint32_t p, int b, int lb) {
+  return g0 + (p & (uint32_t)(b - 1)) * (32u >> lb) + (p >> lb);
+}
+
+// J: chunks per thread; S: seeds per step; HQ: rows loaded per seed and chunk
+// before the XOR (J * S * HQ 16-byte loads in flight per thread).
+template <int J, int S, int HQ, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    wide_probe_kernel(const DevIndex* __restrict__ gix, const ColorLoc* __restrict__ color_loc,
+                      const uint64_t* __restrict__ keys,
+                      const unsigned long long* __restrict__ nkeys, int smem_counters,
+                      uint32_t* __restrict__ partial, uint64_t* __restrict__ counts,
+                      unsigned long long* __restrict__ total) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  DevIndex* six = reinterpret_cast<DevIndex*>(smem);
+  uint8_t* p = smem + FusedSmem::ix_bytes;
+  const uint32_t colors = gix->colors, classes = gix->classes;
+  uint32_t* scount = nullptr;
+  if (smem_counters) {
+    scount = reinterpret_cast<uint32_t*>(p);
+    p += FusedSmem::counter_bytes(colors, 1);
+  }
+  uint32_t* pattern = reinterpret_cast<uint32_t*>(p);
+  uint32_t* rows = pattern + kWideSeeds;
+  load_index_smem(gix, six);
+  if (scount)
+    for (uint32_t c = threadIdx.x; c < colors; c += blockDim.x) scount[c] = 0;
+  __syncthreads();
+  const DevIndex& ix = *six;
+  const WideCounters cnt{scount, counts};
+  const int H = ix.hashes, Hp = (H + 3) & ~3, b = ix.bits, lb = log2_bits(b);
+  const uint32_t ones = field_ones(b), hi = ones << (b - 1);
+  const uint32_t fmask = b == 32 ? 0xFFFFFFFFu : (1u << b) - 1u;
+  const uint32_t per_seed = classes * (uint32_t)Hp;
+  const uint32_t T = blockDim.x, tid = threadIdx.x;
+
+  // The chunks this thread owns, their class and masks.
+  const uint8_t* col[J];
+  uint32_t stride[J], roff[J], g0[J], valid[J], multi[J], cls[J];
+  uint32_t planes[J][kWidePlanes];
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    col[j] = nullptr;
+    stride[j] = roff[j] = g0[j] = valid[j] = multi[j] = cls[j] = 0;
+#pragma unroll
+    for (int k = 0; k < kWidePlanes; ++k) planes[j][k] = 0;
+    uint32_t g = tid + (uint32_t)j * T, start = 0;
+    for (uint32_t ci = 0; ci < classes; ++ci) {
+      const DevClass& C = ix.cls[ci];
+      if (g < start + C.fp_chunks) {
+        const uint32_t k = g - start;
+        col[j] = C.data + (uint64_t)k * 16u;
+        stride[j] = C.row_stride;
+        roff[j] = ci * (uint32_t)Hp;
+        cls[j] = ci;
+        g0[j] = k * (128u >> lb);
+        for (uint32_t bit = 0; bit < 32; ++bit) {
+          if ((bit & (uint32_t)(b - 1)) >= 4u) continue;
+          const uint32_t grp = wide_group(g0[j], bit, b, lb);
+          if (grp >= C.groups) continue;
+          valid[j] |= 1u << bit;
+          if (__ldg(C.group_color + grp) & kMultiGroup) multi[j] |= 1u << bit;
+        }
+        break;
+      }
+      start += C.fp_chunks;
+    }
+  }
+
+  auto flush = [&]() {
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      uint32_t any = 0;
+#pragma unroll
+      for (int k = 0; k < kWidePlanes; ++k) any |= planes[j][k];
+      if (!any) continue;
+      const DevClass& C = ix.cls[cls[j]];
+      while (any) {
+        const uint32_t bit = __ffs(any) - 1;
+        any &= any - 1;
+        uint32_t v = 0;
+#pragma unroll
+        for (int k = 0; k < kWidePlanes; ++k) v |= ((planes[j][k] >> bit) & 1u) << k;
+        cnt.add(__ldg(C.group_color + wide_group(g0[j], bit, b, lb)), v);
+      }
+#pragma unroll
+      for (int k = 0; k < kWidePlanes; ++k) planes[j][k] = 0;
+    }
+  };
+
+  const uint64_t nk = *nkeys;
+  unsigned long long seeds = 0;
+  uint32_t steps = 0;
+  for (uint64_t base = (uint64_t)blockIdx.x * kWideSeeds; base < nk;
+       base += (uint64_t)gridDim.x * kWideSeeds) {
+    const uint32_t n =
+        nk - base < (uint64_t)kWideSeeds ? (uint32_t)(nk - base) : (uint32_t)kWideSeeds;
+    // Descriptors: pattern and row indices of each seed; recovered origins
+    // the filter misses are counted by the seed's owner.
+    for (uint32_t i = tid; i < n; i += T) {
+      const uint64_t key = keys[base + i];
+      const uint64_t first = mixsplit(key, ix.seed), step = splitmix64(first);
+      const uint32_t fp = (uint32_t)fingerprint(key, ix.seed, b);
+      pattern[i] = fp * ones;
+      uint32_t* my = rows + i * per_seed;
+      for (uint32_t ci = 0; ci < classes; ++ci) {
+        const DevClass& C = ix.cls[ci];
+        const uint32_t part = C.partitions > 1 ? partition_id(key, ix.seed, C.partitions) : 0;
+        const uint64_t count = C.slots / C.seg - (uint64_t)H + 1;
+        const uint32_t seg = (uint32_t)C.seg;
+        const uint32_t row0 = (uint32_t)((uint64_t)part * C.slots + mulhi64(first, count) * C.seg);
+        uint64_t h = first;
+        for (int r = 0; r < H; ++r, h += step)
+          my[ci * Hp + r] = row0 + (uint32_t)r * seg + (((uint32_t)h ^ (uint32_t)(h >> 33)) & (seg - 1));
+      }
+      const RecHit rec = recovery_lookup(ix.rec, recovery_hash(key, ix.seed));
+      for (uint32_t o = 0; o < rec.len; ++o) {
+        const uint32_t c = rec.at(o);
+        const ColorLoc loc = color_loc[c];
+        bool hit = false;
+        if (loc.cls_member != 0xFFFFFFFFu) {
+          const uint32_t ci = loc.cls_member & 0xFFu, mi = loc.cls_member >> 8, g = loc.group;
+          const DevClass& C = ix.cls[ci];
+          const uint32_t* rr = my + ci * Hp;
+          uint64_t fx = 0;
+          for (int r = 0; r < H; ++r)
+            fx ^= row_bits(C.data + (uint64_t)rr[r] * C.row_stride, g * (uint32_t)b, (uint32_t)b);
+          hit = (uint32_t)fx == (fp & fmask);
+          const uint32_t gc = __ldg(C.group_color + g);
+          if (hit && (gc & kMultiGroup)) {
+            const uint32_t* mg = C.multi + 3 * (gc & ~kMultiGroup);
+            const uint32_t off = __ldg(mg), w = __ldg(mg + 1);
+            uint64_t mx = 0;
+            for (int r = 0; r < H; ++r) mx ^= row_bits(C.data + (uint64_t)rr[r] * C.row_stride, off, w);
+            hit = (mx >> mi) & 1u;
+          }
+        }
+        if (!hit) cnt.add(c, 1);
+      }
+    }
+    if (tid == 0) seeds += n;
+    __syncthreads();
+    for (uint32_t s0 = 0; s0 < n; s0 += S) {
+      uint4 acc[J][S];
+#pragma unroll
+      for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int s = 0; s < S; ++s) acc[j][s] = make_uint4(0, 0, 0, 0);
+      for (int i0 = 0; i0 < H; i0 += HQ) {
+        uint4 v[J][S][HQ];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const uint32_t sd = min(s0 + (uint32_t)s, n - 1);
+          const bool live = s0 + (uint32_t)s < n;
+#pragma unroll
+          for (int j = 0; j < J; ++j) {
+            uint32_t ri[HQ];
+#pragma unroll
+            for (int q = 0; q < HQ; q += 4) {
+              const uint4 r4 = *reinterpret_cast<const uint4*>(rows + sd * per_seed + roff[j] + i0 + q);
+              ri[q] = r4.x; ri[q + 1] = r4.y; ri[q + 2] = r4.z; ri[q + 3] = r4.w;
+            }
+#pragma unroll
+            for (int q = 0; q < HQ; ++q) {
+              v[j][s][q] = make_uint4(0, 0, 0, 0);
+              if (live && col[j] && i0 + q < H) v[j][s][q] = ld_row_chunk(col[j] + (uint64_t)ri[q] * stride[j]);
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+          for (int s = 0; s < S; ++s)
+#pragma unroll
+            for (int q = 0; q < HQ; ++q) {
+              acc[j][s].x ^= v[j][s][q].x; acc[j][s].y ^= v[j][s][q].y;
+              acc[j][s].z ^= v[j][s][q].z; acc[j][s].w ^= v[j][s][q].w;
+            }
+      }
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const uint32_t sd = s0 + (uint32_t)s;
+        if (sd >= n) continue;
+        const uint32_t pat = pattern[sd];
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+          const uint32_t w4[4] = {acc[j][s].x, acc[j][s].y, acc[j][s].z, acc[j][s].w};
+          uint32_t d = 0;
+#pragma unroll
+          for (int w = 0; w < 4; ++w) d |= zero_fields_hi(w4[w] ^ pat, hi) >> (uint32_t)(b - 1 - w);
+          d &= valid[j];
+          const uint32_t slow = d & multi[j];
+          uint32_t m = d & ~slow;
+#pragma unroll
+          for (int k = 0; k < kWidePlanes; ++k) {
+            const uint32_t t = planes[j][k] & m;
+            planes[j][k] ^= m;
+            m = t;
+          }
+          for (uint32_t x = slow; x; x &= x - 1) {
+            const DevClass& C = ix.cls[cls[j]];
+            const uint32_t g = wide_group(g0[j], __ffs(x) - 1, b, lb);
+            const uint32_t gc = __ldg(C.group_color + g);
+            const uint32_t* mg = C.multi + 3 * (gc & ~kMultiGroup);
+            const uint32_t off = __ldg(mg), w = __ldg(mg + 1), firstm = __ldg(mg + 2);
+            const uint32_t* rr = rows + sd * per_seed + roff[j];
+            uint64_t mx = 0;
+            for (int r = 0; r < H; ++r) mx ^= row_bits(C.data + (uint64_t)rr[r] * C.row_stride, off, w);
+            while (mx) {
+              const uint32_t mb = __ffsll((long long)mx) - 1;
+              mx &= mx - 1;
+              cnt.add(__ldg(C.members + firstm + mb), 1);
+            }
+          }
+        }
+        if (++steps == kWideFlush) {
+          flush();
+          steps = 0;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  flush();
+  if (tid == 0 && seeds) atomicAdd(total, seeds);
+  __syncthreads();
+  if (scount)
+    for (uint32_t c = threadIdx.x; c < colors; c += blockDim.x)
+      partial[(uint64_t)blockIdx.x * colors + c] = scount[c];
+}
+
+}  // namespace zx
