@@ -79,10 +79,18 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     if force or _stale(cli, [cli_src, so] + build_src + heads):
         _run(["g++", "-O3", "-std=c++17", "-Wall", "-o", cli, cli_src, *build_src, *host_objs,
               f"-L{LIB}", "-lzindex_b200", f"-Wl,-rpath,$ORIGIN", *LIBS], verbose)
+    # The device builder (zx_build --device) is CUDA: compiled by nvcc and
+    # linked into zx_build only.
+    dbo = objdir / "device_builder.cu.o"
+    dbs = CSRC / "builder" / "device_builder.cu"
+    if force or _stale(dbo, [dbs] + heads):
+        _run([nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexpr", "-c", dbs,
+              "-o", dbo], verbose)
     zb = LIB / "zx_build"
     zb_src = [CSRC / "builder" / "zx_build_main.cpp", CSRC / "builder" / "builder.cpp"]
-    if force or _stale(zb, zb_src + heads + host_objs):
-        _run(["g++", "-O3", "-std=c++17", "-Wall", "-o", zb, *zb_src, *host_objs, *LIBS], verbose)
+    if force or _stale(zb, zb_src + heads + host_objs + [dbo]):
+        _run([nvcc, *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-Wall", "-o", zb, *zb_src, dbo,
+              *host_objs, *LIBS], verbose)
     zs = LIB / "zx_synth"
     zs_src = CSRC / "builder" / "zx_synth.cpp"
     if force or _stale(zs, [zs_src] + heads):

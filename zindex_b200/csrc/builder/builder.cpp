@@ -5,7 +5,9 @@
 // "first active key in a minimum-degree cell" cycle breaking
 // (src/bin/zorindex.rs:634-841), fingerprint-first row packing
 // (storage.rs:1721-1878) and the ZORABN2 recovery file (storage.rs:1882-2128).
-#include "builder.h"
+// The phases shared with the device builder are in namespace zx::build
+// (builder_internal.h).
+#include "builder_internal.h"
 
 #include <sys/stat.h>
 
@@ -29,11 +31,8 @@
 #include "synth.h"
 
 namespace zx {
+namespace build {
 namespace {
-
-struct Input {
-  std::string name, path;
-};
 
 std::string strip_name(const std::string& path) {
   std::string name = path.substr(path.find_last_of('/') == std::string::npos
@@ -89,61 +88,7 @@ std::vector<Input> read_fof(const std::string& path) {
   return out;
 }
 
-uint64_t next_pow2(uint64_t v) {
-  uint64_t p = 1;
-  while (p < v) p <<= 1;
-  return p;
-}
 int ilog2(uint64_t v) { return 63 - __builtin_clzll(v); }
-
-struct Group {
-  std::vector<uint32_t> members;  // sorted dataset ids; bit i <-> members[i]
-  uint64_t width = 0;
-  uint64_t cardinality = 0;
-  uint64_t slots = 0;  // after promotion
-  std::vector<uint64_t> keys, masks;
-  // Filled during construction.
-  uint64_t abandoned = 0;
-  size_t cls = 0, column = 0;
-  uint64_t offset = 0;
-};
-
-struct ClassLayout {
-  uint64_t source_slots = 0, local_slots = 0, partitions = 1;
-  std::vector<size_t> groups;  // in column order
-  uint64_t row_bits = 0;
-  std::vector<std::vector<uint64_t>> rows;  // per partition: slots * row_bytes bytes as u64 words
-};
-
-struct Abandoned {
-  uint32_t hash;
-  uint32_t group;
-  uint64_t mask;
-};
-
-template <class F>
-void parallel_for(size_t n, int threads, F&& body) {
-  std::atomic<size_t> next{0};
-  std::vector<std::thread> pool;
-  std::mutex mu;
-  std::exception_ptr error;
-  auto worker = [&] {
-    for (size_t i; (i = next.fetch_add(1)) < n;) {
-      try {
-        body(i);
-      } catch (...) {
-        std::lock_guard<std::mutex> lock(mu);
-        if (!error) error = std::current_exception();
-        next = n;
-      }
-    }
-  };
-  int t = std::max(1, std::min<int>(threads, (int)n));
-  for (int i = 1; i < t; ++i) pool.emplace_back(worker);
-  worker();
-  for (auto& th : pool) th.join();
-  if (error) std::rethrow_exception(error);
-}
 
 // ZOR construction of one filter: peel the H-uniform hypergraph, abandon
 // keys when the peel stalls, assign cells in reverse peel order so every
@@ -272,100 +217,35 @@ void write_var(std::vector<uint8_t>& out, uint32_t v) {
   out.push_back((uint8_t)v);
 }
 
+
+
+}  // namespace
+
+uint64_t next_pow2(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
 double seconds_since(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
 }
 
-}  // namespace
-
-std::vector<uint64_t> promotion_targets(const std::vector<uint64_t>& slots,
-                                        const std::vector<uint64_t>& docs,
-                                        const std::vector<uint64_t>& widths, uint64_t minimum,
-                                        int64_t maximum) {
-  const size_t n = slots.size();
-  bool all_big = true;
-  for (uint64_t d : docs) all_big &= d >= minimum;
-  if ((minimum == 1 || all_big) && (maximum < 0 || (int64_t)n <= maximum)) return slots;
-  uint64_t total = 0;
-  for (uint64_t d : docs) total += d;
-  minimum = std::min(minimum, total);
-  using Cost = unsigned __int128;
-  auto bank_cost = [&](size_t end, uint64_t width) {
-    return (Cost)slots[end - 1] * (Cost)((width + 7) / 8) * 8;
-  };
-  std::vector<uint64_t> targets(n, 0);
-  if (maximum >= 0 && (int64_t)n > maximum) {
-    size_t limit = (size_t)maximum;
-    struct Cell {
-      bool ok = false;
-      Cost cost = 0;
-      size_t start = 0;
-    };
-    std::vector<std::vector<Cell>> best(limit + 1, std::vector<Cell>(n + 1));
-    best[0][0] = Cell{true, 0, 0};
-    for (size_t count = 1; count <= limit; ++count)
-      for (size_t end = count; end <= n; ++end) {
-        uint64_t d = 0, w = 0;
-        for (size_t s = end; s-- > 0;) {
-          d += docs[s];
-          w += widths[s];
-          if (d < minimum || !best[count - 1][s].ok) continue;
-          Cost c = best[count - 1][s].cost + bank_cost(end, w);
-          Cell& cur = best[count][end];
-          if (!cur.ok || c < cur.cost || (c == cur.cost && s < cur.start)) cur = Cell{true, c, s};
-        }
-      }
-    size_t count = 0;
-    Cost bestc = 0;
-    for (size_t c = 1; c <= limit; ++c)
-      if (best[c][n].ok && (!count || best[c][n].cost < bestc)) {
-        count = c;
-        bestc = best[c][n].cost;
-      }
-    check(count > 0, kEInval, "no feasible bounded subindex layout");
-    for (size_t end = n; end > 0; --count) {
-      size_t s = best[count][end].start;
-      for (size_t i = s; i < end; ++i) targets[i] = slots[end - 1];
-      end = s;
-    }
-    return targets;
-  }
-  struct Cell {
-    bool ok = false;
-    Cost cost = 0;
-    uint64_t banks = 0;
-    size_t start = 0;
-  };
-  std::vector<Cell> best(n + 1);
-  best[0] = Cell{true, 0, 0, 0};
-  for (size_t end = 1; end <= n; ++end) {
-    uint64_t d = 0, w = 0;
-    for (size_t s = end; s-- > 0;) {
-      d += docs[s];
-      w += widths[s];
-      if (d < minimum || !best[s].ok) continue;
-      Cell cand{true, best[s].cost + bank_cost(end, w), best[s].banks + 1, s};
-      Cell& cur = best[end];
-      bool better = !cur.ok || cand.cost < cur.cost ||
-                    (cand.cost == cur.cost &&
-                     (cand.banks < cur.banks || (cand.banks == cur.banks && s < cur.start)));
-      if (better) cur = cand;
-    }
-  }
-  for (size_t end = n; end > 0;) {
-    check(best[end].ok, kEInval, "no feasible minimum-document layout");
-    size_t s = best[end].start;
-    for (size_t i = s; i < end; ++i) targets[i] = slots[end - 1];
-    end = s;
-  }
-  return targets;
+uint64_t config_slots(const BuildOptions& opt, int H, uint64_t cardinality) {
+  double needed = std::ceil(std::max<double>((double)cardinality, 1.0) * opt.slot_scale);
+  uint64_t s = (uint64_t)needed;
+  s = std::max<uint64_t>(s, next_pow2((uint64_t)H));
+  s = std::max<uint64_t>(s, opt.segment_length * next_pow2((uint64_t)H));
+  return next_pow2(s);
 }
 
-void build_index(const BuildOptions& opt) {
-  const auto t0 = std::chrono::steady_clock::now();
-  const int threads = opt.threads > 0 ? opt.threads : (int)std::thread::hardware_concurrency();
-  const int H = opt.hashes, b = opt.fingerprint_bits;
-  FeatureParams fp = opt.features;
+void prepare(const BuildOptions& opt, Context& bc) {
+  bc.opt = opt;
+  bc.t0 = std::chrono::steady_clock::now();
+  bc.threads = opt.threads > 0 ? opt.threads : (int)std::thread::hardware_concurrency();
+  const int H = bc.H = opt.hashes, b = bc.b = opt.fingerprint_bits;
+  FeatureParams& fp = bc.fp;
+  fp = opt.features;
   check(H >= 2 && H <= kMaxHashes, kEInval, "invalid hash count");
   check(b == 1 || b == 2 || b == 4 || b == 8 || b == 16 || b == 32, kEInval,
         "fingerprint bits must be 1, 2, 4, 8, 16 or 32");
@@ -410,8 +290,8 @@ void build_index(const BuildOptions& opt) {
   check(stat(opt.output.c_str(), &st) != 0, kEInval,
         ("output " + opt.output + " already exists; choose a new directory").c_str());
 
-  std::vector<Input> inputs;
-  synth::GenomeSpec spec;
+  auto& inputs = bc.inputs;
+  auto& spec = bc.spec;
   if (!opt.synth.empty()) {
     check(synth::parse_spec(opt.synth, spec), kEInval, "invalid --synth specification");
     for (uint64_t c = 0; c < spec.colors; ++c)
@@ -419,87 +299,16 @@ void build_index(const BuildOptions& opt) {
   } else {
     inputs = read_fof(opt.fof);
   }
-  const size_t C = inputs.size();
-  std::vector<std::vector<uint64_t>> keys(C);
-  std::vector<uint64_t> occurrences(C, 0);
-  parallel_for(C, threads, [&](size_t c) {
-    std::vector<uint64_t> k;
-    if (!opt.synth.empty()) {
-      std::vector<uint8_t> g;
-      synth::genome(spec, c, g);
-      cpu::sequence_features(g.data(), g.size(), fp, k);
-    } else {
-      RecordBatch rb = read_fastx(inputs[c].path, false);
-      for (size_t r = 0; r < rb.records(); ++r)
-        cpu::sequence_features(rb.bases.data() + rb.offsets[r], rb.offsets[r + 1] - rb.offsets[r],
-                               fp, k);
-    }
-    occurrences[c] = k.size();
-    std::sort(k.begin(), k.end());
-    k.erase(std::unique(k.begin(), k.end()), k.end());
-    keys[c] = std::move(k);
-  });
-  if (!opt.quiet) fprintf(stderr, "extracted %zu datasets in %.3fs\n", C, seconds_since(t0));
+  bc.occurrences.assign(inputs.size(), 0);
+}
 
-  // Groups: explicit multi-member groups, singletons for everything else.
-  std::vector<Group> groups;
-  std::vector<int> grouped(C, 0);
-  if (!opt.groups.empty()) {
-    std::stringstream ss(opt.groups);
-    std::string part;
-    while (std::getline(ss, part, ';')) {
-      Group g;
-      std::stringstream ps(part);
-      std::string id;
-      while (std::getline(ps, id, ',')) {
-        size_t c = std::stoul(id);
-        check(c < C && !grouped[c], kEInval, "invalid or repeated dataset in --groups");
-        grouped[c] = 1;
-        g.members.push_back((uint32_t)c);
-      }
-      std::sort(g.members.begin(), g.members.end());
-      check(!g.members.empty() && g.members.size() <= (size_t)(64 - b), kEInval,
-            "invalid group size");
-      groups.push_back(std::move(g));
-    }
-  }
-  for (size_t c = 0; c < C; ++c)
-    if (!grouped[c]) {
-      Group g;
-      g.members.push_back((uint32_t)c);
-      groups.push_back(std::move(g));
-    }
-  const uint64_t fp_mask = (1ull << b) - 1;
-  parallel_for(groups.size(), threads, [&](size_t gi) {
-    Group& g = groups[gi];
-    g.width = (uint64_t)b + (g.members.size() == 1 ? 0 : g.members.size());
-    if (g.members.size() == 1) {
-      g.keys = std::move(keys[g.members[0]]);  // singleton: no membership masks
-    } else {
-      std::vector<std::pair<uint64_t, uint64_t>> all;
-      for (size_t i = 0; i < g.members.size(); ++i)
-        for (uint64_t key : keys[g.members[i]]) all.emplace_back(key, 1ull << i);
-      std::sort(all.begin(), all.end());
-      for (size_t i = 0; i < all.size();) {
-        size_t j = i;
-        uint64_t mask = 0;
-        while (j < all.size() && all[j].first == all[i].first) mask |= all[j++].second;
-        g.keys.push_back(all[i].first);
-        g.masks.push_back(mask);
-        i = j;
-      }
-    }
-    g.cardinality = g.keys.size();
-    // BuildConfig::slots (mod.rs:319-337).
-    double needed = std::ceil(std::max<double>((double)g.cardinality, 1.0) * opt.slot_scale);
-    uint64_t s = (uint64_t)needed;
-    s = std::max<uint64_t>(s, next_pow2((uint64_t)H));
-    s = std::max<uint64_t>(s, opt.segment_length * next_pow2((uint64_t)H));
-    g.slots = next_pow2(s);
-  });
-  for (auto& k : keys) std::vector<uint64_t>().swap(k);
-
+void plan_layout(Context& bc, bool host_rows) {
   // Promotion of undersized size classes.
+  const BuildOptions& opt = bc.opt;
+  const int H = bc.H;
+  auto& groups = bc.groups;
+  auto& classes = bc.classes;
+  auto& class_order = bc.class_order;
   std::map<uint64_t, std::pair<uint64_t, uint64_t>> sizes;
   for (auto& g : groups) {
     sizes[g.slots].first += g.members.size();
@@ -514,7 +323,8 @@ void build_index(const BuildOptions& opt) {
   std::vector<uint64_t> targets =
       promotion_targets(bs, bd, bw, opt.min_subindex_documents, opt.max_subindexes);
   std::map<uint64_t, uint64_t> promote;
-  size_t promoted = 0;
+  size_t& promoted = bc.promoted;
+  promoted = 0;
   for (size_t i = 0; i < bs.size(); ++i) promote[bs[i]] = targets[i];
   for (auto& g : groups) {
     uint64_t t = promote[g.slots];
@@ -525,7 +335,6 @@ void build_index(const BuildOptions& opt) {
   // Classes (one per final slot count), columns ordered by width then first
   // member (ColumnOrder::Width, storage.rs:1644-1660), hash partitions.
   std::map<uint64_t, size_t> class_of;
-  std::vector<ClassLayout> classes;
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     auto it = class_of.find(groups[gi].slots);
     if (it == class_of.end()) {
@@ -536,12 +345,13 @@ void build_index(const BuildOptions& opt) {
     classes[it->second].groups.push_back(gi);
   }
   // Banks in increasing source-slot order.
-  std::vector<size_t> class_order(classes.size());
+  class_order.assign(classes.size(), 0);
   for (size_t i = 0; i < classes.size(); ++i) class_order[i] = i;
   std::sort(class_order.begin(), class_order.end(),
             [&](size_t a, size_t c) { return classes[a].source_slots < classes[c].source_slots; });
   const uint64_t min_local = opt.segment_length * next_pow2((uint64_t)H);
-  bool partitioned = false;
+  bool& partitioned = bc.partitioned;
+  partitioned = false;
   for (auto& cl : classes) {
     std::sort(cl.groups.begin(), cl.groups.end(), [&](size_t a, size_t c) {
       if (groups[a].width != groups[c].width) return groups[a].width < groups[c].width;
@@ -565,68 +375,28 @@ void build_index(const BuildOptions& opt) {
       partitioned = true;
     }
     cl.partitions = cl.source_slots / cl.local_slots;
-    size_t words = (size_t)((cl.local_slots * row_bytes + 7) / 8 + 2);
-    cl.rows.assign(cl.partitions, std::vector<uint64_t>(words, 0));
+    if (host_rows) {
+      size_t words = (size_t)((cl.local_slots * row_bytes + 7) / 8 + 2);
+      cl.rows.assign(cl.partitions, std::vector<uint64_t>(words, 0));
+    }
   }
   for (size_t ci = 0; ci < classes.size(); ++ci)
     for (size_t gi : classes[ci].groups) groups[gi].cls = ci;
 
-  // Construction jobs: one per (group, partition).
-  struct Job {
-    size_t group;
-    uint64_t partition;
-  };
-  std::vector<Job> jobs;
-  for (size_t gi = 0; gi < groups.size(); ++gi)
-    for (uint64_t p = 0; p < classes[groups[gi].cls].partitions; ++p) jobs.push_back({gi, p});
-  std::vector<std::vector<Abandoned>> dropped(jobs.size());
-  std::vector<uint64_t> dropped_count(jobs.size(), 0);
-  // Largest filters first for load balance.
-  std::sort(jobs.begin(), jobs.end(), [&](const Job& a, const Job& c) {
-    return groups[a.group].cardinality > groups[c.group].cardinality;
-  });
-  parallel_for(jobs.size(), threads, [&](size_t ji) {
-    const Job& job = jobs[ji];
-    Group& g = groups[job.group];
-    ClassLayout& cl = classes[g.cls];
-    std::vector<uint64_t> k, v;
-    for (size_t i = 0; i < g.keys.size(); ++i) {
-      if (cl.partitions > 1 &&
-          partition_id(g.keys[i], fp.seed, (uint32_t)cl.partitions) != job.partition)
-        continue;
-      k.push_back(g.keys[i]);
-      v.push_back(fingerprint(g.keys[i], fp.seed, b) |
-                  (g.members.size() == 1 ? 0 : g.masks[i] << b));
-    }
-    std::vector<uint64_t> cells;
-    std::vector<uint32_t> lost =
-        construct_filter(k, v, cl.local_slots, H, opt.segment_length, fp.seed, cells);
-    dropped_count[ji] = lost.size();
-    if (!opt.drop_abandoned)
-      for (uint32_t e : lost)
-        dropped[ji].push_back(Abandoned{recovery_hash(k[e], fp.seed), (uint32_t)job.group,
-                                        g.members.size() == 1 ? 1 : v[e] >> b});
-    // Fingerprint-first packing into this partition's rows (legacy: the
-    // group's whole field, fingerprint in its low bits, at its offset).
-    const uint64_t G = cl.groups.size(), row_bytes = (cl.row_bits + 7) / 8;
-    const uint64_t mem_off = G * (uint64_t)b + g.offset - g.column * (uint64_t)b;
-    uint64_t* words = cl.rows[job.partition].data();
-    for (uint64_t s = 0; s < cl.local_slots; ++s) {
-      uint64_t cell = cells[s];
-      if (!cell) continue;
-      uint64_t base = s * row_bytes * 8;
-      if (opt.legacy_layout) {
-        or_bits(words, base + g.offset, (uint64_t)b, cell & fp_mask);
-        if (g.width > (uint64_t)b) or_bits(words, base + g.offset + b, g.width - b, cell >> b);
-        continue;
-      }
-      or_bits(words, base + g.column * (uint64_t)b, (uint64_t)b, cell & fp_mask);
-      if (g.width > (uint64_t)b) or_bits(words, base + mem_off, g.width - b, cell >> b);
-    }
-  });
-  for (size_t ji = 0; ji < jobs.size(); ++ji) groups[jobs[ji].group].abandoned += dropped_count[ji];
-  if (!opt.quiet) fprintf(stderr, "constructed %zu filters in %.3fs\n", jobs.size(), seconds_since(t0));
+}
 
+void write_index(Context& bc, const PayloadFn& payload_fn, int payload_threads) {
+  const BuildOptions& opt = bc.opt;
+  auto& groups = bc.groups;
+  auto& classes = bc.classes;
+  const FeatureParams& fp = bc.fp;
+  const int H = bc.H, b = bc.b;
+  const auto t0 = bc.t0;
+  const size_t C = bc.inputs.size();
+  const auto& inputs = bc.inputs;
+  const auto& occurrences = bc.occurrences;
+  const bool partitioned = bc.partitioned;
+  const size_t promoted = bc.promoted;
   // Staging directory, renamed into place at the end (storage.rs:466-475).
   std::string stage = opt.output + ".building";
   mkdir(stage.c_str(), 0755);
@@ -636,7 +406,7 @@ void build_index(const BuildOptions& opt) {
     std::string file;
   };
   std::vector<BankOut> banks;
-  for (size_t ci : class_order) {
+  for (size_t ci : bc.class_order) {
     const ClassLayout& cl = classes[ci];
     for (uint64_t p = 0; p < cl.partitions; ++p) {
       char name[128];
@@ -649,7 +419,7 @@ void build_index(const BuildOptions& opt) {
       banks.push_back({ci, p, name});
     }
   }
-  parallel_for(banks.size(), threads, [&](size_t bi) {
+  parallel_for(banks.size(), payload_threads, [&](size_t bi) {
     const ClassLayout& cl = classes[banks[bi].cls];
     const uint64_t row_bytes = (cl.row_bits + 7) / 8, payload = cl.local_slots * row_bytes;
     FramedWriter w(stage + "/" + banks[bi].file, opt.zstd_level);
@@ -659,15 +429,14 @@ void build_index(const BuildOptions& opt) {
     for (int i = 0; i < 4; ++i)
       for (int j = 0; j < 8; ++j) header[8 + 8 * i + j] = (uint8_t)(fields[i] >> (8 * j));
     w.write(header, 40);
-    w.write(cl.rows[banks[bi].partition].data(), payload);
+    payload_fn(banks[bi].cls, banks[bi].partition, w);
     w.finish();
   });
 
   // Recovery map: origins of every abandoned hash, unioned across groups.
   uint64_t hashes = 0, associations = 0;
   if (!opt.drop_abandoned) {
-    std::vector<Abandoned> all;
-    for (auto& d : dropped) all.insert(all.end(), d.begin(), d.end());
+    std::vector<Abandoned>& all = bc.abandoned;
     std::sort(all.begin(), all.end(),
               [](const Abandoned& a, const Abandoned& c) { return a.hash < c.hash; });
     std::vector<uint8_t> out;
@@ -829,6 +598,255 @@ void build_index(const BuildOptions& opt) {
             opt.output.c_str(), seconds_since(t0), banks.size(), groups.size(),
             (unsigned long long)bytes, (unsigned long long)abandoned, (unsigned long long)hashes);
   }
+}
+
+}  // namespace build
+
+std::vector<uint64_t> promotion_targets(const std::vector<uint64_t>& slots,
+                                        const std::vector<uint64_t>& docs,
+                                        const std::vector<uint64_t>& widths, uint64_t minimum,
+                                        int64_t maximum) {
+  const size_t n = slots.size();
+  bool all_big = true;
+  for (uint64_t d : docs) all_big &= d >= minimum;
+  if ((minimum == 1 || all_big) && (maximum < 0 || (int64_t)n <= maximum)) return slots;
+  uint64_t total = 0;
+  for (uint64_t d : docs) total += d;
+  minimum = std::min(minimum, total);
+  using Cost = unsigned __int128;
+  auto bank_cost = [&](size_t end, uint64_t width) {
+    return (Cost)slots[end - 1] * (Cost)((width + 7) / 8) * 8;
+  };
+  std::vector<uint64_t> targets(n, 0);
+  if (maximum >= 0 && (int64_t)n > maximum) {
+    size_t limit = (size_t)maximum;
+    struct Cell {
+      bool ok = false;
+      Cost cost = 0;
+      size_t start = 0;
+    };
+    std::vector<std::vector<Cell>> best(limit + 1, std::vector<Cell>(n + 1));
+    best[0][0] = Cell{true, 0, 0};
+    for (size_t count = 1; count <= limit; ++count)
+      for (size_t end = count; end <= n; ++end) {
+        uint64_t d = 0, w = 0;
+        for (size_t s = end; s-- > 0;) {
+          d += docs[s];
+          w += widths[s];
+          if (d < minimum || !best[count - 1][s].ok) continue;
+          Cost c = best[count - 1][s].cost + bank_cost(end, w);
+          Cell& cur = best[count][end];
+          if (!cur.ok || c < cur.cost || (c == cur.cost && s < cur.start)) cur = Cell{true, c, s};
+        }
+      }
+    size_t count = 0;
+    Cost bestc = 0;
+    for (size_t c = 1; c <= limit; ++c)
+      if (best[c][n].ok && (!count || best[c][n].cost < bestc)) {
+        count = c;
+        bestc = best[c][n].cost;
+      }
+    check(count > 0, kEInval, "no feasible bounded subindex layout");
+    for (size_t end = n; end > 0; --count) {
+      size_t s = best[count][end].start;
+      for (size_t i = s; i < end; ++i) targets[i] = slots[end - 1];
+      end = s;
+    }
+    return targets;
+  }
+  struct Cell {
+    bool ok = false;
+    Cost cost = 0;
+    uint64_t banks = 0;
+    size_t start = 0;
+  };
+  std::vector<Cell> best(n + 1);
+  best[0] = Cell{true, 0, 0, 0};
+  for (size_t end = 1; end <= n; ++end) {
+    uint64_t d = 0, w = 0;
+    for (size_t s = end; s-- > 0;) {
+      d += docs[s];
+      w += widths[s];
+      if (d < minimum || !best[s].ok) continue;
+      Cell cand{true, best[s].cost + bank_cost(end, w), best[s].banks + 1, s};
+      Cell& cur = best[end];
+      bool better = !cur.ok || cand.cost < cur.cost ||
+                    (cand.cost == cur.cost &&
+                     (cand.banks < cur.banks || (cand.banks == cur.banks && s < cur.start)));
+      if (better) cur = cand;
+    }
+  }
+  for (size_t end = n; end > 0;) {
+    check(best[end].ok, kEInval, "no feasible minimum-document layout");
+    size_t s = best[end].start;
+    for (size_t i = s; i < end; ++i) targets[i] = slots[end - 1];
+    end = s;
+  }
+  return targets;
+}
+
+// Programs linked without device_builder.cu (the zorindex command line) get
+// this definition; zx_build links the device builder's.
+__attribute__((weak)) void build_index_device(const BuildOptions&) {
+  raise(kEUnsupported, "this program was built without the device builder: use zx_build --device");
+}
+
+void build_index(const BuildOptions& opt) {
+  if (opt.device) {
+    build_index_device(opt);
+    return;
+  }
+  using namespace build;
+  Context bc;
+  prepare(opt, bc);
+  const auto t0 = bc.t0;
+  const int threads = bc.threads;
+  const int H = bc.H, b = bc.b;
+  const FeatureParams& fp = bc.fp;
+  const auto& inputs = bc.inputs;
+  const auto& spec = bc.spec;
+  auto& occurrences = bc.occurrences;
+  const size_t C = inputs.size();
+  std::vector<std::vector<uint64_t>> keys(C);
+  parallel_for(C, threads, [&](size_t c) {
+    std::vector<uint64_t> k;
+    if (!opt.synth.empty()) {
+      std::vector<uint8_t> g;
+      synth::genome(spec, c, g);
+      cpu::sequence_features(g.data(), g.size(), fp, k);
+    } else {
+      RecordBatch rb = read_fastx(inputs[c].path, false);
+      for (size_t r = 0; r < rb.records(); ++r)
+        cpu::sequence_features(rb.bases.data() + rb.offsets[r], rb.offsets[r + 1] - rb.offsets[r],
+                               fp, k);
+    }
+    occurrences[c] = k.size();
+    std::sort(k.begin(), k.end());
+    k.erase(std::unique(k.begin(), k.end()), k.end());
+    keys[c] = std::move(k);
+  });
+  if (!opt.quiet) fprintf(stderr, "extracted %zu datasets in %.3fs\n", C, seconds_since(t0));
+
+  // Groups: explicit multi-member groups, singletons for everything else.
+  auto& groups = bc.groups;
+  std::vector<int> grouped(C, 0);
+  if (!opt.groups.empty()) {
+    std::stringstream ss(opt.groups);
+    std::string part;
+    while (std::getline(ss, part, ';')) {
+      Group g;
+      std::stringstream ps(part);
+      std::string id;
+      while (std::getline(ps, id, ',')) {
+        size_t c = std::stoul(id);
+        check(c < C && !grouped[c], kEInval, "invalid or repeated dataset in --groups");
+        grouped[c] = 1;
+        g.members.push_back((uint32_t)c);
+      }
+      std::sort(g.members.begin(), g.members.end());
+      check(!g.members.empty() && g.members.size() <= (size_t)(64 - b), kEInval,
+            "invalid group size");
+      groups.push_back(std::move(g));
+    }
+  }
+  for (size_t c = 0; c < C; ++c)
+    if (!grouped[c]) {
+      Group g;
+      g.members.push_back((uint32_t)c);
+      groups.push_back(std::move(g));
+    }
+  const uint64_t fp_mask = (1ull << b) - 1;
+  parallel_for(groups.size(), threads, [&](size_t gi) {
+    Group& g = groups[gi];
+    g.width = (uint64_t)b + (g.members.size() == 1 ? 0 : g.members.size());
+    if (g.members.size() == 1) {
+      g.keys = std::move(keys[g.members[0]]);  // singleton: no membership masks
+    } else {
+      std::vector<std::pair<uint64_t, uint64_t>> all;
+      for (size_t i = 0; i < g.members.size(); ++i)
+        for (uint64_t key : keys[g.members[i]]) all.emplace_back(key, 1ull << i);
+      std::sort(all.begin(), all.end());
+      for (size_t i = 0; i < all.size();) {
+        size_t j = i;
+        uint64_t mask = 0;
+        while (j < all.size() && all[j].first == all[i].first) mask |= all[j++].second;
+        g.keys.push_back(all[i].first);
+        g.masks.push_back(mask);
+        i = j;
+      }
+    }
+    g.cardinality = g.keys.size();
+    g.slots = config_slots(opt, H, g.cardinality);
+  });
+  for (auto& k : keys) std::vector<uint64_t>().swap(k);
+
+  plan_layout(bc, true);
+  auto& classes = bc.classes;
+  // Construction jobs: one per (group, partition).
+  struct Job {
+    size_t group;
+    uint64_t partition;
+  };
+  std::vector<Job> jobs;
+  for (size_t gi = 0; gi < groups.size(); ++gi)
+    for (uint64_t p = 0; p < classes[groups[gi].cls].partitions; ++p) jobs.push_back({gi, p});
+  std::vector<std::vector<Abandoned>> dropped(jobs.size());
+  std::vector<uint64_t> dropped_count(jobs.size(), 0);
+  // Largest filters first for load balance.
+  std::sort(jobs.begin(), jobs.end(), [&](const Job& a, const Job& c) {
+    return groups[a.group].cardinality > groups[c.group].cardinality;
+  });
+  parallel_for(jobs.size(), threads, [&](size_t ji) {
+    const Job& job = jobs[ji];
+    Group& g = groups[job.group];
+    ClassLayout& cl = classes[g.cls];
+    std::vector<uint64_t> k, v;
+    for (size_t i = 0; i < g.keys.size(); ++i) {
+      if (cl.partitions > 1 &&
+          partition_id(g.keys[i], fp.seed, (uint32_t)cl.partitions) != job.partition)
+        continue;
+      k.push_back(g.keys[i]);
+      v.push_back(fingerprint(g.keys[i], fp.seed, b) |
+                  (g.members.size() == 1 ? 0 : g.masks[i] << b));
+    }
+    std::vector<uint64_t> cells;
+    std::vector<uint32_t> lost =
+        construct_filter(k, v, cl.local_slots, H, opt.segment_length, fp.seed, cells);
+    dropped_count[ji] = lost.size();
+    if (!opt.drop_abandoned)
+      for (uint32_t e : lost)
+        dropped[ji].push_back(Abandoned{recovery_hash(k[e], fp.seed), (uint32_t)job.group,
+                                        g.members.size() == 1 ? 1 : v[e] >> b});
+    // Fingerprint-first packing into this partition's rows (legacy: the
+    // group's whole field, fingerprint in its low bits, at its offset).
+    const uint64_t G = cl.groups.size(), row_bytes = (cl.row_bits + 7) / 8;
+    const uint64_t mem_off = G * (uint64_t)b + g.offset - g.column * (uint64_t)b;
+    uint64_t* words = cl.rows[job.partition].data();
+    for (uint64_t s = 0; s < cl.local_slots; ++s) {
+      uint64_t cell = cells[s];
+      if (!cell) continue;
+      uint64_t base = s * row_bytes * 8;
+      if (opt.legacy_layout) {
+        or_bits(words, base + g.offset, (uint64_t)b, cell & fp_mask);
+        if (g.width > (uint64_t)b) or_bits(words, base + g.offset + b, g.width - b, cell >> b);
+        continue;
+      }
+      or_bits(words, base + g.column * (uint64_t)b, (uint64_t)b, cell & fp_mask);
+      if (g.width > (uint64_t)b) or_bits(words, base + mem_off, g.width - b, cell >> b);
+    }
+  });
+  for (size_t ji = 0; ji < jobs.size(); ++ji) groups[jobs[ji].group].abandoned += dropped_count[ji];
+  if (!opt.quiet) fprintf(stderr, "constructed %zu filters in %.3fs\n", jobs.size(), seconds_since(t0));
+
+  for (auto& d : dropped) bc.abandoned.insert(bc.abandoned.end(), d.begin(), d.end());
+
+  write_index(
+      bc,
+      [&](size_t ci, uint64_t part, FramedWriter& w) {
+        const ClassLayout& cl = classes[ci];
+        w.write(cl.rows[part].data(), cl.local_slots * ((cl.row_bits + 7) / 8));
+      },
+      threads);
 }
 
 }  // namespace zx

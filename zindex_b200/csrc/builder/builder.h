@@ -37,6 +37,12 @@ struct BuildOptions {
   // fingerprint then membership at each group's offset) instead of
   // fingerprint-first ("ZORPOW3").
   bool legacy_layout = false;
+  // Construct on the GPU (build_index_device): distinct keys extracted,
+  // sorted and deduplicated on the device and every filter peeled by one
+  // device thread. Singleton groups of k-mer, minimizer and modimizer
+  // indexes; the same directory format.
+  bool device = false;
+  int gpu = 0;  // CUDA device of the device builder
 };
 
 // Builds the index; throws zx::Error.

@@ -35,16 +35,21 @@ inline uint64_t genome_length(const GenomeSpec& s, uint64_t g) {
   return (uint64_t)std::floor(std::exp(lo + u * (hi - lo)));
 }
 
-inline char genome_base(const GenomeSpec& s, uint64_t g, uint64_t pos) {
-  static const char acgt[] = "ACGT";
-  if (s.kind == "uniform") return acgt[splitmix64(pos ^ (s.seed + g)) & 3];
+// Base `pos` of genome g (host and device: the device builder generates the
+// same genomes in place).
+ZX_HD char synth_base(bool pool, uint64_t seed, uint64_t g, uint64_t pos) {
+  if (!pool) return "ACGT"[splitmix64(pos ^ (seed + g)) & 3];
   uint64_t block = pos / kBlock, off = pos % kBlock;
-  uint64_t r = splitmix64(splitmix64(s.seed ^ 0x626c6f636bull) ^ (g << 24) ^ block);
+  uint64_t r = splitmix64(splitmix64(seed ^ 0x626c6f636bull) ^ (g << 24) ^ block);
   if (r % 1000 < 300) {
     uint64_t core = (r >> 32) % kCoreSegments;
-    return acgt[splitmix64(off ^ splitmix64(s.seed ^ 0x636f7265ull ^ (core << 40))) & 3];
+    return "ACGT"[splitmix64(off ^ splitmix64(seed ^ 0x636f7265ull ^ (core << 40))) & 3];
   }
-  return acgt[splitmix64(pos ^ splitmix64(s.seed ^ 0x67656e6f6dull ^ (g << 20))) & 3];
+  return "ACGT"[splitmix64(pos ^ splitmix64(seed ^ 0x67656e6f6dull ^ (g << 20))) & 3];
+}
+
+inline char genome_base(const GenomeSpec& s, uint64_t g, uint64_t pos) {
+  return synth_base(s.kind != "uniform", s.seed, g, pos);
 }
 
 inline void genome(const GenomeSpec& s, uint64_t g, std::vector<uint8_t>& out) {

@@ -62,12 +62,14 @@ int main(int argc, char** argv) {
     else if (a == "--groups") o.groups = val();
     else if (a == "--synth") o.synth = val();
     else if (a == "-q" || a == "--quiet") o.quiet = true;
+    else if (a == "--device") o.device = true;
+    else if (a == "--gpu") o.gpu = std::stoi(val());
     else {
       fprintf(stderr,
               "usage: zx_build -f FOF -o DIR [-k K] [-m M] [-H H] [-b BITS] [-s SEED]\n"
               "  [-i kmers|minimizers|modimizers|findere] [-z Z] [-d D] [-c] [-p PATTERN] [-S SCALE]\n"
               "  [-L SEG] [-D MIN_DOCS] [-N MAX_SUBINDEXES] [-X MAX_SIZE] [-R] [-t THREADS]\n"
-              "  [--groups 0,1;2,3]\n");
+              "  [--groups 0,1;2,3] [--device [--gpu N]]\n");
       return 2;
     }
   }
