@@ -77,7 +77,7 @@ typedef struct zx_launch {
                          (more resident warps); applies to the row-index form (planes 1, no
                          staged gather) and is ignored elsewhere */
   int wide;           /* 1 = wide-row form (fingerprint bits >= 4, k-mer, minimizer and
-                         modimizer indexes with rows of at most 2 x warps x 32 chunks): seeds
+                         modimizer indexes with rows of at most 4 x warps x 32 chunks): seeds
                          are extracted into a dense list and probed by blocks whose threads
                          each own fixed 16-byte chunks of every row, counting in registers;
                          team, planes, stage_bytes and split are then unused */

@@ -21,11 +21,13 @@ CASES = [
     dict(colors=600, H=2, b=8, k=25, groups="1,2"),
     dict(colors=1500, H=4, b=4, k=31, groups="0,1,2;7,9"),
     dict(colors=2048, H=3, b=16, k=25, groups="5,6,7,8"),
-    dict(colors=4096, H=8, b=4, k=31, max_size="256KiB"),
+    dict(colors=4096, H=8, b=4, k=31, max_size="2MiB"),
     dict(colors=700, H=5, b=16, mode="minimizers", k=31, m=21),
     dict(colors=1000, H=3, b=32, mode="modimizers", k=31, d=4),
     dict(colors=800, H=4, b=8, k=45, groups="3,4"),
     dict(colors=300, H=13, b=4, k=21),
+    dict(colors=6000, H=8, b=4, k=25),    # three chunks per thread with 8 warps
+    dict(colors=4000, H=3, b=16, k=25),  # four chunks per thread with 8 warps
 ]
 
 
@@ -110,8 +112,8 @@ def test_wide_form_refuses_what_it_cannot_run(gpu, tmp_path_factory):
         with pytest.raises(zx.ZxError) as err:
             index.set_launch(wide=1, warps=8)  # 2-bit fingerprints
         assert err.value.code == 1
-    ix, _ = _index(tmp_path_factory, 4096, H=3, b=16, k=25)  # 512 chunks per row
+    ix, _ = _index(tmp_path_factory, 8192, H=3, b=16, k=25)  # about 1,024 chunks per row
     with zx.Index(ix) as index:
         with pytest.raises(zx.ZxError):
-            index.set_launch(wide=1, warps=4)  # more than 2 chunks per thread
+            index.set_launch(wide=1, warps=4)  # more than 4 chunks per thread
         index.set_launch(wide=1, warps=8)

@@ -146,7 +146,9 @@ using DenseExtractFn = void (*)(BatchView, SeedParams, uint64_t*, unsigned long 
 // loaded per seed and chunk (16 loads in flight per thread).
 WideFn wide_fn(int J, int HQ) {
   if (J == 1) return HQ == 8 ? wide_probe_kernel<1, 2, 8, 2> : wide_probe_kernel<1, 4, 4, 2>;
-  return HQ == 8 ? wide_probe_kernel<2, 1, 8, 2> : wide_probe_kernel<2, 2, 4, 2>;
+  if (J == 2) return HQ == 8 ? wide_probe_kernel<2, 1, 8, 2> : wide_probe_kernel<2, 2, 4, 2>;
+  if (J == 3) return wide_probe_kernel<3, 1, 4, 2>;
+  return wide_probe_kernel<4, 1, 4, 2>;
 }
 
 DenseExtractFn dense_extract_for(int mode) {
@@ -873,8 +875,8 @@ QueryLaunch Engine::default_launch() const {
   QueryLaunch l = default_fused_launch();
   // Wide rows (2 KiB and more of fingerprint planes per cell over all
   // classes): the block-team probe, one 16-byte chunk per thread for rows of
-  // up to 256 chunks (4 warps up to 128), two beyond; colour counters in
-  // shared memory while they leave room for two blocks per SM.
+  // up to 256 chunks (4 warps up to 128), up to four beyond; colour counters
+  // in shared memory while they leave room for two blocks per SM.
   if (wide_eligible(8) && wide_chunks() >= 128) {
     l.wide = 1;
     l.warps = wide_chunks() <= 128 ? 4 : 8;
@@ -950,7 +952,7 @@ uint32_t Engine::wide_chunks() const {
 
 bool Engine::wide_eligible(int warps) const {
   return m_.fingerprint_bits >= 4 && sp_.mode >= 0 && sp_.mode <= 2 && !sp_.strobe_max &&
-         (warps == 4 || warps == 8) && wide_chunks() <= 2u * (uint32_t)warps * 32u &&
+         (warps == 4 || warps == 8) && wide_chunks() <= 4u * (uint32_t)warps * 32u &&
          WideSmem::total((uint32_t)m_.colors.size(), host_ix_.classes, m_.hashes, 0) <= 200 * 1024;
 }
 
@@ -960,7 +962,7 @@ void Engine::wide_shape(const QueryLaunch& l, int& J, int& HQ) const {
   const uint32_t T = (uint32_t)l.warps * 32u;
   J = (int)((wide_chunks() + T - 1) / T);
   const int Hp = (m_.hashes + 3) & ~3;
-  HQ = Hp % 8 == 0 ? 8 : 4;
+  HQ = Hp % 8 == 0 && J <= 2 ? 8 : 4;
 }
 
 void Engine::check_not_strobes() const {
