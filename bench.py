@@ -89,6 +89,21 @@ CONFIGS = {
         # 64 KiB of rows per seed: fewer served requests keep the run bounded.
         "served": {"closed": 100, "open": 300, "rate": 200.0},
     },
+    "c4": {
+        "workload": {"workload": "served-large-resident-index", "colors": 16384,
+                     "genome_len_bp": [1_000_000, 6_000_000],
+                     "genome_model": "70% iid + 30% core-pool", "k": 31, "hashes": 8,
+                     "fingerprint_bits": 4, "index_mode": "kmers", "reads": 50_000,
+                     "read_len_bp": 150, "sourced": 0.6, "substitutions": 0.005,
+                     "index_build": "zx_build --device (the GPU builder)"},
+        "synth": "pool:16384:1000000:6000000:1",
+        "build": ["-k", "31", "-H", "8", "-b", "4", "--device"],
+        "reads": ["--kind", "short", "--reads", "50000", "--length", "150", "--sourced", "0.6",
+                  "--subst", "0.005"],
+        "served": {"closed": 100, "open": 300, "rate": 200.0},
+        # 16,384 dense counts per read: a bounded per-record sample.
+        "per_record_reads": 5_000,
+    },
 }
 CONFIG = CONFIGS["c2"]
 WORKLOAD = CONFIG["workload"]
@@ -669,6 +684,22 @@ def ours(args):
     served = served_form(zx, ix, make_requests(bases, offsets, lb, lo, sv["closed"], 11 + rank),
                          make_requests(bases, offsets, lb, lo, sv["open"], 23 + rank), sv["rate"])
 
+    log("stage: query file")
+    # The drop-in's own path: zx_query_file on the whole batch as a FASTA file
+    # (page cache): parsing, host-to-device copies, the query and the counts.
+    qfile = records_fasta(Path(args.cache), rank, args.config, bases, offsets, records)
+    ix.query_file(qfile)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        c_file, t_file, _ = ix.query_file(qfile)
+        times.append(time.perf_counter() - t0)
+    assert t_file == seeds and np.array_equal(c_file, counts_dev), "file and device paths disagree"
+    query_file = {"seeds_per_s": seeds / statistics.median(times),
+                  "seconds": statistics.median(times), "file_bytes": qfile.stat().st_size,
+                  "note": "zx_query_file of the batch as FASTA (one record per read, in the page "
+                          "cache): read, parse, copy, query, counts back"}
+
     log("stage: plain form")
     # Plain form: one record per launch, on a prefix.
     n_plain = min(4000, records)
@@ -683,7 +714,7 @@ def ours(args):
     # every read through zx_query_per_record (host buffers, copies inside the
     # timed region), then the compact report of a FASTA file end to end
     # (reading, counting, formatting, writing to /dev/null).
-    n_rec = min(PER_RECORD_READS, records)
+    n_rec = min(CONFIG.get("per_record_reads", PER_RECORD_READS), records)
     rb, ro = bases[: int(offsets[n_rec])], offsets[: n_rec + 1]
     pr_counts, pr_totals = ix.query_per_record(rb, ro)
     agg_counts, agg_total = ix.query_records(rb, ro)
@@ -789,6 +820,7 @@ def ours(args):
                       "served_seeds_per_s": served["closed_loop"]["seeds_per_s"],
                       "planned_seeds_per_s": world * planned["seeds_per_s"],
                       "served": served, "planned": planned, "per_record": per_record},
+            "query_file": query_file,
             "index_load": {"seconds": load_s, "banks_s": info.load_banks_s,
                            "recovery_s": info.load_recovery_s, "file_bytes": file_bytes,
                            "resident_bytes": int(info.resident_bytes),

@@ -97,9 +97,18 @@ def test_planner_gain_over_default_and_regret(gpu):
     timed = float(np.mean([r["timed_per_setting"] for r in dev]))
     cands = float(np.mean([r["candidates_per_setting"] for r in dev]))
     e2e_gain = gm([r["gain_over_default"] for r in e2e])
+    guarded = gm([r["top1_guarded_gain_over_default"] for r in dev])
+    rand = gm([r["random_shortlist_gain_over_default"] for r in dev])
+    heur = gm([r["heuristic_shortlist_gain_over_default"] for r in dev])
     print(f"launch: gain over the default {gain:.3f}, regret {regret:.3f} with {timed:.1f} of "
-          f"{cands:.0f} candidates timed (network's top pick alone: {top1:.3f}); "
+          f"{cands:.0f} candidates timed (network's top pick alone: {top1:.3f}, guarded by a "
+          f"{pl.TOP1_MARGIN:.0%} margin: {guarded:.3f}); the same budget without the network: "
+          f"random shortlist {rand:.3f}, nearest-to-default shortlist {heur:.3f}; "
           f"cut: gain over the default {e2e_gain:.3f}")
+    # What the network earns: its shortlist against untrained shortlists of
+    # the same size (both also time the default).
+    assert gain >= rand and gain >= heur - 0.005
+    assert guarded >= 0.99
     # The default launch is itself fitted to these measurements, so the gain
     # is over a strong baseline; the shortlist can only match or beat it.
     assert gain >= 1.02

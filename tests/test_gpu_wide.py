@@ -117,3 +117,56 @@ def test_wide_form_refuses_what_it_cannot_run(gpu, tmp_path_factory):
         with pytest.raises(zx.ZxError):
             index.set_launch(wide=1, warps=4)  # more than 4 chunks per thread
         index.set_launch(wide=1, warps=8)
+
+
+def test_wide_form_serves_coalesced_requests(gpu, oracle, tmp_path_factory):
+    """Coalesced requests on a wide-row index (each request its own wide-form
+    launch sequence) and the request server on it: every request's counts are
+    the oracle's for that request alone, and a batch of more requests than
+    the per-request path takes goes through the fused segmented launch."""
+    import threading
+
+    import torch
+
+    import zindex_b200 as zx
+    from test_gpu_serving import requests_for
+
+    ix, genomes = _index(tmp_path_factory, 2048, H=3, b=16, k=31)
+    reqs = requests_for(genomes, 90, seed=13)
+    with zx.Index(ix) as index:
+        assert index.launch()["wide"] == 1
+        dev = torch.device("cuda", 0)
+        for part in (reqs[:20], reqs):  # 20 requests: per request; 90: fused segmented
+            flat = [r for recs in part for r in recs]
+            seg = np.zeros(len(part) + 1, dtype=np.uint64)
+            seg[1:] = np.cumsum([len(recs) for recs in part])
+            bases, offsets = zx.pack_records(flat)
+            d_bases = torch.from_numpy(bases if len(bases) else np.zeros(1, np.uint8)).to(dev)
+            d_off = torch.from_numpy(offsets.view(np.int64)).to(dev)
+            counts = torch.zeros((len(part), index.colors), dtype=torch.int64, device=dev)
+            totals = torch.zeros(len(part), dtype=torch.int64, device=dev)
+            index.query_segments(d_bases.data_ptr(), len(bases), d_off.data_ptr(), len(flat), seg,
+                                 counts.data_ptr(), totals.data_ptr())
+            torch.cuda.synchronize(dev)
+            got, got_t = counts.cpu().numpy().astype(np.uint64), totals.cpu().numpy()
+            for i in range(0, len(part), 3):
+                want, want_total = oracle.query_records(ix, *zx.pack_records(part[i]))
+                assert int(got_t[i]) == want_total, i
+                np.testing.assert_array_equal(got[i], want, err_msg=f"request {i}")
+        with zx.Server(index, slots=3, slot_bases=200000, slot_requests=7) as server:
+            tickets = [None] * len(reqs)
+
+            def submitter(p):
+                for i in range(p, len(reqs), 3):
+                    tickets[i] = server.submit(*zx.pack_records(reqs[i]))
+
+            threads = [threading.Thread(target=submitter, args=(p,)) for p in range(3)]
+            for t in threads:
+                t.start()
+            for t in threads:
+                t.join()
+            results = [server.wait(t) for t in tickets]
+    for i in range(0, len(reqs), 4):
+        want, want_total = oracle.query_records(ix, *zx.pack_records(reqs[i]))
+        assert results[i][1] == want_total, i
+        np.testing.assert_array_equal(results[i][0], want, err_msg=f"served request {i}")

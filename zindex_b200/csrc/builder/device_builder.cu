@@ -798,17 +798,19 @@ void build_index_device(const BuildOptions& opt) {
   if (!opt.quiet)
     fprintf(stderr, "constructed %zu filters in %.3fs (%llu bytes of rows on the device)\n", C,
             seconds_since(bc.t0), (unsigned long long)row_total);
-  // Bank payloads streamed from the device through one pinned buffer.
+  // Bank payloads streamed from the device, one writer per bank, each through
+  // its own pinned buffer.
   constexpr uint64_t kPiece = 64ull << 20;
-  uint8_t* pinned = nullptr;
-  cu(cudaMallocHost((void**)&pinned, kPiece), "cudaMallocHost");
-  struct PinnedFree {
-    uint8_t* p;
-    ~PinnedFree() { cudaFreeHost(p); }
-  } pinned_free{pinned};
   write_index(
       bc,
       [&](size_t ci, uint64_t part, FramedWriter& w) {
+        cu(cudaSetDevice(opt.gpu), "cudaSetDevice");
+        uint8_t* pinned = nullptr;
+        cu(cudaMallocHost((void**)&pinned, kPiece), "cudaMallocHost");
+        struct PinnedFree {
+          uint8_t* p;
+          ~PinnedFree() { cudaFreeHost(p); }
+        } pinned_free{pinned};
         const ClassLayout& cl = bc.classes[ci];
         const uint64_t bytes = cl.local_slots * ((cl.row_bits + 7) / 8);
         for (uint64_t at = 0; at < bytes; at += kPiece) {
@@ -817,7 +819,7 @@ void build_index_device(const BuildOptions& opt) {
           w.write(pinned, len);
         }
       },
-      1);
+      bc.threads);
 }
 
 }  // namespace zx

@@ -1370,6 +1370,18 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   for (uint32_t i = 0; i < segments; ++i)
     check(seg_records[i] <= seg_records[i + 1], kEInval, "segment records must be non-decreasing");
   ensure_capacity(ws, nbases, records);
+  // Wide-row indexes: a few coalesced requests (a serving batch) each get the
+  // wide form's own launch sequence into their counters; batches of many
+  // small requests (per-record queries) take the fused segmented launch.
+  constexpr uint32_t kWideSegments = 64;
+  if (wide_form(launch_) && segments <= kWideSegments) {
+    const uint64_t colors = m_.colors.size();
+    for (uint32_t i = 0; i < segments; ++i) {
+      const uint64_t r0 = seg_records[i], n = seg_records[i + 1] - r0;
+      if (n) enqueue(ws, bases, nbases, offsets + r0, n, recover, counts + i * colors, totals + i, s);
+    }
+    return;
+  }
   QueryLaunch l = fused_launch(launch_);
   l.split = 0;  // every segment extracts its own tiles in the fused kernel
   if (warps > 0 && warps < l.warps) l.warps = warps;

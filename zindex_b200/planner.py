@@ -250,6 +250,17 @@ def launch_key(l: Dict[str, int]) -> Tuple:
     return tuple(sorted((k, int(v)) for k, v in l.items() if k != "blocks"))
 
 
+# A single untimed pick leaves the default only for a predicted win above this.
+TOP1_MARGIN = 0.05
+
+
+def _launch_distance(l: Dict[str, int], d: Dict[str, int]) -> float:
+    """Steps between two launches in the default rule's own parameters."""
+    step = lambda a, b: abs(np.log2(max(a, 1)) - np.log2(max(b, 1)))
+    return (step(l["team"], d["team"]) + step(l["warps"], d["warps"]) +
+            abs(l["min_blocks"] - d["min_blocks"]) + 2 * abs(l["planes"] - d["planes"]))
+
+
 def evaluate(planner: Planner, rows: Sequence[Row], default: Dict[str, int],
              e2e: bool = False, k: int = SHORTLIST) -> Dict[str, float]:
     """Scores the planner on measured rows of one kind, per setting, against
@@ -263,6 +274,8 @@ def evaluate(planner: Planner, rows: Sequence[Row], default: Dict[str, int],
         if r.e2e == e2e:
             by.setdefault(r.setting, []).append(r)
     regrets, gains, top_gains, timed = [], [], [], []
+    rand_gains, heur_gains, guard_gains = [], [], []
+    rng = np.random.default_rng(12345)
     dkey = launch_key(default)
     for setting, rs in by.items():
         table = {launch_key(r.launch): r for r in rs}
@@ -280,11 +293,31 @@ def evaluate(planner: Planner, rows: Sequence[Row], default: Dict[str, int],
             chosen = min(table[launch_key(l)].ms for l in short)
             top = planner.choose(rs[0].features, launches)
             top_gains.append(table[dkey].ms / table[launch_key(top)].ms)
+            guard = planner.choose(rs[0].features, launches, default=default,
+                                   margin=TOP1_MARGIN)
+            guard_gains.append(table[dkey].ms / table[launch_key(guard)].ms)
             timed.append(len(short))
+            # The same timing budget without the network: k random candidates
+            # plus the default (mean over draws), and the k candidates nearest
+            # the default launch in its own parameters (the rule the default
+            # follows, one step off in team size, warps or budget).
+            others = [l for l in launches if launch_key(l) != dkey]
+            draws = []
+            for _ in range(64):
+                pick = rng.choice(len(others), size=min(k, len(others)), replace=False)
+                draws.append(min([table[dkey].ms] + [table[launch_key(others[i])].ms for i in pick]))
+            rand_gains.append(float(np.exp(np.mean(np.log(table[dkey].ms / np.array(draws))))))
+            near = sorted(others, key=lambda l: _launch_distance(l, default))[:k]
+            heur_gains.append(table[dkey].ms / min([table[dkey].ms] +
+                                                   [table[launch_key(l)].ms for l in near]))
         regrets.append(chosen / best)
         gains.append(table[dkey].ms / chosen)
     gm = lambda v: float(np.exp(np.mean(np.log(v)))) if v else float("nan")
     return {"settings": len(gains), "regret": gm(regrets) - 1.0, "gain_over_default": gm(gains),
             "worst_gain": min(gains) if gains else float("nan"),
-            "top1_gain_over_default": gm(top_gains), "timed_per_setting": float(np.mean(timed)),
+            "top1_gain_over_default": gm(top_gains),
+            "top1_guarded_gain_over_default": gm(guard_gains),
+            "random_shortlist_gain_over_default": gm(rand_gains),
+            "heuristic_shortlist_gain_over_default": gm(heur_gains),
+            "timed_per_setting": float(np.mean(timed)),
             "candidates_per_setting": float(np.mean([len(v) for v in by.values()]))}
