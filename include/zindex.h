@@ -196,6 +196,10 @@ int zx_extract_seeds(zx_index* index, const uint8_t* bases, const uint64_t* offs
 int zx_get_launch(const zx_index* index, zx_launch* out);
 int zx_set_launch(zx_index* index, const zx_launch* launch);
 int zx_default_launch(const zx_index* index, zx_launch* out);
+/* The default launch of the fused kernel's forms (wide = 0): what a launch
+ * that leaves the wide-row form starts from; the same as zx_default_launch
+ * for indexes whose default is not the wide-row form. */
+int zx_default_fused_launch(const zx_index* index, zx_launch* out);
 
 /* Status of the asynchronous zx_query_device / zx_query_device_noalloc calls
  * of this index since the last status call: ZX_OK; ZX_EINVAL when record

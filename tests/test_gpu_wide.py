@@ -112,11 +112,14 @@ def test_wide_form_refuses_what_it_cannot_run(gpu, tmp_path_factory):
         with pytest.raises(zx.ZxError) as err:
             index.set_launch(wide=1, warps=8)  # 2-bit fingerprints
         assert err.value.code == 1
-    ix, _ = _index(tmp_path_factory, 8192, H=3, b=16, k=25)  # about 1,024 chunks per row
+    ix, _ = _index(tmp_path_factory, 6000, H=3, b=16, k=25)  # about 750 chunks per row
     with zx.Index(ix) as index:
         with pytest.raises(zx.ZxError):
             index.set_launch(wide=1, warps=4)  # more than 4 chunks per thread
         index.set_launch(wide=1, warps=8)
+        # Back to the fused kernel: its own default fields, not the wide form's.
+        index.set_launch(wide=0)
+        assert index.launch() == dict(index.default_fused_launch(), blocks=0)
 
 
 def test_wide_form_serves_coalesced_requests(gpu, oracle, tmp_path_factory):

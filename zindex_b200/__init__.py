@@ -215,6 +215,12 @@ class Index:
         _lib.check(_lib.load().zx_default_launch(self._h, byref(l)))
         return self._launch_dict(l)
 
+    def default_fused_launch(self) -> dict:
+        """The default launch with the wide-row form off."""
+        l = ZxLaunch()
+        _lib.check(_lib.load().zx_default_fused_launch(self._h, byref(l)))
+        return self._launch_dict(l)
+
     def set_launch(self, team: int = None, warps: int = None, blocks: int = 0,
                    smem_counters: Optional[int] = None, stage_bytes: Optional[int] = None,
                    stages: Optional[int] = None, bulk: Optional[int] = None,
@@ -230,6 +236,8 @@ class Index:
         if wide is None:
             fused = any(v is not None for v in (team, planes, stage_bytes, split, min_blocks))
             wide = 0 if fused else d["wide"]
+        if not wide and d["wide"]:
+            d = self.default_fused_launch()
         if min_blocks is None and d["min_blocks"] == 1 and (planes == 0 or (stage_bytes or 0) > 0):
             d["min_blocks"] = 2
         l = ZxLaunch(int(d["team"] if team is None else team), int(d["warps"] if warps is None else warps),

@@ -32,7 +32,7 @@ EXPORTED = (
     "zx_server_submit", "zx_server_wait", "zx_server_stats", "zx_server_stop", "zx_mlp_create",
     "zx_mlp_destroy", "zx_mlp_param_count", "zx_mlp_get_params", "zx_mlp_set_params",
     "zx_mlp_loss_grad", "zx_mlp_train", "zx_mlp_predict", "zx_query_per_record",
-    "zx_query_records_report",
+    "zx_query_records_report", "zx_default_fused_launch",
 )
 
 
@@ -108,6 +108,7 @@ def load() -> ctypes.CDLL:
         "zx_get_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
         "zx_set_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
         "zx_default_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
+        "zx_default_fused_launch": (c_int, [c_void_p, POINTER(ZxLaunch)]),
         "zx_set_timing": (c_int, [c_void_p, c_int]),
         "zx_query_status": (c_int, [c_void_p]),
         "zx_last_kernel_ms": (c_int, [c_void_p, POINTER(ctypes.c_float)]),

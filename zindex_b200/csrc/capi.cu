@@ -327,6 +327,13 @@ int zx_default_launch(const zx_index* index, zx_launch* out) {
   });
 }
 
+int zx_default_fused_launch(const zx_index* index, zx_launch* out) {
+  return guarded([&] {
+    zx::check(index && out, zx::kEInval, "null argument");
+    fill_launch(index->engine->default_fused_launch(), out);
+  });
+}
+
 int zx_set_launch(zx_index* index, const zx_launch* l) {
   return guarded([&] {
     zx::check(index && l, zx::kEInval, "null argument");

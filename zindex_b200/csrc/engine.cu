@@ -1050,7 +1050,7 @@ void Engine::set_launch(const QueryLaunch& l) {
   check(!l.wide || wide_eligible(l.warps), kEInval,
         "the wide-row form needs fingerprints of at least 4 bits, a k-mer, minimizer or "
         "modimizer index without strobes, 4 or 8 warps per block and rows of at most "
-        "2 x 32 x warps chunks");
+        "4 x 32 x warps chunks");
   check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
   check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
   std::lock_guard<std::mutex> lock(mu_);
