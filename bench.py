@@ -202,11 +202,17 @@ def launches_per_step(ix, nbases: int, records: int) -> int:
     """Kernels one batched query launches (all compiled into libzindex_b200.so):
     pack, count_tiles, the two kernels of the CUB tile scan and fill_tiles;
     then the fused query kernel and, with shared counters, the counter
-    reduction, once or once per round of a split minimizer query (plus the
-    extraction kernel each round)."""
+    reduction, once or once per round of a split minimizer query or of the
+    wide-row form (plus the extraction kernel each round)."""
     lc, info = ix.launch(), ix.info
     plan = 5
     probe = 1 + (1 if lc["smem_counters"] else 0)
+    tiles_bound = nbases // 256 + records + nbases // 16384 + 1
+    if lc.get("wide"):
+        # Wide-row form: per round the dense extraction, the probe and (with
+        # shared counters) the reduction.
+        rounds = -(-tiles_bound // 262144)
+        return plan + rounds * (1 + probe)
     if lc.get("split") and info.index_mode == 1 and lc["planes"] == 1 and lc["stage_bytes"] == 0:
         tiles_bound = nbases // 256 + records + nbases // 16384 + 1
         rounds = -(-tiles_bound // 262144)

@@ -59,7 +59,7 @@ def test_wide_form_matches_oracle(gpu, oracle, tmp_path_factory, case):
     bases, offsets = zx.pack_records(reads)
     with zx.Index(ix) as index:
         chunks_ok = []
-        for warps in (4, 8):
+        for warps in (4, 8, 9):
             try:
                 index.set_launch(wide=1, warps=warps)
                 chunks_ok.append(warps)

@@ -144,8 +144,14 @@ using DenseExtractFn = void (*)(BatchView, SeedParams, uint64_t*, unsigned long 
 
 // Wide-row probe variant: J chunks per thread, S seeds per step, HQ rows
 // loaded per seed and chunk (16 loads in flight per thread).
-WideFn wide_fn(int J, int HQ) {
-  if (J == 1) return HQ == 8 ? wide_probe_kernel<1, 2, 8, 2> : wide_probe_kernel<1, 4, 4, 2>;
+// Blocks of up to 288 threads (9 warps) keep rows a few partial chunks over
+// 256 or 512 at one or two chunks per thread; their register budget (96 at
+// two blocks per SM) holds 16 loads in flight for one chunk, 8 for two.
+WideFn wide_fn(int J, int HQ, int T) {
+  if (J == 1)
+    return HQ == 8 ? wide_probe_kernel<1, 2, 8, 2, 288> : wide_probe_kernel<1, 4, 4, 2, 288>;
+  if (J == 2 && T > 256)
+    return HQ == 8 ? wide_probe_kernel<2, 1, 8, 2, 288> : wide_probe_kernel<2, 1, 4, 2, 288>;
   if (J == 2) return HQ == 8 ? wide_probe_kernel<2, 1, 8, 2> : wide_probe_kernel<2, 2, 4, 2>;
   if (J == 3) return wide_probe_kernel<3, 1, 4, 2>;
   return wide_probe_kernel<4, 1, 4, 2>;
@@ -878,8 +884,9 @@ QueryLaunch Engine::default_launch() const {
   // up to 256 chunks (4 warps up to 128), up to four beyond; colour counters
   // in shared memory while they leave room for two blocks per SM.
   if (wide_eligible(8) && wide_chunks() >= 128) {
+    const uint32_t nc = wide_chunks();
     l.wide = 1;
-    l.warps = wide_chunks() <= 128 ? 4 : 8;
+    l.warps = nc <= 128 ? 4 : ((nc > 256 && nc <= 288) || (nc > 512 && nc <= 576) ? 9 : 8);
     l.smem_counters = 1;
     if (m_.colors.size() > 16384 || fused_smem_bytes(l) > 110 * 1024) l.smem_counters = 0;
   }
@@ -951,8 +958,9 @@ uint32_t Engine::wide_chunks() const {
 }
 
 bool Engine::wide_eligible(int warps) const {
+  const uint32_t max_j = warps == 9 ? 2u : 4u;
   return m_.fingerprint_bits >= 4 && sp_.mode >= 0 && sp_.mode <= 2 && !sp_.strobe_max &&
-         (warps == 4 || warps == 8) && wide_chunks() <= 4u * (uint32_t)warps * 32u &&
+         (warps == 4 || warps == 8 || warps == 9) && wide_chunks() <= max_j * (uint32_t)warps * 32u &&
          WideSmem::total((uint32_t)m_.colors.size(), host_ix_.classes, m_.hashes, 0) <= 200 * 1024;
 }
 
@@ -996,7 +1004,7 @@ int Engine::max_blocks(const QueryLaunch& l) const {
   if (wide_form(l)) {
     int J, HQ;
     wide_shape(l, J, HQ);
-    WideFn fn = wide_fn(J, HQ);
+    WideFn fn = wide_fn(J, HQ, l.warps * 32);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, l.warps * 32, smem),
                "occupancy");
@@ -1032,7 +1040,8 @@ float Engine::last_fused_ms() {
 void Engine::set_launch(const QueryLaunch& l) {
   check(l.team >= 1 && l.team <= 32 && (l.team & (l.team - 1)) == 0, kEInval,
         "team size must be a power of two in 1..32");
-  check(l.warps >= 1 && l.warps <= 8, kEInval, "warps per block must be in 1..8");
+  check((l.warps >= 1 && l.warps <= 8) || (l.wide && l.warps == 9), kEInval,
+        "warps per block must be in 1..8 (or 9 for the wide-row form)");
   check(l.smem_counters == 0 || m_.colors.size() <= 16384, kEInval,
         "shared-memory counters support at most 16384 colours");
   check(l.stage_bytes == 0 || (l.stage_bytes % 16 == 0 && l.stage_bytes >= 16 * m_.hashes &&
@@ -1049,8 +1058,8 @@ void Engine::set_launch(const QueryLaunch& l) {
   check(l.wide == 0 || l.wide == 1, kEInval, "wide must be 0 or 1");
   check(!l.wide || wide_eligible(l.warps), kEInval,
         "the wide-row form needs fingerprints of at least 4 bits, a k-mer, minimizer or "
-        "modimizer index without strobes, 4 or 8 warps per block and rows of at most "
-        "4 x 32 x warps chunks");
+        "modimizer index without strobes, 4, 8 or 9 warps per block and rows of at most "
+        "4 x 32 x warps chunks (2 x 288 with 9 warps)");
   check(l.warps * 32 * l.min_blocks <= 2048 || l.warps <= 8, kEInval, "too many threads");
   check(fused_smem_bytes(l) <= 227 * 1024, kEInval, "launch needs too much shared memory");
   std::lock_guard<std::mutex> lock(mu_);
@@ -1272,7 +1281,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     ensure_split_capacity(ws);
     int J, HQ;
     wide_shape(l, J, HQ);
-    WideFn wfn = wide_fn(J, HQ);
+    WideFn wfn = wide_fn(J, HQ, l.warps * 32);
     cuda_check(cudaFuncSetAttribute(wfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                "cudaFuncSetAttribute");
     const int ewarps = 4;

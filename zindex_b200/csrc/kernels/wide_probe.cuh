@@ -106,9 +106,11 @@ __device__ __forceinline__ uint32_t wide_group(uint32_t g0, uint32_t p, int b, i
 }
 
 // J: chunks per thread; S: seeds per step; HQ: rows loaded per seed and chunk
-// before the XOR (J * S * HQ 16-byte loads in flight per thread).
-template <int J, int S, int HQ, int MINB>
-__global__ void __launch_bounds__(256, MINB)
+// before the XOR (J * S * HQ 16-byte loads in flight per thread); MAXT: the
+// largest block (256, or 288 so that rows a few partial chunks over 256 or
+// 512 keep one or two chunks per thread).
+template <int J, int S, int HQ, int MINB, int MAXT = 256>
+__global__ void __launch_bounds__(MAXT, MINB)
     wide_probe_kernel(const DevIndex* __restrict__ gix, const ColorLoc* __restrict__ color_loc,
                       const uint64_t* __restrict__ keys,
                       const unsigned long long* __restrict__ nkeys, int smem_counters,
