@@ -112,8 +112,9 @@ METRIC = "query seeds/s"
 # one ncu capture of a slice of the same batch (dram__bytes_read.sum +
 # dram__bytes_write.sum over the seeds of the slice); the line scales them by the
 # seeds of a launch (for a fixed index the traffic grows with the seeds).
-# c2: 12.034 GB read + 7.0 MB written over a 1.2e7-seed slice.
-TRAFFIC_BYTES_PER_SEED = {"c2": 12.041e9 / 1.2e7}
+# c2: 12.034 GB read + 7.0 MB written over a 1.2e7-seed slice; c3: the wide-row probe
+# kernel, 56.050 GB read + 6.7 MB written over a 4,854,580-seed slice (20,000 reads).
+TRAFFIC_BYTES_PER_SEED = {"c2": 12.041e9 / 1.2e7, "c3": 56.0566e9 / 4854580}
 # Per-record form: reads counted one by one, and the compact report threshold.
 PER_RECORD_READS = 200_000
 PER_RECORD_CPU_READS = 20_000

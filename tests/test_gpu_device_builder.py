@@ -26,7 +26,7 @@ CASES = [
     dict(mode="minimizers", k=31, m=21, H=3, b=16),
     dict(mode="modimizers", k=31, H=4, b=4, d=4),
     dict(k=45, H=5, b=32),
-    dict(k=21, H=2, b=1, pattern="##_#_##"),
+    dict(k=11, H=2, b=1, pattern="####_#_####"),
 ]
 
 LAYOUT = ("file", "slots", "row_bits", "routing")

@@ -1285,7 +1285,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     cuda_check(cudaFuncSetAttribute(wfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                "cudaFuncSetAttribute");
     const int ewarps = 4;
-    const size_t esmem = 256 * 8 + ewarps * FusedSmem::warp_bytes(sp_.mode, sp_.k, 0);
+    const size_t esmem = DenseSmem::total(sp_.mode, sp_.k, ewarps);
     DenseExtractFn efn = dense_extract_for(sp_.mode);
     cuda_check(cudaFuncSetAttribute(efn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem),
                "cudaFuncSetAttribute");

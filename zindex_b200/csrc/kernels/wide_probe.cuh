@@ -46,6 +46,21 @@ struct ColorLoc {
   uint32_t group;
 };
 
+// Shared memory of the dense extraction per warp: one tile's keys (and the
+// staging of long k-mer hashes) and, for minimizers, the open-closed
+// minimizer scratch; no probe descriptors. The block adds the 256-entry inner
+// hash table.
+struct DenseSmem {
+  static __host__ __device__ size_t warp_bytes(int mode, int k) {
+    size_t b = FusedSmem::key_bytes(mode, k, false);
+    if (mode == 1) b += 2 * FusedSmem::ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
+    return (b + 15) / 16 * 16;
+  }
+  static __host__ __device__ size_t total(int mode, int k, int warps) {
+    return 256 * 8 + (size_t)warps * warp_bytes(mode, k);
+  }
+};
+
 // Appends the seeds of tiles [tile_lo, tile_hi) (tile_hi 0 = to the end) to
 // out[], one atomic cursor bump per warp and tile. out holds at least
 // (tile_hi - tile_lo) * kTileWindows keys.
@@ -56,9 +71,9 @@ __global__ void extract_dense_kernel(BatchView bv, SeedParams sp, uint64_t* __re
   uint64_t* inner = reinterpret_cast<uint64_t*>(smem);
   uint8_t* p = smem + 256 * 8;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint8_t* wbase = p + (size_t)warp * FusedSmem::warp_bytes(MODE, sp.k, 0, 0, 0, 4, 0, 0, false);
+  uint8_t* wbase = p + (size_t)warp * DenseSmem::warp_bytes(MODE, sp.k);
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
-  uint8_t* ocm = wbase + FusedSmem::key_bytes(MODE, sp.k, false) + FusedSmem::probe_bytes(0);
+  uint8_t* ocm = wbase + FusedSmem::key_bytes(MODE, sp.k, false);
   build_inner_table(sp, inner);
   __syncthreads();
   uint32_t ntiles = *bv.ntiles;
