@@ -100,15 +100,17 @@ def test_planner_gain_over_default_and_regret(gpu):
     guarded = gm([r["top1_guarded_gain_over_default"] for r in dev])
     rand = gm([r["random_shortlist_gain_over_default"] for r in dev])
     heur = gm([r["heuristic_shortlist_gain_over_default"] for r in dev])
+    wide = gm([r["network_over_all_launches_gain_over_default"] for r in dev])
     print(f"launch: gain over the default {gain:.3f}, regret {regret:.3f} with {timed:.1f} of "
-          f"{cands:.0f} candidates timed (network's top pick alone: {top1:.3f}, guarded by a "
-          f"{pl.TOP1_MARGIN:.0%} margin: {guarded:.3f}); the same budget without the network: "
-          f"random shortlist {rand:.3f}, nearest-to-default shortlist {heur:.3f}; "
-          f"cut: gain over the default {e2e_gain:.3f}")
-    # What the network earns: its shortlist against untrained shortlists of
-    # the same size (both also time the default).
-    assert gain >= rand and gain >= heur - 0.005
-    assert guarded >= 0.99
+          f"{cands:.0f} candidates timed (network ranking every launch: {wide:.3f}; its top "
+          f"pick alone, untimed: {top1:.3f}, guarded by a {pl.TOP1_MARGIN:.0%} margin: "
+          f"{guarded:.3f}); the same budget without the network: random shortlist {rand:.3f}, "
+          f"nearest-to-default shortlist {heur:.3f}; cut: gain over the default {e2e_gain:.3f}")
+    # What the network earns: its shortlist (ranking the default's
+    # neighbourhood) against untrained shortlists of the same size, all of
+    # which also time the default.
+    assert gain > rand
+    assert gain >= heur - 0.01
     # The default launch is itself fitted to these measurements, so the gain
     # is over a strong baseline; the shortlist can only match or beat it.
     assert gain >= 1.02

@@ -461,13 +461,16 @@ Workspace::~Workspace() {
                  keys_count, error,    fstate,    hp_starts, hp_keep,    hp_pos,
                  hp_bases,   hp_offsets, hp_scan_tmp, seg_blocks, seg_tiles, seg_records,
                  rec_counts, rec_totals, rec_hits, rec_first, rec_scan_tmp, hit_colors,
-                 hit_counts, split_keys, split_counts, wide_cursor};
+                 hit_counts, split_keys, split_counts, wide_cursor, wide_keys2};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total, h_seg_blocks, h_seg_records};
   for (void* p : host)
     if (p) cudaFreeHost(p);
   if (seg_staged) cudaEventDestroy(seg_staged);
+  for (cudaEvent_t e : {wide_fork, wide_ext[0], wide_ext[1], wide_probe[0], wide_probe[1]})
+    if (e) cudaEventDestroy(e);
+  if (aux_stream) cudaStreamDestroy(aux_stream);
   for (cudaEvent_t e : chunk_events) cudaEventDestroy(e);
   if (copy_stream) cudaStreamDestroy(copy_stream);
   if (stream) cudaStreamDestroy(stream);
@@ -1079,6 +1082,8 @@ void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
   const uint64_t colors = m_.colors.size();
   // Split minimizer and wide-row queries: key slots allocated before any graph capture.
   if (kernel_mode(launch_) == 4 || wide_form(launch_)) ensure_split_capacity(ws);
+  if (wide_form(launch_) && nbases / kTileWindows + records + nbases / kFindereTask + 1 > kSplitTiles)
+    ensure_wide_pipeline(ws);
   if (nbases > ws.cap_bases || !ws.bases) {
     uint64_t cap = std::max<uint64_t>({nbases, ws.cap_bases * 3 / 2, 4096});
     cap = round_up(cap, 4096);
@@ -1292,15 +1297,34 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     const int egrid = (int)std::min<uint64_t>((kSplitTiles + ewarps - 1) / ewarps,
                                               (uint64_t)sms_ * 8);
     const int wblocks = l.blocks > 0 ? std::min(l.blocks, blocks_cap) : blocks_cap;
-    for (uint64_t lo = 0; lo < tiles_bound; lo += kSplitTiles) {
+    const uint64_t rounds = (tiles_bound + kSplitTiles - 1) / kSplitTiles;
+    // Several rounds: extraction (compute-bound) of round r + 1 runs on the
+    // auxiliary stream beside the probe (memory-bound) of round r, the rounds
+    // alternating between two key lists; events order each list's reuse.
+    const bool overlap = rounds > 1;
+    if (overlap) ensure_wide_pipeline(ws);
+    cudaStream_t xs = overlap ? ws.aux_stream : s;
+    if (overlap) {
+      cuda_check(cudaEventRecord(ws.wide_fork, s), "cudaEventRecord");
+      cuda_check(cudaStreamWaitEvent(xs, ws.wide_fork, 0), "cudaStreamWaitEvent");
+    }
+    for (uint64_t r = 0; r < rounds; ++r) {
+      const int b = overlap ? (int)(r & 1) : 0;
+      uint64_t* keys = b ? ws.wide_keys2 : ws.split_keys;
       BatchView rb = bv;
-      rb.tile_lo = (uint32_t)lo;
-      rb.tile_hi = (uint32_t)std::min<uint64_t>(lo + kSplitTiles, tiles_bound);
-      cuda_check(cudaMemsetAsync(ws.wide_cursor, 0, 8, s), "memset");
-      efn<<<egrid, ewarps * 32, esmem, s>>>(rb, sp_, ws.split_keys, ws.wide_cursor, ewarps);
+      rb.tile_lo = (uint32_t)(r * kSplitTiles);
+      rb.tile_hi = (uint32_t)std::min<uint64_t>((r + 1) * kSplitTiles, tiles_bound);
+      if (overlap && r >= 2)
+        cuda_check(cudaStreamWaitEvent(xs, ws.wide_probe[b], 0), "cudaStreamWaitEvent");
+      cuda_check(cudaMemsetAsync(ws.wide_cursor + b, 0, 8, xs), "memset");
+      efn<<<egrid, ewarps * 32, esmem, xs>>>(rb, sp_, keys, ws.wide_cursor + b, ewarps);
       cuda_check(cudaGetLastError(), "extract_dense_kernel");
+      if (overlap) {
+        cuda_check(cudaEventRecord(ws.wide_ext[b], xs), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(s, ws.wide_ext[b], 0), "cudaStreamWaitEvent");
+      }
       wfn<<<wblocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, d_color_loc_,
-                                              ws.split_keys, ws.wide_cursor, l.smem_counters,
+                                              keys, ws.wide_cursor + b, l.smem_counters,
                                               ws.partial, counts, total);
       cuda_check(cudaGetLastError(), "wide_probe_kernel");
       if (l.smem_counters) {
@@ -1308,6 +1332,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
             ws.partial, wblocks, colors, counts);
         cuda_check(cudaGetLastError(), "reduce_counters_kernel");
       }
+      if (overlap) cuda_check(cudaEventRecord(ws.wide_probe[b], s), "cudaEventRecord");
     }
     if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
     return;
@@ -1349,11 +1374,21 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
 }
 
+void Engine::ensure_wide_pipeline(Workspace& ws) {
+  if (ws.aux_stream) return;
+  dev_alloc(&ws.wide_keys2, kSplitTiles * kTileWindows, "second dense key list");
+  cuda_check(cudaStreamCreateWithFlags(&ws.aux_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (cudaEvent_t* e : {&ws.wide_fork, &ws.wide_ext[0], &ws.wide_ext[1], &ws.wide_probe[0],
+                         &ws.wide_probe[1]})
+    cuda_check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+  ws.release_graphs();
+}
+
 void Engine::ensure_split_capacity(Workspace& ws) {
   if (ws.split_keys) return;
   dev_alloc(&ws.split_keys, kSplitTiles * kTileWindows, "split key slots");
   dev_alloc(&ws.split_counts, kSplitTiles, "split key counts");
-  dev_alloc(&ws.wide_cursor, 1, "dense key cursor");
+  dev_alloc(&ws.wide_cursor, 2, "dense key cursors");
   ws.release_graphs();
 }
 

@@ -68,7 +68,10 @@ struct Workspace {
   // Split minimizer queries: key slots of one round of tiles.
   uint64_t* split_keys = nullptr;
   uint32_t* split_counts = nullptr;
-  unsigned long long* wide_cursor = nullptr;  // wide-row queries: keys in the dense list
+  unsigned long long* wide_cursor = nullptr;  // wide-row queries: keys in the dense lists (2)
+  uint64_t* wide_keys2 = nullptr;  // second dense key list (rounds alternate)
+  cudaStream_t aux_stream = nullptr;  // wide-row queries: extraction beside the probe
+  cudaEvent_t wide_fork = nullptr, wide_ext[2] = {}, wide_probe[2] = {};
   // Per-record queries: counters of one record group (records x colours).
   uint64_t* rec_counts = nullptr;
   unsigned long long* rec_totals = nullptr;
@@ -245,6 +248,9 @@ class Engine {
   // seeds) for split minimizer queries.
   int kernel_mode(const QueryLaunch& l) const;
   void ensure_split_capacity(Workspace& ws);
+  // Wide-row queries of several rounds: the second key list, the auxiliary
+  // stream and the events of the extraction / probe pipeline.
+  void ensure_wide_pipeline(Workspace& ws);
   // Runs host records in device groups (one segment per record): after each
   // group's launch, on_group(r0, n) enqueues its read-back on ws.stream; the
   // stream is then synchronised and the error word checked.
