@@ -26,6 +26,7 @@ CASES = [
     dict(colors=1000, H=3, b=32, mode="modimizers", k=31, d=4),
     dict(colors=800, H=4, b=8, k=45, groups="3,4"),
     dict(colors=300, H=13, b=4, k=21),
+    dict(colors=256, H=4, b=8, k=31),     # rows of few chunks: teams of 32 threads
     dict(colors=6000, H=8, b=4, k=25),    # three chunks per thread with 8 warps
     dict(colors=4000, H=3, b=16, k=25),  # four chunks per thread with 8 warps
 ]

@@ -139,7 +139,8 @@ FusedFn fused_for(int mode, const QueryLaunch& l) {
 }
 
 using WideFn = void (*)(const DevIndex*, const ColorLoc*, const uint64_t*,
-                       const unsigned long long*, int, uint32_t*, uint64_t*, unsigned long long*);
+                       const unsigned long long*, int, uint32_t, uint32_t*, uint64_t*,
+                       unsigned long long*);
 using DenseExtractFn = void (*)(BatchView, SeedParams, uint64_t*, unsigned long long*, int);
 
 // Wide-row probe variant: J chunks per thread, S seeds per step, HQ rows
@@ -969,9 +970,17 @@ bool Engine::wide_eligible(int warps) const {
 
 bool Engine::wide_form(const QueryLaunch& l) const { return l.wide && wide_eligible(l.warps); }
 
-void Engine::wide_shape(const QueryLaunch& l, int& J, int& HQ) const {
-  const uint32_t T = (uint32_t)l.warps * 32u;
-  J = (int)((wide_chunks() + T - 1) / T);
+void Engine::wide_shape(const QueryLaunch& l, int& J, int& HQ, uint32_t* team) const {
+  const uint32_t T = (uint32_t)l.warps * 32u, nc = wide_chunks();
+  // Rows of at most half a block of chunks: teams of the next power of two of
+  // threads, one chunk each; wider rows: the whole block.
+  uint32_t tt = T;
+  if (2 * nc <= T) {
+    tt = 1;
+    while (tt < nc) tt <<= 1;
+  }
+  if (team) *team = tt;
+  J = (int)((nc + tt - 1) / tt);
   const int Hp = (m_.hashes + 3) & ~3;
   HQ = Hp % 8 == 0 && J <= 2 ? 8 : 4;
 }
@@ -1285,7 +1294,8 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     // probe counts them, and the block counters are added up.
     ensure_split_capacity(ws);
     int J, HQ;
-    wide_shape(l, J, HQ);
+    uint32_t wteam = 0;
+    wide_shape(l, J, HQ, &wteam);
     WideFn wfn = wide_fn(J, HQ, l.warps * 32);
     cuda_check(cudaFuncSetAttribute(wfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                "cudaFuncSetAttribute");
@@ -1324,7 +1334,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
         cuda_check(cudaStreamWaitEvent(s, ws.wide_ext[b], 0), "cudaStreamWaitEvent");
       }
       wfn<<<wblocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, d_color_loc_,
-                                              keys, ws.wide_cursor + b, l.smem_counters,
+                                              keys, ws.wide_cursor + b, l.smem_counters, wteam,
                                               ws.partial, counts, total);
       cuda_check(cudaGetLastError(), "wide_probe_kernel");
       if (l.smem_counters) {

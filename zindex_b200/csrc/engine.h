@@ -136,7 +136,7 @@ class Engine {
   uint32_t wide_chunks() const;
   bool wide_eligible(int warps) const;
   bool wide_form(const QueryLaunch& l) const;
-  void wide_shape(const QueryLaunch& l, int& J, int& HQ) const;
+  void wide_shape(const QueryLaunch& l, int& J, int& HQ, uint32_t* team = nullptr) const;
   size_t fused_smem_bytes(const QueryLaunch& l) const;
   int max_blocks(const QueryLaunch& l) const;
   // Bytes of fingerprint planes gathered per seed, summed over classes.

@@ -129,8 +129,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
     wide_probe_kernel(const DevIndex* __restrict__ gix, const ColorLoc* __restrict__ color_loc,
                       const uint64_t* __restrict__ keys,
                       const unsigned long long* __restrict__ nkeys, int smem_counters,
-                      uint32_t* __restrict__ partial, uint64_t* __restrict__ counts,
-                      unsigned long long* __restrict__ total) {
+                      uint32_t team_threads, uint32_t* __restrict__ partial,
+                      uint64_t* __restrict__ counts, unsigned long long* __restrict__ total) {
   extern __shared__ __align__(16) uint8_t smem[];
   DevIndex* six = reinterpret_cast<DevIndex*>(smem);
   uint8_t* p = smem + FusedSmem::ix_bytes;
@@ -153,6 +153,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
   const uint32_t fmask = b == 32 ? 0xFFFFFFFFu : (1u << b) - 1u;
   const uint32_t per_seed = classes * (uint32_t)Hp;
   const uint32_t T = blockDim.x, tid = threadIdx.x;
+  // Teams of TT threads (the whole block for wide rows; fewer threads for
+  // rows of few chunks, each team then walking its own share of the round's
+  // seeds). Thread tt of a team owns chunks tt, tt + TT, ...
+  const uint32_t TT = team_threads && team_threads < T ? team_threads : T;
+  const uint32_t tt = tid % TT, team = tid / TT, teams = T / TT;
 
   // The chunks this thread owns, their class and masks.
   const uint8_t* col[J];
@@ -164,7 +169,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
     stride[j] = roff[j] = g0[j] = valid[j] = multi[j] = cls[j] = 0;
 #pragma unroll
     for (int k = 0; k < kWidePlanes; ++k) planes[j][k] = 0;
-    uint32_t g = tid + (uint32_t)j * T, start = 0;
+    uint32_t g = tt + (uint32_t)j * TT, start = 0;
     for (uint32_t ci = 0; ci < classes; ++ci) {
       const DevClass& C = ix.cls[ci];
       if (g < start + C.fp_chunks) {
@@ -260,7 +265,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
     if (tid == 0) seeds += n;
     __syncthreads();
-    for (uint32_t s0 = 0; s0 < n; s0 += S) {
+    const uint32_t per = (n + teams - 1) / teams;
+    const uint32_t lo = min(n, team * per), hi = min(n, lo + per);
+    for (uint32_t s0 = lo; s0 < hi; s0 += S) {
       uint4 acc[J][S];
 #pragma unroll
       for (int j = 0; j < J; ++j)
@@ -270,8 +277,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
         uint4 v[J][S][HQ];
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-          const uint32_t sd = min(s0 + (uint32_t)s, n - 1);
-          const bool live = s0 + (uint32_t)s < n;
+          const uint32_t sd = min(s0 + (uint32_t)s, hi - 1);
+          const bool live = s0 + (uint32_t)s < hi;
 #pragma unroll
           for (int j = 0; j < J; ++j) {
             uint32_t ri[HQ];
@@ -300,7 +307,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
       for (int s = 0; s < S; ++s) {
         const uint32_t sd = s0 + (uint32_t)s;
-        if (sd >= n) continue;
+        if (sd >= hi) continue;
         const uint32_t pat = pattern[sd];
 #pragma unroll
         for (int j = 0; j < J; ++j) {
