@@ -204,7 +204,9 @@ def launches_per_step(ix, nbases: int, records: int) -> int:
     pack, count_tiles, the two kernels of the CUB tile scan and fill_tiles;
     then the fused query kernel and, with shared counters, the counter
     reduction, once or once per round of a split minimizer query or of the
-    wide-row form (plus the extraction kernel each round)."""
+    wide-row form (plus the extraction kernel each round, and for ordered
+    wide rounds the CUB radix sort's kernels: histogram, scan and three
+    onesweep passes over 20 bits)."""
     lc, info = ix.launch(), ix.info
     plan = 5
     probe = 1 + (1 if lc["smem_counters"] else 0)
@@ -213,7 +215,8 @@ def launches_per_step(ix, nbases: int, records: int) -> int:
         # Wide-row form: per round the dense extraction, the probe and (with
         # shared counters) the reduction.
         rounds = -(-tiles_bound // 262144)
-        return plan + rounds * (1 + probe)
+        sort = 5 if lc.get("order") else 0
+        return plan + rounds * (1 + sort + probe)
     if lc.get("split") and info.index_mode == 1 and lc["planes"] == 1 and lc["stage_bytes"] == 0:
         tiles_bound = nbases // 256 + records + nbases // 16384 + 1
         rounds = -(-tiles_bound // 262144)
@@ -271,7 +274,12 @@ def planned_form(ix, bases, offsets, seeds, step_ms, e2e_ms):
     default = dict(ix.default_launch(), blocks=0)
     lengths = np.diff(offsets.astype(np.int64))
     feats = tn.Autotuner.features(ix, lengths, seeds)
-    cands = [dict(default, **l, stage_bytes=0) for l in tn.REGISTER_LAUNCHES]
+    # The network's candidates are the fused kernel's launches; an index whose
+    # default is the wide-row form has that default as one more candidate.
+    fused = dict(ix.default_fused_launch(), blocks=0)
+    cands = [dict(fused, **l, stage_bytes=0, wide=0) for l in tn.REGISTER_LAUNCHES]
+    if default["wide"]:
+        cands.append(default)
     timed = {}
 
     def timed_ms(launch):
@@ -296,11 +304,11 @@ def planned_form(ix, bases, offsets, seeds, step_ms, e2e_ms):
     t_pick = timed_ms(pick)
     t_default = timed_ms(default)
     return pick, {
-        "chosen": {k: pick[k] for k in ("team", "warps", "min_blocks", "planes", "cut")},
+        "chosen": {k: pick[k] for k in ("team", "warps", "min_blocks", "planes", "cut", "wide")},
         "ms_per_step": t_pick, "default_ms_per_step": t_default,
         "exhaustive_best_ms_per_step": timed[best_key],
-        "exhaustive_best": dict((k, v) for k, v in best_key if k in ("team", "warps", "min_blocks",
-                                                                      "planes")),
+        "exhaustive_best": dict((k, v) for k, v in best_key
+                                if k in ("team", "warps", "min_blocks", "planes", "wide")),
         "regret": t_pick / timed[best_key] - 1.0, "gain_over_default": t_default / t_pick,
         "timed": len(short), "cuts_timed": len(cuts), "candidates": len(cands),
         "train_rows": len(rows),
@@ -324,25 +332,8 @@ def served_form(zx, ix, requests_closed, requests_open, rate):
         out["closed_loop"] = {"requests": len(tickets), "seconds": dt, "seeds_per_s": seeds / dt,
                               "bases_per_s": st["bases"] / dt, "batches": st["batches"],
                               "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3}
-        rng = np.random.default_rng(5)
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(requests_open)))
-        tickets = [None] * len(requests_open)
-        start = time.perf_counter()
-
-        def submitter():
-            for i, (b, o) in enumerate(requests_open):
-                delay = start + arrivals[i] - time.perf_counter()
-                if delay > 0:
-                    time.sleep(delay)
-                tickets[i] = server.submit(b, o)
-
-        th = threading.Thread(target=submitter)
-        th.start()
-        th.join()
-        seeds = sum(server.wait(t)[1] for t in tickets)
-        dt = time.perf_counter() - start
-        st = server.stats(reset=True)
-        out["poisson"] = {"rate_req_per_s": rate, "requests": len(tickets), "seconds": dt,
+        dt, seeds, st = poisson_run(server, requests_open, rate, 5)
+        out["poisson"] = {"rate_req_per_s": rate, "requests": len(requests_open), "seconds": dt,
                           "seeds_per_s": seeds / dt, "batches": st["batches"],
                           "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
                           "max_ms": st["max_s"] * 1e3,
@@ -862,6 +853,9 @@ def main():
                     help="query only the first N reads (smaller case for profiler captures)")
     ap.add_argument("--slice", type=int, default=None,
                     help="profiler case: three plain launches over the first N reads, no timing")
+    ap.add_argument("--serve-sweep", action="store_true",
+                    help="serving rate sweep: p50/p99 latency against the offered Poisson rate "
+                         "and the sustainable request rate of the config (one JSON line)")
     args = ap.parse_args()
     global CONFIG, WORKLOAD
     CONFIG = CONFIGS[args.config]
@@ -870,10 +864,103 @@ def main():
         args.warmup = 3
     if args.slice:
         profile_slice(args)
+    elif args.serve_sweep:
+        serve_sweep(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:
         ours(args)
+
+
+def poisson_run(server, requests, rate, seed):
+    """Requests submitted at Poisson arrivals of `rate` per second; returns
+    the seconds from the first arrival to the last completion, the seeds and
+    the server's latency statistics."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(requests)))
+    tickets = [None] * len(requests)
+    server.stats(reset=True)
+    start = time.perf_counter()
+
+    def submitter():
+        for i, (b, o) in enumerate(requests):
+            delay = start + arrivals[i] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            tickets[i] = server.submit(b, o)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    seeds = sum(server.wait(t)[1] for t in tickets)
+    return time.perf_counter() - start, seeds, server.stats(reset=True)
+
+
+# A rate is sustained when the p99 latency stays within this many times the
+# p50 service time of a request served alone and the server completes at
+# least SUSTAIN_FRACTION of the offered rate.
+SUSTAIN_LATENCY = 10.0
+SUSTAIN_FRACTION = 0.9
+
+
+def serve_sweep(args):
+    """Serving rate sweep on the config's request mix (half 1-10,000 short
+    reads, half 1-10 long records): the service time of a request alone, the
+    closed-loop capacity, then open Poisson streams at fractions of that
+    capacity and at the config's stated rate. The sustainable rate is the
+    highest swept rate at which the p99 latency stays within SUSTAIN_LATENCY
+    x the alone-p50 and completions keep up with arrivals."""
+    import torch
+
+    build_native()
+    import zindex_b200 as zx
+
+    cache = Path(args.cache)
+    index_dir, bases, offsets = prepare(cache, 0, args.config)
+    lb, lo = long_pool(cache, 0, args.config)
+    sv = CONFIG.get("served", {"closed": 400, "open": 1000, "rate": 200.0})
+    pool = make_requests(bases, offsets, lb, lo, 400, 31)
+    out = {"config": dict(WORKLOAD), "mix": "half 1-10,000 reads of the batch, half 1-10 long "
+           "records (lognormal, median 30 kbp)", "sustain_rule": {
+               "p99_within_alone_p50_x": SUSTAIN_LATENCY, "completed_over_offered_min":
+               SUSTAIN_FRACTION}}
+    with zx.Index(index_dir) as ix, zx.Server(ix, slots=3) as server:
+        out["launch"] = ix.launch()
+        for b, o in pool[:10]:  # warm-up
+            server.wait(server.submit(b, o))
+        alone = []
+        for b, o in pool[10:50]:
+            alone.append(server.wait(server.submit(b, o))[2])
+        alone_p50 = float(np.median(alone))
+        out["alone"] = {"requests": len(alone), "p50_ms": alone_p50 * 1e3,
+                        "p99_ms": float(np.percentile(alone, 99)) * 1e3}
+        server.stats(reset=True)
+        t0 = time.perf_counter()
+        tickets = [server.submit(b, o) for b, o in pool[:sv["closed"]]]
+        seeds = sum(server.wait(t)[1] for t in tickets)
+        dt = time.perf_counter() - t0
+        capacity = len(tickets) / dt
+        out["closed_loop"] = {"requests": len(tickets), "req_per_s": capacity,
+                              "seeds_per_s": seeds / dt}
+        rates = sorted({round(capacity * f, 1) for f in (0.2, 0.4, 0.6, 0.8, 0.9, 1.0, 1.1)} |
+                       {float(sv["rate"])})
+        rows, sustained = [], 0.0
+        for i, rate in enumerate(rates):
+            n = int(min(len(pool), max(60, rate * 4)))
+            reqs = [pool[j % len(pool)] for j in range(n)]
+            dt, seeds, st = poisson_run(server, reqs, rate, 100 + i)
+            achieved = st["completed"] / dt
+            ok = st["p99_s"] <= SUSTAIN_LATENCY * alone_p50 and achieved >= SUSTAIN_FRACTION * rate
+            if ok:
+                sustained = max(sustained, rate)
+            rows.append({"offered_req_per_s": rate, "requests": n, "completed_req_per_s": achieved,
+                         "seeds_per_s": seeds / dt, "p50_ms": st["p50_s"] * 1e3,
+                         "p99_ms": st["p99_s"] * 1e3, "max_ms": st["max_s"] * 1e3,
+                         "batches": st["batches"], "sustained": bool(ok)})
+        out["rates"] = rows
+        out["sustainable_req_per_s"] = sustained
+        out["stated_rate_req_per_s"] = float(sv["rate"])
+    print(json.dumps({"serve_sweep": out}))
 
 
 def profile_slice(args):

@@ -81,6 +81,10 @@ typedef struct zx_launch {
                          are extracted into a dense list and probed by blocks whose threads
                          each own fixed 16-byte chunks of every row, counting in registers;
                          team, planes, stage_bytes and split are then unused */
+  int order;          /* wide-row form, unsegmented queries: 1 = each round's seeds are sorted
+                         by their first hash before the probe (every class's row index grows
+                         with it, so consecutive seeds read neighbouring rows); ignored
+                         elsewhere. Counts do not depend on it */
 } zx_launch;
 
 /* Thread-local message of the last failed call on this thread. */
@@ -254,10 +258,13 @@ typedef struct zx_server_report {
   double p50_s, p99_s, mean_s, max_s; /* submit-to-completion latency */
   double elapsed_s;                   /* since start or the last reset */
   uint64_t device_bytes;              /* device memory held by the slots */
+  uint64_t pinned_bytes;              /* page-locked host memory: the request ring
+                                         ((slots + 2) x slot_bases) and the slots */
 } zx_server_report;
 
 int zx_server_start(zx_index* index, const zx_server_options* options, zx_server** out);
-/* Queue one request (host buffers, copied before returning); ZX_EINVAL if it
+/* Queue one request (host buffers, copied before returning into the server's
+ * page-locked ring, waiting while the ring is full); ZX_EINVAL if it
  * does not fit one batch slot. */
 int zx_server_submit(zx_server* server, const uint8_t* bases, const uint64_t* offsets,
                      uint64_t records, int recover, uint64_t* ticket);

@@ -7,7 +7,8 @@ cover every fingerprint width it takes (4, 8, 16, 32), hash counts whose
 row loads fold by 4 and by 8 (H 2, 3, 5, 8, 13), one and two chunks per
 thread, multi-member groups, hash partitions, several size classes, k-mers
 (short and long), minimizers and modimizers, recovery on and off, shared and
-global colour counters, and device batches replayed from a CUDA graph.
+global colour counters, seeds probed in extraction order and sorted by
+their first hash, and device batches replayed from a CUDA graph.
 """
 import numpy as np
 import pytest
@@ -70,11 +71,11 @@ def test_wide_form_matches_oracle(gpu, oracle, tmp_path_factory, case):
         for recover in (True, False):
             want, want_total = oracle.query_records(ix, bases, offsets, recover=recover)
             for warps in chunks_ok:
-                for counters in (1, 0):
-                    index.set_launch(wide=1, warps=warps, smem_counters=counters)
-                    assert index.launch()["wide"] == 1
+                for counters, order in ((1, 1), (1, 0), (0, 1)):
+                    index.set_launch(wide=1, warps=warps, smem_counters=counters, order=order)
+                    assert index.launch()["wide"] == 1 and index.launch()["order"] == order
                     got, total = index.query_records(bases, offsets, recover=recover)
-                    assert total == want_total, (warps, counters, recover)
+                    assert total == want_total, (warps, counters, order, recover)
                     np.testing.assert_array_equal(got, want)
 
 
@@ -124,10 +125,12 @@ def test_wide_form_refuses_what_it_cannot_run(gpu, tmp_path_factory):
 
 
 def test_wide_form_serves_coalesced_requests(gpu, oracle, tmp_path_factory):
-    """Coalesced requests on a wide-row index (each request its own wide-form
-    launch sequence) and the request server on it: every request's counts are
-    the oracle's for that request alone, and a batch of more requests than
-    the per-request path takes goes through the fused segmented launch."""
+    """Coalesced requests on a wide-row index (one segmented wide-form query:
+    each request's seeds in its own part of the key list, probe rounds that
+    never straddle requests, each block's counters added to the request it
+    leaves) and the request server on it: every request's counts are the
+    oracle's for that request alone, with shared and global counters and on
+    rows of few chunks (teams of threads)."""
     import threading
 
     import torch
@@ -140,7 +143,8 @@ def test_wide_form_serves_coalesced_requests(gpu, oracle, tmp_path_factory):
     with zx.Index(ix) as index:
         assert index.launch()["wide"] == 1
         dev = torch.device("cuda", 0)
-        for part in (reqs[:20], reqs):  # 20 requests: per request; 90: fused segmented
+        for counters, part in ((1, reqs[:20]), (1, reqs), (0, reqs)):
+            index.set_launch(wide=1, smem_counters=counters)
             flat = [r for recs in part for r in recs]
             seg = np.zeros(len(part) + 1, dtype=np.uint64)
             seg[1:] = np.cumsum([len(recs) for recs in part])
@@ -157,6 +161,7 @@ def test_wide_form_serves_coalesced_requests(gpu, oracle, tmp_path_factory):
                 want, want_total = oracle.query_records(ix, *zx.pack_records(part[i]))
                 assert int(got_t[i]) == want_total, i
                 np.testing.assert_array_equal(got[i], want, err_msg=f"request {i}")
+        index.set_launch(wide=1)
         with zx.Server(index, slots=3, slot_bases=200000, slot_requests=7) as server:
             tickets = [None] * len(reqs)
 
@@ -174,3 +179,81 @@ def test_wide_form_serves_coalesced_requests(gpu, oracle, tmp_path_factory):
         want, want_total = oracle.query_records(ix, *zx.pack_records(reqs[i]))
         assert results[i][1] == want_total, i
         np.testing.assert_array_equal(results[i][0], want, err_msg=f"served request {i}")
+
+
+@pytest.mark.parametrize("colors,opts", [(2048, dict(H=3, b=16, k=31)), (256, dict(H=4, b=8, k=31))],
+                         ids=["c2048-b16", "c256-teams"])
+def test_wide_segments_across_extraction_rounds(gpu, oracle, tmp_path_factory, colors, opts):
+    """A segmented wide-row query of more tiles than one extraction round
+    holds (two rounds on two key lists, the second extracted beside the
+    first's probe): 1,000 requests of 300 short records, one of them cut by
+    the round boundary. The requests' counts add up to the oracle's count of
+    the whole batch, and a sample (the boundary's requests among them) equals
+    the oracle's per request. The same batch unsegmented (seeds sorted per
+    round, and in extraction order) gives the oracle's count."""
+    import torch
+
+    import zindex_b200 as zx
+
+    ix, genomes = _index(tmp_path_factory, colors, **opts)
+    rng = np.random.default_rng(21)
+    n_req, per = 1000, 300
+    reads = sample_reads(genomes, rng, n_req * per, 40, n_runs=0.05)
+    bases, offsets = zx.pack_records(reads)
+    seg = (np.arange(n_req + 1, dtype=np.uint64) * per).astype(np.uint64)
+    dev = torch.device("cuda", 0)
+    d_bases = torch.from_numpy(bases).to(dev)
+    d_off = torch.from_numpy(offsets.view(np.int64)).to(dev)
+    with zx.Index(ix) as index:
+        index.set_launch(wide=1)
+        counts = torch.zeros((n_req, index.colors), dtype=torch.int64, device=dev)
+        totals = torch.zeros(n_req, dtype=torch.int64, device=dev)
+        index.query_segments(d_bases.data_ptr(), len(bases), d_off.data_ptr(), len(reads), seg,
+                             counts.data_ptr(), totals.data_ptr())
+        torch.cuda.synchronize(dev)
+        got, got_t = counts.cpu().numpy().astype(np.uint64), totals.cpu().numpy()
+        # The same batch unsegmented: two ordered rounds, and two in
+        # extraction order.
+        whole = []
+        for order in (1, 0):
+            index.set_launch(wide=1, order=order)
+            c1 = torch.zeros(index.colors, dtype=torch.int64, device=dev)
+            t1 = torch.zeros(1, dtype=torch.int64, device=dev)
+            index.query_device(d_bases.data_ptr(), len(bases), d_off.data_ptr(), len(reads),
+                               c1.data_ptr(), t1.data_ptr())
+            torch.cuda.synchronize(dev)
+            whole.append((c1.cpu().numpy().astype(np.uint64), int(t1.item())))
+    want, want_total = oracle.query_records(ix, bases, offsets)
+    assert int(got_t.sum()) == want_total
+    np.testing.assert_array_equal(got.sum(axis=0, dtype=np.uint64), want)
+    for c1, t1 in whole:
+        assert t1 == want_total
+        np.testing.assert_array_equal(c1, want)
+    boundary = (1 << 18) // per  # one tile per 40-base record; 2^18 tiles per round
+    for i in sorted({0, 1, boundary - 1, boundary, boundary + 1, n_req - 1, 417}):
+        sub = reads[i * per:(i + 1) * per]
+        w, wt = oracle.query_records(ix, *zx.pack_records(sub))
+        assert int(got_t[i]) == wt, i
+        np.testing.assert_array_equal(got[i], w, err_msg=f"request {i}")
+
+
+def test_wide_form_per_record(gpu, oracle, tmp_path_factory):
+    """Per-record queries on a wide-row index (one segment per record, most
+    records one probe round, so one block writes their counters) equal the
+    oracle's query of each record alone."""
+    import zindex_b200 as zx
+
+    ix, genomes = _index(tmp_path_factory, 2048, H=3, b=16, k=31)
+    rng = np.random.default_rng(31)
+    recs = sample_reads(genomes, rng, 150, 150, n_runs=0.1)
+    recs += sample_reads(genomes, rng, 12, 2500) + [b"", b"ACGT", b"N" * 60]
+    order = rng.permutation(len(recs))
+    recs = [recs[i] for i in order]
+    bases, offsets = zx.pack_records(recs)
+    with zx.Index(ix) as index:
+        assert index.launch()["wide"] == 1
+        counts, totals = index.query_per_record(bases, offsets)
+    for i, r in enumerate(recs):
+        want, want_total = oracle.query_records(ix, *zx.pack_records([r]))
+        assert int(totals[i]) == want_total, i
+        np.testing.assert_array_equal(counts[i], want, err_msg=f"record {i}")

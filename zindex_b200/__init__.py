@@ -203,7 +203,8 @@ class Index:
         return {"team": l.team, "warps": l.warps, "blocks": l.blocks,
                 "smem_counters": l.smem_counters, "stage_bytes": l.stage_bytes,
                 "stages": l.stages, "bulk": l.bulk, "min_blocks": l.min_blocks,
-                "planes": l.planes, "cut": l.cut, "split": l.split, "wide": l.wide}
+                "planes": l.planes, "cut": l.cut, "split": l.split, "wide": l.wide,
+                "order": l.order}
 
     def launch(self) -> dict:
         l = ZxLaunch()
@@ -226,7 +227,7 @@ class Index:
                    stages: Optional[int] = None, bulk: Optional[int] = None,
                    min_blocks: Optional[int] = None, planes: Optional[int] = None,
                    cut: Optional[int] = None, split: Optional[int] = None,
-                   wide: Optional[int] = None, **_ignored):
+                   wide: Optional[int] = None, order: Optional[int] = None, **_ignored):
         """Change the launch configuration (never changes results); unset
         fields keep their default values (a default 255-register budget,
         min_blocks 1, becomes 2 when the per-hit or staged form is asked for;
@@ -248,7 +249,8 @@ class Index:
                      int(d["min_blocks"] if min_blocks is None else min_blocks),
                      int(d["planes"] if planes is None else planes),
                      int(d["cut"] if cut is None else cut),
-                     int(d["split"] if split is None else split), int(wide))
+                     int(d["split"] if split is None else split), int(wide),
+                     int(d["order"] if order is None else order))
         _lib.check(_lib.load().zx_set_launch(self._h, byref(l)))
 
     def query_status(self) -> None:

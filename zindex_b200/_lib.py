@@ -51,7 +51,8 @@ class ZxInfo(ctypes.Structure):
 class ZxLaunch(ctypes.Structure):
     _fields_ = [("team", c_int), ("warps", c_int), ("blocks", c_int), ("smem_counters", c_int),
                 ("stage_bytes", c_int), ("stages", c_int), ("bulk", c_int), ("min_blocks", c_int),
-                ("planes", c_int), ("cut", c_int), ("split", c_int), ("wide", c_int)]
+                ("planes", c_int), ("cut", c_int), ("split", c_int), ("wide", c_int),
+                ("order", c_int)]
 
 
 class ZxServerOptions(ctypes.Structure):
@@ -63,7 +64,8 @@ class ZxServerStats(ctypes.Structure):
     _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("failed", c_uint64),
                 ("batches", c_uint64), ("seeds", c_uint64), ("bases", c_uint64),
                 ("p50_s", c_double), ("p99_s", c_double), ("mean_s", c_double),
-                ("max_s", c_double), ("elapsed_s", c_double), ("device_bytes", c_uint64)]
+                ("max_s", c_double), ("elapsed_s", c_double), ("device_bytes", c_uint64),
+                ("pinned_bytes", c_uint64)]
 
 
 class ZxError(RuntimeError):

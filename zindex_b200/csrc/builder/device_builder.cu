@@ -37,6 +37,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -284,17 +285,36 @@ __global__ void peel_kernel(const Filter* __restrict__ f, uint32_t nf,
       ++nab;
     }
     positions(K[e], seed, M, H, seg, pos);
-    for (int h = 0; h < H; ++h) {
-      const uint32_t t = (uint32_t)pos[h];
-      X[t] ^= e;
-      if (--D[t] == 1) {
-        if (top >= M) {
-          atomicOr(err, kErrQueue);
-          sp = n;
-          break;
+    // A key's H cells lie in H different segments, so they are distinct: the
+    // degrees and XORs of 8 cells are loaded together, then updated.
+    bool full = false;
+    for (int h0 = 0; h0 < H && !full; h0 += 8) {
+      uint32_t dv[8], xv[8], tv[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        tv[i] = h0 + i < H ? (uint32_t)pos[h0 + i] : 0u;
+        if (h0 + i < H) {
+          dv[i] = D[tv[i]];
+          xv[i] = X[tv[i]];
         }
-        Q[top++] = t;
       }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (h0 + i >= H) continue;
+        X[tv[i]] = xv[i] ^ e;
+        D[tv[i]] = dv[i] - 1;
+        if (dv[i] == 2) {
+          if (top >= M) {
+            full = true;
+            break;
+          }
+          Q[top++] = tv[i];
+        }
+      }
+    }
+    if (full) {
+      atomicOr(err, kErrQueue);
+      break;
     }
   }
   abandoned[fi] = nab;
@@ -395,6 +415,17 @@ class DeviceBuilder {
     if (s_) cudaStreamDestroy(s_);
   }
 
+  // Seconds per build phase, summed over batches (measured at stream
+  // synchronisations when the build is not quiet).
+  enum Phase { kExtract, kSort, kUnique, kOrder, kAccumulate, kPeel, kPack, kAbandoned, kPhases };
+  void report(FILE* f) const {
+    static const char* names[kPhases] = {"extract", "sort", "unique", "order", "accumulate",
+                                         "peel", "assign+pack", "abandoned"};
+    fprintf(f, "device phases:");
+    for (int i = 0; i < kPhases; ++i) fprintf(f, " %s %.2fs", names[i], phase_[i]);
+    fprintf(f, "\n");
+  }
+
   // Bases of dataset d (its records' bases for file inputs).
   uint64_t dataset_bases(uint32_t d) {
     if (!bc_.opt.synth.empty()) return synth::genome_length(bc_.spec, d);
@@ -408,6 +439,7 @@ class DeviceBuilder {
   void distinct(const Batch& b, std::vector<uint64_t>& unique, std::vector<uint64_t>& occ,
                 bool dense_out, const std::vector<uint64_t>* dense_start) {
     const uint32_t nd = b.d1 - b.d0;
+    tick();
     // Records: one per synthetic genome; the files' records otherwise.
     std::vector<uint64_t> rec_off{0}, region(nd + 1, 0), genome(nd);
     std::vector<uint32_t> rec_ds;
@@ -499,6 +531,7 @@ class DeviceBuilder {
     std::vector<unsigned long long> cur(nd);
     cu(cudaMemcpyAsync(cur.data(), cursor_.p, nd * 8, cudaMemcpyDeviceToHost, s_), "D2H");
     cu(cudaStreamSynchronize(s_), "extraction");
+    tock(kExtract);
     // Radix sort of each dataset's region.
     uint64_t largest = 1;
     for (auto c : cur) largest = std::max<uint64_t>(largest, c);
@@ -513,6 +546,7 @@ class DeviceBuilder {
                                         sorted_.p + region[j], (int)cur[j], 0, 64, s_),
          "sort");
     }
+    tock(kSort);
     d_counts_.need(nd, "counts");
     d_dense_.need(nd + 1, "dense offsets");
     std::vector<uint64_t> local_dense(nd, 0);
@@ -527,6 +561,7 @@ class DeviceBuilder {
     std::vector<uint64_t> cnt(nd);
     cu(cudaMemcpyAsync(cnt.data(), d_counts_.p, nd * 8, cudaMemcpyDeviceToHost, s_), "D2H");
     cu(cudaStreamSynchronize(s_), "unique");
+    tock(kUnique);
     for (uint32_t j = 0; j < nd; ++j) {
       unique[b.d0 + j] = cnt[j];
       occ[b.d0 + j] = cur[j];
@@ -545,6 +580,7 @@ class DeviceBuilder {
     const int H = bc_.H;
     const uint64_t seg = bc_.opt.segment_length, seed = bc_.fp.seed;
     if (!n) return;
+    tick();
     // Per-dataset filter geometry.
     std::vector<uint64_t> dense(nd + 1), local(nd);
     std::vector<uint32_t> parts(nd);
@@ -596,6 +632,7 @@ class DeviceBuilder {
     std::vector<unsigned long long> hist((uint64_t)nd * maxp);
     cu(cudaMemcpyAsync(hist.data(), hist_.p, hist.size() * 8, cudaMemcpyDeviceToHost, s_), "D2H");
     cu(cudaStreamSynchronize(s_), "filter order");
+    tock(kOrder);
     // Filter table: dataset-major, partitions in order (the keys' order).
     std::vector<Filter> filters;
     uint64_t cells = 0;
@@ -638,10 +675,12 @@ class DeviceBuilder {
     accumulate_kernel<<<grid_for(n, sms_), 256, 0, s_>>>(d_filters_.p, nf, keys_.p, n, seed, H, seg,
                                                          deg_.p, xr_.p);
     cu(cudaGetLastError(), "accumulate_kernel");
+    tock(kAccumulate);
     const int pb = 32, pg = (int)((nf + pb - 1) / pb);
     peel_kernel<<<pg, pb, 0, s_>>>(d_filters_.p, nf, keys_.p, seed, H, seg, deg_.p, xr_.p, queue_.p,
                                    state_.p, stack_.p, nab_.p, err_.p);
     cu(cudaGetLastError(), "peel_kernel");
+    tock(kPeel);
     assign_kernel<<<pg, pb, 0, s_>>>(d_filters_.p, nf, keys_.p, seed, H, seg, bc_.b, deg_.p,
                                      stack_.p);
     cu(cudaGetLastError(), "assign_kernel");
@@ -650,6 +689,7 @@ class DeviceBuilder {
     std::vector<uint32_t> nab(nf);
     cu(cudaMemcpyAsync(nab.data(), nab_.p, nf * 4, cudaMemcpyDeviceToHost, s_), "D2H");
     cu(cudaStreamSynchronize(s_), "construction");
+    tock(kPack);
     check_error();
     std::vector<uint64_t> first(nf + 1, 0);
     for (uint32_t i = 0; i < nf; ++i) {
@@ -670,6 +710,7 @@ class DeviceBuilder {
       cu(cudaStreamSynchronize(s_), "abandoned keys");
       for (const uint2& x : lost) bc_.abandoned.push_back(build::Abandoned{x.x, x.y, 1});
     }
+    tock(kAbandoned);
   }
 
   cudaStream_t stream() const { return s_; }
@@ -690,7 +731,22 @@ class DeviceBuilder {
     return file_;
   }
 
+  void tick() {
+    if (bc_.opt.quiet) return;
+    cu(cudaStreamSynchronize(s_), "phase timing");
+    tp_ = std::chrono::steady_clock::now();
+  }
+  void tock(Phase i) {
+    if (bc_.opt.quiet) return;
+    cu(cudaStreamSynchronize(s_), "phase timing");
+    const auto now = std::chrono::steady_clock::now();
+    phase_[i] += std::chrono::duration<double>(now - tp_).count();
+    tp_ = now;
+  }
+
   Context& bc_;
+  double phase_[kPhases] = {};
+  std::chrono::steady_clock::time_point tp_;
   int sms_ = 1;
   cudaStream_t s_ = nullptr;
   SeedParams sp_{};
@@ -795,9 +851,12 @@ void build_index_device(const BuildOptions& opt) {
   }
   for (size_t d = 0; d < C; ++d)
     check(unique_again[d] == unique[d], kEInval, "distinct keys differ between passes");
-  if (!opt.quiet)
+  if (!opt.quiet) {
     fprintf(stderr, "constructed %zu filters in %.3fs (%llu bytes of rows on the device)\n", C,
             seconds_since(bc.t0), (unsigned long long)row_total);
+    dev.report(stderr);
+  }
+  const double t_write = seconds_since(bc.t0);
   // Bank payloads streamed from the device, one writer per bank, each through
   // its own pinned buffer.
   constexpr uint64_t kPiece = 64ull << 20;
@@ -820,6 +879,9 @@ void build_index_device(const BuildOptions& opt) {
         }
       },
       bc.threads);
+  if (!opt.quiet)
+    fprintf(stderr, "wrote the index in %.3fs (%zu abandoned keys)\n", seconds_since(bc.t0) - t_write,
+            bc.abandoned.size());
 }
 
 }  // namespace zx

@@ -63,6 +63,7 @@ void fill_launch(const zx::QueryLaunch& l, zx_launch* out) {
   out->cut = l.cut;
   out->split = l.split;
   out->wide = l.wide;
+  out->order = l.order;
 }
 
 }  // namespace
@@ -340,7 +341,8 @@ int zx_set_launch(zx_index* index, const zx_launch* l) {
     std::lock_guard<std::mutex> lock(index->mu);
     index->engine->set_launch(
         zx::QueryLaunch{l->team, l->warps, l->blocks, l->smem_counters, l->stage_bytes, l->stages,
-                        l->bulk, l->min_blocks, l->planes, l->cut, l->split, l->wide});
+                        l->bulk, l->min_blocks, l->planes, l->cut, l->split, l->wide,
+                        l->order});
   });
 }
 
@@ -443,6 +445,7 @@ int zx_server_stats(zx_server* server, int reset, zx_server_report* out) {
     out->max_s = st.max_s;
     out->elapsed_s = st.elapsed_s;
     out->device_bytes = st.device_bytes;
+    out->pinned_bytes = st.pinned_bytes;
   });
 }
 

@@ -9,6 +9,7 @@
 // storage.rs:3745-3766): HBM holds the whole filter payload.
 #include "engine.h"
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "kernels/query_kernels.cuh"
@@ -140,8 +141,9 @@ FusedFn fused_for(int mode, const QueryLaunch& l) {
 
 using WideFn = void (*)(const DevIndex*, const ColorLoc*, const uint64_t*,
                        const unsigned long long*, int, uint32_t, uint32_t*, uint64_t*,
-                       unsigned long long*);
-using DenseExtractFn = void (*)(BatchView, SeedParams, uint64_t*, unsigned long long*, int);
+                       unsigned long long*, WideRound);
+using DenseExtractFn = void (*)(BatchView, SeedParams, uint64_t*, unsigned long long*, int,
+                                WideRound);
 
 // Wide-row probe variant: J chunks per thread, S seeds per step, HQ rows
 // loaded per seed and chunk (16 loads in flight per thread).
@@ -462,7 +464,9 @@ Workspace::~Workspace() {
                  keys_count, error,    fstate,    hp_starts, hp_keep,    hp_pos,
                  hp_bases,   hp_offsets, hp_scan_tmp, seg_blocks, seg_tiles, seg_records,
                  rec_counts, rec_totals, rec_hits, rec_first, rec_scan_tmp, hit_colors,
-                 hit_counts, split_keys, split_counts, wide_cursor, wide_keys2};
+                 hit_counts, split_keys, split_counts, wide_cursor, wide_keys2,
+                 wide_seg_cursor, wide_round_first, wide_sk[0], wide_sk[1], wide_sk_alt[0],
+                 wide_sk_alt[1], wide_keys_alt[0], wide_keys_alt[1], wide_sort_tmp};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total, h_seg_blocks, h_seg_records};
@@ -890,6 +894,7 @@ QueryLaunch Engine::default_launch() const {
   if (wide_eligible(8) && wide_chunks() >= 128) {
     const uint32_t nc = wide_chunks();
     l.wide = 1;
+    l.order = 1;
     l.warps = nc <= 128 ? 4 : ((nc > 256 && nc <= 288) || (nc > 512 && nc <= 576) ? 9 : 8);
     l.smem_counters = 1;
     if (m_.colors.size() > 16384 || fused_smem_bytes(l) > 110 * 1024) l.smem_counters = 0;
@@ -933,6 +938,7 @@ QueryLaunch Engine::default_fused_launch() const {
   l.planes = 1;
   l.cut = 4;
   l.wide = 0;
+  l.order = 0;
   // Minimizer seeds are extracted by a kernel of their own: the probe kernel
   // then needs no extraction scratch and keeps twice the warps resident
   // (C3 slice on B200: 22.3 ms against 36.7 ms for the fused kernel).
@@ -1068,6 +1074,7 @@ void Engine::set_launch(const QueryLaunch& l) {
   check(l.cut >= 1 && l.cut <= 64, kEInval, "cut must be in 1..64");
   check(l.split == 0 || l.split == 1, kEInval, "split must be 0 or 1");
   check(l.wide == 0 || l.wide == 1, kEInval, "wide must be 0 or 1");
+  check(l.order == 0 || l.order == 1, kEInval, "order must be 0 or 1");
   check(!l.wide || wide_eligible(l.warps), kEInval,
         "the wide-row form needs fingerprints of at least 4 bits, a k-mer, minimizer or "
         "modimizer index without strobes, 4, 8 or 9 warps per block and rows of at most "
@@ -1091,8 +1098,12 @@ void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
   const uint64_t colors = m_.colors.size();
   // Split minimizer and wide-row queries: key slots allocated before any graph capture.
   if (kernel_mode(launch_) == 4 || wide_form(launch_)) ensure_split_capacity(ws);
-  if (wide_form(launch_) && nbases / kTileWindows + records + nbases / kFindereTask + 1 > kSplitTiles)
-    ensure_wide_pipeline(ws);
+  const bool rounds = nbases / kTileWindows + records + nbases / kFindereTask + 1 > kSplitTiles;
+  if (wide_form(launch_) && rounds) ensure_wide_pipeline(ws);
+  if (wide_form(launch_) && launch_.order) {
+    ensure_order_capacity(ws, 0);
+    if (rounds) ensure_order_capacity(ws, 1);
+  }
   if (nbases > ws.cap_bases || !ws.bases) {
     uint64_t cap = std::max<uint64_t>({nbases, ws.cap_bases * 3 / 2, 4096});
     cap = round_up(cap, 4096);
@@ -1289,61 +1300,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     cuda_check(cudaGetLastError(), "reduce_counters_kernel");
   };
   if (wide_form(l)) {
-    // Wide-row query: rounds of up to kSplitTiles tiles; per round the
-    // extraction kernel appends the tiles' seeds to one dense list, the wide
-    // probe counts them, and the block counters are added up.
-    ensure_split_capacity(ws);
-    int J, HQ;
-    uint32_t wteam = 0;
-    wide_shape(l, J, HQ, &wteam);
-    WideFn wfn = wide_fn(J, HQ, l.warps * 32);
-    cuda_check(cudaFuncSetAttribute(wfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-               "cudaFuncSetAttribute");
-    const int ewarps = 4;
-    const size_t esmem = DenseSmem::total(sp_.mode, sp_.k, ewarps);
-    DenseExtractFn efn = dense_extract_for(sp_.mode);
-    cuda_check(cudaFuncSetAttribute(efn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem),
-               "cudaFuncSetAttribute");
-    const int egrid = (int)std::min<uint64_t>((kSplitTiles + ewarps - 1) / ewarps,
-                                              (uint64_t)sms_ * 8);
-    const int wblocks = l.blocks > 0 ? std::min(l.blocks, blocks_cap) : blocks_cap;
-    const uint64_t rounds = (tiles_bound + kSplitTiles - 1) / kSplitTiles;
-    // Several rounds: extraction (compute-bound) of round r + 1 runs on the
-    // auxiliary stream beside the probe (memory-bound) of round r, the rounds
-    // alternating between two key lists; events order each list's reuse.
-    const bool overlap = rounds > 1;
-    if (overlap) ensure_wide_pipeline(ws);
-    cudaStream_t xs = overlap ? ws.aux_stream : s;
-    if (overlap) {
-      cuda_check(cudaEventRecord(ws.wide_fork, s), "cudaEventRecord");
-      cuda_check(cudaStreamWaitEvent(xs, ws.wide_fork, 0), "cudaStreamWaitEvent");
-    }
-    for (uint64_t r = 0; r < rounds; ++r) {
-      const int b = overlap ? (int)(r & 1) : 0;
-      uint64_t* keys = b ? ws.wide_keys2 : ws.split_keys;
-      BatchView rb = bv;
-      rb.tile_lo = (uint32_t)(r * kSplitTiles);
-      rb.tile_hi = (uint32_t)std::min<uint64_t>((r + 1) * kSplitTiles, tiles_bound);
-      if (overlap && r >= 2)
-        cuda_check(cudaStreamWaitEvent(xs, ws.wide_probe[b], 0), "cudaStreamWaitEvent");
-      cuda_check(cudaMemsetAsync(ws.wide_cursor + b, 0, 8, xs), "memset");
-      efn<<<egrid, ewarps * 32, esmem, xs>>>(rb, sp_, keys, ws.wide_cursor + b, ewarps);
-      cuda_check(cudaGetLastError(), "extract_dense_kernel");
-      if (overlap) {
-        cuda_check(cudaEventRecord(ws.wide_ext[b], xs), "cudaEventRecord");
-        cuda_check(cudaStreamWaitEvent(s, ws.wide_ext[b], 0), "cudaStreamWaitEvent");
-      }
-      wfn<<<wblocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, d_color_loc_,
-                                              keys, ws.wide_cursor + b, l.smem_counters, wteam,
-                                              ws.partial, counts, total);
-      cuda_check(cudaGetLastError(), "wide_probe_kernel");
-      if (l.smem_counters) {
-        reduce_counters_kernel<<<std::max(1u, (colors + 255) / 256), 256, 0, s>>>(
-            ws.partial, wblocks, colors, counts);
-        cuda_check(cudaGetLastError(), "reduce_counters_kernel");
-      }
-      if (overlap) cuda_check(cudaEventRecord(ws.wide_probe[b], s), "cudaEventRecord");
-    }
+    run_wide(ws, bv, tiles_bound, recover, counts, total, 0, s);
     if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
     return;
   }
@@ -1382,6 +1339,157 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     reduce();
   }
   if (timed) cuda_check(cudaEventRecord(ev_end_, s), "cudaEventRecord");
+}
+
+void Engine::run_wide(Workspace& ws, const BatchView& bv, uint64_t tiles_bound, bool recover,
+                      uint64_t* counts, unsigned long long* total, uint32_t segments,
+                      cudaStream_t s) {
+  // Rounds of up to kSplitTiles tiles; per round the extraction kernel
+  // appends the tiles' seeds to one dense list (segmented: each segment's
+  // seeds to its own part of it), the wide probe counts them, and the block
+  // counters are added up (segmented: each block adds its counters to the
+  // segment it leaves).
+  const QueryLaunch& l = launch_;
+  ensure_split_capacity(ws);
+  const size_t smem = fused_smem_bytes(l);
+  const int blocks_cap = max_blocks(l);
+  int J, HQ;
+  uint32_t wteam = 0;
+  wide_shape(l, J, HQ, &wteam);
+  WideFn wfn = wide_fn(J, HQ, l.warps * 32);
+  cuda_check(cudaFuncSetAttribute(wfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  const int ewarps = 4;
+  const size_t esmem = DenseSmem::total(sp_.mode, sp_.k, ewarps);
+  DenseExtractFn efn = dense_extract_for(sp_.mode);
+  cuda_check(cudaFuncSetAttribute(efn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem),
+             "cudaFuncSetAttribute");
+  const int egrid = (int)std::min<uint64_t>((kSplitTiles + ewarps - 1) / ewarps,
+                                            (uint64_t)sms_ * 8);
+  // A tile holds at most 256 seeds: one probe round.
+  const int wblocks = l.blocks > 0 ? std::min(l.blocks, blocks_cap)
+                                   : (int)std::min<uint64_t>(blocks_cap, std::max<uint64_t>(tiles_bound, 1));
+  const uint32_t colors = (uint32_t)m_.colors.size();
+  const uint64_t rounds = (tiles_bound + kSplitTiles - 1) / kSplitTiles;
+  // Several rounds: extraction (compute-bound) of round r + 1 runs on the
+  // auxiliary stream beside the probe (memory-bound) of round r, the rounds
+  // alternating between two key lists; events order each list's reuse.
+  const bool overlap = rounds > 1;
+  if (overlap) ensure_wide_pipeline(ws);
+  cudaStream_t xs = overlap ? ws.aux_stream : s;
+  if (overlap) {
+    cuda_check(cudaEventRecord(ws.wide_fork, s), "cudaEventRecord");
+    cuda_check(cudaStreamWaitEvent(xs, ws.wide_fork, 0), "cudaStreamWaitEvent");
+  }
+  for (uint64_t r = 0; r < rounds; ++r) {
+    const int b = overlap ? (int)(r & 1) : 0;
+    uint64_t* keys = b ? ws.wide_keys2 : ws.split_keys;
+    BatchView rb = bv;
+    rb.tile_lo = (uint32_t)(r * kSplitTiles);
+    rb.tile_hi = (uint32_t)std::min<uint64_t>((r + 1) * kSplitTiles, tiles_bound);
+    WideRound sg;
+    if (segments) {
+      sg.seg_tiles = ws.seg_tiles;
+      sg.cursor = ws.wide_seg_cursor + (uint64_t)b * ws.cap_segments;
+      sg.round_first = ws.wide_round_first + (uint64_t)b * ws.cap_segments;
+      sg.totals = total;
+      sg.nseg = segments;
+      sg.tile_lo = rb.tile_lo;
+    }
+    // Ordered round: every slot the round may fill gets a sort key (the
+    // unfilled ones all ones, so a stable sort leaves them behind the keys).
+    const bool ordered = l.order && !segments;
+    const uint64_t slots = (uint64_t)(rb.tile_hi - rb.tile_lo) * kTileWindows;
+    if (ordered) {
+      ensure_order_capacity(ws, b);
+      sg.order_keys = ws.wide_sk[b];
+      sg.seed = host_ix_.seed;
+    }
+    if (overlap && r >= 2)
+      cuda_check(cudaStreamWaitEvent(xs, ws.wide_probe[b], 0), "cudaStreamWaitEvent");
+    if (segments)
+      cuda_check(cudaMemsetAsync(sg.cursor, 0, segments * 8ull, xs), "memset");
+    else
+      cuda_check(cudaMemsetAsync(ws.wide_cursor + b, 0, 8, xs), "memset");
+    if (ordered) cuda_check(cudaMemsetAsync(sg.order_keys, 0xFF, slots * 4, xs), "memset");
+    efn<<<egrid, ewarps * 32, esmem, xs>>>(rb, sp_, keys, ws.wide_cursor + b, ewarps, sg);
+    cuda_check(cudaGetLastError(), "extract_dense_kernel");
+    const uint64_t* probe_keys = keys;
+    if (ordered && slots) {
+      // Stable radix sort of the round's slots by the first hash's top 20
+      // bits: the keys come first, in row-address order of every class.
+      cub::DoubleBuffer<uint32_t> sk(ws.wide_sk[b], ws.wide_sk_alt[b]);
+      cub::DoubleBuffer<uint64_t> kv(keys, ws.wide_keys_alt[b]);
+      size_t bytes = ws.wide_sort_bytes;
+      cuda_check(cub::DeviceRadixSort::SortPairs(ws.wide_sort_tmp, bytes, sk, kv, (int)slots,
+                                                 kOrderBit, 32, xs),
+                 "round sort");
+      probe_keys = kv.Current();
+    }
+    if (segments) {
+      wide_rounds_kernel<<<1, 1024, 0, xs>>>(sg.cursor, segments,
+                                             const_cast<uint32_t*>(sg.round_first));
+      cuda_check(cudaGetLastError(), "wide_rounds_kernel");
+    }
+    if (overlap) {
+      cuda_check(cudaEventRecord(ws.wide_ext[b], xs), "cudaEventRecord");
+      cuda_check(cudaStreamWaitEvent(s, ws.wide_ext[b], 0), "cudaStreamWaitEvent");
+    }
+    wfn<<<wblocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, d_color_loc_,
+                                            probe_keys, ws.wide_cursor + b, l.smem_counters,
+                                            wteam, ws.partial, counts, segments ? nullptr : total,
+                                            sg);
+    cuda_check(cudaGetLastError(), "wide_probe_kernel");
+    if (l.smem_counters && !segments) {
+      reduce_counters_kernel<<<std::max(1u, (colors + 255) / 256), 256, 0, s>>>(
+          ws.partial, wblocks, colors, counts);
+      cuda_check(cudaGetLastError(), "reduce_counters_kernel");
+    }
+    if (overlap) cuda_check(cudaEventRecord(ws.wide_probe[b], s), "cudaEventRecord");
+  }
+}
+
+void Engine::ensure_order_capacity(Workspace& ws, int b) {
+  if (ws.wide_sk[b]) return;
+  const uint64_t slots = (uint64_t)kSplitTiles * kTileWindows;
+  dev_alloc(&ws.wide_sk[b], slots, "round sort keys");
+  dev_alloc(&ws.wide_sk_alt[b], slots, "round sort keys (second buffer)");
+  dev_alloc(&ws.wide_keys_alt[b], slots, "round keys (second buffer)");
+  if (!ws.wide_sort_tmp) {
+    cub::DoubleBuffer<uint32_t> sk(ws.wide_sk[b], ws.wide_sk_alt[b]);
+    cub::DoubleBuffer<uint64_t> kv(ws.split_keys, ws.wide_keys_alt[b]);
+    size_t bytes = 0;
+    cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, bytes, sk, kv, (int)slots, kOrderBit, 32),
+               "sort scratch size");
+    dev_alloc((uint8_t**)&ws.wide_sort_tmp, std::max<size_t>(bytes, 16), "round sort scratch");
+    ws.wide_sort_bytes = std::max<size_t>(bytes, 16);
+  }
+  ws.release_graphs();
+}
+
+void Engine::ensure_segment_capacity(Workspace& ws, uint32_t segments) {
+  if (segments + 1 > ws.cap_segments || !ws.seg_blocks) {
+    const uint64_t c = std::max<uint64_t>(segments + 1, 256);
+    for (void* p : {(void*)ws.seg_blocks, (void*)ws.seg_tiles, (void*)ws.seg_records,
+                    (void*)ws.wide_seg_cursor, (void*)ws.wide_round_first})
+      if (p) cudaFree(p);
+    for (void* p : {(void*)ws.h_seg_blocks, (void*)ws.h_seg_records})
+      if (p) cudaFreeHost(p);
+    ws.wide_seg_cursor = nullptr;
+    ws.wide_round_first = nullptr;
+    dev_alloc(&ws.seg_blocks, c, "segment blocks");
+    dev_alloc(&ws.seg_tiles, c, "segment tiles");
+    dev_alloc(&ws.seg_records, c, "segment records");
+    host_alloc(&ws.h_seg_blocks, c);
+    host_alloc(&ws.h_seg_records, c);
+    ws.cap_segments = c;
+  }
+  if (wide_form(launch_) && !ws.wide_seg_cursor) {
+    dev_alloc(&ws.wide_seg_cursor, 2 * ws.cap_segments, "segment key cursors");
+    dev_alloc(&ws.wide_round_first, 2 * ws.cap_segments, "segment probe rounds");
+  }
+  if (!ws.seg_staged)
+    cuda_check(cudaEventCreateWithFlags(&ws.seg_staged, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 void Engine::ensure_wide_pipeline(Workspace& ws) {
@@ -1424,16 +1532,30 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   for (uint32_t i = 0; i < segments; ++i)
     check(seg_records[i] <= seg_records[i + 1], kEInval, "segment records must be non-decreasing");
   ensure_capacity(ws, nbases, records);
-  // Wide-row indexes: a few coalesced requests (a serving batch) each get the
-  // wide form's own launch sequence into their counters; batches of many
-  // small requests (per-record queries) take the fused segmented launch.
-  constexpr uint32_t kWideSegments = 64;
-  if (wide_form(launch_) && segments <= kWideSegments) {
-    const uint64_t colors = m_.colors.size();
-    for (uint32_t i = 0; i < segments; ++i) {
-      const uint64_t r0 = seg_records[i], n = seg_records[i + 1] - r0;
-      if (n) enqueue(ws, bases, nbases, offsets + r0, n, recover, counts + i * colors, totals + i, s);
-    }
+  ensure_segment_capacity(ws, segments);
+  // The pinned staging is reused: wait until the previous call's copies ran.
+  cuda_check(cudaEventSynchronize(ws.seg_staged), "segment staging");
+  if (wide_form(launch_)) {
+    // Wide-row indexes: one wide-form query over the whole batch, each
+    // request's seeds in its own part of the key lists and its own counters.
+    for (uint32_t i = 0; i <= segments; ++i) ws.h_seg_records[i] = seg_records[i];
+    cuda_check(cudaMemcpyAsync(ws.seg_records, ws.h_seg_records, (segments + 1) * 8ull,
+                               cudaMemcpyHostToDevice, s),
+               "H2D");
+    cuda_check(cudaEventRecord(ws.seg_staged, s), "cudaEventRecord");
+    if (m_.homopolymer_compression) compress_homopolymers(ws, bases, nbases, offsets, records, s);
+    const uint64_t words = nbases / 32 + 2;
+    int grid = (int)std::min<uint64_t>((words + 255) / 256, (uint64_t)sms_ * 16);
+    pack_kernel<<<std::max(grid, 1), 256, 0, s>>>(bases, nbases, ws.packed, ws.invalid, words);
+    cuda_check(cudaGetLastError(), "pack_kernel");
+    plan_tiles(ws, offsets, records, nbases, s);
+    segment_tiles_kernel<<<(segments + 256) / 256, 256, 0, s>>>(ws.tile_first, ws.seg_records,
+                                                                segments, ws.seg_tiles);
+    cuda_check(cudaGetLastError(), "segment_tiles_kernel");
+    BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records,
+                 ws.fstate};
+    const uint64_t tiles_bound = nbases / kTileWindows + records + nbases / kFindereTask + 1;
+    run_wide(ws, bv, tiles_bound, recover, counts, totals, segments, s);
     return;
   }
   QueryLaunch l = fused_launch(launch_);
@@ -1445,23 +1567,6 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   // at most one warp per tile.
   uint64_t est_total = 0;
   for (uint32_t i = 0; i < segments; ++i) est_total += est_tiles[i];
-  if (segments + 1 > ws.cap_segments || !ws.seg_blocks) {
-    const uint64_t c = std::max<uint64_t>(segments + 1, 256);
-    for (void* p : {(void*)ws.seg_blocks, (void*)ws.seg_tiles, (void*)ws.seg_records})
-      if (p) cudaFree(p);
-    for (void* p : {(void*)ws.h_seg_blocks, (void*)ws.h_seg_records})
-      if (p) cudaFreeHost(p);
-    dev_alloc(&ws.seg_blocks, c, "segment blocks");
-    dev_alloc(&ws.seg_tiles, c, "segment tiles");
-    dev_alloc(&ws.seg_records, c, "segment records");
-    host_alloc(&ws.h_seg_blocks, c);
-    host_alloc(&ws.h_seg_records, c);
-    ws.cap_segments = c;
-  }
-  // The pinned staging is reused: wait until the previous call's copies ran.
-  if (!ws.seg_staged)
-    cuda_check(cudaEventCreateWithFlags(&ws.seg_staged, cudaEventDisableTiming), "cudaEventCreate");
-  cuda_check(cudaEventSynchronize(ws.seg_staged), "segment staging");
   uint32_t blocks = 0;
   for (uint32_t i = 0; i < segments; ++i) {
     ws.h_seg_blocks[i] = blocks;

@@ -18,6 +18,7 @@
 
 namespace zx {
 struct ColorLoc;
+struct BatchView;
 }
 
 namespace zx {
@@ -69,6 +70,17 @@ struct Workspace {
   uint64_t* split_keys = nullptr;
   uint32_t* split_counts = nullptr;
   unsigned long long* wide_cursor = nullptr;  // wide-row queries: keys in the dense lists (2)
+  // Segmented wide-row queries, per key list: keys of each segment and the
+  // first probe round of each segment (2 x cap_segments each).
+  unsigned long long* wide_seg_cursor = nullptr;
+  uint32_t* wide_round_first = nullptr;
+  // Ordered wide-row rounds, per key list: sort keys and the radix sort's
+  // second buffers (keys and sort keys), and its scratch.
+  uint32_t* wide_sk[2] = {};
+  uint32_t* wide_sk_alt[2] = {};
+  uint64_t* wide_keys_alt[2] = {};
+  void* wide_sort_tmp = nullptr;
+  size_t wide_sort_bytes = 0;
   uint64_t* wide_keys2 = nullptr;  // second dense key list (rounds alternate)
   cudaStream_t aux_stream = nullptr;  // wide-row queries: extraction beside the probe
   cudaEvent_t wide_fork = nullptr, wide_ext[2] = {}, wide_probe[2] = {};
@@ -251,6 +263,17 @@ class Engine {
   // Wide-row queries of several rounds: the second key list, the auxiliary
   // stream and the events of the extraction / probe pipeline.
   void ensure_wide_pipeline(Workspace& ws);
+  // Ordered wide-row rounds: sort buffers of key list b (0 or 1).
+  void ensure_order_capacity(Workspace& ws, int b);
+  // Wide-row form over the planned tiles of a packed batch: rounds of up to
+  // kSplitTiles tiles, each a dense extraction and a wide probe. segments = 0:
+  // one query into counts / *total; segments > 0: a segmented query, request
+  // s into counts + s x colours and total[s] (the segment tables and their
+  // per-round cursors already in ws).
+  void run_wide(Workspace& ws, const BatchView& bv, uint64_t tiles_bound, bool recover,
+                uint64_t* counts, unsigned long long* total, uint32_t segments, cudaStream_t s);
+  // Device tables of a segmented launch for `segments` requests.
+  void ensure_segment_capacity(Workspace& ws, uint32_t segments);
   // Runs host records in device groups (one segment per record): after each
   // group's launch, on_group(r0, n) enqueues its read-back on ws.stream; the
   // stream is then synchronised and the error word checked.

@@ -50,6 +50,8 @@ struct QueryLaunch {
                       // then probed by a kernel without the extraction scratch (more warps per SM)
   int wide;           // 1 = wide-row form: seeds extracted into a dense list, probed by blocks
                       // whose threads own fixed 16-byte chunks of every row (wide_probe.cuh)
+  int order;          // wide-row form: 1 = each round's seeds sorted by their first hash, so
+                      // consecutive seeds read neighbouring rows of every class
 };
 
 }  // namespace zx

@@ -37,6 +37,9 @@ namespace zx {
 constexpr int kWideSeeds = 256;      // seeds per descriptor round of a block
 constexpr int kWidePlanes = 6;       // register planes: counts up to 63 per field
 constexpr uint32_t kWideFlush = 63;  // seeds between plane flushes
+// Ordered rounds compare bits [kOrderBit, 32) of the sort keys (the first
+// hash's top 32 bits): about a million row-order buckets.
+constexpr int kOrderBit = 12;
 
 // Colour location for recovered-origin point probes: cls_member = class |
 // member index << 8 (member index within a multi-member group, 0 for
@@ -61,12 +64,78 @@ struct DenseSmem {
   }
 };
 
+// Largest s < n with first[s] <= x (first[] non-decreasing, first[0] <= x):
+// the segment holding tile or round x, empty segments sharing its start
+// coming before it.
+__device__ __forceinline__ uint32_t segment_of(const uint32_t* __restrict__ first, uint32_t n,
+                                               uint32_t x) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(first + mid) <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Per-round tables of a wide-row query.
+// Segmented (several requests in one launch): per extraction round, segment
+// s's keys sit at out[(max(seg_tiles[s], tile_lo) - tile_lo) * kTileWindows
+// ...], their number in cursor[s]; the probe's rounds of 256 seeds never
+// straddle segments (round_first[s] = first round of segment s). nseg = 0:
+// one unsegmented list, one cursor.
+// Ordered (unsegmented only): the extraction also writes each key's sort key,
+// the top 32 bits of its first hash, at the same index of order_keys.
+struct WideRound {
+  const uint32_t* seg_tiles = nullptr;    // first tile of each segment (nseg + 1)
+  unsigned long long* cursor = nullptr;   // keys of each segment in this round
+  const uint32_t* round_first = nullptr;  // first probe round of each segment (nseg + 1)
+  unsigned long long* totals = nullptr;   // seeds of each segment
+  uint32_t nseg = 0;
+  uint32_t tile_lo = 0;                   // first tile of the extraction round
+  uint32_t* order_keys = nullptr;         // sort keys of the dense list (ordered rounds)
+  uint64_t seed = 0;                      // the index seed (first hash)
+};
+
+__device__ __forceinline__ uint64_t wide_seg_base(const WideRound& sg, uint32_t s) {
+  const uint32_t t = __ldg(sg.seg_tiles + s);
+  return (uint64_t)(t > sg.tile_lo ? t - sg.tile_lo : 0u) * kTileWindows;
+}
+
+// round_first[] of a segmented round: exclusive scan of each segment's
+// ceil(keys / 256) probe rounds (one block).
+__global__ void wide_rounds_kernel(const unsigned long long* __restrict__ cursor, uint32_t nseg,
+                                   uint32_t* __restrict__ round_first) {
+  __shared__ uint32_t part[1024];
+  const uint32_t T = blockDim.x, tid = threadIdx.x;
+  const uint32_t per = (nseg + T - 1) / T;
+  const uint32_t lo = min(nseg, tid * per), hi = min(nseg, lo + per);
+  uint32_t sum = 0;
+  for (uint32_t s = lo; s < hi; ++s) sum += (uint32_t)((cursor[s] + kWideSeeds - 1) / kWideSeeds);
+  part[tid] = sum;
+  __syncthreads();
+  for (uint32_t off = 1; off < T; off <<= 1) {
+    const uint32_t v = tid >= off ? part[tid - off] : 0u;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  uint32_t run = tid ? part[tid - 1] : 0u;
+  for (uint32_t s = lo; s < hi; ++s) {
+    round_first[s] = run;
+    run += (uint32_t)((cursor[s] + kWideSeeds - 1) / kWideSeeds);
+  }
+  if (tid == T - 1) round_first[nseg] = part[T - 1];
+}
+
 // Appends the seeds of tiles [tile_lo, tile_hi) (tile_hi 0 = to the end) to
 // out[], one atomic cursor bump per warp and tile. out holds at least
-// (tile_hi - tile_lo) * kTileWindows keys.
+// (tile_hi - tile_lo) * kTileWindows keys. Segmented (sg.nseg > 0): each
+// tile's seeds go to its segment's part of out[] and cursor.
 template <int MODE>
 __global__ void extract_dense_kernel(BatchView bv, SeedParams sp, uint64_t* __restrict__ out,
-                                     unsigned long long* __restrict__ cursor, int warps_per_block) {
+                                     unsigned long long* __restrict__ cursor, int warps_per_block,
+                                     WideRound sg) {
   extern __shared__ __align__(16) uint8_t smem[];
   uint64_t* inner = reinterpret_cast<uint64_t*>(smem);
   uint8_t* p = smem + 256 * 8;
@@ -84,9 +153,19 @@ __global__ void extract_dense_kernel(BatchView bv, SeedParams sp, uint64_t* __re
     const uint32_t n = extract_tile<MODE>(bv, sp, bv.tiles[t], keys, ocm, inner, lane);
     __syncwarp();
     unsigned long long at = 0;
-    if (lane == 0 && n) at = atomicAdd(cursor, (unsigned long long)n);
+    uint64_t* dst = out;
+    unsigned long long* cur = cursor;
+    if (sg.nseg) {
+      const uint32_t seg = segment_of(sg.seg_tiles, sg.nseg, t);
+      dst = out + wide_seg_base(sg, seg);
+      cur = sg.cursor + seg;
+    }
+    if (lane == 0 && n) at = atomicAdd(cur, (unsigned long long)n);
     at = __shfl_sync(0xFFFFFFFFu, at, 0);
-    for (uint32_t i = lane; i < n; i += 32) out[at + i] = keys[i];
+    for (uint32_t i = lane; i < n; i += 32) dst[at + i] = keys[i];
+    if (sg.order_keys)
+      for (uint32_t i = lane; i < n; i += 32)
+        sg.order_keys[at + i] = (uint32_t)(mixsplit(keys[i], sg.seed) >> 32);
     __syncwarp();
   }
 }
@@ -107,7 +186,7 @@ struct WideSmem {
 
 struct WideCounters {
   uint32_t* smem;
-  uint64_t* gmem;
+  uint64_t* gmem;  // the current segment's counters when smem is null
   __device__ __forceinline__ void add(uint32_t c, uint32_t n) const {
     if (smem) atomicAdd(smem + c, n);
     else atomicAdd(reinterpret_cast<unsigned long long*>(gmem + c), (unsigned long long)n);
@@ -130,7 +209,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
                       const uint64_t* __restrict__ keys,
                       const unsigned long long* __restrict__ nkeys, int smem_counters,
                       uint32_t team_threads, uint32_t* __restrict__ partial,
-                      uint64_t* __restrict__ counts, unsigned long long* __restrict__ total) {
+                      uint64_t* __restrict__ counts, unsigned long long* __restrict__ total,
+                      WideRound sg) {
   extern __shared__ __align__(16) uint8_t smem[];
   DevIndex* six = reinterpret_cast<DevIndex*>(smem);
   uint8_t* p = smem + FusedSmem::ix_bytes;
@@ -147,7 +227,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
     for (uint32_t c = threadIdx.x; c < colors; c += blockDim.x) scount[c] = 0;
   __syncthreads();
   const DevIndex& ix = *six;
-  const WideCounters cnt{scount, counts};
+  WideCounters cnt{scount, counts};
   const int H = ix.hashes, Hp = (H + 3) & ~3, b = ix.bits, lb = log2_bits(b);
   const uint32_t ones = field_ones(b), hi = ones << (b - 1);
   const uint32_t fmask = b == 32 ? 0xFFFFFFFFu : (1u << b) - 1u;
@@ -213,13 +293,51 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
   };
 
-  const uint64_t nk = *nkeys;
   unsigned long long seeds = 0;
   uint32_t steps = 0;
-  for (uint64_t base = (uint64_t)blockIdx.x * kWideSeeds; base < nk;
-       base += (uint64_t)gridDim.x * kWideSeeds) {
-    const uint32_t n =
-        nk - base < (uint64_t)kWideSeeds ? (uint32_t)(nk - base) : (uint32_t)kWideSeeds;
+  // Segmented: the block's counters belong to one segment at a time. They
+  // go to that segment's counts when the block moves on (a plain add when
+  // the segment has one round, so this block is its only writer).
+  uint32_t cur = 0xFFFFFFFFu;
+  auto leave_segment = [&]() {
+    flush();
+    steps = 0;
+    if (!scount) return;
+    __syncthreads();
+    if (cur != 0xFFFFFFFFu) {
+      uint64_t* out = counts + (uint64_t)cur * colors;
+      const bool owner = __ldg(sg.round_first + cur + 1) - __ldg(sg.round_first + cur) == 1u;
+      for (uint32_t c = tid; c < colors; c += T) {
+        const uint32_t v = scount[c];
+        if (!v) continue;
+        if (owner) out[c] += v;
+        else atomicAdd(reinterpret_cast<unsigned long long*>(out + c), (unsigned long long)v);
+        scount[c] = 0;
+      }
+    }
+    __syncthreads();
+  };
+  const uint64_t nk = sg.nseg ? 0 : *nkeys;
+  const uint64_t nrounds = sg.nseg ? (uint64_t)__ldg(sg.round_first + sg.nseg)
+                                   : (nk + kWideSeeds - 1) / kWideSeeds;
+  for (uint64_t r = blockIdx.x; r < nrounds; r += gridDim.x) {
+    uint64_t base = r * kWideSeeds;
+    uint32_t n;
+    if (sg.nseg) {
+      const uint32_t seg = segment_of(sg.round_first, sg.nseg, (uint32_t)r);
+      const uint64_t k = (uint64_t)((uint32_t)r - __ldg(sg.round_first + seg)) * kWideSeeds;
+      const uint64_t have = sg.cursor[seg];
+      base = wide_seg_base(sg, seg) + k;
+      n = have - k < (uint64_t)kWideSeeds ? (uint32_t)(have - k) : (uint32_t)kWideSeeds;
+      if (seg != cur) {  // uniform across the block
+        leave_segment();
+        cur = seg;
+        cnt.gmem = counts + (uint64_t)seg * colors;
+      }
+      if (tid == 0) atomicAdd(sg.totals + seg, (unsigned long long)n);
+    } else {
+      n = nk - base < (uint64_t)kWideSeeds ? (uint32_t)(nk - base) : (uint32_t)kWideSeeds;
+    }
     // Descriptors: pattern and row indices of each seed; recovered origins
     // the filter misses are counted by the seed's owner.
     for (uint32_t i = tid; i < n; i += T) {
@@ -263,11 +381,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
         if (!hit) cnt.add(c, 1);
       }
     }
-    if (tid == 0) seeds += n;
+    if (tid == 0 && !sg.nseg) seeds += n;
     __syncthreads();
     const uint32_t per = (n + teams - 1) / teams;
-    const uint32_t lo = min(n, team * per), hi = min(n, lo + per);
-    for (uint32_t s0 = lo; s0 < hi; s0 += S) {
+    const uint32_t first_seed = min(n, team * per), end_seed = min(n, first_seed + per);
+    for (uint32_t s0 = first_seed; s0 < end_seed; s0 += S) {
       uint4 acc[J][S];
 #pragma unroll
       for (int j = 0; j < J; ++j)
@@ -277,8 +395,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
         uint4 v[J][S][HQ];
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-          const uint32_t sd = min(s0 + (uint32_t)s, hi - 1);
-          const bool live = s0 + (uint32_t)s < hi;
+          const uint32_t sd = min(s0 + (uint32_t)s, end_seed - 1);
+          const bool live = s0 + (uint32_t)s < end_seed;
 #pragma unroll
           for (int j = 0; j < J; ++j) {
             uint32_t ri[HQ];
@@ -307,7 +425,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
       for (int s = 0; s < S; ++s) {
         const uint32_t sd = s0 + (uint32_t)s;
-        if (sd >= hi) continue;
+        if (sd >= end_seed) continue;
         const uint32_t pat = pattern[sd];
 #pragma unroll
         for (int j = 0; j < J; ++j) {
@@ -347,6 +465,10 @@ __global__ void __launch_bounds__(MAXT, MINB)
       }
     }
     __syncthreads();
+  }
+  if (sg.nseg) {
+    leave_segment();
+    return;
   }
   flush();
   if (tid == 0 && seeds) atomicAdd(total, seeds);

@@ -55,7 +55,6 @@ Server::Server(Engine& engine, std::mutex& index_mu, const ServerOptions& option
       s.d_offsets = s.ws->offsets;
       s.d_counts = device_array<uint64_t>((uint64_t)opt_.slot_requests * colors_, "counts");
       s.d_totals = device_array<unsigned long long>(opt_.slot_requests, "totals");
-      s.h_bases = pinned_array<uint8_t>(opt_.slot_bases);
       s.h_offsets = pinned_array<uint64_t>(opt_.slot_records + 1);
       s.h_counts = pinned_array<uint64_t>((uint64_t)opt_.slot_requests * colors_);
       s.h_totals = pinned_array<unsigned long long>(opt_.slot_requests);
@@ -64,6 +63,19 @@ Server::Server(Engine& engine, std::mutex& index_mu, const ServerOptions& option
     for (auto& s : slots_) release(s);
     throw;
   }
+  // The ring holds every slot's batch and two more, so submitters rarely wait
+  // while batches run.
+  ring_cap_ = (uint64_t)(opt_.slots + 2) * opt_.slot_bases;
+  spans_ = SpanRing(ring_cap_);
+  try {
+    ring_ = pinned_array<uint8_t>(ring_cap_);
+  } catch (...) {
+    for (auto& s : slots_) release(s);
+    throw;
+  }
+  pinned_bytes_ = ring_cap_ + (uint64_t)opt_.slots *
+                                  ((opt_.slot_records + 1) * 8 +
+                                   (uint64_t)opt_.slot_requests * (colors_ + 1) * 8);
   cuda_check(cudaMemGetInfo(&free_after, &total_mem), "cudaMemGetInfo");
   device_bytes_ = free_before > free_after ? free_before - free_after : 0;
   since_ = Clock::now();
@@ -74,9 +86,28 @@ void Server::release(Slot& s) {
   if (s.done) cudaEventDestroy(s.done);
   if (s.d_counts) cudaFree(s.d_counts);
   if (s.d_totals) cudaFree(s.d_totals);
-  for (void* p : {(void*)s.h_bases, (void*)s.h_offsets, (void*)s.h_counts, (void*)s.h_totals})
+  for (void* p : {(void*)s.h_offsets, (void*)s.h_counts, (void*)s.h_totals})
     if (p) cudaFreeHost(p);
   s = Slot{};
+}
+
+std::pair<uint64_t, uint64_t> Server::ring_reserve(uint64_t n) {
+  std::unique_lock<std::mutex> lk(ring_mu_);
+  uint64_t off = 0, id = 0;
+  for (;;) {
+    check(!ring_stop_, kEInval, "server is stopping");
+    if (spans_.reserve(n, &off, &id)) return {off, id};
+    ring_cv_.wait(lk);
+  }
+}
+
+void Server::ring_release(uint64_t span) {
+  if (!span) return;
+  {
+    std::lock_guard<std::mutex> lk(ring_mu_);
+    spans_.release(span);
+  }
+  ring_cv_.notify_all();
 }
 
 Server::~Server() {
@@ -84,6 +115,11 @@ Server::~Server() {
     std::lock_guard<std::mutex> lk(mu_);
     stop_ = true;
   }
+  {
+    std::lock_guard<std::mutex> lk(ring_mu_);
+    ring_stop_ = true;
+  }
+  ring_cv_.notify_all();
   cv_submit_.notify_all();
   if (thread_.joinable()) thread_.join();
   cudaSetDevice(engine_.device());
@@ -91,6 +127,7 @@ Server::~Server() {
     if (s.stream) cudaStreamSynchronize(s.stream);
     release(s);
   }
+  if (ring_) cudaFreeHost(ring_);
 }
 
 uint64_t Server::submit(const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
@@ -102,20 +139,29 @@ uint64_t Server::submit(const uint8_t* bases, uint64_t nbases, const uint64_t* o
                        std::to_string(opt_.slot_bases) + " bases, " +
                        std::to_string(opt_.slot_records) + " records): split it");
   auto r = std::make_shared<Request>();
-  r->bases.assign(bases, bases + nbases);
+  r->arrival = Clock::now();
   r->offsets.assign(offsets, offsets + records + 1);
   r->recover = recover;
   for (uint64_t i = 0; i < records; ++i) {
     check(offsets[i] <= offsets[i + 1], kEInval, "offsets must not decrease");
     r->est_tiles += engine_.tiles_for_length(offsets[i + 1] - offsets[i]);
   }
+  r->nbases = nbases;
+  if (nbases) {
+    const auto span = ring_reserve(nbases);
+    r->ring_off = span.first;
+    r->span = span.second;
+    memcpy(ring_ + r->ring_off, bases, nbases);
+  }
   uint64_t id;
   {
     std::lock_guard<std::mutex> lk(mu_);
-    check(!stop_, kEInval, "server is stopping");
+    if (stop_) {
+      ring_release(r->span);
+      raise(kEInval, "server is stopping");
+    }
     id = next_id_++;
     r->id = id;
-    r->arrival = Clock::now();
     queue_.push_back(r);
     requests_[id] = r;
     ++submitted_;
@@ -151,6 +197,7 @@ ServerStats Server::stats(bool reset) {
   st.seeds = seeds_;
   st.bases = bases_;
   st.device_bytes = device_bytes_;
+  st.pinned_bytes = pinned_bytes_;
   st.elapsed_s = std::chrono::duration<double>(Clock::now() - since_).count();
   if (!latencies_.empty()) {
     std::vector<double> v = latencies_;
@@ -185,7 +232,7 @@ bool Server::launch(Slot& s) {
     const bool rec = queue_.front()->recover;
     while (!queue_.empty() && batch.size() < opt_.slot_requests) {
       const auto& r = queue_.front();
-      const uint64_t rb = r->bases.size(), rr = r->offsets.size() - 1;
+      const uint64_t rb = r->nbases, rr = r->offsets.size() - 1;
       if (r->recover != rec || nb + rb > opt_.slot_bases || nr + rr > opt_.slot_records) break;
       batch.push_back(r);
       queue_.pop_front();
@@ -197,14 +244,25 @@ bool Server::launch(Slot& s) {
   std::vector<uint64_t> seg_records(n + 1), est(n);
   uint64_t at = 0, rec0 = 0;
   s.h_offsets[0] = 0;
+  // Copies from the ring: one per run of requests adjacent in it.
+  struct Copy {
+    uint64_t dst, src, len;
+  };
+  std::vector<Copy> copies;
   for (uint32_t i = 0; i < n; ++i) {
     const Request& r = *batch[i];
-    if (!r.bases.empty()) memcpy(s.h_bases + at, r.bases.data(), r.bases.size());
+    if (r.nbases) {
+      if (!copies.empty() && copies.back().src + copies.back().len == r.ring_off &&
+          copies.back().dst + copies.back().len == at)
+        copies.back().len += r.nbases;
+      else
+        copies.push_back(Copy{at, r.ring_off, r.nbases});
+    }
     const uint64_t rr = r.offsets.size() - 1;
     for (uint64_t j = 1; j <= rr; ++j) s.h_offsets[rec0 + j] = at + r.offsets[j];
     seg_records[i] = rec0;
     est[i] = r.est_tiles;
-    at += r.bases.size();
+    at += r.nbases;
     rec0 += rr;
   }
   seg_records[n] = rec0;
@@ -212,7 +270,10 @@ bool Server::launch(Slot& s) {
   s.busy = true;
   try {
     std::lock_guard<std::mutex> lock(index_mu_);
-    cuda_check(cudaMemcpyAsync(s.d_bases, s.h_bases, nb, cudaMemcpyHostToDevice, s.stream), "H2D");
+    for (const Copy& c : copies)
+      cuda_check(cudaMemcpyAsync(s.d_bases + c.dst, ring_ + c.src, c.len, cudaMemcpyHostToDevice,
+                                 s.stream),
+                 "H2D");
     cuda_check(cudaMemcpyAsync(s.d_offsets, s.h_offsets, (nr + 1) * 8, cudaMemcpyHostToDevice,
                                s.stream),
                "H2D");
@@ -248,16 +309,16 @@ void Server::finish(Slot& s, const std::string& error) {
         r.total = s.h_totals[i];
         ++completed_;
         seeds_ += r.total;
-        bases_ += r.bases.size();
+        bases_ += r.nbases;
         latencies_.push_back(r.latency);
       } else {
         ++failed_;
       }
-      r.bases.clear();
-      r.bases.shrink_to_fit();
       r.done = true;
     }
   }
+  // The batch's copies have run: its ring spans are free.
+  for (const auto& r : s.batch) ring_release(r->span);
   s.batch.clear();
   s.busy = false;
   cv_done_.notify_all();

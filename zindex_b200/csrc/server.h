@@ -6,16 +6,19 @@
 // zorindex.rs:341-343; query_stream.rs:163-452). A server keeps the filters
 // resident in HBM and accepts requests from any thread:
 //
-// * admission: a request is copied into host memory at submit and queued; it
-//   is admitted into a batch when a slot is free and the batch still has room
+// * admission: a request's bases are copied at submit, on the submitting
+//   thread, into a page-locked ring shared by the slots (submit waits while
+//   the ring is full: back-pressure), and the request is queued; it is
+//   admitted into a batch when a slot is free and the batch still has room
 //   (bases, records, requests) in the slot's device buffers, which are sized
 //   once at start (their bytes are the server's device memory budget);
 // * continuous batching: whenever a slot is free the scheduler takes the
 //   queued requests in arrival order that fit (same recovery flag) and
 //   launches them at once; requests that arrive while others run are taken
 //   by the next free slot, so batches grow with load;
-// * overlap: every slot has its own CUDA stream and pinned staging, so the
-//   copies of one batch overlap the kernels of another;
+// * overlap: every slot has its own CUDA stream; the scheduler only issues
+//   asynchronous copies from the ring (one per run of ring-adjacent
+//   requests), so the copies of one batch overlap the kernels of another;
 // * latency: submit-to-completion time of every request (p50/p99 in stats()).
 //
 // Results are exactly those of a query of the request alone (integer counts;
@@ -35,6 +38,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "host/span_ring.h"
 
 namespace zx {
 
@@ -50,6 +54,7 @@ struct ServerStats {
   double p50_s = 0, p99_s = 0, mean_s = 0, max_s = 0;
   double elapsed_s = 0;       // since start or the last reset
   uint64_t device_bytes = 0;  // device memory held by the slots
+  uint64_t pinned_bytes = 0;  // page-locked host memory of the ring and the slots
 };
 
 class Server {
@@ -73,7 +78,9 @@ class Server {
   using Clock = std::chrono::steady_clock;
   struct Request {
     uint64_t id = 0;
-    std::vector<uint8_t> bases;
+    uint64_t nbases = 0;
+    uint64_t ring_off = 0;          // the bases' span in the ring
+    uint64_t span = 0;              // its ring span id (0: no span, no bases)
     std::vector<uint64_t> offsets;  // records + 1, from 0
     bool recover = true;
     uint64_t est_tiles = 0;
@@ -92,7 +99,6 @@ class Server {
     uint64_t* d_offsets = nullptr;
     uint64_t* d_counts = nullptr;
     unsigned long long* d_totals = nullptr;
-    uint8_t* h_bases = nullptr;
     uint64_t* h_offsets = nullptr;
     uint64_t* h_counts = nullptr;
     unsigned long long* h_totals = nullptr;
@@ -104,6 +110,10 @@ class Server {
   bool launch(Slot& slot);
   void finish(Slot& slot, const std::string& error);
   void release(Slot& slot);
+  // Ring spans: reserve waits until n contiguous bytes of the ring are free
+  // and returns (offset, span id); release frees a span.
+  std::pair<uint64_t, uint64_t> ring_reserve(uint64_t n);
+  void ring_release(uint64_t span);
 
   Engine& engine_;
   std::mutex& index_mu_;
@@ -111,6 +121,14 @@ class Server {
   uint64_t colors_ = 0;
   uint64_t device_bytes_ = 0;
   std::vector<Slot> slots_;
+
+  std::mutex ring_mu_;
+  std::condition_variable ring_cv_;
+  uint8_t* ring_ = nullptr;  // page-locked request bases
+  uint64_t ring_cap_ = 0;
+  SpanRing spans_;
+  bool ring_stop_ = false;
+  uint64_t pinned_bytes_ = 0;
 
   std::mutex mu_;  // queue, requests, stats
   std::condition_variable cv_submit_, cv_done_;

@@ -227,8 +227,13 @@ def collect(work: Path, out: Path, reps: int = 5, settings=None, log=print) -> d
             tuner = Autotuner(reps=reps)
             default = ix.default_launch()
             defaults[name] = dict(default, blocks=0)
-            for launch in REGISTER_LAUNCHES:
-                full = dict(default, **launch, blocks=0, stage_bytes=0)
+            # The fused kernel's launches; a wide-row default is one more row.
+            fused = ix.default_fused_launch()
+            launches = [dict(fused, **launch, blocks=0, stage_bytes=0, wide=0)
+                        for launch in REGISTER_LAUNCHES]
+            if default["wide"]:
+                launches.append(dict(default, blocks=0))
+            for full in launches:
                 ms = tuner.time_config(ix, batch, full)
                 rows.append({"setting": name, "features": feats, "launch": full, "e2e": False,
                              "ms": ms})
