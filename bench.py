@@ -69,9 +69,10 @@ CONFIGS = {
                      "genome_model": "70% iid + 30% core-pool", "k": 49, "m": 31, "hashes": 3,
                      "fingerprint_bits": 16, "index_mode": "minimizers", "reads": 200_000,
                      "read_len_bp": "lognormal median 2000, clipped 100-100000", "sourced": 0.8,
-                     "substitutions": 0.01, "n_runs": 0.1},
+                     "substitutions": 0.01, "n_runs": 0.1,
+                     "index_build": "zx_build --device (the GPU builder)"},
         "synth": "pool:2048:500000:8000000:1",
-        "build": ["-i", "minimizers", "-k", "49", "-m", "31", "-H", "3", "-b", "16"],
+        "build": ["-i", "minimizers", "-k", "49", "-m", "31", "-H", "3", "-b", "16", "--device"],
         "reads": ["--kind", "long", "--reads", "200000", "--length", "2000", "--sourced", "0.8",
                   "--subst", "0.01", "--n-runs", "0.1"],
     },
@@ -81,9 +82,10 @@ CONFIGS = {
                      "genome_model": "70% iid + 30% core-pool", "k": 31, "hashes": 8,
                      "fingerprint_bits": 4, "index_mode": "kmers", "reads": 20_000,
                      "read_len_bp": 150, "sourced": 0.6, "substitutions": 0.005,
-                     "scaled": "genome lengths 1-6 Mbp scaled down 50x (the host builder cannot "
-                               "build the 64 GB index in a run); rows are the full 8 KiB"},
-        "synth": "pool:16384:20000:120000:1", "build": ["-k", "31", "-H", "8", "-b", "4"],
+                     "scaled": "genome lengths 1-6 Mbp scaled down 50x (a fast stand-in for c4); "
+                               "rows are the full 8 KiB",
+                     "index_build": "zx_build --device (the GPU builder)"},
+        "synth": "pool:16384:20000:120000:1", "build": ["-k", "31", "-H", "8", "-b", "4", "--device"],
         "reads": ["--kind", "short", "--reads", "20000", "--length", "150", "--sourced", "0.6",
                   "--subst", "0.005"],
         # 64 KiB of rows per seed: fewer served requests keep the run bounded.
@@ -206,11 +208,16 @@ def launches_per_step(ix, nbases: int, records: int) -> int:
     reduction, once or once per round of a split minimizer query or of the
     wide-row form (plus the extraction kernel each round, and for ordered
     wide rounds the CUB radix sort's kernels: histogram, scan and three
-    onesweep passes over 20 bits)."""
+    onesweep passes over 20 bits). Small batches take two or three."""
     lc, info = ix.launch(), ix.info
     plan = 5
     probe = 1 + (1 if lc["smem_counters"] else 0)
     tiles_bound = nbases // 256 + records + nbases // 16384 + 1
+    split = lc.get("split") and info.index_mode == 1 and lc["planes"] == 1 and lc["stage_bytes"] == 0
+    if records <= 4096 and nbases <= (1 << 20) and not lc.get("wide") and not split:
+        # Small batches: one block packs and plans, then the fused kernel
+        # (adding into the caller's counters for up to 1,024 colours).
+        return 1 + 1 + (1 if lc["smem_counters"] and ix.colors > 1024 else 0)
     if lc.get("wide"):
         # Wide-row form: per round the dense extraction, the probe and (with
         # shared counters) the reduction.
@@ -430,14 +437,17 @@ class CpuOracle:
         self.fast = bool(lib.oracle_fast_serves(self.h))
         self.kind = "port-simd" if self.fast else "port"
 
-    def run(self, bases, offsets, n, colors):
+    def run(self, bases, offsets, n, colors, checker=False):
+        """(seeds, seconds, counts) of the first n records; checker=True takes
+        the scalar lookup (the parity checker) instead of the fast one."""
         if not 0 < n <= len(offsets) - 1:
             raise ValueError(f"oracle sample of {n} records outside a batch of {len(offsets) - 1}")
         ct = self.ct
         off = np.ascontiguousarray(offsets[: n + 1])
         counts = np.zeros(colors, dtype=np.uint64)
         total, secs = ct.c_uint64(), ct.c_double()
-        fn = self.lib.oracle_query_handle_fast if self.fast else self.lib.oracle_query_handle
+        fast = self.fast and not checker
+        fn = self.lib.oracle_query_handle_fast if fast else self.lib.oracle_query_handle
         rc = fn(self.h, bases.ctypes.data_as(ct.c_void_p),
                                           off.ctypes.data_as(ct.POINTER(ct.c_uint64)), n, self.cores,
                                           counts.ctypes.data_as(ct.POINTER(ct.c_uint64)), colors,
@@ -486,6 +496,75 @@ def cpu_baseline(index, bases, offsets, colors, target_s=15.0):
     return {"value": seeds / secs, "unit": "seeds/s", "cores": orc.cores, "kind": orc.kind,
             "sample": f"first {n} of the {len(offsets) - 1:,} query records ({seeds} seeds), query only "
                       f"(index load excluded), {secs:.2f}s"}, n, counts
+
+
+# Configurations measured beside the default line (their batched step, kernel
+# roofline and an oracle parity sample), and the reads of the parity sample.
+OTHER_CONFIGS = {"c3": 300, "c4s": 2000}
+
+
+def other_config(zx, torch, name, cache: Path, steps: int):
+    """The batched step of another configuration: index (GPU builder) and
+    reads prepared like the default line's, device-resident batch, `steps`
+    timed steps (inputs larger than L2), the probe's kernel time against the
+    copy peak, and the first reads' counts against the oracle's."""
+    cfg = CONFIGS[name]
+    index_dir, bases, offsets = prepare(cache, 0, name)
+    records = len(offsets) - 1
+    dev = torch.device("cuda", 0)
+    with zx.Index(index_dir) as ix:
+        info = ix.info
+        d_bases = torch.from_numpy(bases).to(dev)
+        d_off = torch.from_numpy(offsets.view(np.int64)).to(dev)
+        d_counts = torch.zeros(ix.colors, dtype=torch.int64, device=dev)
+        d_total = torch.zeros(1, dtype=torch.int64, device=dev)
+        stream = torch.cuda.current_stream(dev)
+
+        def step(graph=True):
+            d_counts.zero_()
+            d_total.zero_()
+            ix.query_device(d_bases.data_ptr(), len(bases), d_off.data_ptr(), records,
+                            d_counts.data_ptr(), d_total.data_ptr(), stream=stream.cuda_stream,
+                            use_graph=graph)
+
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize(dev)
+        seeds = int(d_total.item())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / steps
+        ix.set_timing(True)
+        kms = []
+        for _ in range(3):
+            step(graph=False)
+            kms.append(ix.last_kernel_ms())
+        ix.set_timing(False)
+        kernel_ms = statistics.median(kms)
+        rec_bytes = 8 if info.abandoned_hashes else 0
+        alg = seeds * (info.gather_bytes_per_seed + rec_bytes) + len(bases) * 3 // 8
+        peak, peak_kind = hbm_peak()
+        n = min(OTHER_CONFIGS[name], records)
+        got, got_total = ix.query_records(bases[: int(offsets[n])], offsets[: n + 1])
+        launch = ix.launch()
+    orc = CpuOracle(index_dir)
+    _, _, want = orc.run(bases, offsets, n, len(got), checker=True)
+    orc.close()
+    achieved = alg / (kernel_ms / 1e3) / 1e9
+    return {"workload": cfg["workload"], "value": seeds / (ms / 1e3), "unit": "seeds/s",
+            "ms_per_step": ms, "steps": steps, "seeds_per_step": seeds,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "kernel_ms": kernel_ms,
+                         "algorithmic_bytes_per_launch": int(alg),
+                         "traffic": (TRAFFIC_BYTES_PER_SEED[name] * seeds / 1e9
+                                     if name in TRAFFIC_BYTES_PER_SEED else None)},
+            "launch": launch, "resident_bytes": int(info.resident_bytes),
+            "parity_vs_oracle_sample": bool(np.array_equal(got, want)),
+            "parity_sample_reads": n}
 
 
 def reference_arm(args):
@@ -832,8 +911,22 @@ def ours(args):
             "cpu_baseline": cb,
             "parity_vs_oracle_sample": parity,
         }
+        if world == 1 and args.config == "c2" and not args.no_other_configs:
+            ix.close()
+            ix = None
+            others = {}
+            for name in OTHER_CONFIGS:
+                log(f"stage: {name}")
+                torch.cuda.empty_cache()
+                try:
+                    others[name] = other_config(zx, torch, name, Path(args.cache),
+                                                max(3, min(args.steps, 5)))
+                except Exception as e:  # reported, never hides the default line
+                    others[name] = {"error": f"{type(e).__name__}: {e}"}
+            line["other_configs"] = others
         print(json.dumps(line), flush=True)
-    ix.close()
+    if ix is not None:
+        ix.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -847,6 +940,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cache", default=os.environ.get("ZX_BENCH_CACHE", "/tmp/zx_bench"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="default line only (no c3 / c4s measurements beside it)")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c2",
                     help="workload: c2 (default line) or another configuration")
     ap.add_argument("--reads", type=int, default=None,

@@ -75,6 +75,32 @@ def test_report_matches_oracle(gpu, oracle, tmp_path_factory, tmp_path, opts):
         assert out.read_bytes() == oracle.records_report(ix, q, recover=False)
 
 
+@pytest.mark.parametrize("colors,opts", [(4096, dict(k=31, H=8, b=4)),
+                                         (2048, dict(k=25, H=3, b=16, groups="4,5,6"))],
+                         ids=["c4096-H8-b4", "c2048-H3-b16-multi"])
+def test_wide_row_report_with_threshold_pruning(gpu, oracle, tmp_path_factory, tmp_path, colors,
+                                                opts):
+    """Per-record reports on wide-row indexes: with min_ratio > 0 the wide
+    probe stops loading the row chunks whose colours can no longer reach the
+    threshold (exact pruning), and the report bytes still equal the oracle's
+    (colours below the threshold are not reported, whatever their partial
+    counts). Long records take several probe rounds (no pruning across
+    blocks); a multi-member group's chunks are never pruned."""
+    import zindex_b200 as zx
+
+    ix, genomes = index_for(tmp_path_factory, colors=colors, length=3000, seed=91, min_docs=1,
+                            **opts)
+    q, _ = query_file(tmp_path / "q.fa", genomes, n=400, seed=9)
+    with zx.Index(ix) as index:
+        assert index.launch()["wide"] == 1
+        for fmt in ("compact", "tsv"):
+            for min_ratio in (1e-9, 0.3, 0.8, 1.0):
+                out = tmp_path / f"w-{fmt}-{min_ratio}.tsv"
+                index.query_records_report(q, out, min_ratio=min_ratio, fmt=fmt)
+                want = oracle.records_report(ix, q, min_ratio=min_ratio, fmt=fmt)
+                assert out.read_bytes() == want, (fmt, min_ratio)
+
+
 def test_batch_sizes_fastq_and_cli(gpu, oracle, tmp_path_factory, tmp_path):
     import zindex_b200 as zx
 

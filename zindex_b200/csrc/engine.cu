@@ -139,6 +139,10 @@ FusedFn fused_for(int mode, const QueryLaunch& l) {
   return v == 2 ? fused_mode<2, 2>(mode) : fused_mode<2, 0>(mode);
 }
 
+// Small batches with at most this many colours count with global atomics
+// into the caller's counters (flushed planes make them rare).
+constexpr size_t kSmallColors = 1024;
+
 using WideFn = void (*)(const DevIndex*, const ColorLoc*, const uint64_t*,
                        const unsigned long long*, int, uint32_t, uint32_t*, uint64_t*,
                        unsigned long long*, WideRound);
@@ -1094,13 +1098,13 @@ std::unique_ptr<Workspace> Engine::make_workspace() {
   return ws;
 }
 
-void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records) {
+void Engine::ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records, bool segmented) {
   const uint64_t colors = m_.colors.size();
   // Split minimizer and wide-row queries: key slots allocated before any graph capture.
   if (kernel_mode(launch_) == 4 || wide_form(launch_)) ensure_split_capacity(ws);
   const bool rounds = nbases / kTileWindows + records + nbases / kFindereTask + 1 > kSplitTiles;
   if (wide_form(launch_) && rounds) ensure_wide_pipeline(ws);
-  if (wide_form(launch_) && launch_.order) {
+  if (wide_form(launch_) && launch_.order && !segmented) {
     ensure_order_capacity(ws, 0);
     if (rounds) ensure_order_capacity(ws, 1);
   }
@@ -1262,13 +1266,24 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                      unsigned long long* total, cudaStream_t s) {
   if (m_.homopolymer_compression) compress_homopolymers(ws, bases, nbases, offsets, records, s);
   const uint64_t words = nbases / 32 + 2;
-  {
+  QueryLaunch l = launch_;
+  // Small batches: one block packs and plans (one launch for pack, count,
+  // scan and fill), and with few colours the fused kernel adds into the
+  // caller's counters (no reduction launch).
+  const bool small = records <= kSmallRecords && nbases <= kSmallBases && !wide_form(l) &&
+                     kernel_mode(l) != 4;
+  if (small) {
+    small_plan_kernel<<<1, 1024, 0, s>>>(bases, nbases, ws.packed, ws.invalid, words, offsets,
+                                         (uint32_t)records, span(), m_.index_mode == kFindere,
+                                         ws.tile_first, ws.tiles, ws.error);
+    cuda_check(cudaGetLastError(), "small_plan_kernel");
+    if (m_.colors.size() <= kSmallColors) l.smem_counters = 0;
+  } else {
     int grid = (int)std::min<uint64_t>((words + 255) / 256, (uint64_t)sms_ * 16);
     pack_kernel<<<std::max(grid, 1), 256, 0, s>>>(bases, nbases, ws.packed, ws.invalid, words);
     cuda_check(cudaGetLastError(), "pack_kernel");
+    plan_tiles(ws, offsets, records, nbases, s);
   }
-  plan_tiles(ws, offsets, records, nbases, s);
-  QueryLaunch l = launch_;
   const int kmode = kernel_mode(l);
   const size_t smem = fused_smem_bytes(l);
   const int blocks_cap = max_blocks(l);
@@ -1343,7 +1358,7 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
 
 void Engine::run_wide(Workspace& ws, const BatchView& bv, uint64_t tiles_bound, bool recover,
                       uint64_t* counts, unsigned long long* total, uint32_t segments,
-                      cudaStream_t s) {
+                      cudaStream_t s, double prune_ratio) {
   // Rounds of up to kSplitTiles tiles; per round the extraction kernel
   // appends the tiles' seeds to one dense list (segmented: each segment's
   // seeds to its own part of it), the wide probe counts them, and the block
@@ -1395,6 +1410,8 @@ void Engine::run_wide(Workspace& ws, const BatchView& bv, uint64_t tiles_bound, 
       sg.totals = total;
       sg.nseg = segments;
       sg.tile_lo = rb.tile_lo;
+      sg.tile_hi = rb.tile_hi;
+      sg.min_ratio = prune_ratio;
     }
     // Ordered round: every slot the round may fill gets a sort key (the
     // unfilled ones all ones, so a stable sort leaves them behind the keys).
@@ -1523,7 +1540,7 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
                             const uint64_t* offsets, uint64_t records, const uint64_t* seg_records,
                             const uint64_t* est_tiles, uint32_t segments, bool recover,
                             uint64_t* counts, unsigned long long* totals, cudaStream_t s,
-                            int warps) {
+                            int warps, double prune_ratio) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   check(segments > 0, kEInval, "a segmented query needs at least one segment");
   check(warps >= 0 && warps <= 8, kEInval, "warps per block must be in 1..8");
@@ -1531,7 +1548,7 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
         "segments must span the records");
   for (uint32_t i = 0; i < segments; ++i)
     check(seg_records[i] <= seg_records[i + 1], kEInval, "segment records must be non-decreasing");
-  ensure_capacity(ws, nbases, records);
+  ensure_capacity(ws, nbases, records, true);
   ensure_segment_capacity(ws, segments);
   // The pinned staging is reused: wait until the previous call's copies ran.
   cuda_check(cudaEventSynchronize(ws.seg_staged), "segment staging");
@@ -1555,7 +1572,7 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
     BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records,
                  ws.fstate};
     const uint64_t tiles_bound = nbases / kTileWindows + records + nbases / kFindereTask + 1;
-    run_wide(ws, bv, tiles_bound, recover, counts, totals, segments, s);
+    run_wide(ws, bv, tiles_bound, recover, counts, totals, segments, s, prune_ratio);
     return;
   }
   QueryLaunch l = fused_launch(launch_);
@@ -1631,6 +1648,7 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
 
 void Engine::record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases,
                            const uint64_t* offsets, uint64_t records, bool recover,
+                           double prune_ratio,
                            const std::function<void(uint64_t, uint64_t)>& on_group) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   check(offsets[0] == 0 && offsets[records] == nbases, kEInval, "offsets must span the bases");
@@ -1679,7 +1697,7 @@ void Engine::record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     while (r1 < records && r1 - r0 < gmax && offsets[r1 + 1] - offsets[r0] <= group_bases)
       tiles += tiles_for_length(offsets[r1 + 1] - offsets[r1]), ++r1;
     const uint64_t n = r1 - r0, b0 = offsets[r0], nb = offsets[r1] - b0;
-    ensure_capacity(ws, nb, n);
+    ensure_capacity(ws, nb, n, true);
     ensure_host_capacity(ws, nb, n);
     seg.resize(n + 1);
     est.resize(n);
@@ -1706,7 +1724,7 @@ void Engine::record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     const uint64_t mean = (tiles + n - 1) / n;
     if (mean < (uint64_t)launch_.warps) warps = mean <= 2 ? 2 : (mean <= 4 ? 4 : 8);
     query_segments(ws, ws.bases, nb, ws.offsets, n, seg.data(), est.data(), (uint32_t)n, recover,
-                   ws.rec_counts, ws.rec_totals, s, warps);
+                   ws.rec_counts, ws.rec_totals, s, warps, prune_ratio);
     on_group(r0, n);
     cuda_check(cudaStreamSynchronize(s), "per-record query");
     check_error_word(ws);
@@ -1720,7 +1738,7 @@ void Engine::query_per_record(Workspace& ws, const uint8_t* bases, uint64_t nbas
   const uint64_t colors = m_.colors.size();
   cudaStream_t s = ws.stream;
   auto run = [&](const uint8_t* b, uint64_t* c, uint64_t* t) {
-    record_groups(ws, b, nbases, offsets, records, recover, [&](uint64_t r0, uint64_t n) {
+    record_groups(ws, b, nbases, offsets, records, recover, 0.0, [&](uint64_t r0, uint64_t n) {
       cuda_check(cudaMemcpyAsync(c + r0 * colors, ws.rec_counts, n * colors * 8,
                                  cudaMemcpyDeviceToHost, s),
                  "D2H");
@@ -1795,7 +1813,10 @@ void Engine::query_record_hits(Workspace& ws, const uint8_t* bases, uint64_t nba
   out.first.assign(records + 1, 0);
   out.colors.clear();
   out.counts.clear();
-  record_groups(ws, bases, nbases, offsets, records, recover, [&](uint64_t r0, uint64_t n) {
+  // Threshold pruning in the wide-row form: colours that cannot reach the
+  // ratio may stop counting early (their counts stay below it).
+  record_groups(ws, bases, nbases, offsets, records, recover, min_ratio,
+                [&](uint64_t r0, uint64_t n) {
     const int grid = (int)std::min<uint64_t>((n + 7) / 8, (uint64_t)sms_ * 16);
     count_record_hits_kernel<<<grid, 256, 0, s>>>(ws.rec_counts, ws.rec_totals, n, colors,
                                                   min_ratio, ws.rec_hits);

@@ -159,9 +159,10 @@ class Engine {
   uint64_t gather_sector_bytes_per_seed() const;
 
   std::unique_ptr<Workspace> make_workspace();
-  // Sizes a workspace's device buffers for batches up to these sizes.
+  // Sizes a workspace's device buffers for segmented batches up to these
+  // sizes (the request server's slots).
   void reserve(Workspace& ws, uint64_t nbases, uint64_t records) {
-    ensure_capacity(ws, nbases, records);
+    ensure_capacity(ws, nbases, records, true);
   }
   Workspace& default_workspace() { return *ws_; }
 
@@ -205,7 +206,8 @@ class Engine {
   void query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
                       uint64_t records, const uint64_t* seg_records, const uint64_t* est_tiles,
                       uint32_t segments, bool recover, uint64_t* counts,
-                      unsigned long long* totals, cudaStream_t stream, int warps = 0);
+                      unsigned long long* totals, cudaStream_t stream, int warps = 0,
+                      double prune_ratio = 0.0);
   // Per-record query of host records (--records): counts (records x colours,
   // row-major) and totals (records) receive each record's own result, exactly
   // as if the record were queried alone. Records run in groups whose device
@@ -244,7 +246,9 @@ class Engine {
  private:
   void load(const std::string& dir, const OpenOptions& options);
   void release();  // frees every device allocation and event of the engine
-  void ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records);
+  // Device buffers of a query of nbases / records (segmented queries do not
+  // sort their rounds: no ordered-round buffers).
+  void ensure_capacity(Workspace& ws, uint64_t nbases, uint64_t records, bool segmented = false);
   // Homopolymer compression on the device (lib.rs:211-222 per ACGT run):
   // replaces (bases, offsets) by the compressed batch in the workspace.
   void compress_homopolymers(Workspace& ws, const uint8_t*& bases, uint64_t nbases,
@@ -270,15 +274,20 @@ class Engine {
   // one query into counts / *total; segments > 0: a segmented query, request
   // s into counts + s x colours and total[s] (the segment tables and their
   // per-round cursors already in ws).
+  // prune_ratio > 0 (segmented per-record reports): threshold pruning of the
+  // colours that cannot reach count / total >= prune_ratio.
   void run_wide(Workspace& ws, const BatchView& bv, uint64_t tiles_bound, bool recover,
-                uint64_t* counts, unsigned long long* total, uint32_t segments, cudaStream_t s);
+                uint64_t* counts, unsigned long long* total, uint32_t segments, cudaStream_t s,
+                double prune_ratio = 0.0);
   // Device tables of a segmented launch for `segments` requests.
   void ensure_segment_capacity(Workspace& ws, uint32_t segments);
   // Runs host records in device groups (one segment per record): after each
   // group's launch, on_group(r0, n) enqueues its read-back on ws.stream; the
   // stream is then synchronised and the error word checked.
+  // prune_ratio > 0: the groups' counts are only exact for the colours with
+  // count / total >= prune_ratio (the others may stop early, below it).
   void record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases, const uint64_t* offsets,
-                     uint64_t records, bool recover,
+                     uint64_t records, bool recover, double prune_ratio,
                      const std::function<void(uint64_t, uint64_t)>& on_group);
 
   Manifest m_;

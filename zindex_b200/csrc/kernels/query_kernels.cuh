@@ -38,20 +38,18 @@ __device__ __forceinline__ uint32_t record_windows(const uint64_t* offsets, uint
 }
 
 // Tiles per record. Findere tiles never cross a 16,384-window task.
+__device__ __forceinline__ uint32_t record_tiles(uint32_t w, int findere) {
+  if (!findere) return (w + kTileWindows - 1) / kTileWindows;
+  const uint32_t full = w / kFindereTask, rest = w % kFindereTask;
+  return full * (kFindereTask / kTileWindows) + (rest + kTileWindows - 1) / kTileWindows;
+}
+
 __global__ void count_tiles_kernel(const uint64_t* __restrict__ offsets, uint64_t records,
                                    uint64_t nbases, int span, int findere,
                                    uint32_t* __restrict__ counts, uint32_t* __restrict__ err) {
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < records;
        r += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t w = record_windows(offsets, r, span, nbases, err);
-    uint32_t n;
-    if (!findere) {
-      n = (w + kTileWindows - 1) / kTileWindows;
-    } else {
-      uint32_t full = w / kFindereTask, rest = w % kFindereTask;
-      n = full * (kFindereTask / kTileWindows) + (rest + kTileWindows - 1) / kTileWindows;
-    }
-    counts[r] = n;
+    counts[r] = record_tiles(record_windows(offsets, r, span, nbases, err), findere);
   }
 }
 
@@ -69,6 +67,50 @@ __global__ void fill_tiles_kernel(const uint64_t* __restrict__ offsets, uint64_t
       w0 = end;
     }
   }
+}
+
+// Small batches (a few thousand records, up to 1 MiB of bases): one block
+// packs the bases and plans the tiles (count, scan and fill), so the query is
+// two launches instead of six.
+constexpr uint32_t kSmallRecords = 4096;
+constexpr uint64_t kSmallBases = 1ull << 20;
+
+__global__ void __launch_bounds__(1024)
+    small_plan_kernel(const uint8_t* __restrict__ bases, uint64_t nbases,
+                      uint64_t* __restrict__ packed, uint32_t* __restrict__ invalid,
+                      uint64_t words, const uint64_t* __restrict__ offsets, uint32_t records,
+                      int span, int findere, uint32_t* __restrict__ tile_first,
+                      Tile* __restrict__ tiles, uint32_t* __restrict__ err) {
+  __shared__ uint32_t sums[1024];
+  const uint32_t T = blockDim.x, tid = threadIdx.x;
+  for (uint64_t w = tid; w < words; w += T) pack_word(bases, nbases, packed, invalid, w);
+  // Each thread plans a contiguous run of records: their tile counts, a
+  // block scan of the runs' sums, then the tiles.
+  const uint32_t per = (records + T - 1) / T;
+  const uint32_t lo = min(records, tid * per), hi = min(records, lo + per);
+  uint32_t mine = 0;
+  for (uint32_t r = lo; r < hi; ++r)
+    mine += record_tiles(record_windows(offsets, r, span, nbases, err), findere);
+  sums[tid] = mine;
+  __syncthreads();
+  for (uint32_t off = 1; off < T; off <<= 1) {
+    const uint32_t v = tid >= off ? sums[tid - off] : 0u;
+    __syncthreads();
+    sums[tid] += v;
+    __syncthreads();
+  }
+  uint32_t t = tid ? sums[tid - 1] : 0u;
+  for (uint32_t r = lo; r < hi; ++r) {
+    tile_first[r] = t;
+    const uint32_t w = record_windows(offsets, r, span, nbases, nullptr);
+    for (uint32_t w0 = 0; w0 < w;) {
+      const uint32_t task = (w0 / kFindereTask) * kFindereTask;
+      const uint32_t end = min(w, min(w0 + kTileWindows, task + kFindereTask));
+      tiles[t++] = Tile{r, w0, end - w0, task};
+      w0 = end;
+    }
+  }
+  if (tid == T - 1) tile_first[records] = sums[T - 1];
 }
 
 struct BatchView {

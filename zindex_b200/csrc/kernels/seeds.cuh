@@ -22,11 +22,10 @@ __device__ __forceinline__ uint32_t dev_code(uint8_t b) { return encode_base(b);
 
 // K0: ASCII bases -> packed 2-bit words + invalid masks. Word w covers bases
 // 32w..32w+31; positions past `n` are marked invalid.
-__global__ void pack_kernel(const uint8_t* __restrict__ bases, uint64_t n,
-                            uint64_t* __restrict__ packed, uint32_t* __restrict__ invalid,
-                            uint64_t words) {
-  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words;
-       w += (uint64_t)gridDim.x * blockDim.x) {
+__device__ __forceinline__ void pack_word(const uint8_t* __restrict__ bases, uint64_t n,
+                                          uint64_t* __restrict__ packed,
+                                          uint32_t* __restrict__ invalid, uint64_t w) {
+  {
     uint64_t base = w * 32, v = 0;
     uint32_t inv = 0;
     if (base + 32 <= n && (((uintptr_t)(bases + base)) & 15) == 0) {
@@ -49,6 +48,14 @@ __global__ void pack_kernel(const uint8_t* __restrict__ bases, uint64_t n,
     packed[w] = v;
     invalid[w] = inv;
   }
+}
+
+__global__ void pack_kernel(const uint8_t* __restrict__ bases, uint64_t n,
+                            uint64_t* __restrict__ packed, uint32_t* __restrict__ invalid,
+                            uint64_t words) {
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words;
+       w += (uint64_t)gridDim.x * blockDim.x)
+    pack_word(bases, n, packed, invalid, w);
 }
 
 struct PackedView {

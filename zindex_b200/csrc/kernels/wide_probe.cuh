@@ -95,7 +95,27 @@ struct WideRound {
   uint32_t tile_lo = 0;                   // first tile of the extraction round
   uint32_t* order_keys = nullptr;         // sort keys of the dense list (ordered rounds)
   uint64_t seed = 0;                      // the index seed (first hash)
+  // Segmented per-record reports: colours reported when count / total >=
+  // min_ratio (> 0 turns on threshold pruning); tile_hi ends the round.
+  double min_ratio = 0.0;
+  uint32_t tile_hi = 0;
 };
+
+// Smallest count c with c / total >= ratio in IEEE double division: the
+// report's own test (minimum_matches, src/power_merge/record_query.rs:12-26).
+__device__ __forceinline__ uint64_t minimum_matches(uint64_t total, double ratio) {
+  if (total == 0 || ratio == 0.0) return 0;
+  uint64_t lo = 0, hi = total;
+  while (lo < hi) {
+    const uint64_t mid = lo + (hi - lo) / 2;
+    if (__ddiv_rn((double)mid, (double)total) >= ratio) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+// Threshold pruning: a chunk's fields are checked every kPruneStep seeds.
+constexpr uint32_t kPruneStep = 16;
 
 __device__ __forceinline__ uint64_t wide_seg_base(const WideRound& sg, uint32_t s) {
   const uint32_t t = __ldg(sg.seg_tiles + s);
@@ -295,6 +315,32 @@ __global__ void __launch_bounds__(MAXT, MINB)
 
   unsigned long long seeds = 0;
   uint32_t steps = 0;
+  // Threshold pruning (record_query.rs:28-107, exact): in a per-record report
+  // a colour is reported only with at least `need` of its record's seeds.
+  // Its final count is at most its block counter plus the segment's seeds
+  // this team has not probed yet (the other rounds' hits are at most their
+  // seeds), so once no field of a chunk can reach `need` the thread stops
+  // loading that chunk for the rest of the segment. Counts of pruned
+  // colours stay below the threshold, so the reported hits are unchanged.
+  // Chunks of multi-member groups are never pruned; segments split across
+  // extraction rounds and global counters turn pruning off.
+  uint32_t alive = (1u << J) - 1u;
+  uint64_t need = 0, seg_total = 0, seen = 0;
+  bool prune = false;
+  auto prune_chunks = [&]() {
+    const uint64_t rest = seg_total - seen;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      if (!((alive >> j) & 1u) || !col[j] || multi[j]) continue;
+      const DevClass& C = ix.cls[cls[j]];
+      uint32_t best = 0;
+      for (uint32_t x = valid[j]; x; x &= x - 1) {
+        const uint32_t c = __ldg(C.group_color + wide_group(g0[j], __ffs(x) - 1, b, lb));
+        best = max(best, scount[c]);
+      }
+      if ((uint64_t)best + rest < need) alive &= ~(1u << j);
+    }
+  };
   // Segmented: the block's counters belong to one segment at a time. They
   // go to that segment's counts when the block moves on (a plain add when
   // the segment has one round, so this block is its only writer).
@@ -333,6 +379,15 @@ __global__ void __launch_bounds__(MAXT, MINB)
         leave_segment();
         cur = seg;
         cnt.gmem = counts + (uint64_t)seg * colors;
+        alive = (1u << J) - 1u;
+        seen = 0;
+        prune = false;
+        if (sg.min_ratio > 0.0 && scount && __ldg(sg.seg_tiles + seg) >= sg.tile_lo &&
+            __ldg(sg.seg_tiles + seg + 1) <= sg.tile_hi) {
+          seg_total = have;  // the whole segment is in this round
+          need = minimum_matches(have, sg.min_ratio);
+          prune = need > 0;
+        }
       }
       if (tid == 0) atomicAdd(sg.totals + seg, (unsigned long long)n);
     } else {
@@ -408,7 +463,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
             for (int q = 0; q < HQ; ++q) {
               v[j][s][q] = make_uint4(0, 0, 0, 0);
-              if (live && col[j] && i0 + q < H) v[j][s][q] = ld_row_chunk(col[j] + (uint64_t)ri[q] * stride[j]);
+              if (live && col[j] && ((alive >> j) & 1u) && i0 + q < H)
+                v[j][s][q] = ld_row_chunk(col[j] + (uint64_t)ri[q] * stride[j]);
             }
           }
         }
@@ -433,7 +489,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
           uint32_t d = 0;
 #pragma unroll
           for (int w = 0; w < 4; ++w) d |= zero_fields_hi(w4[w] ^ pat, hi) >> (uint32_t)(b - 1 - w);
-          d &= valid[j];
+          d &= ((alive >> j) & 1u) ? valid[j] : 0u;
           const uint32_t slow = d & multi[j];
           uint32_t m = d & ~slow;
 #pragma unroll
@@ -458,9 +514,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
             }
           }
         }
-        if (++steps == kWideFlush) {
+        ++seen;
+        if (++steps == kWideFlush || (prune && seen % kPruneStep == 0)) {
           flush();
           steps = 0;
+          if (prune) prune_chunks();
         }
       }
     }
