@@ -207,8 +207,8 @@ def launches_per_step(ix, nbases: int, records: int) -> int:
     then the fused query kernel and, with shared counters, the counter
     reduction, once or once per round of a split minimizer query or of the
     wide-row form (plus the extraction kernel each round, and for ordered
-    wide rounds the CUB radix sort's kernels: histogram, scan and three
-    onesweep passes over 20 bits). Small batches take two or three."""
+    wide rounds the counting sort's bucket count, scan and scatter). Small
+    batches take two or three."""
     lc, info = ix.launch(), ix.info
     plan = 5
     probe = 1 + (1 if lc["smem_counters"] else 0)
@@ -222,7 +222,7 @@ def launches_per_step(ix, nbases: int, records: int) -> int:
         # Wide-row form: per round the dense extraction, the probe and (with
         # shared counters) the reduction.
         rounds = -(-tiles_bound // 262144)
-        sort = 5 if lc.get("order") else 0
+        sort = 3 if lc.get("order") else 0
         return plan + rounds * (1 + sort + probe)
     if lc.get("split") and info.index_mode == 1 and lc["planes"] == 1 and lc["stage_bytes"] == 0:
         tiles_bound = nbases // 256 + records + nbases // 16384 + 1
@@ -742,6 +742,11 @@ def ours(args):
         return statistics.median(ts) * 1e3
 
     default_launch = ix.launch()
+    # Ordered wide-row rounds against extraction order (same launch otherwise).
+    unordered = None
+    if default_launch.get("wide") and default_launch.get("order"):
+        unordered = seeds / (step_ms(dict(default_launch, order=0)) / 1e3)
+        ix.set_launch(**default_launch)
     pick, planned = planned_form(ix, bases, offsets, seeds, step_ms, e2e_ms)
     ix.set_launch(**pick)
     times = []
@@ -896,6 +901,7 @@ def ours(args):
             "forms": {"plain_seeds_per_s": plain_rate, "batched_seeds_per_s": value / world,
                       "served_seeds_per_s": served["closed_loop"]["seeds_per_s"],
                       "planned_seeds_per_s": world * planned["seeds_per_s"],
+                      "unordered_seeds_per_s": unordered,
                       "served": served, "planned": planned, "per_record": per_record},
             "query_file": query_file,
             "index_load": {"seconds": load_s, "banks_s": info.load_banks_s,

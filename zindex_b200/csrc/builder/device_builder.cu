@@ -339,8 +339,15 @@ __global__ void assign_kernel(const Filter* __restrict__ f, uint32_t nf,
     const uint64_t key = K[es.x];
     uint32_t v = (uint32_t)fingerprint(key, seed, bits);
     positions(key, seed, F.slots, H, seg, pos);
-    for (int h = 0; h < H; ++h)
-      if ((uint32_t)pos[h] != es.y) v ^= C[pos[h]];
+    // The key's cells are distinct: 8 of them are loaded together.
+    for (int h0 = 0; h0 < H; h0 += 8) {
+      uint32_t cv[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        cv[i] = h0 + i < H && (uint32_t)pos[h0 + i] != es.y ? C[pos[h0 + i]] : 0u;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v ^= cv[i];
+    }
     C[es.y] = v;
   }
 }

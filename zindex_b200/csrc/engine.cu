@@ -410,7 +410,9 @@ void Engine::query_device_noalloc(const uint8_t* bases, uint64_t nbases, const u
   int blocks = (int)std::min<uint64_t>((uint64_t)std::max(1, per_sm) * sms_, std::max<uint64_t>(want, 1));
   l.blocks = blocks;
   const uint64_t fstate_bytes =
-      m_.index_mode == kFindere ? (uint64_t)blocks * l.warps * 2 * m_.colors.size() * 4 : 0;
+      m_.index_mode == kFindere && m_.colors.size() > kFindereSmemColors
+          ? (uint64_t)blocks * l.warps * 2 * m_.colors.size() * 4
+          : 0;
   // Scratch layout, every region 256-byte aligned.
   size_t scan_bytes = 0;
   cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr,
@@ -469,8 +471,8 @@ Workspace::~Workspace() {
                  hp_bases,   hp_offsets, hp_scan_tmp, seg_blocks, seg_tiles, seg_records,
                  rec_counts, rec_totals, rec_hits, rec_first, rec_scan_tmp, hit_colors,
                  hit_counts, split_keys, split_counts, wide_cursor, wide_keys2,
-                 wide_seg_cursor, wide_round_first, wide_sk[0], wide_sk[1], wide_sk_alt[0],
-                 wide_sk_alt[1], wide_keys_alt[0], wide_keys_alt[1], wide_sort_tmp};
+                 wide_seg_cursor, wide_round_first, wide_keys_alt[0], wide_keys_alt[1],
+                 wide_hist[0], wide_hist[1]};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total, h_seg_blocks, h_seg_records};
@@ -1294,7 +1296,9 @@ void Engine::enqueue(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   l.blocks = blocks;
   BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records,
                ws.fstate};
-  if (m_.index_mode == kFindere)
+  // Findere round state: in shared memory for up to kFindereSmemColors
+  // colours, else in this zeroed scratch.
+  if (m_.index_mode == kFindere && m_.colors.size() > kFindereSmemColors)
     cuda_check(cudaMemsetAsync(ws.fstate, 0,
                                (uint64_t)blocks * l.warps * 2 * m_.colors.size() * 4, s),
                "memset");
@@ -1413,35 +1417,31 @@ void Engine::run_wide(Workspace& ws, const BatchView& bv, uint64_t tiles_bound, 
       sg.tile_hi = rb.tile_hi;
       sg.min_ratio = prune_ratio;
     }
-    // Ordered round: every slot the round may fill gets a sort key (the
-    // unfilled ones all ones, so a stable sort leaves them behind the keys).
     const bool ordered = l.order && !segments;
-    const uint64_t slots = (uint64_t)(rb.tile_hi - rb.tile_lo) * kTileWindows;
-    if (ordered) {
-      ensure_order_capacity(ws, b);
-      sg.order_keys = ws.wide_sk[b];
-      sg.seed = host_ix_.seed;
-    }
+    if (ordered) ensure_order_capacity(ws, b);
     if (overlap && r >= 2)
       cuda_check(cudaStreamWaitEvent(xs, ws.wide_probe[b], 0), "cudaStreamWaitEvent");
     if (segments)
       cuda_check(cudaMemsetAsync(sg.cursor, 0, segments * 8ull, xs), "memset");
     else
       cuda_check(cudaMemsetAsync(ws.wide_cursor + b, 0, 8, xs), "memset");
-    if (ordered) cuda_check(cudaMemsetAsync(sg.order_keys, 0xFF, slots * 4, xs), "memset");
     efn<<<egrid, ewarps * 32, esmem, xs>>>(rb, sp_, keys, ws.wide_cursor + b, ewarps, sg);
     cuda_check(cudaGetLastError(), "extract_dense_kernel");
     const uint64_t* probe_keys = keys;
-    if (ordered && slots) {
-      // Stable radix sort of the round's slots by the first hash's top 20
-      // bits: the keys come first, in row-address order of every class.
-      cub::DoubleBuffer<uint32_t> sk(ws.wide_sk[b], ws.wide_sk_alt[b]);
-      cub::DoubleBuffer<uint64_t> kv(keys, ws.wide_keys_alt[b]);
-      size_t bytes = ws.wide_sort_bytes;
-      cuda_check(cub::DeviceRadixSort::SortPairs(ws.wide_sort_tmp, bytes, sk, kv, (int)slots,
-                                                 kOrderBit, 32, xs),
-                 "round sort");
-      probe_keys = kv.Current();
+    if (ordered) {
+      // Counting sort of the round's keys by their first hash's top bits
+      // (row-address order of every class), the key count read on the device.
+      const int ogrid = sms_ * 8;
+      cuda_check(cudaMemsetAsync(ws.wide_hist[b], 0, kOrderBuckets * 4, xs), "memset");
+      order_count_kernel<<<ogrid, 256, 0, xs>>>(keys, ws.wide_cursor + b, host_ix_.seed,
+                                                ws.wide_hist[b]);
+      cuda_check(cudaGetLastError(), "order_count_kernel");
+      order_scan_kernel<<<1, 1024, 0, xs>>>(ws.wide_hist[b]);
+      cuda_check(cudaGetLastError(), "order_scan_kernel");
+      order_scatter_kernel<<<ogrid, 256, 0, xs>>>(keys, ws.wide_cursor + b, host_ix_.seed,
+                                                  ws.wide_hist[b], ws.wide_keys_alt[b]);
+      cuda_check(cudaGetLastError(), "order_scatter_kernel");
+      probe_keys = ws.wide_keys_alt[b];
     }
     if (segments) {
       wide_rounds_kernel<<<1, 1024, 0, xs>>>(sg.cursor, segments,
@@ -1467,20 +1467,9 @@ void Engine::run_wide(Workspace& ws, const BatchView& bv, uint64_t tiles_bound, 
 }
 
 void Engine::ensure_order_capacity(Workspace& ws, int b) {
-  if (ws.wide_sk[b]) return;
-  const uint64_t slots = (uint64_t)kSplitTiles * kTileWindows;
-  dev_alloc(&ws.wide_sk[b], slots, "round sort keys");
-  dev_alloc(&ws.wide_sk_alt[b], slots, "round sort keys (second buffer)");
-  dev_alloc(&ws.wide_keys_alt[b], slots, "round keys (second buffer)");
-  if (!ws.wide_sort_tmp) {
-    cub::DoubleBuffer<uint32_t> sk(ws.wide_sk[b], ws.wide_sk_alt[b]);
-    cub::DoubleBuffer<uint64_t> kv(ws.split_keys, ws.wide_keys_alt[b]);
-    size_t bytes = 0;
-    cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, bytes, sk, kv, (int)slots, kOrderBit, 32),
-               "sort scratch size");
-    dev_alloc((uint8_t**)&ws.wide_sort_tmp, std::max<size_t>(bytes, 16), "round sort scratch");
-    ws.wide_sort_bytes = std::max<size_t>(bytes, 16);
-  }
+  if (ws.wide_keys_alt[b]) return;
+  dev_alloc(&ws.wide_keys_alt[b], (uint64_t)kSplitTiles * kTileWindows, "round keys in order");
+  dev_alloc(&ws.wide_hist[b], kOrderBuckets, "round order buckets");
   ws.release_graphs();
 }
 
@@ -1629,7 +1618,7 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   const size_t smem = fused_smem_bytes(l);
   BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records,
                ws.fstate, segments, ws.seg_blocks, ws.seg_tiles};
-  if (m_.index_mode == kFindere)
+  if (m_.index_mode == kFindere && colors > kFindereSmemColors)
     cuda_check(cudaMemsetAsync(ws.fstate, 0, (uint64_t)blocks * wpb * 2 * colors * 4, s), "memset");
   FusedFn fn = fused_for(sp_.mode, l);
   cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),

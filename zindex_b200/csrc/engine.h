@@ -74,13 +74,10 @@ struct Workspace {
   // first probe round of each segment (2 x cap_segments each).
   unsigned long long* wide_seg_cursor = nullptr;
   uint32_t* wide_round_first = nullptr;
-  // Ordered wide-row rounds, per key list: sort keys and the radix sort's
-  // second buffers (keys and sort keys), and its scratch.
-  uint32_t* wide_sk[2] = {};
-  uint32_t* wide_sk_alt[2] = {};
+  // Ordered wide-row rounds, per key list: the keys in bucket order and the
+  // buckets' counts / next places.
   uint64_t* wide_keys_alt[2] = {};
-  void* wide_sort_tmp = nullptr;
-  size_t wide_sort_bytes = 0;
+  uint32_t* wide_hist[2] = {};
   uint64_t* wide_keys2 = nullptr;  // second dense key list (rounds alternate)
   cudaStream_t aux_stream = nullptr;  // wide-row queries: extraction beside the probe
   cudaEvent_t wide_fork = nullptr, wide_ext[2] = {}, wide_probe[2] = {};

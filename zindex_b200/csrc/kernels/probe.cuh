@@ -876,20 +876,23 @@ struct FindereSink {
 // Sweeps the round masks of positions r0 .. r0 + len - 1 (bit i = r0 + i):
 // counts the positions whose run of consecutive hits is at least z + 1 long
 // and clears the masks; run[c] carries the run length at the round's end (0
-// after the tile's last round).
+// after the tile's last round). SHARED: the warp's masks and run lengths are
+// in shared memory (the caller synchronised the warp after the hits).
+template <bool SHARED>
 __device__ __forceinline__ void findere_sweep(uint32_t* mask, uint32_t* run, uint32_t colors, int z,
                                               uint32_t len, bool last, const Counters& cnt,
                                               int lane) {
-  // The masks are set by L2 atomics of every lane: read them past L1 and
+  // Global masks are set by L2 atomics of every lane: read them past L1 and
   // clear them atomically. run[c] belongs to lane c % 32.
   for (uint32_t c = (uint32_t)lane; c < colors; c += 32) {
-    uint32_t m = __ldcg(mask + c);
+    uint32_t m = SHARED ? mask[c] : __ldcg(mask + c);
     const uint32_t r = run[c];
     if (!m) {
       if (r) run[c] = 0;
       continue;
     }
-    m = atomicExch(mask + c, 0u);
+    if (SHARED) mask[c] = 0u;
+    else m = atomicExch(mask + c, 0u);
     uint32_t y = m;
     for (int t = 1; t <= z && y; ++t) y &= t < 32 ? (m << t) : 0u;
     uint32_t n = __popc(y);

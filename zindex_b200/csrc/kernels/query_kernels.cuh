@@ -19,6 +19,9 @@ namespace zx {
 
 constexpr uint32_t kTileWindows = 256;
 constexpr uint32_t kFindereTask = 16384;  // src/findere.rs:13-16
+// Findere indexes of up to this many colours keep each warp's round masks and
+// run lengths in shared memory (8 bytes per colour and warp).
+constexpr uint32_t kFindereSmemColors = 512;
 constexpr uint32_t kSplitTiles = 1u << 18;  // tiles per round of a split minimizer query
 constexpr uint32_t kMaxStrobeSpan = 256;    // largest randstrobemer partner distance on the GPU
 
@@ -170,13 +173,20 @@ struct FusedSmem {
     const bool staged = mode == 3 || ((mode == 0 || mode == 2) && k > 32);
     return (staged ? 2 : 1) * (size_t)kTileWindows * 8;
   }
+  // Findere round masks and run lengths of a warp in shared memory (indexes
+  // of up to kFindereSmemColors colours; else in the global scratch).
+  static __host__ __device__ size_t findere_state_bytes(uint32_t colors) {
+    return colors <= kFindereSmemColors ? (size_t)colors * 8 : 0;
+  }
   static __host__ __device__ size_t warp_bytes(int mode, int k, uint32_t classes, int stage_bytes = 0,
                                                int stages = 0, int hashes = 4, int planes = 0,
-                                               uint32_t shared_words = 0, bool strobes = false) {
+                                               uint32_t shared_words = 0, bool strobes = false,
+                                               uint32_t colors = 0) {
     size_t b = key_bytes(mode, k, strobes) + probe_bytes(classes, hashes, planes) +
                ring_bytes(stage_bytes, stages) + shared_plane_bytes(shared_words);
     if (mode == 1) b += 2 * ocm_entries(k) * sizeof(Rank16) + (kTileWindows + 1) * 4 + 16;
-    if (mode == 3) b += 64;  // findere: valid bits of up to 512 s-mer positions
+    // Findere: valid bits of up to 512 s-mer positions, then the round state.
+    if (mode == 3) b += 64 + findere_state_bytes(colors);
     return (b + 15) / 16 * 16;
   }
   // Findere always runs the row-index probe without a staged ring.
@@ -188,7 +198,7 @@ struct FusedSmem {
     return ix_bytes + map_bytes + counter_bytes(colors, l.smem_counters) +
            (mode == 1 ? 256 * 8 : 0) +
            (size_t)l.warps * warp_bytes(mode, k, classes, fin ? 0 : l.stage_bytes, l.stages, hashes,
-                                        fin ? 1 : l.planes, shared_words, strobes);
+                                        fin ? 1 : l.planes, shared_words, strobes, colors);
   }
   // Shared-plane words per lane a launch uses (0 unless the row-index form
   // counts in planes).
@@ -284,13 +294,18 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   const int stage_bytes = MODE == 3 ? 0 : lc.stage_bytes;
   const uint32_t swords = VARIANT == 2 ? FusedSmem::shared_words(MODE, *gix, lc) : 0u;
   const size_t wstride = FusedSmem::warp_bytes(MODE, sp.k, classes, stage_bytes, lc.stages, hashes,
-                                               ROWS, swords, sp.strobe_max != 0);
+                                               ROWS, swords, sp.strobe_max != 0, colors);
   uint8_t* wbase = p + (size_t)warp * wstride;
   uint64_t* keys = reinterpret_cast<uint64_t*>(wbase);
   SeedDesc* desc = reinterpret_cast<SeedDesc*>(wbase + FusedSmem::key_bytes(MODE, sp.k, sp.strobe_max != 0));
   uint64_t* row0s = reinterpret_cast<uint64_t*>(desc + 64);
   uint8_t* ring_base = wbase + FusedSmem::key_bytes(MODE, sp.k, sp.strobe_max != 0) + FusedSmem::probe_bytes(classes, hashes, ROWS);
   uint8_t* ocm = ring_base + FusedSmem::ring_bytes(stage_bytes, lc.stages);
+  if (MODE == 3 && colors <= kFindereSmemColors) {
+    uint32_t* fst = reinterpret_cast<uint32_t*>(ocm + 64);
+    for (uint32_t c = lane; c < 2 * colors; c += 32) fst[c] = 0;
+    __syncwarp();
+  }
   SharedPlanes splanes{reinterpret_cast<uint32_t*>(wbase + wstride - FusedSmem::shared_plane_bytes(swords)),
                        swords, 0u};
   StageRing ring{ring_base + 64, reinterpret_cast<uint64_t*>(ring_base), (uint32_t)lc.stage_bytes,
@@ -353,12 +368,16 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
         const uint32_t bal = __ballot_sync(0xFFFFFFFFu, ok);
         if (lane == 0) seeds += __popc(bal);
       }
-      uint32_t* fmask = bv.fstate + (uint64_t)gwarp * 2 * colors;
+      const bool fshared = colors <= kFindereSmemColors;
+      uint32_t* fmask = fshared ? reinterpret_cast<uint32_t*>(ocm + 64)
+                                : bv.fstate + (uint64_t)gwarp * 2 * colors;
       uint32_t* frun = fmask + colors;
       const FindereSink fs{fmask};
       probe_rows<MINB == 1>(ix, keys, npos, kvalid, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
                  splanes, pbase, fs, lane, [&](uint32_t r0, uint32_t m) {
-                   findere_sweep(fmask, frun, colors, z, m, r0 + m >= npos, cnt, lane);
+                   __syncwarp();
+                   if (fshared) findere_sweep<true>(fmask, frun, colors, z, m, r0 + m >= npos, cnt, lane);
+                   else findere_sweep<false>(fmask, frun, colors, z, m, r0 + m >= npos, cnt, lane);
                    __syncwarp();
                  });
       continue;

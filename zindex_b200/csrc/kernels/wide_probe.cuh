@@ -37,9 +37,11 @@ namespace zx {
 constexpr int kWideSeeds = 256;      // seeds per descriptor round of a block
 constexpr int kWidePlanes = 6;       // register planes: counts up to 63 per field
 constexpr uint32_t kWideFlush = 63;  // seeds between plane flushes
-// Ordered rounds compare bits [kOrderBit, 32) of the sort keys (the first
-// hash's top 32 bits): about a million row-order buckets.
-constexpr int kOrderBit = 12;
+// Ordered rounds: a counting sort of a round's dense key list by the top
+// kOrderBits bits of each key's first hash (every class's row index grows
+// with the first hash). Keys keep no particular order within a bucket.
+constexpr int kOrderBits = 16;
+constexpr uint32_t kOrderBuckets = 1u << kOrderBits;
 
 // Colour location for recovered-origin point probes: cls_member = class |
 // member index << 8 (member index within a multi-member group, 0 for
@@ -84,8 +86,6 @@ __device__ __forceinline__ uint32_t segment_of(const uint32_t* __restrict__ firs
 // ...], their number in cursor[s]; the probe's rounds of 256 seeds never
 // straddle segments (round_first[s] = first round of segment s). nseg = 0:
 // one unsegmented list, one cursor.
-// Ordered (unsegmented only): the extraction also writes each key's sort key,
-// the top 32 bits of its first hash, at the same index of order_keys.
 struct WideRound {
   const uint32_t* seg_tiles = nullptr;    // first tile of each segment (nseg + 1)
   unsigned long long* cursor = nullptr;   // keys of each segment in this round
@@ -93,8 +93,6 @@ struct WideRound {
   unsigned long long* totals = nullptr;   // seeds of each segment
   uint32_t nseg = 0;
   uint32_t tile_lo = 0;                   // first tile of the extraction round
-  uint32_t* order_keys = nullptr;         // sort keys of the dense list (ordered rounds)
-  uint64_t seed = 0;                      // the index seed (first hash)
   // Segmented per-record reports: colours reported when count / total >=
   // min_ratio (> 0 turns on threshold pruning); tile_hi ends the round.
   double min_ratio = 0.0;
@@ -183,10 +181,55 @@ __global__ void extract_dense_kernel(BatchView bv, SeedParams sp, uint64_t* __re
     if (lane == 0 && n) at = atomicAdd(cur, (unsigned long long)n);
     at = __shfl_sync(0xFFFFFFFFu, at, 0);
     for (uint32_t i = lane; i < n; i += 32) dst[at + i] = keys[i];
-    if (sg.order_keys)
-      for (uint32_t i = lane; i < n; i += 32)
-        sg.order_keys[at + i] = (uint32_t)(mixsplit(keys[i], sg.seed) >> 32);
     __syncwarp();
+  }
+}
+
+__device__ __forceinline__ uint32_t order_bucket(uint64_t key, uint64_t seed) {
+  return (uint32_t)(mixsplit(key, seed) >> (64 - kOrderBits));
+}
+
+// Ordered rounds, step 1: keys per bucket (hist zeroed before).
+__global__ void order_count_kernel(const uint64_t* __restrict__ keys,
+                                   const unsigned long long* __restrict__ nkeys, uint64_t seed,
+                                   uint32_t* __restrict__ hist) {
+  const uint64_t n = *nkeys;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(hist + order_bucket(keys[i], seed), 1u);
+}
+
+// Step 2 (one block of 1,024 threads): the buckets' first places, in place.
+__global__ void order_scan_kernel(uint32_t* __restrict__ hist) {
+  __shared__ uint32_t part[1024];
+  const uint32_t T = blockDim.x, tid = threadIdx.x, per = kOrderBuckets / T;
+  uint32_t sum = 0;
+  for (uint32_t j = 0; j < per; ++j) sum += hist[tid * per + j];
+  part[tid] = sum;
+  __syncthreads();
+  for (uint32_t off = 1; off < T; off <<= 1) {
+    const uint32_t v = tid >= off ? part[tid - off] : 0u;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  uint32_t run = tid ? part[tid - 1] : 0u;
+  for (uint32_t j = 0; j < per; ++j) {
+    const uint32_t c = hist[tid * per + j];
+    hist[tid * per + j] = run;
+    run += c;
+  }
+}
+
+// Step 3: every key to its bucket's next place in out[].
+__global__ void order_scatter_kernel(const uint64_t* __restrict__ keys,
+                                     const unsigned long long* __restrict__ nkeys, uint64_t seed,
+                                     uint32_t* __restrict__ next, uint64_t* __restrict__ out) {
+  const uint64_t n = *nkeys;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    out[atomicAdd(next + order_bucket(k, seed), 1u)] = k;
   }
 }
 
@@ -363,11 +406,18 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
     __syncthreads();
   };
+  // Unsegmented: block b takes the seeds b, b + G, b + 2G, ... of the dense
+  // list (G blocks), 256 per round, so the blocks work on neighbouring seeds
+  // at the same time: in an ordered list their rows overlap in a few
+  // megabytes and the repeated reads of a row are L2 hits. Segmented: rounds
+  // of 256 consecutive seeds of one segment, round-robin over the blocks.
+  const uint64_t G = gridDim.x;
   const uint64_t nk = sg.nseg ? 0 : *nkeys;
+  const uint64_t mine = sg.nseg || nk <= blockIdx.x ? 0 : (nk - blockIdx.x + G - 1) / G;
   const uint64_t nrounds = sg.nseg ? (uint64_t)__ldg(sg.round_first + sg.nseg)
-                                   : (nk + kWideSeeds - 1) / kWideSeeds;
-  for (uint64_t r = blockIdx.x; r < nrounds; r += gridDim.x) {
-    uint64_t base = r * kWideSeeds;
+                                   : (mine + kWideSeeds - 1) / kWideSeeds;
+  for (uint64_t r = sg.nseg ? blockIdx.x : 0; r < nrounds; r += sg.nseg ? G : 1) {
+    uint64_t base, kstride = 1;  // seed i of the round: keys[base + i * kstride]
     uint32_t n;
     if (sg.nseg) {
       const uint32_t seg = segment_of(sg.round_first, sg.nseg, (uint32_t)r);
@@ -391,12 +441,15 @@ __global__ void __launch_bounds__(MAXT, MINB)
       }
       if (tid == 0) atomicAdd(sg.totals + seg, (unsigned long long)n);
     } else {
-      n = nk - base < (uint64_t)kWideSeeds ? (uint32_t)(nk - base) : (uint32_t)kWideSeeds;
+      base = r * kWideSeeds * G + blockIdx.x;
+      kstride = G;
+      const uint64_t left = mine - r * kWideSeeds;
+      n = left < (uint64_t)kWideSeeds ? (uint32_t)left : (uint32_t)kWideSeeds;
     }
     // Descriptors: pattern and row indices of each seed; recovered origins
     // the filter misses are counted by the seed's owner.
     for (uint32_t i = tid; i < n; i += T) {
-      const uint64_t key = keys[base + i];
+      const uint64_t key = keys[base + (uint64_t)i * kstride];
       const uint64_t first = mixsplit(key, ix.seed), step = splitmix64(first);
       const uint32_t fp = (uint32_t)fingerprint(key, ix.seed, b);
       pattern[i] = fp * ones;
