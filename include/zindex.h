@@ -83,8 +83,10 @@ typedef struct zx_launch {
                          team, planes, stage_bytes and split are then unused */
   int order;          /* wide-row form, unsegmented queries: 1 = each round's seeds are sorted
                          by their first hash before the probe (every class's row index grows
-                         with it, so consecutive seeds read neighbouring rows); ignored
-                         elsewhere. Counts do not depend on it */
+                         with it, so consecutive seeds read neighbouring rows), each block
+                         probing runs of 256 consecutive seeds; 2 = sorted, and block b
+                         probes seeds b, b + blocks, ... (all blocks on neighbouring seeds);
+                         0 = extraction order; ignored elsewhere. Counts do not depend on it */
 } zx_launch;
 
 /* Thread-local message of the last failed call on this thread. */

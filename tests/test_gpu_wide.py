@@ -71,7 +71,7 @@ def test_wide_form_matches_oracle(gpu, oracle, tmp_path_factory, case):
         for recover in (True, False):
             want, want_total = oracle.query_records(ix, bases, offsets, recover=recover)
             for warps in chunks_ok:
-                for counters, order in ((1, 1), (1, 0), (0, 1)):
+                for counters, order in ((1, 1), (1, 0), (0, 1), (1, 2)):
                     index.set_launch(wide=1, warps=warps, smem_counters=counters, order=order)
                     assert index.launch()["wide"] == 1 and index.launch()["order"] == order
                     got, total = index.query_records(bases, offsets, recover=recover)
@@ -212,10 +212,10 @@ def test_wide_segments_across_extraction_rounds(gpu, oracle, tmp_path_factory, c
                              counts.data_ptr(), totals.data_ptr())
         torch.cuda.synchronize(dev)
         got, got_t = counts.cpu().numpy().astype(np.uint64), totals.cpu().numpy()
-        # The same batch unsegmented: two ordered rounds, and two in
-        # extraction order.
+        # The same batch unsegmented: two ordered rounds (each block on its
+        # own seeds, then interleaved seeds), and two in extraction order.
         whole = []
-        for order in (1, 0):
+        for order in (1, 2, 0):
             index.set_launch(wide=1, order=order)
             c1 = torch.zeros(index.colors, dtype=torch.int64, device=dev)
             t1 = torch.zeros(1, dtype=torch.int64, device=dev)

@@ -1080,7 +1080,7 @@ void Engine::set_launch(const QueryLaunch& l) {
   check(l.cut >= 1 && l.cut <= 64, kEInval, "cut must be in 1..64");
   check(l.split == 0 || l.split == 1, kEInval, "split must be 0 or 1");
   check(l.wide == 0 || l.wide == 1, kEInval, "wide must be 0 or 1");
-  check(l.order == 0 || l.order == 1, kEInval, "order must be 0 or 1");
+  check(l.order >= 0 && l.order <= 2, kEInval, "order must be 0, 1 or 2");
   check(!l.wide || wide_eligible(l.warps), kEInval,
         "the wide-row form needs fingerprints of at least 4 bits, a k-mer, minimizer or "
         "modimizer index without strobes, 4, 8 or 9 warps per block and rows of at most "
@@ -1419,6 +1419,7 @@ void Engine::run_wide(Workspace& ws, const BatchView& bv, uint64_t tiles_bound, 
     }
     const bool ordered = l.order && !segments;
     if (ordered) ensure_order_capacity(ws, b);
+    sg.interleave = !segments && l.order == 2 ? 1u : 0u;
     if (overlap && r >= 2)
       cuda_check(cudaStreamWaitEvent(xs, ws.wide_probe[b], 0), "cudaStreamWaitEvent");
     if (segments)

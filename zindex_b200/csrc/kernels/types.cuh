@@ -51,7 +51,8 @@ struct QueryLaunch {
   int wide;           // 1 = wide-row form: seeds extracted into a dense list, probed by blocks
                       // whose threads own fixed 16-byte chunks of every row (wide_probe.cuh)
   int order;          // wide-row form: 1 = each round's seeds sorted by their first hash, so
-                      // consecutive seeds read neighbouring rows of every class
+                      // consecutive seeds read neighbouring rows of every class (2: and the
+                      // blocks take interleaved seeds)
 };
 
 }  // namespace zx

@@ -93,6 +93,8 @@ struct WideRound {
   unsigned long long* totals = nullptr;   // seeds of each segment
   uint32_t nseg = 0;
   uint32_t tile_lo = 0;                   // first tile of the extraction round
+  // Unsegmented: 1 = blocks take interleaved seeds (see the probe loop).
+  uint32_t interleave = 0;
   // Segmented per-record reports: colours reported when count / total >=
   // min_ratio (> 0 turns on threshold pruning); tile_hi ends the round.
   double min_ratio = 0.0;
@@ -406,17 +408,20 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
     __syncthreads();
   };
-  // Unsegmented: block b takes the seeds b, b + G, b + 2G, ... of the dense
-  // list (G blocks), 256 per round, so the blocks work on neighbouring seeds
-  // at the same time: in an ordered list their rows overlap in a few
-  // megabytes and the repeated reads of a row are L2 hits. Segmented: rounds
+  // Rounds of 256 seeds. Unsegmented, contiguous: round r is seeds 256r ..
+  // 256r + 255 of the dense list, round-robin over the blocks (in an ordered
+  // list each block walks its own neighbourhood of rows). Unsegmented,
+  // interleaved: block b takes the seeds b, b + G, b + 2G, ... (G blocks), so
+  // all blocks work on neighbouring seeds at the same time. Segmented: rounds
   // of 256 consecutive seeds of one segment, round-robin over the blocks.
   const uint64_t G = gridDim.x;
+  const bool inter = !sg.nseg && sg.interleave;
   const uint64_t nk = sg.nseg ? 0 : *nkeys;
-  const uint64_t mine = sg.nseg || nk <= blockIdx.x ? 0 : (nk - blockIdx.x + G - 1) / G;
+  const uint64_t mine = !inter || nk <= blockIdx.x ? 0 : (nk - blockIdx.x + G - 1) / G;
   const uint64_t nrounds = sg.nseg ? (uint64_t)__ldg(sg.round_first + sg.nseg)
-                                   : (mine + kWideSeeds - 1) / kWideSeeds;
-  for (uint64_t r = sg.nseg ? blockIdx.x : 0; r < nrounds; r += sg.nseg ? G : 1) {
+                           : inter ? (mine + kWideSeeds - 1) / kWideSeeds
+                                   : (nk + kWideSeeds - 1) / kWideSeeds;
+  for (uint64_t r = inter ? 0 : blockIdx.x; r < nrounds; r += inter ? 1 : G) {
     uint64_t base, kstride = 1;  // seed i of the round: keys[base + i * kstride]
     uint32_t n;
     if (sg.nseg) {
@@ -440,11 +445,14 @@ __global__ void __launch_bounds__(MAXT, MINB)
         }
       }
       if (tid == 0) atomicAdd(sg.totals + seg, (unsigned long long)n);
-    } else {
+    } else if (inter) {
       base = r * kWideSeeds * G + blockIdx.x;
       kstride = G;
       const uint64_t left = mine - r * kWideSeeds;
       n = left < (uint64_t)kWideSeeds ? (uint32_t)left : (uint32_t)kWideSeeds;
+    } else {
+      base = r * kWideSeeds;
+      n = nk - base < (uint64_t)kWideSeeds ? (uint32_t)(nk - base) : (uint32_t)kWideSeeds;
     }
     // Descriptors: pattern and row indices of each seed; recovered origins
     // the filter misses are counted by the seed's owner.
