@@ -1,10 +1,14 @@
 """Randstrobemer queries on the GPU against the oracle.
 
-k-mer strobes are extracted per tile on the device (each anchor's partner up
-to strobe_max windows downstream, across tile boundaries), the reverse-
-complement strand is queried too, and every record keeps per colour the larger
-strand count (query_stream.rs:516-534, 690-701). Aggregates, per-record counts
-and per-record reports must equal the oracle's.
+Candidates (every canonical k-mer, or the selected minimizer positions of a
+run, once each) are marked in a per-base table on the device and each tile's
+candidates are linked by a forward scan of it (partners strobe_min..
+strobe_max bases downstream in the same run, for distances above 256 too,
+across tile boundaries); the reverse-complement strand is queried too, and
+every record keeps per colour the larger strand count (query_stream.rs:
+516-534, 690-701). Aggregates, per-record counts and per-record reports must
+equal the oracle's, for k-mer and minimizer strobes, spaced seeds and
+homopolymer compression.
 """
 import numpy as np
 import pytest
@@ -54,6 +58,12 @@ CASES = [
     dict(k=31, lo=5, hi=200),
     dict(k=15, pattern="##_#_#_#_#_#_##"),
     dict(k=25, homopolymer=True, lo=10, hi=90),
+    dict(k=21, lo=300, hi=1200),                      # distances above 256
+    dict(mode="minimizers", k=31, m=15),
+    dict(mode="minimizers", k=31, m=19, lo=20, hi=400),
+    dict(mode="minimizers", k=21, m=21),              # k == m: every m-mer
+    dict(mode="minimizers", k=31, m=15, pattern="#####_###_#####"),
+    dict(mode="minimizers", k=29, m=13, lo=100, hi=2000, homopolymer=True),
 ]
 
 
@@ -102,5 +112,7 @@ def test_strobe_indexes_refuse_single_strand_device_paths(gpu, tmp_path_factory)
             index.query_device(d_bases.data_ptr(), 100, d_off.data_ptr(), 1, d_counts.data_ptr(),
                                d_total.data_ptr())
     mix, _ = strobe_index(tmp_path_factory, k=31, mode="minimizers", m=15)
-    with pytest.raises(zx.ZxError):
-        zx.Index(mix)  # minimizer strobes are not linked on the GPU
+    with zx.Index(mix) as index:
+        with pytest.raises(zx.ZxError):
+            index.query_device(d_bases.data_ptr(), 100, d_off.data_ptr(), 1, d_counts.data_ptr(),
+                               d_total.data_ptr())

@@ -14,6 +14,7 @@
 
 #include "kernels/query_kernels.cuh"
 #include "kernels/record_hits.cuh"
+#include "kernels/strobes.cuh"
 #include "kernels/wide_probe.cuh"
 
 #include <algorithm>
@@ -472,7 +473,8 @@ Workspace::~Workspace() {
                  rec_counts, rec_totals, rec_hits, rec_first, rec_scan_tmp, hit_colors,
                  hit_counts, split_keys, split_counts, wide_cursor, wide_keys2,
                  wide_seg_cursor, wide_round_first, wide_keys_alt[0], wide_keys_alt[1],
-                 wide_hist[0], wide_hist[1]};
+                 wide_hist[0], wide_hist[1], strobe_anchors, strobe_hashes, strobe_slots,
+                 strobe_count};
   for (void* p : dev)
     if (p) cudaFree(p);
   void* host[] = {h_bases, h_offsets, h_counts, h_total, h_seg_blocks, h_seg_records};
@@ -624,10 +626,15 @@ void Engine::load(const std::string& dir, const OpenOptions& options) {
   }
   sp_.strobe_min = sp_.strobe_max = 0;
   if (m_.has_randstrobemers) {
-    check(m_.index_mode == kKmers && m_.k <= 32, kEUnsupported,
-          "the GPU query path links randstrobemers over k-mers with k <= 32 only");
-    check(m_.strobe_max <= kMaxStrobeSpan, kEUnsupported,
-          "randstrobemer distances above 256 are not supported by the GPU query path");
+    // Candidates of k-mer (k <= 32) or minimizer indexes; a minimizer window
+    // can select up to w - 1 positions past a record's last window start.
+    check((m_.index_mode == kKmers && m_.k <= 32) ||
+              (m_.index_mode == kMinimizers && m_.minimizer_size <= 32 &&
+               m_.k - m_.minimizer_size <= kStrobeExtra),
+          kEUnsupported,
+          "the GPU query path links randstrobemers over k-mers with k <= 32 and over "
+          "minimizers with m <= 32 and k - m <= 64");
+    check(m_.strobe_max < (1ull << 31), kEUnsupported, "randstrobemer distances below 2^31");
     sp_.strobe_min = (uint32_t)m_.strobe_min;
     sp_.strobe_max = (uint32_t)m_.strobe_max;
   }
@@ -1474,6 +1481,49 @@ void Engine::ensure_order_capacity(Workspace& ws, int b) {
   ws.release_graphs();
 }
 
+void Engine::ensure_strobe_capacity(Workspace& ws, uint64_t nbases, uint64_t tiles) {
+  if (nbases > ws.cap_strobe_bases || !ws.strobe_anchors) {
+    const uint64_t cap = std::max<uint64_t>({nbases, ws.cap_strobe_bases * 3 / 2, 4096});
+    if (ws.strobe_anchors) cudaFree(ws.strobe_anchors);
+    if (ws.strobe_hashes) cudaFree(ws.strobe_hashes);
+    ws.strobe_anchors = nullptr;
+    ws.strobe_hashes = nullptr;
+    dev_alloc(&ws.strobe_anchors, cap / 32 + 2, "strobe candidates");
+    dev_alloc(&ws.strobe_hashes, cap + 1, "strobe hashes");
+    ws.cap_strobe_bases = cap;
+    ws.release_graphs();
+  }
+  if (tiles > ws.cap_strobe_tiles || !ws.strobe_slots) {
+    const uint64_t cap = std::max<uint64_t>({tiles, ws.cap_strobe_tiles * 3 / 2, 1024});
+    if (ws.strobe_slots) cudaFree(ws.strobe_slots);
+    if (ws.strobe_count) cudaFree(ws.strobe_count);
+    ws.strobe_slots = nullptr;
+    ws.strobe_count = nullptr;
+    dev_alloc(&ws.strobe_slots, cap * kStrobeSlot, "strobe seeds");
+    dev_alloc(&ws.strobe_count, cap, "strobe seed counts");
+    ws.cap_strobe_tiles = cap;
+    ws.release_graphs();
+  }
+}
+
+void Engine::link_strobes(Workspace& ws, const BatchView& bv, uint64_t nbases, cudaStream_t s) {
+  cuda_check(cudaMemsetAsync(ws.strobe_anchors, 0, (nbases / 32 + 2) * 4, s), "memset");
+  const int warps = 4;
+  const int mode = sp_.mode == kMinimizers ? 1 : 0;
+  const size_t smem = StrobeSmem::total(mode, sp_.k, warps);
+  auto afn = mode == 1 ? strobe_anchor_kernel<1> : strobe_anchor_kernel<0>;
+  cuda_check(cudaFuncSetAttribute(afn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+  const int grid = sms_ * 8;
+  afn<<<grid, warps * 32, smem, s>>>(bv, sp_, ws.strobe_anchors, ws.strobe_hashes, warps);
+  cuda_check(cudaGetLastError(), "strobe_anchor_kernel");
+  const int len = mode == 1 ? sp_.m : sp_.klen;
+  const uint32_t extra = mode == 1 && sp_.k != sp_.m ? (uint32_t)sp_.ocm.w - 1 : 0u;
+  strobe_link_kernel<<<grid, 256, 0, s>>>(bv, sp_, ws.strobe_anchors, ws.strobe_hashes, len,
+                                          extra, ws.strobe_slots, ws.strobe_count);
+  cuda_check(cudaGetLastError(), "strobe_link_kernel");
+}
+
 void Engine::ensure_segment_capacity(Workspace& ws, uint32_t segments) {
   if (segments + 1 > ws.cap_segments || !ws.seg_blocks) {
     const uint64_t c = std::max<uint64_t>(segments + 1, 256);
@@ -1568,6 +1618,18 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
   QueryLaunch l = fused_launch(launch_);
   l.split = 0;  // every segment extracts its own tiles in the fused kernel
   if (warps > 0 && warps < l.warps) l.warps = warps;
+  // Randstrobemer indexes: the segments' seeds are linked beforehand
+  // (strobes.cuh) and probed from their tile slots (mode 4, row-index form).
+  const bool strobes = sp_.strobe_max != 0;
+  if (strobes) {
+    l.planes = 1;
+    l.stage_bytes = 0;
+    uint64_t tiles = 0;
+    for (uint32_t i = 0; i < segments; ++i) tiles += est_tiles[i];
+    check(tiles <= kSplitTiles, kEInval,
+          "a randstrobemer query holds at most 262,144 tiles (about 64 Mbases) per launch");
+    ensure_strobe_capacity(ws, nbases, std::max<uint64_t>(tiles, 1));
+  }
   const int cap = max_blocks(l);
   const uint32_t wpb = (uint32_t)l.warps;
   // Grid shares: proportional to the estimated tiles, at least one block,
@@ -1616,12 +1678,22 @@ void Engine::query_segments(Workspace& ws, const uint8_t* bases, uint64_t nbases
                                                               segments, ws.seg_tiles);
   cuda_check(cudaGetLastError(), "segment_tiles_kernel");
   l.blocks = (int)blocks;
-  const size_t smem = fused_smem_bytes(l);
+  const int kmode = strobes ? 4 : sp_.mode;
+  const size_t smem = strobes ? FusedSmem::total(4, sp_.k, (uint32_t)colors, host_ix_.classes,
+                                                 m_.hashes, l,
+                                                 FusedSmem::shared_words(4, host_ix_, l), true)
+                              : fused_smem_bytes(l);
   BatchView bv{PackedView{ws.packed, ws.invalid}, offsets, ws.tiles, ws.tile_first + records,
                ws.fstate, segments, ws.seg_blocks, ws.seg_tiles};
+  if (strobes) {
+    link_strobes(ws, bv, nbases, s);
+    bv.prekeys = ws.strobe_slots;
+    bv.prekey_count = ws.strobe_count;
+    bv.prekey_stride = kStrobeSlot;
+  }
   if (m_.index_mode == kFindere && colors > kFindereSmemColors)
     cuda_check(cudaMemsetAsync(ws.fstate, 0, (uint64_t)blocks * wpb * 2 * colors * 4, s), "memset");
-  FusedFn fn = fused_for(sp_.mode, l);
+  FusedFn fn = fused_for(kmode, l);
   cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "cudaFuncSetAttribute");
   fn<<<blocks, l.warps * 32, smem, s>>>(recover ? d_ix_rec_ : d_ix_norec_, bv, sp_, l, ws.partial,
@@ -1652,7 +1724,10 @@ void Engine::record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   uint64_t gmax = budget / (colors * 8);
   if (m_.index_mode == kFindere) gmax = std::min<uint64_t>(gmax, budget / (colors * 8 * launch_.warps));
   gmax = std::max<uint64_t>(1, std::min<uint64_t>(gmax, 1ull << 20));
-  const uint64_t group_bases = 256ull << 20;
+  // Randstrobemer groups: one launch's tile slots and a candidate table of
+  // 8 bytes per base (64 Mi bases).
+  const bool strobes = sp_.strobe_max != 0;
+  const uint64_t group_bases = strobes ? (64ull << 20) : (256ull << 20);
   if (gmax > ws.cap_rec_totals || !ws.rec_counts) {
     for (void* p : {(void*)ws.rec_counts, (void*)ws.rec_totals, (void*)ws.rec_hits,
                     (void*)ws.rec_first, ws.rec_scan_tmp})
@@ -1683,9 +1758,18 @@ void Engine::record_groups(Workspace& ws, const uint8_t* bases, uint64_t nbases,
     cudaGetLastError();
   std::vector<uint64_t> seg, est;
   for (uint64_t r0 = 0; r0 < records;) {
-    uint64_t r1 = r0 + 1, tiles = tiles_for_length(offsets[r0 + 1] - offsets[r0]);
-    while (r1 < records && r1 - r0 < gmax && offsets[r1 + 1] - offsets[r0] <= group_bases)
-      tiles += tiles_for_length(offsets[r1 + 1] - offsets[r1]), ++r1;
+    // (Strobe groups count a tile for every record, as the launch's estimate does.)
+    auto tiles_of = [&](uint64_t r) {
+      const uint64_t t = tiles_for_length(offsets[r + 1] - offsets[r]);
+      return strobes ? std::max<uint64_t>(1, t) : t;
+    };
+    uint64_t r1 = r0 + 1, tiles = tiles_of(r0);
+    while (r1 < records && r1 - r0 < gmax && offsets[r1 + 1] - offsets[r0] <= group_bases) {
+      const uint64_t next = tiles_of(r1);
+      if (strobes && tiles + next > kSplitTiles) break;
+      tiles += next;
+      ++r1;
+    }
     const uint64_t n = r1 - r0, b0 = offsets[r0], nb = offsets[r1] - b0;
     ensure_capacity(ws, nb, n, true);
     ensure_host_capacity(ws, nb, n);
@@ -2086,6 +2170,27 @@ void Engine::extract_host(Workspace& ws, const uint8_t* bases, uint64_t nbases,
   cuda_check(cudaStreamSynchronize(s), "tiles");
   if (ntiles == 0) {
     keys.clear();
+    return;
+  }
+  if (sp_.strobe_max) {
+    // Randstrobemer seeds of the forward strand, records and positions in order.
+    ensure_strobe_capacity(ws, nbases, ntiles);
+    BatchView bv{PackedView{ws.packed, ws.invalid}, d_offsets, ws.tiles, ws.tile_first + records,
+                 nullptr};
+    link_strobes(ws, bv, nbases, s);
+    std::vector<uint64_t> all((uint64_t)ntiles * kStrobeSlot);
+    std::vector<uint32_t> cnt(ntiles);
+    cuda_check(cudaMemcpyAsync(all.data(), ws.strobe_slots, all.size() * 8, cudaMemcpyDeviceToHost,
+                               s),
+               "D2H");
+    cuda_check(cudaMemcpyAsync(cnt.data(), ws.strobe_count, ntiles * 4ull, cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaStreamSynchronize(s), "extract");
+    check_error_word(ws);
+    keys.clear();
+    for (uint32_t t = 0; t < ntiles; ++t)
+      keys.insert(keys.end(), all.begin() + (uint64_t)t * kStrobeSlot,
+                  all.begin() + (uint64_t)t * kStrobeSlot + cnt[t]);
     return;
   }
   uint64_t need = (uint64_t)ntiles * kTileWindows;

@@ -78,6 +78,13 @@ struct Workspace {
   // buckets' counts / next places.
   uint64_t* wide_keys_alt[2] = {};
   uint32_t* wide_hist[2] = {};
+  // Randstrobemer queries: candidate bits and strobe hashes per base, each
+  // tile's linked seeds (kStrobeSlot per tile) and their numbers.
+  uint32_t* strobe_anchors = nullptr;
+  uint64_t* strobe_hashes = nullptr;
+  uint64_t* strobe_slots = nullptr;
+  uint32_t* strobe_count = nullptr;
+  uint64_t cap_strobe_bases = 0, cap_strobe_tiles = 0;
   uint64_t* wide_keys2 = nullptr;  // second dense key list (rounds alternate)
   cudaStream_t aux_stream = nullptr;  // wide-row queries: extraction beside the probe
   cudaEvent_t wide_fork = nullptr, wide_ext[2] = {}, wide_probe[2] = {};
@@ -278,6 +285,10 @@ class Engine {
                 double prune_ratio = 0.0);
   // Device tables of a segmented launch for `segments` requests.
   void ensure_segment_capacity(Workspace& ws, uint32_t segments);
+  // Randstrobemer seeds of a planned batch (strobes.cuh): candidates, then
+  // each tile's linked seeds into ws.strobe_slots / strobe_count.
+  void ensure_strobe_capacity(Workspace& ws, uint64_t nbases, uint64_t tiles);
+  void link_strobes(Workspace& ws, const BatchView& bv, uint64_t nbases, cudaStream_t s);
   // Runs host records in device groups (one segment per record): after each
   // group's launch, on_group(r0, n) enqueues its read-back on ws.stream; the
   // stream is then synchronised and the error word checked.

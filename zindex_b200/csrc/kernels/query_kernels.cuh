@@ -23,7 +23,10 @@ constexpr uint32_t kFindereTask = 16384;  // src/findere.rs:13-16
 // run lengths in shared memory (8 bytes per colour and warp).
 constexpr uint32_t kFindereSmemColors = 512;
 constexpr uint32_t kSplitTiles = 1u << 18;  // tiles per round of a split minimizer query
-constexpr uint32_t kMaxStrobeSpan = 256;    // largest randstrobemer partner distance on the GPU
+// Randstrobemer seeds of a tile (strobes.cuh): its windows' positions plus up
+// to kStrobeExtra minimizer positions past a record's last window start.
+constexpr uint32_t kStrobeExtra = 64;
+constexpr uint32_t kStrobeSlot = 256 + kStrobeExtra;
 
 // Windows of record r: k-windows fully inside the record. A record whose
 // offsets decrease, pass the end of the bases or span 2^31 bases or more has
@@ -130,10 +133,12 @@ struct BatchView {
   const uint32_t* seg_tiles;
   // Tile range of a launch over part of the list: tiles tile_lo .. tile_hi-1
   // (tile_hi 0 = to the end). Seeds extracted beforehand (MODE 4): tile t's
-  // keys are prekeys[(t - tile_lo) * kTileWindows ...], prekey_count[t - tile_lo] of them.
+  // keys are prekeys[(t - tile_lo) * stride ...], prekey_count[t - tile_lo] of
+  // them (stride = prekey_stride, or kTileWindows when 0).
   uint32_t tile_lo, tile_hi;
   const uint64_t* prekeys;
   const uint32_t* prekey_count;
+  uint32_t prekey_stride;
 };
 
 // Shared memory of the fused kernel, in order: DevIndex copy, counters,
@@ -164,12 +169,9 @@ struct FusedSmem {
   }
   // Key buffer of a warp: one tile's keys, plus the lane-run staging of the
   // polynomial k-mer hashes (modes 0 and 2 with k > 32) and of findere s-mers.
-  // Randstrobemers (mode 0) add the strobe hashes of a tile's windows and of
-  // up to kMaxStrobeSpan windows past it, with their validity bits.
+  // Randstrobemer seeds (probed in mode 4): one tile's slot of kStrobeSlot.
   static __host__ __device__ size_t key_bytes(int mode, int k, bool strobes = false) {
-    if (strobes && mode == 0)
-      return (size_t)kTileWindows * 8 + (kTileWindows + kMaxStrobeSpan) * 8 +
-             (kTileWindows + kMaxStrobeSpan) / 8;
+    if (strobes) return (size_t)kStrobeSlot * 8;
     const bool staged = mode == 3 || ((mode == 0 || mode == 2) && k > 32);
     return (staged ? 2 : 1) * (size_t)kTileWindows * 8;
   }
@@ -225,12 +227,6 @@ __device__ __forceinline__ uint32_t extract_tile(const BatchView& bv, const Seed
       uint32_t* pos = reinterpret_cast<uint32_t*>(suf + FusedSmem::ocm_entries(sp.k));
       n = tile_ocm(bv.pv, rb, t.w0, t.nw, sp, inner, pre, suf, pos, keys, lane);
     }
-  } else if (MODE == 0 && sp.strobe_max) {
-    const uint64_t len = bv.offsets[t.record + 1] - rb;
-    const uint32_t windows = (uint32_t)(len - (uint64_t)sp.klen + 1);  // tiles exist: len >= k
-    return tile_strobes(bv.pv, rb, t.w0, t.nw, windows - t.w0, sp, keys, keys + kTileWindows,
-                        reinterpret_cast<uint32_t*>(keys + 2 * kTileWindows + kMaxStrobeSpan),
-                        lane);
   } else if (sp.klen <= 32) {
     n = tile_kmers_short(bv.pv, rb, t.w0, t.nw, sp.klen, MODE == 2, sp.seed, sp.sampling, keys,
                          lane);
@@ -385,7 +381,8 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
     uint32_t n;
     if constexpr (MODE == 4) {
       // Seeds extracted beforehand into this tile's slot.
-      const uint64_t slot = (uint64_t)(t - bv.tile_lo) * kTileWindows;
+      const uint64_t slot =
+          (uint64_t)(t - bv.tile_lo) * (bv.prekey_stride ? bv.prekey_stride : kTileWindows);
       n = bv.prekey_count[t - bv.tile_lo];
       for (uint32_t i = lane; i < n; i += 32) keys[i] = bv.prekeys[slot + i];
     } else {

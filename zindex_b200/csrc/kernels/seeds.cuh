@@ -152,65 +152,6 @@ __device__ __forceinline__ uint32_t tile_kmers_short(const PackedView& pv, uint6
   return count;
 }
 
-// Randstrobemers over canonical k-mers (k <= 32; src/anchors.rs:182-256,
-// 265-347): windows [w0, w0+nw) of a record are the anchors, `rest` windows
-// of the record remain from w0. Each valid window's strobe hash (of its
-// canonical k-mer, or of its spaced-seed key) goes to hash[] for the tile and
-// up to strobe_max windows past it, validity bits to vmask[]. An anchor's
-// partner is the first window strobe_min..strobe_max downstream, in the same
-// ACGT run (every window in between valid), with the fewest differing low 8
-// hash bits; without one the anchor pairs with itself. Key = h/2 + partner/2,
-// one per valid anchor, in window order. hash holds nw + kMaxStrobeSpan
-// entries, vmask as many bits; strobe_max <= kMaxStrobeSpan.
-__device__ __forceinline__ uint32_t tile_strobes(const PackedView& pv, uint64_t rb, uint32_t w0,
-                                                 uint32_t nw, uint32_t rest, const SeedParams& sp,
-                                                 uint64_t* keys, uint64_t* hash, uint32_t* vmask,
-                                                 int lane) {
-  const int k = sp.klen;
-  const uint32_t span = min(rest, nw + sp.strobe_max);
-  for (uint32_t j0 = 0; j0 < span; j0 += 32) {
-    const uint32_t j = j0 + lane;
-    bool ok = false;
-    if (j < span) {
-      const uint64_t p = rb + w0 + j;
-      ok = pv.valid(p, k);
-      uint64_t key = 0;
-      if (ok) {
-        key = canonical_at(pv, p, k);
-        if (sp.spaced) key = spaced_canonical(sp.pattern, key);
-      }
-      hash[j] = ok ? strobe_hash(key) : 0;
-    }
-    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, ok);
-    if (lane == 0) vmask[j0 >> 5] = bal;
-  }
-  __syncwarp();
-  auto valid = [&](uint32_t j) { return (vmask[j >> 5] >> (j & 31)) & 1u; };
-  uint32_t count = 0;
-  for (uint32_t i0 = 0; i0 < nw; i0 += 32) {
-    const uint32_t i = i0 + lane;
-    bool keep = false;
-    uint64_t key = 0;
-    if (i < nw && valid(i)) {
-      const uint64_t h = hash[i];
-      uint64_t partner = h;
-      int fewest = 9;
-      for (uint32_t j = i + 1; j < span && j - i <= sp.strobe_max && valid(j) && fewest; ++j) {
-        if (j - i < sp.strobe_min) continue;
-        const int d = __popcll((h ^ hash[j]) & 0xFFull);
-        if (d < fewest) {
-          fewest = d;
-          partner = hash[j];
-        }
-      }
-      key = (h >> 1) + (partner >> 1);
-      keep = true;
-    }
-    count = warp_append(keys, count, keep, key, lane);
-  }
-  return count;
-}
-
 // Polynomial hashes (k > 32): each lane rolls over a contiguous run of
 // windows, restarting with a direct evaluation after invalid bases. Lane runs
 // are staged in `tmp` (nw entries) and concatenated in lane order.
@@ -342,14 +283,15 @@ __device__ __forceinline__ Rank16 rank_min(const Rank16& a, const Rank16& b) {
 
 constexpr uint32_t kOcmTile = 256;  // windows per minimizer tile
 
-// Minimizers of windows [w0, w0+nw) (nw <= kOcmTile). pre/suf hold at least
-// nw + W entries each; inner is the 4^s-entry inner hash table; pos holds
-// nw + 1 entries. Emits in window order, dropping repeats of the previous
-// window's selected position within a run.
-__device__ uint32_t tile_ocm(const PackedView& pv, uint64_t rb, uint32_t w0, uint32_t nw,
-                             const SeedParams& sp, const uint64_t* inner, Rank16* pre,
-                             Rank16* suf, uint32_t* pos, uint64_t* buf, int lane) {
-  const int k = sp.k, m = sp.m, t = sp.ocm.t, s = sp.ocm.s, w = sp.ocm.w;
+// Selected minimizer positions of windows w0 - 1 .. w0 + nw - 1 (nw <=
+// kOcmTile): pos[i] is window w0 - 1 + i's selected m-mer, as an index j
+// into the tile's anchors (record position w0 - 1 + j), or ~0 for an invalid
+// window. pre/suf hold at least nw + W entries each; inner is the
+// 4^s-entry inner hash table; pos holds nw + 1 entries.
+__device__ void tile_ocm_select(const PackedView& pv, uint64_t rb, uint32_t w0, uint32_t nw,
+                                const SeedParams& sp, const uint64_t* inner, Rank16* pre,
+                                Rank16* suf, uint32_t* pos, int lane) {
+  const int k = sp.k, t = sp.ocm.t, s = sp.ocm.s, w = sp.ocm.w;
   const uint32_t W = (uint32_t)(k - t + 1);
   // Anchor index j <-> anchor position w0 - 1 + j (record coordinates).
   const uint32_t anchors = nw + W;
@@ -403,6 +345,16 @@ __device__ uint32_t tile_ocm(const PackedView& pv, uint64_t rb, uint32_t w0, uin
     pos[i] = sel;
   }
   __syncwarp();
+}
+
+// Minimizers of windows [w0, w0+nw) (nw <= kOcmTile), buffers as for
+// tile_ocm_select. Emits in window order, dropping repeats of the previous
+// window's selected position within a run.
+__device__ uint32_t tile_ocm(const PackedView& pv, uint64_t rb, uint32_t w0, uint32_t nw,
+                             const SeedParams& sp, const uint64_t* inner, Rank16* pre,
+                             Rank16* suf, uint32_t* pos, uint64_t* buf, int lane) {
+  const int m = sp.m;
+  tile_ocm_select(pv, rb, w0, nw, sp, inner, pre, suf, pos, lane);
   uint32_t count = 0;
   for (uint32_t i0 = 1; i0 <= nw; i0 += 32) {
     uint32_t i = i0 + lane;

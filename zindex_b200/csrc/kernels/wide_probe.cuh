@@ -304,16 +304,21 @@ __global__ void __launch_bounds__(MAXT, MINB)
   const uint32_t TT = team_threads && team_threads < T ? team_threads : T;
   const uint32_t tt = tid % TT, team = tid / TT, teams = T / TT;
 
-  // The chunks this thread owns, their class and masks.
+  // The chunks this thread owns, their class and masks (a chunk pruned in a
+  // per-record report loses its row pointer and field mask until the next
+  // segment sets them up again).
   const uint8_t* col[J];
   uint32_t stride[J], roff[J], g0[J], valid[J], multi[J], cls[J];
   uint32_t planes[J][kWidePlanes];
 #pragma unroll
+  for (int j = 0; j < J; ++j)
+#pragma unroll
+    for (int k = 0; k < kWidePlanes; ++k) planes[j][k] = 0;
+  auto setup_chunks = [&]() {
+#pragma unroll
   for (int j = 0; j < J; ++j) {
     col[j] = nullptr;
     stride[j] = roff[j] = g0[j] = valid[j] = multi[j] = cls[j] = 0;
-#pragma unroll
-    for (int k = 0; k < kWidePlanes; ++k) planes[j][k] = 0;
     uint32_t g = tt + (uint32_t)j * TT, start = 0;
     for (uint32_t ci = 0; ci < classes; ++ci) {
       const DevClass& C = ix.cls[ci];
@@ -336,6 +341,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
       start += C.fp_chunks;
     }
   }
+  };
+  setup_chunks();
 
   auto flush = [&]() {
 #pragma unroll
@@ -370,8 +377,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
   // Chunks of multi-member groups are never pruned; segments split across
   // extraction rounds and global counters turn pruning off.
   uint32_t alive = (1u << J) - 1u;
-  uint64_t need = 0, seg_total = 0, seen = 0;
+  uint64_t need = 0, seg_total = 0, seen = 0;  // seen: this team's seeds flushed in the segment
   bool prune = false;
+  uint32_t flush_at = kWideFlush;  // seeds between flushes (kPruneStep while pruning)
   auto prune_chunks = [&]() {
     const uint64_t rest = seg_total - seen;
 #pragma unroll
@@ -383,7 +391,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
         const uint32_t c = __ldg(C.group_color + wide_group(g0[j], __ffs(x) - 1, b, lb));
         best = max(best, scount[c]);
       }
-      if ((uint64_t)best + rest < need) alive &= ~(1u << j);
+      if ((uint64_t)best + rest < need) {
+        alive &= ~(1u << j);
+        col[j] = nullptr;
+        valid[j] = 0;
+      }
     }
   };
   // Segmented: the block's counters belong to one segment at a time. They
@@ -434,14 +446,17 @@ __global__ void __launch_bounds__(MAXT, MINB)
         leave_segment();
         cur = seg;
         cnt.gmem = counts + (uint64_t)seg * colors;
+        if (alive != (1u << J) - 1u) setup_chunks();
         alive = (1u << J) - 1u;
         seen = 0;
         prune = false;
+        flush_at = kWideFlush;
         if (sg.min_ratio > 0.0 && scount && __ldg(sg.seg_tiles + seg) >= sg.tile_lo &&
             __ldg(sg.seg_tiles + seg + 1) <= sg.tile_hi) {
           seg_total = have;  // the whole segment is in this round
           need = minimum_matches(have, sg.min_ratio);
           prune = need > 0;
+          if (prune) flush_at = kPruneStep;
         }
       }
       if (tid == 0) atomicAdd(sg.totals + seg, (unsigned long long)n);
@@ -524,7 +539,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
             for (int q = 0; q < HQ; ++q) {
               v[j][s][q] = make_uint4(0, 0, 0, 0);
-              if (live && col[j] && ((alive >> j) & 1u) && i0 + q < H)
+              if (live && col[j] && i0 + q < H)
                 v[j][s][q] = ld_row_chunk(col[j] + (uint64_t)ri[q] * stride[j]);
             }
           }
@@ -550,7 +565,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
           uint32_t d = 0;
 #pragma unroll
           for (int w = 0; w < 4; ++w) d |= zero_fields_hi(w4[w] ^ pat, hi) >> (uint32_t)(b - 1 - w);
-          d &= ((alive >> j) & 1u) ? valid[j] : 0u;
+          d &= valid[j];
           const uint32_t slow = d & multi[j];
           uint32_t m = d & ~slow;
 #pragma unroll
@@ -575,9 +590,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
             }
           }
         }
-        ++seen;
-        if (++steps == kWideFlush || (prune && seen % kPruneStep == 0)) {
+        if (++steps == flush_at) {
           flush();
+          seen += steps;
           steps = 0;
           if (prune) prune_chunks();
         }
