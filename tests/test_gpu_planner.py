@@ -101,10 +101,12 @@ def test_planner_gain_over_default_and_regret(gpu):
     rand = gm([r["random_shortlist_gain_over_default"] for r in dev])
     heur = gm([r["heuristic_shortlist_gain_over_default"] for r in dev])
     wide = gm([r["network_over_all_launches_gain_over_default"] for r in dev])
+    nearby = gm([r["top1_nearby_guarded_gain_over_default"] for r in dev])
     print(f"launch: gain over the default {gain:.3f}, regret {regret:.3f} with {timed:.1f} of "
           f"{cands:.0f} candidates timed (network ranking every launch: {wide:.3f}; its top "
           f"pick alone, untimed: {top1:.3f}, guarded by a {pl.TOP1_MARGIN:.0%} margin: "
-          f"{guarded:.3f}); the same budget without the network: random shortlist {rand:.3f}, "
+          f"{guarded:.3f}; among the default's {pl.POOL} nearest, guarded: {nearby:.3f}); "
+          f"the same budget without the network: random shortlist {rand:.3f}, "
           f"nearest-to-default shortlist {heur:.3f}; cut: gain over the default {e2e_gain:.3f}")
     # What the network earns: its shortlist (ranking the default's
     # neighbourhood) against untrained shortlists of the same size, all of

@@ -284,7 +284,7 @@ def evaluate(planner: Planner, rows: Sequence[Row], default: Dict[str, int],
         if r.e2e == e2e:
             by.setdefault(r.setting, []).append(r)
     regrets, gains, top_gains, timed = [], [], [], []
-    rand_gains, heur_gains, guard_gains, all_gains = [], [], [], []
+    rand_gains, heur_gains, guard_gains, all_gains, near_top = [], [], [], [], []
     rng = np.random.default_rng(12345)
     dkey = launch_key(default)
     for setting, rs in by.items():
@@ -323,6 +323,11 @@ def evaluate(planner: Planner, rows: Sequence[Row], default: Dict[str, int],
             near = sorted(others, key=lambda l: _launch_distance(l, default))[:k]
             heur_gains.append(table[dkey].ms / min([table[dkey].ms] +
                                                    [table[launch_key(l)].ms for l in near]))
+            # An untimed pick inside the default's neighbourhood, kept only
+            # when predicted faster than the default by the margin.
+            pool = sorted(others, key=lambda l: _launch_distance(l, default))[:POOL]
+            pick = planner.choose(rs[0].features, pool, default=default, margin=TOP1_MARGIN)
+            near_top.append(table[dkey].ms / table[launch_key(pick)].ms)
         regrets.append(chosen / best)
         gains.append(table[dkey].ms / chosen)
     gm = lambda v: float(np.exp(np.mean(np.log(v)))) if v else float("nan")
@@ -330,6 +335,7 @@ def evaluate(planner: Planner, rows: Sequence[Row], default: Dict[str, int],
             "worst_gain": min(gains) if gains else float("nan"),
             "top1_gain_over_default": gm(top_gains),
             "top1_guarded_gain_over_default": gm(guard_gains),
+            "top1_nearby_guarded_gain_over_default": gm(near_top),
             "random_shortlist_gain_over_default": gm(rand_gains),
             "network_over_all_launches_gain_over_default": gm(all_gains),
             "heuristic_shortlist_gain_over_default": gm(heur_gains),
