@@ -868,10 +868,33 @@ struct CountSink {
 // consecutive hits, carrying the run length (saturated at z) into the next
 // round. Windows are the features: total = valid k-windows.
 struct FindereSink {
-  uint32_t* mask;  // colours round masks of this warp
-  __device__ __forceinline__ void hit(uint32_t c, uint32_t s) const { atomicOr(mask + c, 1u << s); }
+  uint32_t* mask;     // colours round masks of this warp
+  uint32_t* touched;  // shared state: bit c set at colour c's first hit of a round (else null)
+  __device__ __forceinline__ void hit(uint32_t c, uint32_t s) const {
+    const uint32_t old = atomicOr(mask + c, 1u << s);
+    if (touched && !old) atomicOr(touched + (c >> 5), 1u << (c & 31));
+  }
   __device__ __forceinline__ void add(uint32_t, uint32_t) const {}
 };
+
+// One colour's round: positions ending a run of at least z + 1 hits (m: the
+// round's hit mask, r: the run carried in), and the run carried out.
+__device__ __forceinline__ uint32_t findere_round(uint32_t m, uint32_t r, int z, uint32_t len,
+                                                  uint32_t* carried) {
+  uint32_t y = m;
+  for (int t = 1; t <= z && y; ++t) y &= t < 32 ? (m << t) : 0u;
+  uint32_t n = __popc(y);
+  const uint32_t lead = m == 0xFFFFFFFFu ? 32u : (uint32_t)(__ffs(~m) - 1);
+  const int lo = max(0, z - (int)r), hi2 = min(z, (int)lead);
+  if (hi2 > lo) n += (uint32_t)(hi2 - lo);
+  if (lead >= len) {
+    *carried = min((uint32_t)z, r + len);
+  } else {
+    const uint32_t mm = len == 32 ? m : (m << (32 - len));
+    *carried = min((uint32_t)z, (uint32_t)__clz(~mm));
+  }
+  return n;
+}
 
 // Sweeps the round masks of positions r0 .. r0 + len - 1 (bit i = r0 + i):
 // counts the positions whose run of consecutive hits is at least z + 1 long
@@ -882,32 +905,47 @@ template <bool SHARED>
 __device__ __forceinline__ void findere_sweep(uint32_t* mask, uint32_t* run, uint32_t colors, int z,
                                               uint32_t len, bool last, const Counters& cnt,
                                               int lane) {
-  // Global masks are set by L2 atomics of every lane: read them past L1 and
-  // clear them atomically. run[c] belongs to lane c % 32.
-  for (uint32_t c = (uint32_t)lane; c < colors; c += 32) {
-    uint32_t m = SHARED ? mask[c] : __ldcg(mask + c);
-    const uint32_t r = run[c];
-    if (!m) {
-      if (r) run[c] = 0;
-      continue;
+  if constexpr (SHARED) {
+    // Only the colours hit this round (touched) or carrying a run (runbits)
+    // can count or change: lane l takes words l, l + 32, ... of the bitmaps.
+    uint32_t* touched = run + colors;
+    uint32_t* runbits = touched + (colors + 31) / 32;
+    for (uint32_t wd = (uint32_t)lane; wd < (colors + 31) / 32; wd += 32) {
+      uint32_t bits = touched[wd] | runbits[wd], carry = 0;
+      touched[wd] = 0;
+      while (bits) {
+        const uint32_t bit = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const uint32_t c = wd * 32 + bit;
+        const uint32_t m = mask[c], r = run[c];
+        uint32_t nr = 0, n = 0;
+        if (m) {
+          mask[c] = 0u;
+          n = findere_round(m, r, z, len, &nr);
+        }
+        if (last) nr = 0;
+        run[c] = nr;
+        if (nr) carry |= 1u << bit;
+        if (n) cnt.add(c, n);
+      }
+      runbits[wd] = carry;
     }
-    if (SHARED) mask[c] = 0u;
-    else m = atomicExch(mask + c, 0u);
-    uint32_t y = m;
-    for (int t = 1; t <= z && y; ++t) y &= t < 32 ? (m << t) : 0u;
-    uint32_t n = __popc(y);
-    const uint32_t lead = m == 0xFFFFFFFFu ? 32u : (uint32_t)(__ffs(~m) - 1);
-    const int lo = max(0, z - (int)r), hi2 = min(z, (int)lead);
-    if (hi2 > lo) n += (uint32_t)(hi2 - lo);
-    uint32_t nr;
-    if (lead >= len) {
-      nr = min((uint32_t)z, r + len);
-    } else {
-      const uint32_t mm = len == 32 ? m : (m << (32 - len));
-      nr = min((uint32_t)z, (uint32_t)__clz(~mm));
+  } else {
+    // Global masks are set by L2 atomics of every lane: read them past L1 and
+    // clear them atomically. run[c] belongs to lane c % 32.
+    for (uint32_t c = (uint32_t)lane; c < colors; c += 32) {
+      uint32_t m = __ldcg(mask + c);
+      const uint32_t r = run[c];
+      if (!m) {
+        if (r) run[c] = 0;
+        continue;
+      }
+      m = atomicExch(mask + c, 0u);
+      uint32_t nr;
+      const uint32_t n = findere_round(m, r, z, len, &nr);
+      run[c] = last ? 0u : nr;
+      if (n) cnt.add(c, n);
     }
-    run[c] = last ? 0u : nr;
-    if (n) cnt.add(c, n);
   }
 }
 

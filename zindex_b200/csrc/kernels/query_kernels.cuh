@@ -178,7 +178,7 @@ struct FusedSmem {
   // Findere round masks and run lengths of a warp in shared memory (indexes
   // of up to kFindereSmemColors colours; else in the global scratch).
   static __host__ __device__ size_t findere_state_bytes(uint32_t colors) {
-    return colors <= kFindereSmemColors ? (size_t)colors * 8 : 0;
+    return colors <= kFindereSmemColors ? (size_t)colors * 8 + (size_t)(colors + 31) / 32 * 8 : 0;
   }
   static __host__ __device__ size_t warp_bytes(int mode, int k, uint32_t classes, int stage_bytes = 0,
                                                int stages = 0, int hashes = 4, int planes = 0,
@@ -298,8 +298,9 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
   uint8_t* ring_base = wbase + FusedSmem::key_bytes(MODE, sp.k, sp.strobe_max != 0) + FusedSmem::probe_bytes(classes, hashes, ROWS);
   uint8_t* ocm = ring_base + FusedSmem::ring_bytes(stage_bytes, lc.stages);
   if (MODE == 3 && colors <= kFindereSmemColors) {
+    // Masks, run lengths, then the touched and run bitmaps of this warp.
     uint32_t* fst = reinterpret_cast<uint32_t*>(ocm + 64);
-    for (uint32_t c = lane; c < 2 * colors; c += 32) fst[c] = 0;
+    for (uint32_t c = lane; c < 2 * colors + 2 * ((colors + 31) / 32); c += 32) fst[c] = 0;
     __syncwarp();
   }
   SharedPlanes splanes{reinterpret_cast<uint32_t*>(wbase + wstride - FusedSmem::shared_plane_bytes(swords)),
@@ -368,7 +369,7 @@ __global__ void __launch_bounds__(256, MINB) fused_query_kernel(const DevIndex* 
       uint32_t* fmask = fshared ? reinterpret_cast<uint32_t*>(ocm + 64)
                                 : bv.fstate + (uint64_t)gwarp * 2 * colors;
       uint32_t* frun = fmask + colors;
-      const FindereSink fs{fmask};
+      const FindereSink fs{fmask, fshared ? frun + colors : nullptr};
       probe_rows<MINB == 1>(ix, keys, npos, kvalid, desc, reinterpret_cast<uint32_t*>(row0s), lc.team, planes,
                  splanes, pbase, fs, lane, [&](uint32_t r0, uint32_t m) {
                    __syncwarp();
