@@ -113,13 +113,13 @@ METRIC = "query seeds/s"
 # DRAM bytes (read + write) per seed of the dominant kernel(s) of each workload, from
 # one ncu capture of a slice of the same batch (dram__bytes_read.sum +
 # dram__bytes_write.sum over the seeds of the slice); the line scales them by the
-# seeds of a launch. c2 (fused kernel): 12.034 GB read + 7.0 MB written over a
-# 1.2e7-seed slice. c3 and c4s (wide-row probe with ordered rounds, whose seeds
-# sharing rows are probed together): 2.333 GB + 8.1 MB over a 4,854,580-seed
-# slice (the first 20,000 reads; an upper bound for the whole batch, whose extra
-# seeds share rows at least as well) and 1.150 GB + 18.9 MB over the whole
-# 2,400,000-seed batch.
-TRAFFIC_BYTES_PER_SEED = {"c2": 12.041e9 / 1.2e7, "c3": 2.3415e9 / 4854580,
+# seeds of a launch. The wide-row probe with ordered rounds (the default of these
+# configurations) probes together the seeds that share rows: c2 1.885 GB read +
+# 7.4 MB written over the first 20,000 reads (2,400,000 seeds), c3 2.333 GB +
+# 8.1 MB over the first 20,000 reads (4,854,580 seeds) - upper bounds for the
+# whole batches, whose extra seeds share rows at least as well - and c4s
+# 1.150 GB + 18.9 MB over its whole 2,400,000-seed batch.
+TRAFFIC_BYTES_PER_SEED = {"c2": 1.89211e9 / 2400000, "c3": 2.3415e9 / 4854580,
                           "c4s": 1.16844e9 / 2400000}
 # Per-record form: reads counted one by one, and the compact report threshold.
 PER_RECORD_READS = 200_000
