@@ -905,15 +905,14 @@ QueryLaunch Engine::default_launch() const {
   // chunk per thread for rows of up to 256 chunks (teams of fewer threads
   // than the block below 128 chunks; 4 warps at 128), up to four beyond;
   // colour counters in shared memory while they leave room for two blocks
-  // per SM. Measured on B200: C2's 16-chunk rows 22.68 ms against 23.64 ms
-  // for the fused kernel, C3 124.3 ms against 212.3 ms.
+  // per SM. Measured on B200: C2's 16-chunk rows 19.75 ms in 4-warp blocks
+  // (22.68 ms in 8-warp blocks, 23.64 ms for the fused kernel), C3 124.3 ms
+  // in 9-warp blocks against 212.3 ms.
   if (wide_eligible(8) && wide_chunks() >= 16) {
     const uint32_t nc = wide_chunks();
     l.wide = 1;
     l.order = 1;
-    l.warps = nc < 128 ? 8
-              : nc == 128 ? 4
-                          : ((nc > 256 && nc <= 288) || (nc > 512 && nc <= 576) ? 9 : 8);
+    l.warps = nc <= 128 ? 4 : ((nc > 256 && nc <= 288) || (nc > 512 && nc <= 576) ? 9 : 8);
     l.smem_counters = 1;
     if (m_.colors.size() > 16384 || fused_smem_bytes(l) > 110 * 1024) l.smem_counters = 0;
   }
