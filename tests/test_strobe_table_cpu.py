@@ -19,8 +19,6 @@ import ctypes
 import numpy as np
 import pytest
 
-import helpers
-
 TILE = 256
 
 
@@ -108,8 +106,8 @@ def candidates(rng, valid, k, length, extra, density):
     ("kmers", 21, 21, 1.0), ("kmers", 31, 31, 1.0),
     ("minimizers", 31, 15, 0.15), ("minimizers", 49, 31, 0.1), ("minimizers", 25, 25, 1.0),
 ])
-def test_table_scan_equals_the_reference_linker(mode, k, length, density):
-    lib = helpers.Oracle().lib
+def test_table_scan_equals_the_reference_linker(oracle, mode, k, length, density):
+    lib = oracle.lib
     lib.oracle_link_strobes.restype = None
     rng = np.random.default_rng(1000 * k + length + (7 if mode == "minimizers" else 0))
     extra = k - length  # 0 for k-mers and for k == m
